@@ -1,0 +1,212 @@
+/*
+ * qublar.h -- C ABI of the B200 simulated-annealing QUBO/Ising solver.
+ *
+ * The boundary replaces the annealing path of QuBLAR:
+ *   - argos::wising::WeightedGraph / anneal / cut_of / energy_scratch
+ *       (src/ising_weighted.hpp:35-42, :173-189, :250-267)
+ *   - argos::gising::make_plan / scaled_budget / run_batch / device_energies
+ *       (src/ising_gpu.cuh:74-111, :396-458, :461-475)
+ *   - argos::BinaryProblem / Schedule / binary_energy / anneal_branch /
+ *     branch_fractions / classify
+ *       (src/engine.hpp:30-49, src/ising_recon.hpp:65-166, :302-309)
+ *
+ * A QUBO goes in (integer Max-Cut graph or residual-form BinaryProblem),
+ * annealed branches, exact energies, per-bit void fractions and the tri-state
+ * map come out. Plain pointers and sizes only; the library owns device memory,
+ * the caller owns host buffers, and no call throws or exits: every failure is
+ * a qb_status with a thread-local message (qb_last_error).
+ *
+ * Differences from the reference that a caller can observe, by design:
+ *   - sweeps visit the bits in colour-class order (a greedy distance-1
+ *     colouring of the conflict graph), not in index order;
+ *   - the Metropolis draw of (branch, bit, sweep) is Philox4x32-10 keyed by the
+ *     branch seed, not the reference's sequential splitmix64 stream.
+ * Energies and fields of any returned configuration are exact (integer) or
+ * fp64 from scratch; trajectories agree with the reference statistically.
+ */
+#ifndef QUBLAR_H
+#define QUBLAR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QUBLAR_ABI_VERSION 1
+
+/* Status codes. The reference exits the process on a CUDA error
+ * (GISING_CUDA, src/ising_gpu.cuh:44-52) and refuses plans through a string
+ * (Plan::refused, src/ising_gpu.cuh:93-94); both become codes here. */
+typedef enum qb_status {
+    QB_OK = 0,
+    QB_EINVAL = 1,      /* malformed input (the refusals of parse_rudy, ising_weighted.hpp:89-123) */
+    QB_ENOMEM = 2,      /* allocation failed or the request exceeds the device budget */
+    QB_EREFUSED = 3,    /* the planner refuses the instance (field bound, all-zero weights, size) */
+    QB_ETIMEDOUT = 4,   /* a bounded wait ran out */
+    QB_ECUDA = 5,       /* a CUDA runtime error; qb_last_error names the call */
+    QB_ENOTSUP = 6,     /* a request this build does not serve */
+    QB_ECANCELLED = 7,  /* a served request was cancelled */
+    QB_EBUSY = 8        /* the result is not ready yet */
+} qb_status;
+
+/* Problem kinds reported by qb_problem_info_get. */
+#define QB_KIND_ISING 1     /* integer-weighted Max-Cut / Ising, E = -cut */
+#define QB_KIND_RESIDUAL 2  /* residual-form QUBO (rays + 6-neighbour prior) */
+
+/* Text of a status code (static storage). */
+const char* qb_status_string(qb_status s);
+/* Detail of the last failure on this host thread (thread-local storage). */
+const char* qb_last_error(void);
+/* QUBLAR_ABI_VERSION of the loaded library. */
+int32_t qb_abi_version(void);
+/* Number of CUDA devices visible, or -1 with qb_last_error set. */
+int32_t qb_device_count(void);
+
+typedef struct qb_problem qb_problem;
+typedef struct qb_result qb_result;
+
+/* Integer-weighted graph; replaces argos::wising::WeightedGraph
+ * (src/ising_weighted.hpp:35-42). Edges are 0-based (u, v, w), u != v, no
+ * duplicates in either orientation, w in int32. E(x) = -sum_e w_e [x_u != x_v]. */
+typedef struct qb_ising_desc {
+    int32_t n;
+    int64_t m;
+    const int32_t* eu;
+    const int32_t* ev;
+    const int32_t* ew;
+} qb_ising_desc;
+
+/* Residual-form QUBO; replaces argos::BinaryProblem (src/engine.hpp:30-49):
+ *   E(x) = 1/2 sum_b w_b (sum_v a_bv x_v - d_b)^2
+ *        + lambda sum_<uv> [x_u != x_v] + sum_v lin_v x_v,
+ * lin_v = field[v] when field != NULL, else kappa (BinaryProblem::lin). The
+ * bit->ray CSR (row_ptr, ray, a) and the symmetric neighbour CSR (nbr_ptr, nbr)
+ * use int32 offsets like the reference. */
+typedef struct qb_residual_desc {
+    int32_t n_vars;
+    int32_t n_rays;
+    const double* d;        /* n_rays */
+    const double* w;        /* n_rays */
+    const int32_t* row_ptr; /* n_vars + 1 */
+    const int32_t* ray;     /* row_ptr[n_vars] */
+    const float* a;         /* row_ptr[n_vars] */
+    const int32_t* nbr_ptr; /* n_vars + 1 */
+    const int32_t* nbr;     /* nbr_ptr[n_vars] */
+    double lambda;
+    double kappa;
+    const double* field;    /* n_vars, or NULL */
+} qb_residual_desc;
+
+/* Geometric schedule: T(s) = t_hot (t_cold/t_hot)^min(1, s/max(1, A-1)) for
+ * s < A, then t_cold for `hold_sweeps` more sweeps -- the expression of
+ * ising_recon.hpp:129-131 and ising_weighted.hpp:255-257. Replaces
+ * argos::Schedule (ising_recon.hpp:81-86) and wising::Budget (:227-232).
+ * refresh_sweeps: residual instances recompute their fp32 residuals from
+ * scratch in fp64 every this many sweeps (0 = at the start only). */
+typedef struct qb_schedule {
+    double t_hot;
+    double t_cold;
+    int32_t anneal_sweeps;
+    int32_t hold_sweeps;
+    int32_t refresh_sweeps;
+} qb_schedule;
+
+/* Per-call options. stream: a cudaStream_t (NULL = the legacy default
+ * stream); device: CUDA ordinal (-1 = current). */
+typedef struct qb_opts {
+    void* stream;
+    int32_t device;
+    uint32_t flags;
+} qb_opts;
+
+/* Upload an integer graph and plan it (colouring, field width).
+ * Replaces gising::make_plan + DeviceGraph (src/ising_gpu.cuh:74-101, :278-336). */
+qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb_opts* opts, qb_problem** out);
+/* Upload a residual-form problem and plan it (conflict colouring of bits that
+ * share a ray or a neighbour bond). Replaces passing a BinaryProblem to
+ * branch_fractions (src/ising_recon.hpp:148). */
+qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts* opts, qb_problem** out);
+void qb_problem_destroy(qb_problem* p);
+
+typedef struct qb_problem_info {
+    int32_t kind;           /* QB_KIND_* */
+    int32_t n;              /* bits */
+    int64_t nnz;            /* directed couplings (ising) or bit-ray entries (residual) */
+    int32_t n_rays;         /* residual only */
+    int32_t n_colours;      /* colour classes of the sweep */
+    int32_t max_class;      /* largest class */
+    int32_t field_bytes;    /* ising: 4 (int32 fields) */
+    int32_t weight_bytes;   /* ising: 1 or 4 */
+    int64_t device_bytes;   /* device memory held by the problem */
+    double sigma;           /* ising: sqrt(2 sum w^2 / n) (ising_gpu.cuh:99) */
+    double w_min;           /* ising: min |w| over w != 0 */
+    int64_t field_bound;    /* ising: max_i sum_j |w_ij| (ising_gpu.cuh:87-92) */
+} qb_problem_info;
+qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* info);
+
+/* The sweep order of the plan: order[k] is the bit (input index) visited k-th
+ * in a sweep, class c is order[class_ptr[c] .. class_ptr[c+1]). Either output
+ * may be NULL; *n_colours receives the class count. */
+qb_status qb_problem_colouring(const qb_problem* p, int32_t* order, int32_t* class_ptr, int32_t* n_colours);
+
+/* Plan only, on the host (no device is touched): the colour-class sweep order
+ * qb_problem_create_* would use for this input. order: n entries; class_ptr:
+ * room for n + 1 entries (the first n_colours + 1 are written). Validates the
+ * input like the create calls. */
+qb_status qb_colour_ising(const qb_ising_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours);
+qb_status qb_colour_residual(const qb_residual_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours);
+
+/* T_hot = sigma, T_cold = 0.1 w_min: the reference's scaled budget
+ * (gising::scaled_budget, src/ising_gpu.cuh:104-111). Ising problems only. */
+qb_status qb_schedule_scaled(const qb_problem* p, int32_t anneal_sweeps, int32_t hold_sweeps, qb_schedule* out);
+
+/* Anneal n_branches branches; branch b uses seed b + 1 + seed_offset, the
+ * reference's convention (ising_recon.hpp:157, gpu_anneal.cu:143). Every
+ * branch starts from x = 0. The kernels are queued on opts->stream; the call
+ * returns without waiting for them. Replaces anneal_branch /
+ * branch_fractions (ising_recon.hpp:121-166), wising::anneal
+ * (ising_weighted.hpp:250) and gising::run_batch (ising_gpu.cuh:396). */
+qb_status qb_solve(qb_problem* p, const qb_schedule* s, uint32_t n_branches, uint64_t seed_offset,
+                   const qb_opts* opts, qb_result** out);
+
+typedef struct qb_result_info {
+    int32_t n;
+    int32_t n_branches;
+    int32_t sweeps;
+    int32_t launches;       /* kernels this solve launched */
+    float anneal_ms;        /* CUDA-event time of the anneal kernels (on the solve's stream) */
+    float total_ms;         /* CUDA-event time of the whole solve */
+    int64_t attempts;       /* n_branches * sweeps * n */
+    double max_drift;       /* residual: max |fp32 residual - fp64 residual| seen at refreshes */
+} qb_result_info;
+/* Waits for the solve. */
+qb_status qb_result_info_get(qb_result* r, qb_result_info* info);
+/* Branches as 0/1 bytes, n_branches x n, bit order of the input. Waits. */
+qb_status qb_result_branches(qb_result* r, uint8_t* x);
+/* Ising: tracked energies E = -cut of every branch (RunOut::energy_tracked). */
+qb_status qb_result_energies_i64(qb_result* r, int64_t* e);
+/* Ising: maintained local fields f_i = sum_j w_ij s_j, n_branches x n (wising::State::f). */
+qb_status qb_result_fields_i64(qb_result* r, int64_t* f);
+/* Energies from scratch in fp64 (binary_energy for residual problems, -cut for ising). */
+qb_status qb_result_energies_f64(qb_result* r, double* e);
+/* Per-bit fraction of branches with x = 1 (branch_fractions, ising_recon.hpp:160-163). */
+qb_status qb_result_marginals(qb_result* r, float* p);
+/* Tri-state per bit: 1 = NotThere (p >= hi), 0 = Exists (p <= lo), 2 = Undecided
+ * (argos::classify, ising_recon.hpp:302-309; defaults lo = 0.1, hi = 0.9). */
+qb_status qb_result_tristate(qb_result* r, float lo, float hi, uint8_t* bits);
+void qb_result_destroy(qb_result* r);
+
+/* Device energies of k caller states (k x n bytes, 0/1) by an independent
+ * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
+qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);
+/* Device fp64 energies of k caller states for a residual problem
+ * (binary_energy, src/ising_recon.hpp:65-79). */
+qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x, int32_t k, double* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUBLAR_H */

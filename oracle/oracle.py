@@ -1,0 +1,315 @@
+"""TEST INFRASTRUCTURE ONLY: Python access to the CPU oracle.
+
+* ``orc``  -- libqb_oracle.so, this project's C restatement (qb_oracle.c);
+* ``ref``  -- oracle/_ref/libqbref.so, the reference's own annealers compiled
+  from its sources (absent when the reference was never built here).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only to check or time the CPU side; the solver never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+ORC_PATH = os.path.join(_HERE, "libqb_oracle.so")
+REF_PATH = os.path.join(_HERE, "_ref", "libqbref.so")
+
+
+class ResidDesc(C.Structure):
+    """The layout of qb_residual_desc / argos::BinaryProblem's arrays."""
+    _fields_ = [("n_vars", C.c_int32), ("n_rays", C.c_int32), ("d", C.c_void_p), ("w", C.c_void_p),
+                ("row_ptr", C.c_void_p), ("ray", C.c_void_p), ("a", C.c_void_p), ("nbr_ptr", C.c_void_p),
+                ("nbr", C.c_void_p), ("lambda_", C.c_double), ("kappa", C.c_double), ("field", C.c_void_p)]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def resid_desc(arr: dict) -> ResidDesc:
+    return ResidDesc(int(arr["row_ptr"].size - 1), int(arr["d"].size), _p(arr["d"]), _p(arr["w"]),
+                     _p(arr["row_ptr"]), _p(arr["ray"]), _p(arr["a"]), _p(arr["nbr_ptr"]), _p(arr["nbr"]),
+                     float(arr["lambda"]), float(arr["kappa"]), _p(arr.get("field")))
+
+
+_orc = None
+_ref = None
+
+
+def orc() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        L = C.CDLL(ORC_PATH)
+        P, I64, U64, D = C.c_void_p, C.c_int64, C.c_uint64, C.c_double
+        sig = {
+            "orc_splitmix": (U64, [P]), "orc_uniform": (D, [P]),
+            "orc_philox4x32_10": (None, [P, P, P]), "orc_draw_u53": (U64, [U64, C.c_uint32, C.c_uint32, C.c_uint32]),
+            "orc_temperature": (D, [D, D, C.c_int, C.c_int]),
+            "orc_build_csr": (None, [C.c_int, I64, P, P, P, P, P, P]),
+            "orc_cut_of": (I64, [I64, P, P, P, P]),
+            "orc_energy_scratch": (I64, [C.c_int, P, P, P, P]),
+            "orc_fields": (None, [C.c_int, P, P, P, P, P]),
+            "orc_wising_anneal": (I64, [C.c_int, P, P, P, D, D, C.c_int, C.c_int, U64, P, P]),
+            "orc_ising_anneal_coloured": (I64, [C.c_int, P, P, P, P, P, C.c_int, U64, P, P, P]),
+            "orc_gray_check": (I64, [C.c_int, I64, P, P, P, P, P, P, P]),
+            "orc_binary_energy": (D, [C.POINTER(ResidDesc), P]),
+            "orc_binary_energy_batch": (None, [C.POINTER(ResidDesc), P, I64, P]),
+            "orc_local_field_dE": (D, [C.POINTER(ResidDesc), P, P, C.c_int]),
+            "orc_anneal_branch": (None, [C.POINTER(ResidDesc), D, D, C.c_int, C.c_int, U64, P, P]),
+            "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, P, P, P]),
+            "orc_classify": (None, [P, I64, C.c_float, C.c_float, P]),
+            "orc_fractions": (None, [P, C.c_int, I64, P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_PATH)
+        P, U64, D = C.c_void_p, C.c_uint64, C.c_double
+        sig = {
+            "ref_graph_parse": (P, [C.c_char_p, C.c_size_t, C.c_char_p, C.c_int]),
+            "ref_graph_free": (None, [P]),
+            "ref_graph_sizes": (None, [P, P, P, P]),
+            "ref_cut_of": (C.c_longlong, [P, P]),
+            "ref_energy_scratch": (C.c_longlong, [P, P]),
+            "ref_wising_anneal_many": (D, [P, D, D, C.c_int, C.c_int, U64, C.c_int, C.c_int, P, P]),
+            "ref_wising_trace": (C.c_longlong, [P, D, D, C.c_int, C.c_int, U64, P, P]),
+            "ref_problem_new": (P, [C.POINTER(ResidDesc)]),
+            "ref_problem_free": (None, [P]),
+            "ref_binary_energy": (D, [P, P]),
+            "ref_local_field_dE": (D, [P, P, P, C.c_int]),
+            "ref_anneal_branch": (None, [P, D, D, C.c_int, C.c_int, U64, P]),
+            "ref_branch_fractions": (D, [P, D, D, C.c_int, C.c_int, C.c_int, C.c_uint, U64, P, P]),
+            "ref_anneal_branch_trace": (None, [P, D, D, C.c_int, C.c_int, U64, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _ref = L
+    return _ref
+
+
+# ---- integer helpers -----------------------------------------------------------------------------
+
+class Graph:
+    """An integer graph with the reference's CSR (parse_rudy's build order)."""
+
+    def __init__(self, n, eu, ev, ew):
+        self.n = int(n)
+        self.eu = np.ascontiguousarray(eu, np.int32)
+        self.ev = np.ascontiguousarray(ev, np.int32)
+        self.ew = np.ascontiguousarray(ew, np.int32)
+        self.m = int(self.eu.size)
+        self.row = np.empty(self.n + 1, np.int64)
+        self.col = np.empty(max(2 * self.m, 1), np.int32)
+        self.w = np.empty(max(2 * self.m, 1), np.int32)
+        orc().orc_build_csr(self.n, self.m, _p(self.eu), _p(self.ev), _p(self.ew), _p(self.row), _p(self.col),
+                            _p(self.w))
+
+    def rudy(self) -> bytes:
+        lines = [f"{self.n} {self.m}"] + [f"{u + 1} {v + 1} {w}" for u, v, w in zip(self.eu, self.ev, self.ew)]
+        return ("\n".join(lines) + "\n").encode()
+
+    def cut(self, x) -> int:
+        x = np.ascontiguousarray(x, np.uint8)
+        return int(orc().orc_cut_of(self.m, _p(self.eu), _p(self.ev), _p(self.ew), _p(x)))
+
+    def energy_scratch(self, x) -> int:
+        x = np.ascontiguousarray(x, np.uint8)
+        return int(orc().orc_energy_scratch(self.n, _p(self.row), _p(self.col), _p(self.w), _p(x)))
+
+    def fields(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.uint8)
+        f = np.empty(self.n, np.int64)
+        orc().orc_fields(self.n, _p(self.row), _p(self.col), _p(self.w), _p(x), _p(f))
+        return f
+
+    def wising_anneal(self, t_hot, t_cold, anneal, hold, seed, trace=False):
+        x = np.empty(self.n, np.uint8)
+        tr = np.empty(anneal + hold, np.float64) if trace else None
+        e = orc().orc_wising_anneal(self.n, _p(self.row), _p(self.col), _p(self.w), t_hot, t_cold, anneal, hold,
+                                    seed, _p(x), _p(tr))
+        return (x, int(e), tr) if trace else (x, int(e))
+
+    def anneal_coloured(self, order, temps, seed, trace=False):
+        order = np.ascontiguousarray(order, np.int32)
+        temps = np.ascontiguousarray(temps, np.float64)
+        x = np.empty(self.n, np.uint8)
+        f = np.empty(self.n, np.int64)
+        tr = np.empty(temps.size, np.float64) if trace else None
+        e = orc().orc_ising_anneal_coloured(self.n, _p(self.row), _p(self.col), _p(self.w), _p(order), _p(temps),
+                                            int(temps.size), seed, _p(x), _p(f), _p(tr))
+        return (x, f, int(e), tr) if trace else (x, f, int(e))
+
+    def gray_check(self):
+        best = C.c_int64(0)
+        bad = orc().orc_gray_check(self.n, self.m, _p(self.eu), _p(self.ev), _p(self.ew), _p(self.row), _p(self.col),
+                                   _p(self.w), C.byref(best))
+        return int(bad), int(best.value)
+
+
+def temperatures(t_hot, t_cold, anneal, hold) -> np.ndarray:
+    return np.array([orc().orc_temperature(t_hot, t_cold, anneal, s) for s in range(anneal + hold)], np.float64)
+
+
+def draw_u53(seed, bit, sweep, stream=0) -> int:
+    return int(orc().orc_draw_u53(seed, bit, sweep, stream))
+
+
+def philox(ctr, key):
+    c = np.array(ctr, np.uint32)
+    k = np.array(key, np.uint32)
+    o = np.empty(4, np.uint32)
+    orc().orc_philox4x32_10(_p(c), _p(k), _p(o))
+    return [int(v) for v in o]
+
+
+# ---- residual helpers -------------------------------------------------------------------------------
+
+def binary_energy(arr: dict, x) -> float:
+    d = resid_desc(arr)
+    x = np.ascontiguousarray(x, np.uint8)
+    return float(orc().orc_binary_energy(C.byref(d), _p(x)))
+
+
+def binary_energies(arr: dict, X) -> np.ndarray:
+    d = resid_desc(arr)
+    X = np.ascontiguousarray(X, np.uint8)
+    n = int(arr["row_ptr"].size - 1)
+    K = X.size // n
+    e = np.empty(K, np.float64)
+    orc().orc_binary_energy_batch(C.byref(d), _p(X), K, _p(e))
+    return e
+
+
+def local_field_dE(arr: dict, x, r, i) -> float:
+    d = resid_desc(arr)
+    return float(orc().orc_local_field_dE(C.byref(d), _p(np.ascontiguousarray(x, np.uint8)),
+                                          _p(np.ascontiguousarray(r, np.float64)), int(i)))
+
+
+def anneal_branch(arr: dict, t_hot, t_cold, anneal, hold, seed, trace=False):
+    d = resid_desc(arr)
+    n = int(arr["row_ptr"].size - 1)
+    x = np.empty(n, np.uint8)
+    tr = np.empty(anneal + hold, np.float64) if trace else None
+    orc().orc_anneal_branch(C.byref(d), t_hot, t_cold, anneal, hold, seed, _p(x), _p(tr))
+    return (x, tr) if trace else x
+
+
+def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False):
+    d = resid_desc(arr)
+    n = int(arr["row_ptr"].size - 1)
+    order = np.ascontiguousarray(order, np.int32)
+    temps = np.ascontiguousarray(temps, np.float64)
+    x = np.empty(n, np.uint8)
+    drift = C.c_float(0.0)
+    tr = np.empty(temps.size, np.float64) if trace else None
+    orc().orc_resid_anneal_coloured(C.byref(d), _p(order), _p(temps), int(temps.size), int(refresh), seed, _p(x),
+                                    C.byref(drift), _p(tr))
+    return (x, float(drift.value), tr) if trace else (x, float(drift.value))
+
+
+def fractions(X) -> np.ndarray:
+    X = np.ascontiguousarray(X, np.uint8)
+    R, n = X.shape
+    f = np.empty(n, np.float32)
+    orc().orc_fractions(_p(X), R, n, _p(f))
+    return f
+
+
+def classify(p, lo=0.1, hi=0.9) -> np.ndarray:
+    p = np.ascontiguousarray(p, np.float32)
+    out = np.empty(p.size, np.uint8)
+    orc().orc_classify(_p(p), p.size, lo, hi, _p(out))
+    return out
+
+
+# ---- the compiled reference -------------------------------------------------------------------------
+
+class RefGraph:
+    """argos::wising::WeightedGraph parsed by the reference's own loader."""
+
+    def __init__(self, text: bytes):
+        err = C.create_string_buffer(256)
+        self.h = ref().ref_graph_parse(text, len(text), err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        n, m, sw = C.c_int(), C.c_longlong(), C.c_longlong()
+        ref().ref_graph_sizes(self.h, C.byref(n), C.byref(m), C.byref(sw))
+        self.n, self.m, self.sum_w = n.value, m.value, sw.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().ref_graph_free(self.h)
+
+    def anneal_many(self, t_hot, t_cold, anneal, hold, seed0, R, threads):
+        X = np.empty((R, self.n), np.uint8)
+        E = np.empty(R, np.int64)
+        wall = ref().ref_wising_anneal_many(self.h, t_hot, t_cold, anneal, hold, seed0, R, threads, _p(X), _p(E))
+        return X, E, wall
+
+    def trace(self, t_hot, t_cold, anneal, hold, seed):
+        x = np.empty(self.n, np.uint8)
+        tr = np.empty(anneal + hold, np.float64)
+        e = ref().ref_wising_trace(self.h, t_hot, t_cold, anneal, hold, seed, _p(x), _p(tr))
+        return x, int(e), tr
+
+    def cut(self, x):
+        return int(ref().ref_cut_of(self.h, _p(np.ascontiguousarray(x, np.uint8))))
+
+    def energy_scratch(self, x):
+        return int(ref().ref_energy_scratch(self.h, _p(np.ascontiguousarray(x, np.uint8))))
+
+
+class RefProblem:
+    """argos::BinaryProblem with the reference's evaluators and annealers."""
+
+    def __init__(self, arr: dict):
+        self.arr = arr
+        self.desc = resid_desc(arr)
+        self.h = ref().ref_problem_new(C.byref(self.desc))
+        self.n = int(arr["row_ptr"].size - 1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().ref_problem_free(self.h)
+
+    def energy(self, x):
+        return float(ref().ref_binary_energy(self.h, _p(np.ascontiguousarray(x, np.uint8))))
+
+    def local_field_dE(self, x, r, i):
+        return float(ref().ref_local_field_dE(self.h, _p(np.ascontiguousarray(x, np.uint8)),
+                                              _p(np.ascontiguousarray(r, np.float64)), int(i)))
+
+    def anneal_branch(self, t_hot, t_cold, anneal, hold, seed):
+        x = np.empty(self.n, np.uint8)
+        ref().ref_anneal_branch(self.h, t_hot, t_cold, anneal, hold, seed, _p(x))
+        return x
+
+    def branch_fractions(self, t_hot, t_cold, anneal, hold, n_branches, n_threads, seed_offset=0, keep=True):
+        frac = np.empty(self.n, np.float32)
+        X = np.empty((n_branches, self.n), np.uint8) if keep else None
+        wall = ref().ref_branch_fractions(self.h, t_hot, t_cold, anneal, hold, n_branches, n_threads, seed_offset,
+                                          _p(frac), _p(X))
+        return frac, X, wall
+
+    def trace(self, t_hot, t_cold, anneal, hold, seed):
+        x = np.empty(self.n, np.uint8)
+        tr = np.empty(anneal + hold, np.float64)
+        ref().ref_anneal_branch_trace(self.h, t_hot, t_cold, anneal, hold, seed, _p(x), _p(tr))
+        return x, tr

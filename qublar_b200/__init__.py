@@ -1,0 +1,318 @@
+"""qublar_b200 -- a B200-native simulated-annealing QUBO/Ising solver.
+
+Host-side mirror of the reference's solver interface (QuBLAR): every call goes
+through the C ABI of ``libqublar_b200.so`` (include/qublar.h) into
+hand-written sm_100a kernels. Names and argument meanings follow the
+reference:
+
+* :class:`Schedule` / :func:`branch_fractions` / :func:`anneal_branch` /
+  :func:`classify` -- ``argos::Schedule``, ``branch_fractions``,
+  ``anneal_branch``, ``classify`` (src/ising_recon.hpp:81-166, :302-309)
+* :class:`Budget` / :func:`anneal` / :func:`run_batch` -- ``wising::Budget``,
+  ``wising::anneal`` (src/ising_weighted.hpp:227-267) and ``gising::run_batch``
+  (src/ising_gpu.cuh:396-458)
+
+Errors raise :class:`QBError` carrying the library's status and message; no
+call falls back to a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._abi import (KIND_ISING, KIND_RESIDUAL, IsingDesc, Opts, ProblemInfo, QBError, ResidualDesc, ResultInfo,
+                   ScheduleC, check, lib, ptr)
+
+__all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "Result", "RunOut", "BatchOut",
+           "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib"]
+
+
+@dataclass
+class Schedule:
+    """argos::Schedule (ising_recon.hpp:81-86): anneal T_hot -> T_cold, then hold.
+
+    ``refresh_sweeps``: residual problems recompute their fp32 residuals in fp64
+    every this many sweeps."""
+    t_hot: float = 50.0
+    t_cold: float = 1.0
+    anneal_sweeps: int = 200
+    hold_sweeps: int = 50
+    refresh_sweeps: int = 50
+
+    def to_c(self) -> ScheduleC:
+        return ScheduleC(float(self.t_hot), float(self.t_cold), int(self.anneal_sweeps), int(self.hold_sweeps),
+                         int(self.refresh_sweeps))
+
+    @property
+    def sweeps(self) -> int:
+        return int(self.anneal_sweeps) + int(self.hold_sweeps)
+
+
+@dataclass
+class Budget(Schedule):
+    """wising::Budget (ising_weighted.hpp:227-232): the integer engine's defaults."""
+    t_hot: float = 5.0
+    t_cold: float = 1e-3
+    anneal_sweeps: int = 400
+    hold_sweeps: int = 20
+    refresh_sweeps: int = 0
+
+
+def device_count() -> int:
+    return int(lib().qb_device_count())
+
+
+def _opts(device: int = -1, stream=None) -> Opts:
+    s = None
+    if stream is not None:
+        s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", stream))
+    return Opts(s, int(device), 0)
+
+
+def _c32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Result:
+    """One qb_solve: device-resident branches and their read-outs."""
+
+    def __init__(self, handle, problem):
+        self._h = C.c_void_p(handle)
+        self.problem = problem
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().qb_result_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> ResultInfo:
+        i = ResultInfo()
+        check(lib().qb_result_info_get(self._h, C.byref(i)))
+        return i
+
+    @property
+    def n(self) -> int:
+        return self.problem.n
+
+    def branches(self) -> np.ndarray:
+        R = self.info().n_branches
+        x = np.empty((R, self.n), dtype=np.uint8)
+        check(lib().qb_result_branches(self._h, ptr(x)))
+        return x
+
+    def energies_tracked(self) -> np.ndarray:
+        e = np.empty(self.info().n_branches, dtype=np.int64)
+        check(lib().qb_result_energies_i64(self._h, ptr(e)))
+        return e
+
+    def fields(self) -> np.ndarray:
+        R = self.info().n_branches
+        f = np.empty((R, self.n), dtype=np.int64)
+        check(lib().qb_result_fields_i64(self._h, ptr(f)))
+        return f
+
+    def energies(self) -> np.ndarray:
+        e = np.empty(self.info().n_branches, dtype=np.float64)
+        check(lib().qb_result_energies_f64(self._h, ptr(e)))
+        return e
+
+    def marginals(self) -> np.ndarray:
+        p = np.empty(self.n, dtype=np.float32)
+        check(lib().qb_result_marginals(self._h, ptr(p)))
+        return p
+
+    def tristate(self, lo: float = 0.1, hi: float = 0.9) -> np.ndarray:
+        t = np.empty(self.n, dtype=np.uint8)
+        check(lib().qb_result_tristate(self._h, C.c_float(lo), C.c_float(hi), ptr(t)))
+        return t
+
+
+class _Problem:
+    kind = 0
+
+    def __init__(self):
+        self._h = C.c_void_p(None)
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().qb_problem_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> ProblemInfo:
+        i = ProblemInfo()
+        check(lib().qb_problem_info_get(self._h, C.byref(i)))
+        return i
+
+    def colouring(self):
+        """(order, class_ptr): the sweep order of the plan."""
+        order = np.empty(self.n, dtype=np.int32)
+        cptr = np.empty(self.n + 1, dtype=np.int32)
+        nc = C.c_int32(0)
+        check(lib().qb_problem_colouring(self._h, ptr(order), ptr(cptr), C.byref(nc)))
+        return order, cptr[: nc.value + 1].copy()
+
+    def solve(self, schedule: Schedule, n_branches: int, seed_offset: int = 0, stream=None) -> Result:
+        out = C.c_void_p()
+        o = _opts(-1, stream)
+        s = schedule.to_c()
+        check(lib().qb_solve(self._h, C.byref(s), int(n_branches), int(seed_offset), C.byref(o), C.byref(out)))
+        return Result(out.value, self)
+
+
+class IsingProblem(_Problem):
+    """An integer Max-Cut / Ising instance on the device (WeightedGraph + DeviceGraph)."""
+    kind = KIND_ISING
+
+    def __init__(self, n: int, eu, ev, ew, device: int = -1, stream=None):
+        super().__init__()
+        self.n = int(n)
+        self.eu, self.ev, self.ew = _c32(eu), _c32(ev), _c32(ew)
+        self.m = int(self.eu.size)
+        d = self.desc()
+        h = C.c_void_p()
+        o = _opts(device, stream)
+        check(lib().qb_problem_create_ising(C.byref(d), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def desc(self) -> IsingDesc:
+        return IsingDesc(self.n, self.m, ptr(self.eu), ptr(self.ev), ptr(self.ew))
+
+    def scaled_schedule(self, anneal_sweeps: int, hold_sweeps: int) -> Budget:
+        s = ScheduleC()
+        check(lib().qb_schedule_scaled(self._h, int(anneal_sweeps), int(hold_sweeps), C.byref(s)))
+        return Budget(s.t_hot, s.t_cold, s.anneal_sweeps, s.hold_sweeps, 0)
+
+    def energies(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.uint8).reshape(-1, self.n)
+        e = np.empty(X.shape[0], dtype=np.int64)
+        check(lib().qb_energies_ising(self._h, ptr(X), int(X.shape[0]), ptr(e)))
+        return e
+
+
+class ResidualProblem(_Problem):
+    """A residual-form QUBO (argos::BinaryProblem, engine.hpp:30-49) on the device."""
+    kind = KIND_RESIDUAL
+
+    def __init__(self, d, w, row_ptr, ray, a, nbr_ptr, nbr, lam: float, kappa: float, field=None,
+                 device: int = -1, stream=None):
+        super().__init__()
+        self.d = np.ascontiguousarray(d, dtype=np.float64)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.row_ptr, self.ray = _c32(row_ptr), _c32(ray)
+        self.a = np.ascontiguousarray(a, dtype=np.float32)
+        self.nbr_ptr, self.nbr = _c32(nbr_ptr), _c32(nbr)
+        self.lam, self.kappa = float(lam), float(kappa)
+        self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float64)
+        self.n = int(self.row_ptr.size - 1)
+        self.n_rays = int(self.d.size)
+        d_ = self.desc()
+        h = C.c_void_p()
+        o = _opts(device, stream)
+        check(lib().qb_problem_create_residual(C.byref(d_), C.byref(o), C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_arrays(cls, arrays: dict, **kw) -> "ResidualProblem":
+        return cls(arrays["d"], arrays["w"], arrays["row_ptr"], arrays["ray"], arrays["a"], arrays["nbr_ptr"],
+                   arrays["nbr"], arrays["lambda"], arrays["kappa"], arrays.get("field"), **kw)
+
+    def desc(self) -> ResidualDesc:
+        return ResidualDesc(self.n, self.n_rays, ptr(self.d), ptr(self.w), ptr(self.row_ptr), ptr(self.ray),
+                            ptr(self.a), ptr(self.nbr_ptr), ptr(self.nbr), self.lam, self.kappa, ptr(self.field))
+
+    def energies(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.uint8).reshape(-1, self.n)
+        e = np.empty(X.shape[0], dtype=np.float64)
+        check(lib().qb_energies_residual(self._h, ptr(X), int(X.shape[0]), ptr(e)))
+        return e
+
+
+# ---- the reference's call shapes ------------------------------------------------------------
+
+@dataclass
+class RunOut:
+    """wising::RunOut (ising_weighted.hpp:245-248)."""
+    x: np.ndarray
+    energy_tracked: int
+
+
+@dataclass
+class BatchOut:
+    """gising::BatchOut (ising_gpu.cuh:345-359): x(r) -> 0/1, energies, timing."""
+    X: np.ndarray
+    energy: np.ndarray
+    kernel_ms: float
+    launches: int
+
+    @property
+    def R(self) -> int:
+        return int(self.X.shape[0])
+
+    def x(self, r: int) -> np.ndarray:
+        return self.X[r]
+
+
+def branch_fractions(problem: ResidualProblem, schedule: Schedule, n_branches: int, n_threads: int = 0,
+                     keep: bool = False, seed_offset: int = 0):
+    """branch_fractions (ising_recon.hpp:148-166): the per-bit fraction of
+    n_branches annealed branches with x = 1; branch b uses seed b + 1 +
+    seed_offset. ``n_threads`` is accepted for call compatibility and ignored.
+    Returns ``frac`` or ``(frac, branches)`` when keep is true."""
+    r = problem.solve(schedule, n_branches, seed_offset)
+    try:
+        frac = r.marginals()
+        return (frac, r.branches()) if keep else frac
+    finally:
+        r.close()
+
+
+def anneal_branch(problem: ResidualProblem, schedule: Schedule, seed: int) -> np.ndarray:
+    """anneal_branch (ising_recon.hpp:121-144): one branch with seed ``seed``."""
+    r = problem.solve(schedule, 1, int(seed) - 1)
+    try:
+        return r.branches()[0]
+    finally:
+        r.close()
+
+
+def anneal(graph: IsingProblem, budget: Budget, seed: int) -> RunOut:
+    """wising::anneal (ising_weighted.hpp:250-267) for one seed."""
+    r = graph.solve(budget, 1, int(seed) - 1)
+    try:
+        return RunOut(r.branches()[0], int(r.energies_tracked()[0]))
+    finally:
+        r.close()
+
+
+def run_batch(graph: IsingProblem, budget: Budget, seed_base: int, R: int) -> BatchOut:
+    """gising::run_batch (ising_gpu.cuh:396-458): replicas with seeds
+    seed_base .. seed_base + R - 1."""
+    r = graph.solve(budget, int(R), int(seed_base) - 1)
+    try:
+        info = r.info()
+        return BatchOut(r.branches(), r.energies_tracked(), float(info.anneal_ms), int(info.launches))
+    finally:
+        r.close()
+
+
+def classify(p, lo: float = 0.1, hi: float = 0.9) -> np.ndarray:
+    """classify (ising_recon.hpp:305-309) on the host: 1 NotThere, 0 Exists, 2 Undecided."""
+    p = np.asarray(p, dtype=np.float32)
+    out = np.full(p.shape, 2, dtype=np.uint8)
+    out[p <= np.float32(lo)] = 0
+    out[p >= np.float32(hi)] = 1
+    return out

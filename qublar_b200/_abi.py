@@ -1,0 +1,135 @@
+"""ctypes binding of the C ABI in include/qublar.h and include/qublar_synth.h.
+
+The shared library is built in-tree (qublar_b200/libqublar_b200.so, by
+``__graft_entry__.build()``). Loading fails loudly when it is missing: there is
+no pure-Python or CPU fallback of the solver.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqublar_b200.so")
+
+QB_OK = 0
+STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4: "QB_ETIMEDOUT",
+                5: "QB_ECUDA", 6: "QB_ENOTSUP", 7: "QB_ECANCELLED", 8: "QB_EBUSY"}
+KIND_ISING = 1
+KIND_RESIDUAL = 2
+
+
+class QBError(RuntimeError):
+    """A non-OK qb_status, with the library's thread-local message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class IsingDesc(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m", C.c_int64), ("eu", C.c_void_p), ("ev", C.c_void_p), ("ew", C.c_void_p)]
+
+
+class ResidualDesc(C.Structure):
+    _fields_ = [("n_vars", C.c_int32), ("n_rays", C.c_int32), ("d", C.c_void_p), ("w", C.c_void_p),
+                ("row_ptr", C.c_void_p), ("ray", C.c_void_p), ("a", C.c_void_p), ("nbr_ptr", C.c_void_p),
+                ("nbr", C.c_void_p), ("lambda_", C.c_double), ("kappa", C.c_double), ("field", C.c_void_p)]
+
+
+class ScheduleC(C.Structure):
+    _fields_ = [("t_hot", C.c_double), ("t_cold", C.c_double), ("anneal_sweeps", C.c_int32),
+                ("hold_sweeps", C.c_int32), ("refresh_sweeps", C.c_int32)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("stream", C.c_void_p), ("device", C.c_int32), ("flags", C.c_uint32)]
+
+
+class ProblemInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64), ("n_rays", C.c_int32),
+                ("n_colours", C.c_int32), ("max_class", C.c_int32), ("field_bytes", C.c_int32),
+                ("weight_bytes", C.c_int32), ("device_bytes", C.c_int64), ("sigma", C.c_double),
+                ("w_min", C.c_double), ("field_bound", C.c_int64)]
+
+
+class ResultInfo(C.Structure):
+    _fields_ = [("n", C.c_int32), ("n_branches", C.c_int32), ("sweeps", C.c_int32), ("launches", C.c_int32),
+                ("anneal_ms", C.c_float), ("total_ms", C.c_float), ("attempts", C.c_int64),
+                ("max_drift", C.c_double)]
+
+
+class TomoParams(C.Structure):
+    _fields_ = [("target_bits", C.c_int32), ("target_rays", C.c_int32), ("voxel", C.c_double),
+                ("half_base", C.c_double), ("height", C.c_double), ("n_detectors", C.c_int32),
+                ("det", C.c_double * 12), ("n_theta", C.c_int32), ("n_phi", C.c_int32),
+                ("theta_min", C.c_double), ("theta_max", C.c_double), ("phi_half", C.c_double),
+                ("sub_rays", C.c_int32), ("mu_rock", C.c_double), ("void_center", C.c_double * 3),
+                ("void_side", C.c_double), ("exposure", C.c_double), ("min_open", C.c_double),
+                ("lambda_", C.c_double), ("kappa", C.c_double), ("seed", C.c_uint64)]
+
+
+_P = C.c_void_p
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "qb_status_string": (C.c_char_p, [C.c_int]),
+    "qb_last_error": (C.c_char_p, []),
+    "qb_abi_version": (C.c_int32, []),
+    "qb_device_count": (C.c_int32, []),
+    "qb_problem_create_ising": (C.c_int, [C.POINTER(IsingDesc), C.POINTER(Opts), C.POINTER(_P)]),
+    "qb_problem_create_residual": (C.c_int, [C.POINTER(ResidualDesc), C.POINTER(Opts), C.POINTER(_P)]),
+    "qb_problem_destroy": (None, [_P]),
+    "qb_problem_info_get": (C.c_int, [_P, C.POINTER(ProblemInfo)]),
+    "qb_problem_colouring": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32)]),
+    "qb_schedule_scaled": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(ScheduleC)]),
+    "qb_solve": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, C.POINTER(Opts), C.POINTER(_P)]),
+    "qb_result_info_get": (C.c_int, [_P, C.POINTER(ResultInfo)]),
+    "qb_result_branches": (C.c_int, [_P, _P]),
+    "qb_result_energies_i64": (C.c_int, [_P, _P]),
+    "qb_result_fields_i64": (C.c_int, [_P, _P]),
+    "qb_result_energies_f64": (C.c_int, [_P, _P]),
+    "qb_result_marginals": (C.c_int, [_P, _P]),
+    "qb_result_tristate": (C.c_int, [_P, C.c_float, C.c_float, _P]),
+    "qb_result_destroy": (None, [_P]),
+    "qb_energies_ising": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "qb_energies_residual": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
+    "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
+    "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),
+    "qb_synth_tomography": (C.c_int, [C.POINTER(TomoParams), C.POINTER(_P)]),
+    "qb_tomo_sizes": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int64)]),
+    "qb_tomo_arrays": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "qb_tomo_desc": (C.c_int, [_P, C.POINTER(ResidualDesc)]),
+    "qb_tomo_destroy": (None, [_P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library (loaded once). Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() (make -C qublar_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != QB_OK:
+        raise QBError(status, lib().qb_last_error().decode("utf-8", "replace"))
+
+
+def ptr(a) -> int | None:
+    """Address of a contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    return a.ctypes.data

@@ -1,0 +1,643 @@
+// The C ABI (include/qublar.h): validation, planning, upload, solve, results.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "qb_internal.hpp"
+#include "qb_kernels.hpp"
+
+using namespace qb;
+
+namespace {
+
+cudaStream_t stream_of(const qb_opts* o) { return o ? static_cast<cudaStream_t>(o->stream) : nullptr; }
+
+qb_status select_device(const qb_opts* o, int* dev_out) {
+    int dev = 0;
+    if (o && o->device >= 0) {
+        QB_CUDA(cudaSetDevice(o->device));
+        dev = o->device;
+    } else {
+        QB_CUDA(cudaGetDevice(&dev));
+    }
+    *dev_out = dev;
+    return QB_OK;
+}
+
+// Stream-ordered allocation for per-solve buffers: no device-wide
+// synchronisation inside a timed loop.
+qb_status alloc_async(DevBuf& b, size_t bytes, cudaStream_t st) {
+    b.release();
+    if (bytes == 0) return QB_OK;
+    QB_CUDA(cudaMallocAsync(&b.p, bytes, st));
+    b.bytes = bytes;
+    return QB_OK;
+}
+
+void free_async(DevBuf& b, cudaStream_t st) {
+    if (b.p) cudaFreeAsync(b.p, st);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+// The temperature of every sweep by the reference's expression
+// (ising_recon.hpp:129-131, ising_weighted.hpp:255-257); `volatile` keeps the
+// double rounding of gising::temperatures (ising_gpu.cuh:114-124).
+std::vector<double> temperatures(const qb_schedule& s) {
+    const int total = s.anneal_sweeps + s.hold_sweeps;
+    std::vector<double> t(size_t(total), 0.0);
+    for (int sweep = 0; sweep < total; ++sweep) {
+        const double frac = std::min(1.0, double(sweep) / std::max(1, s.anneal_sweeps - 1));
+        volatile double temp = sweep < s.anneal_sweeps ? s.t_hot * std::pow(s.t_cold / s.t_hot, frac) : s.t_cold;
+        t[size_t(sweep)] = temp;
+    }
+    return t;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+
+// ---- ising planning -------------------------------------------------------------------
+
+qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
+    const int n = g->n;
+    const int64_t m = g->m;
+    if (n <= 0) return fail(QB_EINVAL, "ising: n must be positive");
+    if (m < 0) return fail(QB_EINVAL, "ising: m must be non-negative");
+    if (m > 0 && (!g->eu || !g->ev || !g->ew)) return fail(QB_EINVAL, "ising: null edge arrays");
+    if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "ising: more than 2^30 edges");
+    // loader refusals of parse_rudy (ising_weighted.hpp:113-133)
+    std::vector<uint64_t> key(static_cast<size_t>(m));
+    for (int64_t e = 0; e < m; ++e) {
+        const int32_t u = g->eu[e], v = g->ev[e];
+        if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "ising: vertex index out of range");
+        if (u == v) return fail(QB_EINVAL, "ising: self-loop");
+        key[size_t(e)] = (uint64_t(std::min(u, v)) << 32) | uint64_t(std::max(u, v));
+    }
+    std::sort(key.begin(), key.end());
+    for (size_t k = 1; k < key.size(); ++k)
+        if (key[k] == key[k - 1]) return fail(QB_EINVAL, "ising: duplicate edge");
+    P.n = n;
+    P.m = m;
+    P.nnz = 2 * m;
+    // symmetric CSR in edge order, as parse_rudy builds it (ising_weighted.hpp:135-147)
+    std::vector<int64_t> row(size_t(n) + 1, 0);
+    for (int64_t e = 0; e < m; ++e) { row[size_t(g->eu[e]) + 1]++; row[size_t(g->ev[e]) + 1]++; }
+    for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
+    std::vector<int32_t> col(size_t(2 * m)), w(size_t(2 * m));
+    std::vector<int64_t> fill(row.begin(), row.end() - 1);
+    for (int64_t e = 0; e < m; ++e) {
+        const int32_t a = g->eu[e], b = g->ev[e], wt = g->ew[e];
+        col[size_t(fill[size_t(a)])] = b; w[size_t(fill[size_t(a)]++)] = wt;
+        col[size_t(fill[size_t(b)])] = a; w[size_t(fill[size_t(b)]++)] = wt;
+    }
+    // plan figures of gising::make_plan (ising_gpu.cuh:74-101)
+    double sum_w2 = 0.0;
+    P.w_min = 0;
+    P.max_w = 0;
+    for (int64_t e = 0; e < m; ++e) {
+        const int64_t a = std::llabs(int64_t(g->ew[e]));
+        sum_w2 += double(a) * double(a);
+        P.max_w = std::max(P.max_w, a);
+        if (a != 0 && (P.w_min == 0 || a < P.w_min)) P.w_min = a;
+    }
+    P.B = 0;
+    for (int i = 0; i < n; ++i) {
+        int64_t acc = 0;
+        for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k) acc += std::llabs(int64_t(w[size_t(k)]));
+        P.B = std::max(P.B, acc);
+    }
+    if (P.B > 2147483647LL) return fail(QB_EREFUSED, "ising: field bound exceeds int32");
+    P.sigma = std::sqrt(2.0 * sum_w2 / double(n));
+    P.weight_bytes = P.max_w <= 127 ? 1 : 4;
+    P.col = colour_graph(n, row, col);
+    // sweep-order CSR
+    const Colouring& C = P.col;
+    P.row.assign(size_t(n) + 1, 0);
+    P.adj.resize(size_t(2 * m));
+    P.wgt.resize(size_t(2 * m));
+    P.f0.assign(size_t(n), 0);
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        int32_t pos = P.row[size_t(k)];
+        int64_t acc = 0;
+        for (int64_t e = row[size_t(i)]; e < row[size_t(i) + 1]; ++e) {
+            P.adj[size_t(pos)] = C.inverse[size_t(col[size_t(e)])];
+            P.wgt[size_t(pos)] = w[size_t(e)];
+            acc -= w[size_t(e)];
+            ++pos;
+        }
+        P.row[size_t(k) + 1] = pos;
+        P.f0[size_t(k)] = int32_t(acc);   // x = 0: s = -1 everywhere (wising::State, ising_weighted.hpp:199-208)
+    }
+    return QB_OK;
+}
+
+qb_status upload_ising(IsingPlan& P, const qb_ising_desc* g, cudaStream_t st, int64_t* bytes) {
+    qb_status s;
+    if ((s = upload_vec(P.d_row, P.row, st))) return s;
+    if ((s = upload_vec(P.d_adj, P.adj, st))) return s;
+    if (P.weight_bytes == 1) {
+        std::vector<int8_t> w8(P.wgt.size());
+        for (size_t k = 0; k < w8.size(); ++k) w8[k] = int8_t(P.wgt[k]);
+        if ((s = upload_vec(P.d_w, w8, st))) return s;
+        QB_CUDA(cudaStreamSynchronize(st));   // w8 is a local
+    } else if ((s = upload_vec(P.d_w, P.wgt, st))) {
+        return s;
+    }
+    if ((s = upload_vec(P.d_f0, P.f0, st))) return s;
+    if ((s = upload_vec(P.d_order, P.col.order, st))) return s;
+    if ((s = upload_vec(P.d_class_ptr, P.col.class_ptr, st))) return s;
+    if ((s = upload(P.d_eu, g->eu, size_t(P.m) * 4, st))) return s;
+    if ((s = upload(P.d_ev, g->ev, size_t(P.m) * 4, st))) return s;
+    if ((s = upload(P.d_ew, g->ew, size_t(P.m) * 4, st))) return s;
+    QB_CUDA(cudaStreamSynchronize(st));
+    *bytes = int64_t(P.d_row.bytes + P.d_adj.bytes + P.d_w.bytes + P.d_f0.bytes + P.d_order.bytes +
+                     P.d_class_ptr.bytes + P.d_eu.bytes + P.d_ev.bytes + P.d_ew.bytes);
+    return QB_OK;
+}
+
+// ---- residual planning ------------------------------------------------------------------
+
+qb_status check_residual(const qb_residual_desc* d) {
+    if (d->n_vars <= 0) return fail(QB_EINVAL, "residual: n_vars must be positive");
+    if (d->n_rays < 0) return fail(QB_EINVAL, "residual: n_rays must be non-negative");
+    if (!d->row_ptr || !d->nbr_ptr) return fail(QB_EINVAL, "residual: null CSR offsets");
+    if (d->n_rays > 0 && (!d->d || !d->w)) return fail(QB_EINVAL, "residual: null d or w");
+    const int n = d->n_vars;
+    if (d->row_ptr[0] != 0 || d->nbr_ptr[0] != 0) return fail(QB_EINVAL, "residual: CSR offsets must start at 0");
+    for (int i = 0; i < n; ++i) {
+        if (d->row_ptr[i + 1] < d->row_ptr[i]) return fail(QB_EINVAL, "residual: row_ptr decreases");
+        if (d->nbr_ptr[i + 1] < d->nbr_ptr[i]) return fail(QB_EINVAL, "residual: nbr_ptr decreases");
+    }
+    const int64_t nnz = d->row_ptr[n];
+    if (nnz > 0 && (!d->ray || !d->a)) return fail(QB_EINVAL, "residual: null ray or a");
+    if (d->nbr_ptr[n] > 0 && !d->nbr) return fail(QB_EINVAL, "residual: null nbr");
+    std::vector<int32_t> stamp(size_t(std::max(d->n_rays, 1)), -1);
+    for (int i = 0; i < n; ++i) {
+        for (int k = d->row_ptr[i]; k < d->row_ptr[i + 1]; ++k) {
+            const int b = d->ray[k];
+            if (b < 0 || b >= d->n_rays) return fail(QB_EINVAL, "residual: ray index out of range");
+            if (stamp[size_t(b)] == i) return fail(QB_EINVAL, "residual: a bit lists a ray twice");
+            stamp[size_t(b)] = i;
+            if (!std::isfinite(d->a[k])) return fail(QB_EINVAL, "residual: non-finite a");
+        }
+        for (int k = d->nbr_ptr[i]; k < d->nbr_ptr[i + 1]; ++k) {
+            const int j = d->nbr[k];
+            if (j < 0 || j >= n || j == i) return fail(QB_EINVAL, "residual: neighbour index out of range");
+            bool back = false;
+            for (int q = d->nbr_ptr[j]; q < d->nbr_ptr[j + 1]; ++q) back |= d->nbr[q] == i;
+            if (!back) return fail(QB_EINVAL, "residual: the neighbour lists are not symmetric");
+        }
+    }
+    for (int b = 0; b < d->n_rays; ++b)
+        if (!std::isfinite(d->d[b]) || !std::isfinite(d->w[b])) return fail(QB_EINVAL, "residual: non-finite d or w");
+    return QB_OK;
+}
+
+qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P) {
+    const int n = d->n_vars;
+    P.n = n;
+    P.n_rays = d->n_rays;
+    P.nnz = d->row_ptr[n];
+    P.n_nbr = d->nbr_ptr[n];
+    P.lambda = d->lambda;
+    P.col = colour_residual(n, d->n_rays, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
+    const Colouring& C = P.col;
+    const int nc = C.n_colours();
+    // cluster decomposition: the smallest cluster whose shared memory holds
+    // the branch (QB_RESID_CLUSTER overrides)
+    int CL = env_int("QB_RESID_CLUSTER", 0);
+    const int candidates[2] = {8, 16};
+    for (int t = 0; t < 2 && CL == 0; ++t) {
+        const int c = candidates[t];
+        int bits = 0;
+        for (int k = 0; k < nc; ++k) bits += (C.class_ptr[size_t(k) + 1] - C.class_ptr[size_t(k)] + c - 1) / c;
+        const size_t bytes = size_t((d->n_rays + c - 1) / c) * 8 + size_t(bits);
+        if (bytes <= size_t(200) * 1024) CL = c;
+    }
+    if (CL == 0) return fail(QB_ENOTSUP, "residual: the problem exceeds one cluster's shared memory");
+    if (CL != 4 && CL != 8 && CL != 16) return fail(QB_EINVAL, "residual: cluster size must be 4, 8 or 16");
+    P.CL = CL;
+    P.ray_slots = (d->n_rays + CL - 1) / CL;
+    P.slot_base.assign(size_t(nc) * size_t(CL), 0);
+    P.bit_home.assign(size_t(n), 0);
+    std::vector<int32_t> used(size_t(CL), 0);
+    for (int c = 0; c < nc; ++c) {
+        const int cs = C.class_ptr[size_t(c)], ce = C.class_ptr[size_t(c) + 1];
+        const int chunk = (ce - cs + CL - 1) / CL;
+        for (int t = 0; t < CL; ++t) {
+            P.slot_base[size_t(c) * CL + size_t(t)] = used[size_t(t)];
+            const int b0 = cs + t * chunk, b1 = std::min(b0 + chunk, ce);
+            for (int i = b0; i < b1; ++i) P.bit_home[size_t(i)] = (uint32_t(t) << 27) | uint32_t(used[size_t(t)]++);
+        }
+    }
+    P.bit_slots = *std::max_element(used.begin(), used.end());
+    if (P.bit_slots >= (1 << 27)) return fail(QB_EREFUSED, "residual: too many bits per CTA");
+    return QB_OK;
+}
+
+qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes) {
+    const int n = P.n, nr = P.n_rays;
+    const Colouring& C = P.col;
+    std::vector<int32_t> row(size_t(n) + 1, 0), ray(static_cast<size_t>(P.nnz)), nbr_ptr(size_t(n) + 1, 0);
+    std::vector<float> a(static_cast<size_t>(P.nnz)), lin(static_cast<size_t>(n)), q(static_cast<size_t>(n));
+    std::vector<uint32_t> nbr_home(static_cast<size_t>(P.n_nbr));
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        int32_t pos = row[size_t(k)];
+        double qd = 0.0;
+        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
+            ray[size_t(pos)] = d->ray[e];
+            a[size_t(pos)] = d->a[e];
+            qd += 0.5 * d->w[d->ray[e]] * double(d->a[e]) * double(d->a[e]);
+            ++pos;
+        }
+        row[size_t(k) + 1] = pos;
+        q[size_t(k)] = float(qd);
+        lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
+        int32_t np = nbr_ptr[size_t(k)];
+        for (int e = d->nbr_ptr[i]; e < d->nbr_ptr[i + 1]; ++e)
+            nbr_home[size_t(np++)] = P.bit_home[size_t(C.inverse[size_t(d->nbr[e])])];
+        nbr_ptr[size_t(k) + 1] = np;
+    }
+    // ray-major CSR, bits ascending in input order inside a ray: the refresh
+    // (bits by home) and the energy verifier (bits by input index)
+    std::vector<int32_t> rrow(size_t(nr) + 1, 0);
+    for (int64_t e = 0; e < P.nnz; ++e) rrow[size_t(d->ray[e]) + 1]++;
+    for (int b = 0; b < nr; ++b) rrow[size_t(b) + 1] += rrow[size_t(b)];
+    std::vector<int32_t> rfill(rrow.begin(), rrow.end() - 1), rbit_o(static_cast<size_t>(P.nnz));
+    std::vector<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
+    std::vector<float> ra(static_cast<size_t>(P.nnz));
+    for (int i = 0; i < n; ++i)
+        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
+            const int32_t k = rfill[size_t(d->ray[e])]++;
+            rbit_o[size_t(k)] = i;
+            rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
+            ra[size_t(k)] = d->a[e];
+        }
+    std::vector<float> wf(static_cast<size_t>(nr));
+    for (int b = 0; b < nr; ++b) wf[size_t(b)] = float(d->w[b]);
+    std::vector<double> o_lin(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) o_lin[size_t(i)] = d->field ? d->field[i] : d->kappa;
+    qb_status s;
+#define QB_UP(buf, vec) if ((s = upload_vec(P.buf, vec, st))) return s
+    QB_UP(d_row, row); QB_UP(d_ray, ray); QB_UP(d_a, a); QB_UP(d_lin, lin); QB_UP(d_q, q);
+    QB_UP(d_nbr_ptr, nbr_ptr); QB_UP(d_nbr_home, nbr_home); QB_UP(d_order, C.order);
+    QB_UP(d_class_ptr, C.class_ptr); QB_UP(d_slot_base, P.slot_base);
+    QB_UP(d_wf, wf); QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra);
+    QB_UP(d_o_rrow, rrow); QB_UP(d_o_rbit, rbit_o); QB_UP(d_o_ra, ra); QB_UP(d_o_lin, o_lin);
+#undef QB_UP
+    if ((s = upload(P.d_d, d->d, size_t(nr) * 8, st))) return s;
+    if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
+    if ((s = upload(P.d_o_nbr_ptr, d->nbr_ptr, (size_t(n) + 1) * 4, st))) return s;
+    if ((s = upload(P.d_o_nbr, d->nbr, size_t(P.n_nbr) * 4, st))) return s;
+    QB_CUDA(cudaStreamSynchronize(st));   // the host vectors above are locals
+    const DevBuf* all[] = {&P.d_row, &P.d_ray, &P.d_a, &P.d_lin, &P.d_q, &P.d_nbr_ptr, &P.d_nbr_home, &P.d_order,
+                           &P.d_class_ptr, &P.d_slot_base, &P.d_d, &P.d_w64, &P.d_wf, &P.d_rrow, &P.d_rbit,
+                           &P.d_ra, &P.d_o_rrow, &P.d_o_rbit, &P.d_o_ra, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin};
+    int64_t tot = 0;
+    for (const DevBuf* b : all) tot += int64_t(b->bytes);
+    *bytes = tot;
+    return QB_OK;
+}
+
+qb_status check_schedule(const qb_schedule* s) {
+    if (!s) return fail(QB_EINVAL, "schedule: null");
+    if (s->anneal_sweeps < 0 || s->hold_sweeps < 0 || s->anneal_sweeps + s->hold_sweeps < 1)
+        return fail(QB_EINVAL, "schedule: needs at least one sweep");
+    if (!(s->t_hot > 0.0) || !(s->t_cold > 0.0) || !std::isfinite(s->t_hot) || !std::isfinite(s->t_cold))
+        return fail(QB_EINVAL, "schedule: temperatures must be positive and finite");
+    if (s->refresh_sweeps < 0) return fail(QB_EINVAL, "schedule: refresh_sweeps must be non-negative");
+    return QB_OK;
+}
+
+qb_status wait(qb_result* r) {
+    if (!r->synced) {
+        QB_CUDA(cudaStreamSynchronize(r->stream));
+        r->synced = true;
+    }
+    return QB_OK;
+}
+
+qb_status download(qb_result* r, void* dst, const DevBuf& src, size_t bytes) {
+    if (!dst) return fail(QB_EINVAL, "result: null output buffer");
+    if (!src.p || src.bytes < bytes) return fail(QB_EINVAL, "result: this output is not available for the problem kind");
+    QB_CUDA(cudaSetDevice(r->device));
+    QB_CUDA(cudaMemcpyAsync(dst, src.p, bytes, cudaMemcpyDeviceToHost, r->stream));
+    QB_CUDA(cudaStreamSynchronize(r->stream));
+    r->synced = true;
+    return QB_OK;
+}
+
+}  // namespace
+
+// ---- problems ------------------------------------------------------------------------------
+
+extern "C" qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb_opts* opts, qb_problem** out) {
+    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_ising: null argument");
+    *out = nullptr;
+    qb_problem* p = new (std::nothrow) qb_problem();
+    if (!p) return fail(QB_ENOMEM, "qb_problem_create_ising: out of host memory");
+    p->kind = QB_KIND_ISING;
+    qb_status s = plan_ising(desc, p->ising);
+    if (s == QB_OK && p->ising.w_min == 0) s = fail(QB_EREFUSED, "ising: all weights are zero");   // ising_gpu.cuh:94
+    if (s == QB_OK) s = select_device(opts, &p->device);
+    if (s == QB_OK) s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
+    if (s != QB_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return QB_OK;
+}
+
+extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts* opts, qb_problem** out) {
+    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_residual: null argument");
+    *out = nullptr;
+    qb_status s = check_residual(desc);
+    if (s != QB_OK) return s;
+    qb_problem* p = new (std::nothrow) qb_problem();
+    if (!p) return fail(QB_ENOMEM, "qb_problem_create_residual: out of host memory");
+    p->kind = QB_KIND_RESIDUAL;
+    s = plan_residual(desc, p->resid);
+    if (s == QB_OK) s = select_device(opts, &p->device);
+    if (s == QB_OK) s = resid_check_fit(p->resid);
+    if (s == QB_OK) s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
+    if (s != QB_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return QB_OK;
+}
+
+extern "C" void qb_problem_destroy(qb_problem* p) {
+    if (!p) return;
+    cudaSetDevice(p->device);
+    delete p;
+}
+
+extern "C" qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* info) {
+    if (!p || !info) return fail(QB_EINVAL, "qb_problem_info_get: null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->kind = p->kind;
+    info->device_bytes = p->device_bytes;
+    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->resid.col;
+    info->n_colours = C.n_colours();
+    for (int k = 0; k < C.n_colours(); ++k)
+        info->max_class = std::max(info->max_class, C.class_ptr[size_t(k) + 1] - C.class_ptr[size_t(k)]);
+    if (p->kind == QB_KIND_ISING) {
+        const IsingPlan& P = p->ising;
+        info->n = P.n;
+        info->nnz = P.nnz;
+        info->field_bytes = 4;
+        info->weight_bytes = P.weight_bytes;
+        info->sigma = P.sigma;
+        info->w_min = double(P.w_min);
+        info->field_bound = P.B;
+    } else {
+        const ResidualPlan& P = p->resid;
+        info->n = P.n;
+        info->nnz = P.nnz;
+        info->n_rays = P.n_rays;
+        info->field_bytes = 4;
+        info->weight_bytes = 4;
+    }
+    return QB_OK;
+}
+
+extern "C" qb_status qb_problem_colouring(const qb_problem* p, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
+    if (!p) return fail(QB_EINVAL, "qb_problem_colouring: null problem");
+    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->resid.col;
+    if (order) std::memcpy(order, C.order.data(), C.order.size() * sizeof(int32_t));
+    if (class_ptr) std::memcpy(class_ptr, C.class_ptr.data(), C.class_ptr.size() * sizeof(int32_t));
+    if (n_colours) *n_colours = C.n_colours();
+    return QB_OK;
+}
+
+extern "C" qb_status qb_colour_ising(const qb_ising_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
+    if (!desc) return fail(QB_EINVAL, "qb_colour_ising: null descriptor");
+    IsingPlan P;
+    qb_status s = plan_ising(desc, P);
+    if (s != QB_OK) return s;
+    if (order) std::memcpy(order, P.col.order.data(), P.col.order.size() * sizeof(int32_t));
+    if (class_ptr) std::memcpy(class_ptr, P.col.class_ptr.data(), P.col.class_ptr.size() * sizeof(int32_t));
+    if (n_colours) *n_colours = P.col.n_colours();
+    return QB_OK;
+}
+
+extern "C" qb_status qb_colour_residual(const qb_residual_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
+    if (!desc) return fail(QB_EINVAL, "qb_colour_residual: null descriptor");
+    qb_status s = check_residual(desc);
+    if (s != QB_OK) return s;
+    const Colouring c = colour_residual(desc->n_vars, desc->n_rays, desc->row_ptr, desc->ray, desc->nbr_ptr, desc->nbr);
+    if (order) std::memcpy(order, c.order.data(), c.order.size() * sizeof(int32_t));
+    if (class_ptr) std::memcpy(class_ptr, c.class_ptr.data(), c.class_ptr.size() * sizeof(int32_t));
+    if (n_colours) *n_colours = c.n_colours();
+    return QB_OK;
+}
+
+extern "C" qb_status qb_schedule_scaled(const qb_problem* p, int32_t anneal_sweeps, int32_t hold_sweeps, qb_schedule* out) {
+    if (!p || !out) return fail(QB_EINVAL, "qb_schedule_scaled: null argument");
+    if (p->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_schedule_scaled: ising problems only");
+    out->t_hot = p->ising.sigma;
+    out->t_cold = 0.1 * double(p->ising.w_min);
+    out->anneal_sweeps = anneal_sweeps;
+    out->hold_sweeps = hold_sweeps;
+    out->refresh_sweeps = 0;
+    return QB_OK;
+}
+
+// ---- solve ---------------------------------------------------------------------------------------
+
+extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_branches, uint64_t seed_offset,
+                              const qb_opts* opts, qb_result** out) {
+    if (!p || !out) return fail(QB_EINVAL, "qb_solve: null argument");
+    *out = nullptr;
+    qb_status s = check_schedule(sch);
+    if (s != QB_OK) return s;
+    if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_solve: n_branches must be in [1, 2^20]");
+    QB_CUDA(cudaSetDevice(p->device));
+    cudaStream_t st = stream_of(opts);
+    qb_result* r = new (std::nothrow) qb_result();
+    if (!r) return fail(QB_ENOMEM, "qb_solve: out of host memory");
+    r->prob = p;
+    r->device = p->device;
+    r->stream = st;
+    r->R = int(n_branches);
+    r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
+    const int R = r->R;
+    const int n = p->kind == QB_KIND_ISING ? p->ising.n : p->resid.n;
+    r->n = n;
+    const uint64_t seed0 = 1 + seed_offset;   // branch b: seed b + 1 + offset (ising_recon.hpp:157)
+    auto bail = [&](qb_status e) {
+        qb_result_destroy(r);
+        return e;
+    };
+    const bool same = p->d_temp.p && p->temp_sched.t_hot == sch->t_hot && p->temp_sched.t_cold == sch->t_cold &&
+                      p->temp_sched.anneal_sweeps == sch->anneal_sweeps && p->temp_sched.hold_sweeps == sch->hold_sweeps;
+    if (!same) {
+        const std::vector<double> temp = temperatures(*sch);
+        QB_CUDA(cudaStreamSynchronize(st));   // a solve in flight may still read the old table
+        if ((s = upload_vec(p->d_temp, temp, st))) return bail(s);
+        QB_CUDA(cudaStreamSynchronize(st));
+        p->temp_sched = *sch;
+    }
+    if ((s = alloc_async(r->d_x, size_t(R) * size_t(n), st))) return bail(s);
+    if ((s = alloc_async(r->d_e_f64, size_t(R) * sizeof(double), st))) return bail(s);
+    if ((s = alloc_async(r->d_p, size_t(n) * sizeof(float), st))) return bail(s);
+    if (cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+        cudaEventCreate(&r->ev2) != cudaSuccess)
+        return bail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
+    SolveBuffers b;
+    b.x = r->d_x.as<uint8_t>();
+    b.e_f64 = r->d_e_f64.as<double>();
+    b.p = r->d_p.as<float>();
+    b.temp = p->d_temp.as<double>();
+    if (p->kind == QB_KIND_ISING) {
+        const IsingPlan& P = p->ising;
+        if ((s = alloc_async(r->d_f, size_t(R) * size_t(n) * 4, st))) return bail(s);
+        if ((s = alloc_async(r->d_e_i64, size_t(R) * 8, st))) return bail(s);
+        if ((s = alloc_async(r->d_e_scr, size_t(R) * 8, st))) return bail(s);
+        if (ising_smem_bytes(P) == 0 && (s = alloc_async(r->d_scratch, size_t(R) * size_t(n) * 5, st))) return bail(s);
+        b.f = r->d_f.as<int32_t>();
+        b.e_i64 = r->d_e_i64.as<long long>();
+        b.scratch = r->d_scratch.p;
+        cudaEventRecord(r->ev0, st);
+        if ((s = launch_ising_anneal(P, b, R, r->sweeps, seed0, st))) return bail(s);
+        cudaEventRecord(r->ev1, st);
+        if ((s = launch_ising_energies(P, b.x, R, r->d_e_scr.as<long long>(), st))) return bail(s);
+        if ((s = launch_i64_to_f64(r->d_e_scr.as<long long>(), R, b.e_f64, st))) return bail(s);
+        r->launches = 3;
+    } else {
+        const ResidualPlan& P = p->resid;
+        if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
+        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess)
+            return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+        b.drift = r->d_drift.as<float>();
+        cudaEventRecord(r->ev0, st);
+        if ((s = launch_resid_anneal(P, b, R, r->sweeps, sch->refresh_sweeps, seed0, st))) return bail(s);
+        cudaEventRecord(r->ev1, st);
+        if ((s = launch_resid_energies(P, b.x, R, b.e_f64, st))) return bail(s);
+        r->launches = 2;
+    }
+    if ((s = launch_marginals(b.x, R, n, b.p, st))) return bail(s);
+    r->launches += 1;
+    cudaEventRecord(r->ev2, st);
+    *out = r;
+    return QB_OK;
+}
+
+extern "C" qb_status qb_result_info_get(qb_result* r, qb_result_info* info) {
+    if (!r || !info) return fail(QB_EINVAL, "qb_result_info_get: null argument");
+    QB_CUDA(cudaSetDevice(r->device));
+    qb_status s = wait(r);
+    if (s != QB_OK) return s;
+    std::memset(info, 0, sizeof(*info));
+    info->n = r->n;
+    info->n_branches = r->R;
+    info->sweeps = r->sweeps;
+    info->launches = r->launches;
+    info->attempts = int64_t(r->R) * int64_t(r->sweeps) * int64_t(r->n);
+    QB_CUDA(cudaEventElapsedTime(&info->anneal_ms, r->ev0, r->ev1));
+    QB_CUDA(cudaEventElapsedTime(&info->total_ms, r->ev0, r->ev2));
+    if (r->prob->kind == QB_KIND_RESIDUAL) {
+        std::vector<float> dr(static_cast<size_t>(r->R));
+        QB_CUDA(cudaMemcpy(dr.data(), r->d_drift.p, dr.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (float v : dr) info->max_drift = std::max(info->max_drift, double(v));
+    }
+    return QB_OK;
+}
+
+extern "C" qb_status qb_result_branches(qb_result* r, uint8_t* x) {
+    if (!r) return fail(QB_EINVAL, "qb_result_branches: null result");
+    return download(r, x, r->d_x, size_t(r->R) * size_t(r->n));
+}
+
+extern "C" qb_status qb_result_energies_i64(qb_result* r, int64_t* e) {
+    if (!r) return fail(QB_EINVAL, "qb_result_energies_i64: null result");
+    if (r->prob->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_result_energies_i64: ising problems only");
+    return download(r, e, r->d_e_i64, size_t(r->R) * 8);
+}
+
+extern "C" qb_status qb_result_fields_i64(qb_result* r, int64_t* f) {
+    if (!r || !f) return fail(QB_EINVAL, "qb_result_fields_i64: null argument");
+    if (r->prob->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_result_fields_i64: ising problems only");
+    std::vector<int32_t> f32(size_t(r->R) * size_t(r->n));
+    qb_status s = download(r, f32.data(), r->d_f, f32.size() * 4);
+    if (s != QB_OK) return s;
+    for (size_t k = 0; k < f32.size(); ++k) f[k] = f32[k];
+    return QB_OK;
+}
+
+extern "C" qb_status qb_result_energies_f64(qb_result* r, double* e) {
+    if (!r) return fail(QB_EINVAL, "qb_result_energies_f64: null result");
+    return download(r, e, r->d_e_f64, size_t(r->R) * 8);
+}
+
+extern "C" qb_status qb_result_marginals(qb_result* r, float* p) {
+    if (!r) return fail(QB_EINVAL, "qb_result_marginals: null result");
+    return download(r, p, r->d_p, size_t(r->n) * 4);
+}
+
+extern "C" qb_status qb_result_tristate(qb_result* r, float lo, float hi, uint8_t* bits) {
+    if (!r || !bits) return fail(QB_EINVAL, "qb_result_tristate: null argument");
+    if (!(lo <= hi)) return fail(QB_EINVAL, "qb_result_tristate: needs lo <= hi");
+    QB_CUDA(cudaSetDevice(r->device));
+    DevBuf tmp;
+    qb_status s = alloc_async(tmp, size_t(r->n), r->stream);
+    if (s != QB_OK) return s;
+    s = launch_tristate(r->d_p.as<float>(), r->n, lo, hi, tmp.as<uint8_t>(), r->stream);
+    if (s == QB_OK) s = download(r, bits, tmp, size_t(r->n));
+    free_async(tmp, r->stream);
+    return s;
+}
+
+extern "C" void qb_result_destroy(qb_result* r) {
+    if (!r) return;
+    cudaSetDevice(r->device);
+    cudaStream_t st = r->stream;
+    DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift, &r->d_scratch};
+    for (DevBuf* b : all) free_async(*b, st);
+    if (r->ev0) cudaEventDestroy(r->ev0);
+    if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->ev2) cudaEventDestroy(r->ev2);
+    delete r;
+}
+
+// ---- evaluators -------------------------------------------------------------------------------
+
+extern "C" qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e) {
+    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_ising: bad argument");
+    if (p->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_energies_ising: ising problems only");
+    if (k == 0) return QB_OK;
+    QB_CUDA(cudaSetDevice(p->device));
+    DevBuf dx, de;
+    qb_status s;
+    if ((s = upload(dx, x, size_t(k) * size_t(p->ising.n), nullptr))) return s;
+    if ((s = de.alloc(size_t(k) * 8))) return s;
+    if ((s = launch_ising_energies(p->ising, dx.as<uint8_t>(), k, de.as<long long>(), nullptr))) return s;
+    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+    return QB_OK;
+}
+
+extern "C" qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x, int32_t k, double* e) {
+    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_residual: bad argument");
+    if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_energies_residual: residual problems only");
+    if (k == 0) return QB_OK;
+    QB_CUDA(cudaSetDevice(p->device));
+    DevBuf dx, de;
+    qb_status s;
+    if ((s = upload(dx, x, size_t(k) * size_t(p->resid.n), nullptr))) return s;
+    if ((s = de.alloc(size_t(k) * 8))) return s;
+    if ((s = launch_resid_energies(p->resid, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
+    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+    return QB_OK;
+}

@@ -1,0 +1,116 @@
+// Greedy colourings that turn a sequential Metropolis sweep into a sequence
+// of conflict-free parallel steps.
+//
+// The reference sweeps bits in index order (ising_weighted.hpp:258,
+// ising_recon.hpp:132) and parallelises only across replicas, or speculates
+// on a 32-spin window (ising_gpu.cuh:207-246). Here every bit of a class can
+// be updated at once because no two of them share a coupling (Ising) or a ray
+// or a prior bond (residual form): the dE each one sees is exact.
+#include <algorithm>
+#include <cstring>
+
+#include "qb_internal.hpp"
+
+namespace qb {
+
+void finish_colouring(Colouring& c, int n) {
+    int nc = 0;
+    for (int i = 0; i < n; ++i) nc = std::max(nc, c.colour[size_t(i)] + 1);
+    c.class_ptr.assign(size_t(nc) + 1, 0);
+    for (int i = 0; i < n; ++i) c.class_ptr[size_t(c.colour[size_t(i)]) + 1]++;
+    for (int k = 0; k < nc; ++k) c.class_ptr[size_t(k) + 1] += c.class_ptr[size_t(k)];
+    std::vector<int32_t> fill(c.class_ptr.begin(), c.class_ptr.end() - 1);
+    c.order.assign(size_t(n), 0);
+    c.inverse.assign(size_t(n), 0);
+    for (int i = 0; i < n; ++i) {   // stable: original order inside a class
+        const int k = fill[size_t(c.colour[size_t(i)])]++;
+        c.order[size_t(k)] = i;
+        c.inverse[size_t(i)] = k;
+    }
+}
+
+Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector<int32_t>& col) {
+    Colouring c;
+    c.colour.assign(size_t(n), -1);
+    // Largest degree first (Welsh-Powell order), ties by index: fewer classes
+    // than index order on irregular graphs, identical on regular ones.
+    std::vector<int32_t> vis(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
+    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) {
+        return row[size_t(a) + 1] - row[size_t(a)] > row[size_t(b) + 1] - row[size_t(b)];
+    });
+    std::vector<int32_t> mark;   // mark[colour] == i: colour used by a neighbour of i
+    for (int i : vis) {
+        for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k) {
+            const int cj = c.colour[size_t(col[size_t(k)])];
+            if (cj >= 0) {
+                if (size_t(cj) >= mark.size()) mark.resize(size_t(cj) + 1, -1);
+                mark[size_t(cj)] = i;
+            }
+        }
+        int cc = 0;
+        while (size_t(cc) < mark.size() && mark[size_t(cc)] == i) ++cc;
+        c.colour[size_t(i)] = cc;
+    }
+    finish_colouring(c, n);
+    return c;
+}
+
+Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32_t* ray,
+                          const int32_t* nbr_ptr, const int32_t* nbr) {
+    Colouring c;
+    c.colour.assign(size_t(n), -1);
+    // Per-ray bitset of the colours already on the ray. Grown in 64-colour
+    // words when a bit runs out of free colours.
+    int words = 4;
+    std::vector<uint64_t> used(size_t(n_rays) * size_t(words), 0);
+    std::vector<uint64_t> forbid;
+    auto grow = [&](int new_words) {
+        std::vector<uint64_t> g(size_t(n_rays) * size_t(new_words), 0);
+        for (int b = 0; b < n_rays; ++b)
+            std::memcpy(&g[size_t(b) * size_t(new_words)], &used[size_t(b) * size_t(words)],
+                        sizeof(uint64_t) * size_t(words));
+        used.swap(g);
+        words = new_words;
+    };
+    // Visit bits with the most rays first: long conflict lists get the low
+    // colours, which keeps the class count near the longest ray.
+    std::vector<int32_t> vis(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
+    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) {
+        return row_ptr[a + 1] - row_ptr[a] > row_ptr[b + 1] - row_ptr[b];
+    });
+    for (int i : vis) {
+        for (;;) {
+            forbid.assign(size_t(words), 0);
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+                const uint64_t* u = &used[size_t(ray[k]) * size_t(words)];
+                for (int q = 0; q < words; ++q) forbid[size_t(q)] |= u[q];
+            }
+            for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
+                const int cj = c.colour[size_t(nbr[k])];
+                if (cj >= 0 && cj < 64 * words) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
+            }
+            int cc = -1;
+            for (int q = 0; q < words && cc < 0; ++q)
+                if (~forbid[size_t(q)]) cc = 64 * q + __builtin_ctzll(~forbid[size_t(q)]);
+            if (cc < 0) { grow(words * 2); continue; }
+            c.colour[size_t(i)] = cc;
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+                used[size_t(ray[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
+            break;
+        }
+    }
+    finish_colouring(c, n);
+    return c;
+}
+
+bool colouring_valid_graph(const Colouring& c, const std::vector<int64_t>& row, const std::vector<int32_t>& col) {
+    const int n = int(c.colour.size());
+    for (int i = 0; i < n; ++i)
+        for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k)
+            if (c.colour[size_t(col[size_t(k)])] == c.colour[size_t(i)]) return false;
+    return true;
+}
+
+}  // namespace qb

@@ -1,0 +1,158 @@
+// Internal host-side types of the B200 annealer: problem plans, device
+// buffers, error plumbing. Nothing here crosses the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "qublar.h"
+
+namespace qb {
+
+// ---- errors ------------------------------------------------------------------
+
+void set_error(const std::string& msg);
+qb_status fail(qb_status s, const std::string& msg);
+qb_status cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define QB_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) return ::qb::cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+// ---- device buffer (RAII, library-owned) -------------------------------------
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    qb_status alloc(size_t n);
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+qb_status upload(DevBuf& dst, const void* src, size_t bytes, cudaStream_t st);
+
+template <typename T>
+qb_status upload_vec(DevBuf& dst, const std::vector<T>& v, cudaStream_t st) {
+    return upload(dst, v.data(), v.size() * sizeof(T), st);
+}
+
+// ---- colouring ----------------------------------------------------------------
+
+// A sweep order: bits grouped by colour class. order[k] is the original index
+// of the k-th bit of the sweep; class c occupies order[class_ptr[c] ..
+// class_ptr[c+1]). No two bits of one class interact.
+struct Colouring {
+    std::vector<int32_t> colour;      // per original bit
+    std::vector<int32_t> order;       // new -> old
+    std::vector<int32_t> inverse;     // old -> new
+    std::vector<int32_t> class_ptr;   // n_colours + 1
+    int n_colours() const { return int(class_ptr.size()) - 1; }
+};
+
+// Greedy first-fit distance-1 colouring of a symmetric graph given in CSR.
+Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector<int32_t>& col);
+
+// Colouring of the residual conflict graph: bits conflict when they share a
+// ray or are neighbours in the prior. Rays are cliques, handled with per-ray
+// used-colour bitsets (no explicit conflict graph is built).
+Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32_t* ray,
+                          const int32_t* nbr_ptr, const int32_t* nbr);
+
+void finish_colouring(Colouring& c, int n);
+
+// True when no class holds two interacting bits (test hook).
+bool colouring_valid_graph(const Colouring& c, const std::vector<int64_t>& row, const std::vector<int32_t>& col);
+
+// ---- problems -----------------------------------------------------------------
+
+struct IsingPlan {
+    int n = 0;
+    int64_t m = 0;
+    int64_t nnz = 0;          // 2m
+    int64_t B = 0;            // max_i sum_j |w_ij|
+    int64_t max_w = 0;
+    int64_t w_min = 0;
+    double sigma = 0.0;
+    int weight_bytes = 4;     // 1 (int8) or 4
+    Colouring col;
+    // host copies in sweep (new) order
+    std::vector<int32_t> row;    // n + 1 (int32 offsets: nnz < 2^31 is required)
+    std::vector<int32_t> adj;    // nnz, new indices
+    std::vector<int32_t> wgt;    // nnz
+    std::vector<int32_t> f0;     // fields of x = 0, new order
+    // device
+    DevBuf d_row, d_adj, d_w, d_f0, d_order, d_class_ptr;
+    DevBuf d_eu, d_ev, d_ew;     // edge list as given (energy verifier)
+};
+
+struct ResidualPlan {
+    int n = 0;
+    int n_rays = 0;
+    int64_t nnz = 0;
+    int64_t n_nbr = 0;
+    double lambda = 0.0;
+    Colouring col;
+    // cluster decomposition of one branch: CL CTAs; ray b lives on CTA b % CL,
+    // slot b / CL; bit k of class c belongs to CTA t = (k - class start) / chunk(c)
+    int CL = 8;
+    int ray_slots = 0;
+    int bit_slots = 0;
+    std::vector<int32_t> slot_base;   // n_colours * CL: first slot of (class, CTA)
+    std::vector<uint32_t> bit_home;   // new bit -> (cta << 27) | slot
+    // device arrays in sweep order
+    DevBuf d_row, d_ray, d_a, d_lin, d_q, d_nbr_ptr, d_nbr_home, d_order, d_class_ptr, d_slot_base;
+    DevBuf d_d, d_w64, d_wf;          // per ray
+    DevBuf d_rrow, d_rbit, d_ra;      // ray-major CSR for refresh (bit as home word)
+    // energy verifier (original order)
+    DevBuf d_o_row, d_o_ray, d_o_a, d_o_nbr_ptr, d_o_nbr, d_o_lin;
+    DevBuf d_o_rrow, d_o_rbit, d_o_ra;
+};
+
+}  // namespace qb
+
+struct qb_problem {
+    int kind = 0;
+    int device = 0;
+    qb::IsingPlan ising;
+    qb::ResidualPlan resid;
+    int64_t device_bytes = 0;
+    // temperature table of the last schedule solved (reused while unchanged:
+    // no pageable upload, hence no stream synchronisation, per solve)
+    qb_schedule temp_sched{};
+    qb::DevBuf d_temp;
+};
+
+struct qb_result {
+    qb_problem* prob = nullptr;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0;
+    int R = 0;
+    int sweeps = 0;
+    int launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;   // start, anneal end, solve end
+    qb::DevBuf d_x;          // R x n uint8, original order
+    qb::DevBuf d_f;          // R x n int32 fields (ising), original order
+    qb::DevBuf d_e_i64;      // R tracked energies (ising)
+    qb::DevBuf d_e_scr;      // R energies from scratch over the edge list (ising)
+    qb::DevBuf d_e_f64;      // R energies from scratch
+    qb::DevBuf d_p;          // n marginals
+    qb::DevBuf d_temp;       // sweeps temperatures
+    qb::DevBuf d_drift;      // R floats
+    qb::DevBuf d_scratch;    // per-branch state that does not fit on chip
+    bool synced = false;
+};

@@ -1,0 +1,103 @@
+"""Writes the golden fixtures of tests/golden from the reference.
+
+Run in a checkout where the reference tree is present (QUBLAR_REFERENCE,
+default /root/reference) and oracle/_ref/libqbref.so has been built from it
+(``make -C oracle``). Two kinds of fixtures:
+
+* ree_qubo.json -- the reference's committed REE sequencing QUBOs (six
+  instances), its brute-force minima, its engine_check maxima and its per-seed
+  anneal_branch energies (experiments/ree_cascade/*.csv, *.txt), copied as data;
+* ref_runs.npz -- outputs of the reference's own annealers run here through
+  oracle/_ref: wising::anneal on the 800-node ER Max-Cut instance and
+  anneal_branch on the small pyramid, 64 seeds each (final energies, per-sweep
+  energy traces, per-bit void fractions).
+"""
+import csv
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle as O  # noqa: E402
+from qublar_b200 import synth  # noqa: E402
+
+REF = os.environ.get("QUBLAR_REFERENCE", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+REE_IDS = ["MP_P507-A", "MP_P507-B", "R4_0", "R5_0", "R8_3", "R12_0"]
+SEEDS = 64
+
+
+def ree():
+    base = os.path.join(REF, "experiments", "ree_cascade")
+    inst = {}
+    for iid in REE_IDS:
+        with open(os.path.join(base, f"qubo_{iid}.txt")) as f:
+            head = f.readline().split()
+            nv, nt = int(head[0]), int(head[1])
+            rec = {"n": nv, "offset": float(head[2]), "P": float(head[3]), "opt": float(head[4]), "Qd": [], "cost": [],
+                   "pairs": [], "vals": []}
+            for _ in range(nv):
+                i, qd, c = f.readline().split()
+                rec["Qd"].append(float(qd))
+                rec["cost"].append(float(c))
+            for _ in range(nt):
+                i, j, v = f.readline().split()
+                rec["pairs"].append([int(i), int(j)])
+                rec["vals"].append(float(v))
+        inst[iid] = rec
+    with open(os.path.join(base, "brute_force.csv")) as f:
+        brute = {r["id"]: r for r in csv.DictReader(f)}
+    with open(os.path.join(base, "energy_check.csv")) as f:
+        echeck = {r["id"]: float(r["max_abs_diff"]) for r in csv.DictReader(f) if r["id"] in REE_IDS}
+    runs = {iid: {"seed": [], "energy": [], "hit": []} for iid in REE_IDS}
+    with open(os.path.join(base, "engine_runs.csv")) as f:
+        for r in csv.DictReader(f):
+            if r["id"] in runs:
+                runs[r["id"]]["seed"].append(int(r["seed"]))
+                runs[r["id"]]["energy"].append(r["energy"])
+                runs[r["id"]]["hit"].append(int(r["hit"]))
+    out = {"source": "experiments/ree_cascade (qubo_*.txt, brute_force.csv, energy_check.csv, engine_runs.csv)",
+           "schedule": {"t_hot": 5.0, "t_cold": 1e-3, "anneal_sweeps": 400, "hold_sweeps": 20},
+           "instances": inst, "brute_force": brute, "energy_check": echeck, "engine_runs": runs}
+    with open(os.path.join(OUT, "ree_qubo.json"), "w") as f:
+        json.dump(out, f, indent=0)
+
+
+def ref_runs():
+    res = {}
+    # 800-node ER Max-Cut, T 3 -> 0.05 geometric over 1000 sweeps
+    g = O.Graph(*synth.erdos_renyi(800, 0.06, 1))
+    rg = O.RefGraph(g.rudy())
+    E, T = [], []
+    for s in range(1, SEEDS + 1):
+        x, e, tr = rg.trace(3.0, 0.05, 1000, 0, s)
+        E.append(e)
+        T.append(tr)
+    res["er800_energy"] = np.array(E, np.int64)
+    res["er800_trace_mean"] = np.mean(T, 0)
+    res["er800_trace_var"] = np.var(T, 0, ddof=1)
+    res["er800_m"] = np.int64(g.m)
+    # small pyramid, the posterior schedule 50 -> 1, 200 + 50
+    a = synth.tomography(synth.small_tomo_params())
+    rp = O.RefProblem(a)
+    X, T = [], []
+    for s in range(1, SEEDS + 1):
+        x, tr = rp.trace(50.0, 1.0, 200, 50, s)
+        X.append(x)
+        T.append(tr)
+    X = np.array(X, np.uint8)
+    res["tomo_small_frac"] = X.mean(0)
+    res["tomo_small_energy"] = np.array([t[-1] for t in T])
+    res["tomo_small_trace_mean"] = np.mean(T, 0)
+    res["tomo_small_trace_var"] = np.var(T, 0, ddof=1)
+    res["tomo_small_n"] = np.int64(X.shape[1])
+    np.savez_compressed(os.path.join(OUT, "ref_runs.npz"), **res)
+
+
+if __name__ == "__main__":
+    ree()
+    ref_runs()
+    print("golden fixtures written to", OUT)
