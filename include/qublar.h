@@ -143,7 +143,17 @@ typedef struct qb_problem_info {
     double sigma;           /* ising: sqrt(2 sum w^2 / n) (ising_gpu.cuh:99) */
     double w_min;           /* ising: min |w| over w != 0 */
     int64_t field_bound;    /* ising: max_i sum_j |w_ij| (ising_gpu.cuh:87-92) */
+    int32_t variant;        /* residual: QB_RESID_LOCKSTEP or QB_RESID_CLUSTER */
 } qb_problem_info;
+
+/* Residual sweep variants (qb_problem_info.variant). LOCKSTEP: every branch
+ * on one cooperative grid, residuals in L2, a bounded grid barrier per colour
+ * class; a bit's sum is the even-entry fmaf chain plus the odd-entry chain.
+ * CLUSTER: one thread-block cluster per branch, residuals in distributed
+ * shared memory; a bit's sum is 8 (or, above 64 rays, 32) lane-strided fmaf
+ * chains joined by an xor butterfly. */
+#define QB_RESID_LOCKSTEP 1
+#define QB_RESID_CLUSTER 2
 qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* info);
 
 /* The sweep order of the plan: order[k] is the bit (input index) visited k-th
@@ -180,6 +190,7 @@ typedef struct qb_result_info {
     float total_ms;         /* CUDA-event time of the whole solve */
     int64_t attempts;       /* n_branches * sweeps * n */
     double max_drift;       /* residual: max |fp32 residual - fp64 residual| seen at refreshes */
+    int64_t accepted;       /* residual: accepted flips over all branches and sweeps */
 } qb_result_info;
 /* Waits for the solve. */
 qb_status qb_result_info_get(qb_result* r, qb_result_info* info);

@@ -34,6 +34,7 @@ typedef struct qb_tomo_params {
     double theta_max;
     double phi_half;         /* azimuth half-window around the direction to the axis, radians (pi = all) */
     int32_t sub_rays;        /* chords of a bin are averaged over sub_rays^2 sub-rays (1 = centre line) */
+    double room_radius;      /* cells closer than this to a detector carry no bit (its room) */
     double mu_rock;          /* rock attenuation */
     double void_center[3];   /* cubic void of air with known truth */
     double void_side;

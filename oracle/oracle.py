@@ -60,7 +60,7 @@ def orc() -> C.CDLL:
             "orc_binary_energy_batch": (None, [C.POINTER(ResidDesc), P, I64, P]),
             "orc_local_field_dE": (D, [C.POINTER(ResidDesc), P, P, C.c_int]),
             "orc_anneal_branch": (None, [C.POINTER(ResidDesc), D, D, C.c_int, C.c_int, U64, P, P]),
-            "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, P, P, P]),
+            "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, C.c_int, P, P, P]),
             "orc_classify": (None, [P, I64, C.c_float, C.c_float, P]),
             "orc_fractions": (None, [P, C.c_int, I64, P]),
         }
@@ -211,7 +211,8 @@ def anneal_branch(arr: dict, t_hot, t_cold, anneal, hold, seed, trace=False):
     return (x, tr) if trace else x
 
 
-def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False):
+def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False, mode=1):
+    """mode: the summation order of the kernel variant (1 lockstep, 2 cluster)."""
     d = resid_desc(arr)
     n = int(arr["row_ptr"].size - 1)
     order = np.ascontiguousarray(order, np.int32)
@@ -219,8 +220,8 @@ def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False):
     x = np.empty(n, np.uint8)
     drift = C.c_float(0.0)
     tr = np.empty(temps.size, np.float64) if trace else None
-    orc().orc_resid_anneal_coloured(C.byref(d), _p(order), _p(temps), int(temps.size), int(refresh), seed, _p(x),
-                                    C.byref(drift), _p(tr))
+    orc().orc_resid_anneal_coloured(C.byref(d), _p(order), _p(temps), int(temps.size), int(refresh), seed, int(mode),
+                                    _p(x), C.byref(drift), _p(tr))
     return (x, float(drift.value), tr) if trace else (x, float(drift.value))
 
 

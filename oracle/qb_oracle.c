@@ -12,14 +12,22 @@
  *  2. The coloured-Philox annealers: the same Metropolis rule and evaluators,
  *     visiting bits in the plan's colour-class order with Philox4x32-10 draws
  *     keyed by (seed, bit, sweep), and -- for the residual form -- the same
- *     fp32 operation order as the sm_100a kernels (a 32-lane strided sum and an
- *     xor butterfly). The GPU must match these bit-for-bit.
+ *     fp32 operation order as the sm_100a kernels (lane-strided fmaf chains per
+ *     bit joined by an xor butterfly). The GPU must match these bit-for-bit.
  *
  * Build: gcc -O2 -std=c11 -ffp-contract=off (no FMA contraction: every
  * expression rounds like the reference's host code).
  */
 #include <math.h>
 #include <stdint.h>
+
+/* Lanes that share one bit's sum in the residual kernel (kGroup and kHeavy
+ * in qublar_b200/csrc/qb_kernels.cu): a bit with more than ORC_HEAVY rays is
+ * summed by 32 lanes, any other by ORC_GROUP -- the GPU's summation order. */
+#define ORC_GROUP 8
+#define ORC_HEAVY 64
+/* Entries per segment of the lockstep kernel (kSeg in qb_kernels.cu). */
+#define ORC_SEG 16
 #include <stdlib.h>
 #include <string.h>
 
@@ -307,13 +315,16 @@ void orc_anneal_branch(const orc_resid* p, double t_hot, double t_cold, int anne
 /* The coloured-Philox residual annealer, in the fp32 operation order of the
  * sm_100a cluster kernel:
  *   rw_b = float(w_b * (sum a x - d_b)) (weighted residual), q_i = float(sum
- *   0.5 w a a), lin_i = float(lin); h = 32-lane strided fmaf sum of a * rw with
+ *   0.5 w a a), lin_i = float(lin); h = sum of a * rw over the bit's rays in
+ *   the kernel's order: mode 1 (lockstep) 16-entry segments added in order,
+ *   each the fmaf chain over its even entries plus the chain over its odd
+ *   ones; mode 2 (cluster) G = ORC_GROUP or 32 strided fmaf chains joined by
  *   an xor butterfly; dE = ((delta * (lin + h)) + q) + lambda * (deg - 2
  *   unlike); accept as wising::anneal; scatter rw += (float(w) * a) * delta;
- *   fp64 refresh of rw every `refresh` sweeps (same lane/butterfly order in
- *   double, bits of a ray in ascending index). drift_out: max |fp32 - fp64|. */
+ *   fp64 refresh of rw every `refresh` sweeps (a sequential double sum over
+ *   the ray's set bits in ascending index). drift_out: max |fp32 - fp64|. */
 void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const double* temps, int sweeps, int refresh,
-                               uint64_t seed, uint8_t* x, float* drift_out, double* trace) {
+                               uint64_t seed, int mode, uint8_t* x, float* drift_out, double* trace) {
     const int n = p->n_vars, nr = p->n_rays;
     const int64_t nnz = p->row_ptr[n];
     float* rw = (float*)malloc(sizeof(float) * (size_t)(nr > 0 ? nr : 1));
@@ -352,16 +363,10 @@ void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const d
     for (int sweep = 0; sweep < sweeps; ++sweep) {
         if (refresh > 0 && sweep > 0 && sweep % refresh == 0) {
             for (int b = 0; b < nr; ++b) {
-                double acc[32];
-                for (int l = 0; l < 32; ++l) acc[l] = 0.0;
+                double acc = 0.0;
                 for (int k = rrow[b]; k < rrow[b + 1]; ++k)
-                    if (x[rbit[k]]) acc[(k - rrow[b]) & 31] += (double)ra[k];
-                for (int off = 16; off > 0; off >>= 1) {
-                    double nx[32];
-                    for (int l = 0; l < 32; ++l) nx[l] = acc[l] + acc[l ^ off];
-                    memcpy(acc, nx, sizeof acc);
-                }
-                const float nv = (float)(p->w[b] * (acc[0] - p->d[b]));
+                    if (x[rbit[k]]) acc += (double)ra[k];
+                const float nv = (float)(p->w[b] * (acc - p->d[b]));
                 const float dv = fabsf(nv - rw[b]);
                 if (dv > drift) drift = dv;
                 rw[b] = nv;
@@ -370,23 +375,40 @@ void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const d
         const double T = temps[sweep];
         for (int kk = 0; kk < n; ++kk) {
             const int i = order[kk];
-            float acc[32];
-            for (int l = 0; l < 32; ++l) acc[l] = 0.0f;
+            /* ORC_GROUP lanes: lane l sums entries l, l + G, ... as an fmaf
+             * chain; an xor butterfly (G/2, ..., 1) joins them; lane 0 wins */
+            float hl = 0.0f;
+            if (mode == 1) {
+                /* lockstep kernel: 16-entry segments in order; a segment's
+                 * value is its even-entry fmaf chain plus its odd-entry chain */
+                const int r0 = p->row_ptr[i], r1 = p->row_ptr[i + 1];
+                for (int s0 = r0; s0 < r1; s0 += ORC_SEG) {
+                    const int s1 = s0 + ORC_SEG < r1 ? s0 + ORC_SEG : r1;
+                    float ev = 0.0f, od = 0.0f;
+                    for (int k = s0; k < s1; k += 2) ev = fmaf(p->a[k], rw[p->ray[k]], ev);
+                    for (int k = s0 + 1; k < s1; k += 2) od = fmaf(p->a[k], rw[p->ray[k]], od);
+                    hl = hl + (ev + od);
+                }
+            }
+            const int G = mode == 1 ? 1 : (p->row_ptr[i + 1] - p->row_ptr[i] > ORC_HEAVY ? 32 : ORC_GROUP);
+            float lane[32];
+            for (int l = 0; l < G; ++l) lane[l] = 0.0f;
             for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k) {
-                const int l = (k - p->row_ptr[i]) & 31;
-                acc[l] = fmaf(p->a[k], rw[p->ray[k]], acc[l]);
+                const int l = (k - p->row_ptr[i]) % G;
+                lane[l] = fmaf(p->a[k], rw[p->ray[k]], lane[l]);
             }
-            for (int off = 16; off > 0; off >>= 1) {
+            for (int off = G / 2; off > 0; off >>= 1) {
                 float nx[32];
-                for (int l = 0; l < 32; ++l) nx[l] = acc[l] + acc[l ^ off];
-                memcpy(acc, nx, sizeof acc);
+                for (int l = 0; l < G; ++l) nx[l] = lane[l] + lane[l ^ off];
+                memcpy(lane, nx, sizeof(float) * (size_t)G);
             }
+            const float h = mode == 1 ? hl : lane[0];
             const uint8_t xi = x[i];
             int unlike = 0;
             for (int k = p->nbr_ptr[i]; k < p->nbr_ptr[i + 1]; ++k) unlike += x[p->nbr[k]] != xi;
             const int deg = p->nbr_ptr[i + 1] - p->nbr_ptr[i];
             const float delta = xi ? -1.0f : 1.0f;
-            const float t = linf[i] + acc[0];
+            const float t = linf[i] + h;
             const float prior = lam * (float)(deg - 2 * unlike);
             const float dE = (delta * t + qf[i]) + prior;
             const double dEd = (double)dE;

@@ -17,6 +17,8 @@ STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4:
                 5: "QB_ECUDA", 6: "QB_ENOTSUP", 7: "QB_ECANCELLED", 8: "QB_EBUSY"}
 KIND_ISING = 1
 KIND_RESIDUAL = 2
+RESID_LOCKSTEP = 1
+RESID_CLUSTER = 2
 
 
 class QBError(RuntimeError):
@@ -51,13 +53,13 @@ class ProblemInfo(C.Structure):
     _fields_ = [("kind", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64), ("n_rays", C.c_int32),
                 ("n_colours", C.c_int32), ("max_class", C.c_int32), ("field_bytes", C.c_int32),
                 ("weight_bytes", C.c_int32), ("device_bytes", C.c_int64), ("sigma", C.c_double),
-                ("w_min", C.c_double), ("field_bound", C.c_int64)]
+                ("w_min", C.c_double), ("field_bound", C.c_int64), ("variant", C.c_int32)]
 
 
 class ResultInfo(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_branches", C.c_int32), ("sweeps", C.c_int32), ("launches", C.c_int32),
                 ("anneal_ms", C.c_float), ("total_ms", C.c_float), ("attempts", C.c_int64),
-                ("max_drift", C.c_double)]
+                ("max_drift", C.c_double), ("accepted", C.c_int64)]
 
 
 class TomoParams(C.Structure):
@@ -65,7 +67,7 @@ class TomoParams(C.Structure):
                 ("half_base", C.c_double), ("height", C.c_double), ("n_detectors", C.c_int32),
                 ("det", C.c_double * 12), ("n_theta", C.c_int32), ("n_phi", C.c_int32),
                 ("theta_min", C.c_double), ("theta_max", C.c_double), ("phi_half", C.c_double),
-                ("sub_rays", C.c_int32), ("mu_rock", C.c_double), ("void_center", C.c_double * 3),
+                ("sub_rays", C.c_int32), ("room_radius", C.c_double), ("mu_rock", C.c_double), ("void_center", C.c_double * 3),
                 ("void_side", C.c_double), ("exposure", C.c_double), ("min_open", C.c_double),
                 ("lambda_", C.c_double), ("kappa", C.c_double), ("seed", C.c_uint64)]
 

@@ -1,5 +1,6 @@
 // The C ABI (include/qublar.h): validation, planning, upload, solve, results.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -57,6 +58,10 @@ std::vector<double> temperatures(const qb_schedule& s) {
     }
     return t;
 }
+
+// Slices per class the host-only planner assumes for the lockstep sweep (the
+// SM count of a B200); the order inside a class does not change results.
+constexpr int kHostLockSlices = 148;
 
 int env_int(const char* name, int dflt) {
     const char* v = std::getenv(name);
@@ -201,72 +206,181 @@ qb_status check_residual(const qb_residual_desc* d) {
     return QB_OK;
 }
 
-qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P) {
-    const int n = d->n_vars;
+// Host plan of a residual problem: colour classes, each class split into CL
+// slices of about equal work (longest-processing-time first over bit-ray
+// entries), heavy bits (more than resid_heavy_entries() rays) first inside a
+// slice, slices cut into chunks that fit the kernel's stage buffers, and every
+// device array in sweep order. Reordering bits inside a class changes no
+// result: a class holds no two interacting bits.
+qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_slices) {
+    const int n = d->n_vars, nr = d->n_rays;
     P.n = n;
-    P.n_rays = d->n_rays;
+    P.n_rays = nr;
     P.nnz = d->row_ptr[n];
     P.n_nbr = d->nbr_ptr[n];
     P.lambda = d->lambda;
-    P.col = colour_residual(n, d->n_rays, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
-    const Colouring& C = P.col;
+    P.col = colour_residual(n, nr, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
+    Colouring& C = P.col;
     const int nc = C.n_colours();
-    // cluster decomposition: the smallest cluster whose shared memory holds
-    // the branch (QB_RESID_CLUSTER overrides)
+    auto deg = [&](int i) { return d->row_ptr[i + 1] - d->row_ptr[i]; };
+    // variant: lockstep unless QB_RESID_KERNEL=cluster or no cooperative grid
+    const char* kv = std::getenv("QB_RESID_KERNEL");
+    const bool want_cluster = kv && std::strcmp(kv, "cluster") == 0;
+    P.variant = (lock_slices > 0 && !want_cluster) ? QB_RESID_LOCKSTEP : QB_RESID_CLUSTER;
+    P.lock_grid = P.variant == QB_RESID_LOCKSTEP ? lock_slices : 0;
+    // cluster size: the smallest whose shared memory holds one branch
+    // (QB_RESID_CLUSTER overrides)
     int CL = env_int("QB_RESID_CLUSTER", 0);
     const int candidates[2] = {8, 16};
     for (int t = 0; t < 2 && CL == 0; ++t) {
         const int c = candidates[t];
-        int bits = 0;
-        for (int k = 0; k < nc; ++k) bits += (C.class_ptr[size_t(k) + 1] - C.class_ptr[size_t(k)] + c - 1) / c;
-        const size_t bytes = size_t((d->n_rays + c - 1) / c) * 8 + size_t(bits);
-        if (bytes <= size_t(200) * 1024) CL = c;
+        const size_t bytes = size_t((nr + c - 1) / c) * 4 + size_t(n / c + nc + 64) / 8 + resid_stage_bytes();
+        if (bytes <= size_t(112) * 1024) CL = c;
     }
-    if (CL == 0) return fail(QB_ENOTSUP, "residual: the problem exceeds one cluster's shared memory");
-    if (CL != 4 && CL != 8 && CL != 16) return fail(QB_EINVAL, "residual: cluster size must be 4, 8 or 16");
+    if (P.variant == QB_RESID_CLUSTER) {
+        if (CL == 0) return fail(QB_ENOTSUP, "residual: the problem exceeds one cluster's shared memory");
+        if (CL != 4 && CL != 8 && CL != 16) return fail(QB_EINVAL, "residual: cluster size must be 4, 8 or 16");
+    }
+    if (CL == 0) CL = 16;
     P.CL = CL;
-    P.ray_slots = (d->n_rays + CL - 1) / CL;
-    P.slot_base.assign(size_t(nc) * size_t(CL), 0);
+    P.ray_slots = (nr + CL - 1) / CL;
+    const int S = P.variant == QB_RESID_LOCKSTEP ? P.lock_grid : CL;   // slices per class
+    const int heavy = resid_heavy_entries();
+    // balanced slices
+    std::vector<int32_t> slice_ptr(size_t(nc) * size_t(S + 1), 0);   // per class: CL + 1 offsets
+    {
+        std::vector<int32_t> mem, slot_of;
+        std::vector<std::vector<int32_t>> slices(static_cast<size_t>(S));
+        std::vector<int64_t> load(static_cast<size_t>(S));
+        for (int c = 0; c < nc; ++c) {
+            const int cs = C.class_ptr[size_t(c)], ce = C.class_ptr[size_t(c) + 1];
+            mem.assign(C.order.begin() + cs, C.order.begin() + ce);
+            std::stable_sort(mem.begin(), mem.end(), [&](int a, int b) { return deg(a) > deg(b); });
+            for (auto& v : slices) v.clear();
+            std::fill(load.begin(), load.end(), 0);
+            for (int i : mem) {
+                int t = 0;
+                for (int u = 1; u < S; ++u)
+                    if (load[size_t(u)] < load[size_t(t)]) t = u;
+                slices[size_t(t)].push_back(i);
+                load[size_t(t)] += deg(i) + 8;
+            }
+            int pos = cs;
+            for (int t = 0; t < S; ++t) {
+                auto& v = slices[size_t(t)];
+                std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
+                    const bool ha = deg(a) > heavy, hb = deg(b) > heavy;
+                    return ha != hb ? ha : a < b;
+                });
+                slice_ptr[size_t(c) * (S + 1) + size_t(t)] = pos;
+                for (int i : v) C.order[size_t(pos++)] = i;
+            }
+            slice_ptr[size_t(c) * (S + 1) + size_t(S)] = pos;
+        }
+        for (int k = 0; k < n; ++k) C.inverse[size_t(C.order[size_t(k)])] = k;
+    }
+    const bool lock = P.variant == QB_RESID_LOCKSTEP;
+    // homes (cluster variant): bit k of slice t of class c -> (t << 27) |
+    // running slot of CTA t
+    P.slot_base.assign(size_t(nc) * size_t(S), 0);
     P.bit_home.assign(size_t(n), 0);
-    std::vector<int32_t> used(size_t(CL), 0);
-    for (int c = 0; c < nc; ++c) {
-        const int cs = C.class_ptr[size_t(c)], ce = C.class_ptr[size_t(c) + 1];
-        const int chunk = (ce - cs + CL - 1) / CL;
-        for (int t = 0; t < CL; ++t) {
-            P.slot_base[size_t(c) * CL + size_t(t)] = used[size_t(t)];
-            const int b0 = cs + t * chunk, b1 = std::min(b0 + chunk, ce);
-            for (int i = b0; i < b1; ++i) P.bit_home[size_t(i)] = (uint32_t(t) << 27) | uint32_t(used[size_t(t)]++);
+    std::vector<int32_t> used(size_t(S), 0);
+    for (int c = 0; c < nc; ++c)
+        for (int t = 0; t < S; ++t) {
+            P.slot_base[size_t(c) * S + size_t(t)] = used[size_t(t)];
+            const int b0 = slice_ptr[size_t(c) * (S + 1) + size_t(t)], b1 = slice_ptr[size_t(c) * (S + 1) + size_t(t) + 1];
+            for (int i = b0; i < b1; ++i) {
+                if (!lock) P.bit_home[size_t(i)] = (uint32_t(t) << 27) | uint32_t(used[size_t(t)]);
+                used[size_t(t)]++;
+            }
+        }
+    P.bit_slots = *std::max_element(used.begin(), used.end());
+    if (!lock && P.bit_slots >= (1 << 27)) return fail(QB_EREFUSED, "residual: too many bits per CTA");
+    // sweep-order arrays
+    P.h_row.assign(size_t(n) + 1, 0);
+    P.h_ent.assign(size_t(P.nnz) * 4, 0u);
+    P.h_lin.assign(size_t(n), 0.0f);
+    P.h_q.assign(size_t(n), 0.0f);
+    P.h_nbr_ptr.assign(size_t(n) + 1, 0);
+    P.h_nbr_home.assign(size_t(P.n_nbr), 0u);
+    P.h_nbr_new.assign(size_t(P.n_nbr), 0);
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        int32_t pos = P.h_row[size_t(k)];
+        double qd = 0.0;
+        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
+            const float a = d->a[e];
+            const float wa = float(d->w[d->ray[e]]) * a;   // the fp32 scatter increment
+            P.h_ent[size_t(pos) * 4 + 0] = uint32_t(d->ray[e]);
+            std::memcpy(&P.h_ent[size_t(pos) * 4 + 1], &a, 4);
+            std::memcpy(&P.h_ent[size_t(pos) * 4 + 2], &wa, 4);
+            qd += 0.5 * d->w[d->ray[e]] * double(a) * double(a);
+            ++pos;
+        }
+        P.h_row[size_t(k) + 1] = pos;
+        P.h_q[size_t(k)] = float(qd);
+        P.h_lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
+        int32_t np = P.h_nbr_ptr[size_t(k)];
+        for (int e = d->nbr_ptr[i]; e < d->nbr_ptr[i + 1]; ++e) {
+            P.h_nbr_new[size_t(np)] = C.inverse[size_t(d->nbr[e])];
+            P.h_nbr_home[size_t(np++)] = P.bit_home[size_t(C.inverse[size_t(d->nbr[e])])];
+        }
+        P.h_nbr_ptr[size_t(k) + 1] = np;
+    }
+    if (lock) {
+        P.h_meta.assign(size_t(n) * 8, 0u);
+        for (int k = 0; k < n; ++k) {
+            uint32_t* m = &P.h_meta[size_t(k) * 8];
+            m[0] = uint32_t(P.h_row[size_t(k)]);
+            m[1] = uint32_t(P.h_row[size_t(k) + 1] - P.h_row[size_t(k)]);
+            m[2] = uint32_t(P.h_nbr_ptr[size_t(k)]);
+            m[3] = uint32_t(P.h_nbr_ptr[size_t(k) + 1] - P.h_nbr_ptr[size_t(k)]);
+            std::memcpy(&m[4], &P.h_lin[size_t(k)], 4);
+            std::memcpy(&m[5], &P.h_q[size_t(k)], 4);
+            m[6] = uint32_t(C.order[size_t(k)]);
         }
     }
-    P.bit_slots = *std::max_element(used.begin(), used.end());
-    if (P.bit_slots >= (1 << 27)) return fail(QB_EREFUSED, "residual: too many bits per CTA");
+    // chunk table of every CTA (see ResidualPlan)
+    const int kB = lock ? resid_lockstep_chunk_bits() : resid_chunk_bits();
+    const int kE = lock ? resid_lockstep_chunk_entries() : resid_chunk_entries();
+    const int kN = lock ? resid_lockstep_chunk_nbrs() : resid_chunk_nbrs();
+    const std::vector<int32_t>& row = P.h_row;
+    const std::vector<int32_t>& nbp = P.h_nbr_ptr;
+    const int kSeg = lock ? resid_lockstep_segment() : 1;
+    const int kS = lock ? resid_lockstep_chunk_segments() : INT32_MAX;
+    auto segs = [&](int k) { return (row[size_t(k) + 1] - row[size_t(k)] + kSeg - 1) / kSeg; };
+    P.chunks.clear();
+    P.chunk_ptr.assign(size_t(S) + 1, 0);
+    for (int t = 0; t < S; ++t) {
+        for (int c = 0; c < nc; ++c) {
+            const int b0 = slice_ptr[size_t(c) * (S + 1) + size_t(t)], b1 = slice_ptr[size_t(c) * (S + 1) + size_t(t) + 1];
+            const int slot0 = P.slot_base[size_t(c) * S + size_t(t)];
+            int s0 = b0;
+            do {
+                int e = s0, nseg = 0;
+                while (e < b1 && e - s0 < kB && row[size_t(e) + 1] - row[size_t(s0)] <= kE &&
+                       nbp[size_t(e) + 1] - nbp[size_t(s0)] <= kN && (!lock || nseg + segs(e) <= kS)) {
+                    if (lock) P.h_meta[size_t(e) * 8 + 7] = uint32_t(nseg);   // first segment of the bit
+                    nseg += lock ? segs(e) : 0;
+                    ++e;
+                }
+                if (e == s0 && s0 < b1) return fail(QB_ENOTSUP, "residual: a bit has more rays or neighbours than a chunk holds");
+                int nh = 0;
+                while (s0 + nh < e && row[size_t(s0 + nh) + 1] - row[size_t(s0 + nh)] > heavy) ++nh;
+                const int32_t rec[8] = {s0, e, lock ? nseg : slot0 + (s0 - b0), (e == b1 ? 1 : 0) | (nh << 1),
+                                        row[size_t(s0)], row[size_t(e)], nbp[size_t(s0)], nbp[size_t(e)]};
+                P.chunks.insert(P.chunks.end(), rec, rec + 8);
+                s0 = e;
+            } while (s0 < b1);
+        }
+        P.chunk_ptr[size_t(t) + 1] = int32_t(P.chunks.size() / 8);
+    }
     return QB_OK;
 }
 
 qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
-    std::vector<int32_t> row(size_t(n) + 1, 0), ray(static_cast<size_t>(P.nnz)), nbr_ptr(size_t(n) + 1, 0);
-    std::vector<float> a(static_cast<size_t>(P.nnz)), lin(static_cast<size_t>(n)), q(static_cast<size_t>(n));
-    std::vector<uint32_t> nbr_home(static_cast<size_t>(P.n_nbr));
-    for (int k = 0; k < n; ++k) {
-        const int i = C.order[size_t(k)];
-        int32_t pos = row[size_t(k)];
-        double qd = 0.0;
-        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
-            ray[size_t(pos)] = d->ray[e];
-            a[size_t(pos)] = d->a[e];
-            qd += 0.5 * d->w[d->ray[e]] * double(d->a[e]) * double(d->a[e]);
-            ++pos;
-        }
-        row[size_t(k) + 1] = pos;
-        q[size_t(k)] = float(qd);
-        lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
-        int32_t np = nbr_ptr[size_t(k)];
-        for (int e = d->nbr_ptr[i]; e < d->nbr_ptr[i + 1]; ++e)
-            nbr_home[size_t(np++)] = P.bit_home[size_t(C.inverse[size_t(d->nbr[e])])];
-        nbr_ptr[size_t(k) + 1] = np;
-    }
     // ray-major CSR, bits ascending in input order inside a ray: the refresh
     // (bits by home) and the energy verifier (bits by input index)
     std::vector<int32_t> rrow(size_t(nr) + 1, 0);
@@ -274,37 +388,43 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     for (int b = 0; b < nr; ++b) rrow[size_t(b) + 1] += rrow[size_t(b)];
     std::vector<int32_t> rfill(rrow.begin(), rrow.end() - 1), rbit_o(static_cast<size_t>(P.nnz));
     std::vector<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
+    std::vector<int32_t> rbit_n(static_cast<size_t>(P.nnz));
     std::vector<float> ra(static_cast<size_t>(P.nnz));
     for (int i = 0; i < n; ++i)
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
             const int32_t k = rfill[size_t(d->ray[e])]++;
             rbit_o[size_t(k)] = i;
             rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
+            rbit_n[size_t(k)] = C.inverse[size_t(i)];
             ra[size_t(k)] = d->a[e];
         }
-    std::vector<float> wf(static_cast<size_t>(nr));
-    for (int b = 0; b < nr; ++b) wf[size_t(b)] = float(d->w[b]);
     std::vector<double> o_lin(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) o_lin[size_t(i)] = d->field ? d->field[i] : d->kappa;
     qb_status s;
 #define QB_UP(buf, vec) if ((s = upload_vec(P.buf, vec, st))) return s
-    QB_UP(d_row, row); QB_UP(d_ray, ray); QB_UP(d_a, a); QB_UP(d_lin, lin); QB_UP(d_q, q);
-    QB_UP(d_nbr_ptr, nbr_ptr); QB_UP(d_nbr_home, nbr_home); QB_UP(d_order, C.order);
-    QB_UP(d_class_ptr, C.class_ptr); QB_UP(d_slot_base, P.slot_base);
-    QB_UP(d_wf, wf); QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra);
+    QB_UP(d_ent, P.h_ent); QB_UP(d_row, P.h_row); QB_UP(d_lin, P.h_lin); QB_UP(d_q, P.h_q);
+    QB_UP(d_nbr_ptr, P.h_nbr_ptr); QB_UP(d_nbr_home, P.h_nbr_home); QB_UP(d_order, C.order);
+    QB_UP(d_class_ptr, C.class_ptr); QB_UP(d_chunks, P.chunks); QB_UP(d_chunk_ptr, P.chunk_ptr);
+    QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra);
     QB_UP(d_o_rrow, rrow); QB_UP(d_o_rbit, rbit_o); QB_UP(d_o_ra, ra); QB_UP(d_o_lin, o_lin);
+    if (P.variant == QB_RESID_LOCKSTEP) {
+        QB_UP(d_meta, P.h_meta); QB_UP(d_nbr_new, P.h_nbr_new); QB_UP(d_rbit_new, rbit_n);
+    }
 #undef QB_UP
     if ((s = upload(P.d_d, d->d, size_t(nr) * 8, st))) return s;
     if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
     if ((s = upload(P.d_o_nbr_ptr, d->nbr_ptr, (size_t(n) + 1) * 4, st))) return s;
     if ((s = upload(P.d_o_nbr, d->nbr, size_t(P.n_nbr) * 4, st))) return s;
     QB_CUDA(cudaStreamSynchronize(st));   // the host vectors above are locals
-    const DevBuf* all[] = {&P.d_row, &P.d_ray, &P.d_a, &P.d_lin, &P.d_q, &P.d_nbr_ptr, &P.d_nbr_home, &P.d_order,
-                           &P.d_class_ptr, &P.d_slot_base, &P.d_d, &P.d_w64, &P.d_wf, &P.d_rrow, &P.d_rbit,
-                           &P.d_ra, &P.d_o_rrow, &P.d_o_rbit, &P.d_o_ra, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin};
+    const DevBuf* all[] = {&P.d_row, &P.d_ent, &P.d_lin, &P.d_q, &P.d_nbr_ptr, &P.d_nbr_home, &P.d_order,
+                           &P.d_class_ptr, &P.d_chunks, &P.d_chunk_ptr, &P.d_d, &P.d_w64, &P.d_rrow, &P.d_rbit,
+                           &P.d_ra, &P.d_o_rrow, &P.d_o_rbit, &P.d_o_ra, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin,
+                           &P.d_meta, &P.d_nbr_new, &P.d_rbit_new};
     int64_t tot = 0;
     for (const DevBuf* b : all) tot += int64_t(b->bytes);
     *bytes = tot;
+    // the plan's host copies are not needed after the upload
+    std::vector<uint32_t>().swap(P.h_ent);
     return QB_OK;
 }
 
@@ -366,9 +486,9 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
     qb_problem* p = new (std::nothrow) qb_problem();
     if (!p) return fail(QB_ENOMEM, "qb_problem_create_residual: out of host memory");
     p->kind = QB_KIND_RESIDUAL;
-    s = plan_residual(desc, p->resid);
-    if (s == QB_OK) s = select_device(opts, &p->device);
-    if (s == QB_OK) s = resid_check_fit(p->resid);
+    s = select_device(opts, &p->device);
+    if (s == QB_OK) s = plan_residual(desc, p->resid, resid_lockstep_grid());
+    if (s == QB_OK && p->resid.variant == QB_RESID_CLUSTER) s = resid_check_fit(p->resid);
     if (s == QB_OK) s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
     if (s != QB_OK) {
         delete p;
@@ -409,6 +529,7 @@ extern "C" qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* i
         info->n_rays = P.n_rays;
         info->field_bytes = 4;
         info->weight_bytes = 4;
+        info->variant = P.variant;
     }
     return QB_OK;
 }
@@ -437,7 +558,9 @@ extern "C" qb_status qb_colour_residual(const qb_residual_desc* desc, int32_t* o
     if (!desc) return fail(QB_EINVAL, "qb_colour_residual: null descriptor");
     qb_status s = check_residual(desc);
     if (s != QB_OK) return s;
-    const Colouring c = colour_residual(desc->n_vars, desc->n_rays, desc->row_ptr, desc->ray, desc->nbr_ptr, desc->nbr);
+    ResidualPlan P;
+    if ((s = plan_residual(desc, P, kHostLockSlices)) != QB_OK) return s;
+    const Colouring& c = P.col;
     if (order) std::memcpy(order, c.order.data(), c.order.size() * sizeof(int32_t));
     if (class_ptr) std::memcpy(class_ptr, c.class_ptr.data(), c.class_ptr.size() * sizeof(int32_t));
     if (n_colours) *n_colours = c.n_colours();
@@ -519,14 +642,36 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
     } else {
         const ResidualPlan& P = p->resid;
         if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
-        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess)
+        if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
+        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
+            cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess)
             return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
         b.drift = r->d_drift.as<float>();
+        b.accepts = r->d_accepts.as<unsigned long long>();
+        const int RB = std::min(R, resid_lockstep_max_branches());   // branches per lockstep launch
+        if (P.variant == QB_RESID_LOCKSTEP) {
+            if ((s = alloc_async(r->d_scratch, resid_lockstep_scratch(P, RB), st))) return bail(s);
+            b.scratch = r->d_scratch.p;
+        }
         cudaEventRecord(r->ev0, st);
-        if ((s = launch_resid_anneal(P, b, R, r->sweeps, sch->refresh_sweeps, seed0, st))) return bail(s);
+        int anneal_launches = 0;
+        if (P.variant == QB_RESID_LOCKSTEP) {
+            // blocks of at most RB branches, one cooperative launch each
+            for (int b0 = 0; b0 < R && s == QB_OK; b0 += RB, ++anneal_launches) {
+                SolveBuffers bb = b;
+                bb.x = b.x + size_t(b0) * size_t(n);
+                bb.drift = b.drift + b0;
+                s = launch_resid_lockstep(P, bb, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
+                                          seed0 + uint64_t(b0), st);
+            }
+        } else {
+            s = launch_resid_anneal(P, b, R, r->sweeps, sch->refresh_sweeps, seed0, st);
+            anneal_launches = 1;
+        }
+        if (s != QB_OK) return bail(s);
         cudaEventRecord(r->ev1, st);
         if ((s = launch_resid_energies(P, b.x, R, b.e_f64, st))) return bail(s);
-        r->launches = 2;
+        r->launches = anneal_launches + 1;
     }
     if ((s = launch_marginals(b.x, R, n, b.p, st))) return bail(s);
     r->launches += 1;
@@ -552,6 +697,9 @@ extern "C" qb_status qb_result_info_get(qb_result* r, qb_result_info* info) {
         std::vector<float> dr(static_cast<size_t>(r->R));
         QB_CUDA(cudaMemcpy(dr.data(), r->d_drift.p, dr.size() * sizeof(float), cudaMemcpyDeviceToHost));
         for (float v : dr) info->max_drift = std::max(info->max_drift, double(v));
+        std::vector<unsigned long long> ac(size_t(r->R));
+        QB_CUDA(cudaMemcpy(ac.data(), r->d_accepts.p, ac.size() * 8, cudaMemcpyDeviceToHost));
+        for (unsigned long long v : ac) info->accepted += int64_t(v);
     }
     return QB_OK;
 }
@@ -604,7 +752,7 @@ extern "C" void qb_result_destroy(qb_result* r) {
     if (!r) return;
     cudaSetDevice(r->device);
     cudaStream_t st = r->stream;
-    DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift, &r->d_scratch};
+    DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift, &r->d_accepts, &r->d_scratch};
     for (DevBuf* b : all) free_async(*b, st);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);

@@ -100,6 +100,8 @@ struct IsingPlan {
 };
 
 struct ResidualPlan {
+    int variant = 1;                  // QB_RESID_LOCKSTEP or QB_RESID_CLUSTER
+    int lock_grid = 0;                // lockstep: CTAs of the cooperative grid (= slices per class)
     int n = 0;
     int n_rays = 0;
     int64_t nnz = 0;
@@ -113,10 +115,22 @@ struct ResidualPlan {
     int bit_slots = 0;
     std::vector<int32_t> slot_base;   // n_colours * CL: first slot of (class, CTA)
     std::vector<uint32_t> bit_home;   // new bit -> (cta << 27) | slot
+    // chunk table: CTA t works chunks [chunk_ptr[t], chunk_ptr[t+1]), each two
+    // int4 {b0, b1, slot of b0, last chunk of its class} {e0, e1, n0, n1}
+    // (bits, bit-ray entries and neighbour entries of the chunk, sweep order)
+    std::vector<int32_t> chunks;
+    std::vector<int32_t> chunk_ptr;
+    std::vector<int32_t> h_nbr_new;   // neighbours as sweep-order indices
+    std::vector<uint32_t> h_meta;     // lockstep: per bit 8 words {row start, rays, nbr start, nbrs, lin, q, index, 0}
+    // host copies of the sweep-order arrays (h_ent is released after upload)
+    std::vector<int32_t> h_row, h_nbr_ptr;
+    std::vector<uint32_t> h_ent, h_nbr_home;
+    std::vector<float> h_lin, h_q;
     // device arrays in sweep order
-    DevBuf d_row, d_ray, d_a, d_lin, d_q, d_nbr_ptr, d_nbr_home, d_order, d_class_ptr, d_slot_base;
-    DevBuf d_d, d_w64, d_wf;          // per ray
+    DevBuf d_row, d_ent, d_lin, d_q, d_nbr_ptr, d_nbr_home, d_order, d_class_ptr, d_chunks, d_chunk_ptr;
+    DevBuf d_d, d_w64;                // per ray
     DevBuf d_rrow, d_rbit, d_ra;      // ray-major CSR for refresh (bit as home word)
+    DevBuf d_meta, d_nbr_new, d_rbit_new;   // lockstep tables
     // energy verifier (original order)
     DevBuf d_o_row, d_o_ray, d_o_a, d_o_nbr_ptr, d_o_nbr, d_o_lin;
     DevBuf d_o_rrow, d_o_rbit, d_o_ra;
@@ -153,6 +167,7 @@ struct qb_result {
     qb::DevBuf d_p;          // n marginals
     qb::DevBuf d_temp;       // sweeps temperatures
     qb::DevBuf d_drift;      // R floats
+    qb::DevBuf d_accepts;    // R accepted-flip counts (residual)
     qb::DevBuf d_scratch;    // per-branch state that does not fit on chip
     bool synced = false;
 };

@@ -13,13 +13,13 @@
 //   one thread-block cluster anneals one branch. The branch's weighted
 //   residuals rw_b = w_b (sum_v a_bv x_v - d_b) live in the cluster's
 //   distributed shared memory (ray b on CTA b % CL), its bits on the CTA that
-//   evaluates them. A warp scores a bit with a lane-strided gather over its
-//   rays, dE = delta (lin + sum_k a_k rw_k) + q + lambda (deg - 2 unlike),
-//   q = 1/2 sum_k w a_k^2 (the local_field_dE of src/ising_recon.hpp:105-118
-//   regrouped), and scatters rw += w a delta on accept. A class never holds
-//   two bits of one ray, so the scatter needs no atomics; a cluster barrier
-//   separates classes. Residuals are fp32 and are recomputed from scratch in
-//   fp64 every `refresh` sweeps.
+//   evaluates them. A bit's score is dE = delta (lin + h) + q + lambda (deg -
+//   2 unlike) with h = sum_k a_k rw_k (an fmaf chain over its rays in order)
+//   and q = 1/2 sum_k w a_k^2 -- the local_field_dE of
+//   src/ising_recon.hpp:105-118 regrouped; an accepted flip scatters
+//   rw += w a delta. A class never holds two bits of one ray, so the scatter
+//   needs no atomics; a cluster barrier separates classes. Residuals are fp32
+//   and are recomputed from scratch in fp64 every `refresh` sweeps.
 //
 // Metropolis (both forms): accept if dE <= 0, else if u < exp(-dE/T) in
 // double, u the 53-bit Philox draw of (branch seed, original bit, sweep) --
@@ -28,6 +28,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
 
 #include "qb_kernels.hpp"
 #include "qb_philox.cuh"
@@ -40,7 +43,12 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kIsingThreads = 512;
-constexpr int kResidThreads = 256;
+constexpr int kResidThreads = 512;
+constexpr int kGroup = 8;       // lanes per bit in the residual sweep
+constexpr int kHeavy = 64;      // bits with more rays take a full warp
+constexpr int kChunkB = 1024;   // stage bits per chunk
+constexpr int kChunkE = 8192;   // stage entries per chunk
+constexpr int kChunkN = 6144;   // stage neighbour entries per chunk
 constexpr uint32_t kSlotBits = 27;
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
 
@@ -152,18 +160,16 @@ __global__ void ising_energy_kernel(const int32_t* eu, const int32_t* ev, const 
 struct ResidArgs {
     int n;
     int n_rays;
-    int n_colours;
     int sweeps;
     int refresh;
     int ray_slots;
-    int bit_slots;
+    int bit_words;
     float lambda;
     uint64_t seed0;
-    const int32_t* class_ptr;
-    const int32_t* slot_base;   // n_colours * CL
+    const int4* chunks;         // per CTA rank: 2 x int4 per chunk (see ResidualPlan)
+    const int32_t* chunk_ptr;   // CL + 1
     const int32_t* row;
-    const int32_t* ray;
-    const float* a;
+    const uint4* ent;           // per bit-ray entry: {ray, a bits, float(w_ray) * a bits, 0}
     const float* lin;
     const float* q;
     const int32_t* nbr_ptr;
@@ -171,13 +177,14 @@ struct ResidArgs {
     const int32_t* order;
     const double* d;
     const double* w64;
-    const float* wf;
     const int32_t* rrow;
     const uint32_t* rbit_home;
     const float* ra;
     const double* temp;
     uint8_t* x_out;
     float* drift;
+    unsigned long long* accepts;
+    unsigned long long* phase;  // PHASES builds: per CTA {gather, score, barrier, chunks} clock64 sums
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -188,132 +195,555 @@ __device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
     return r;
 }
-__device__ __forceinline__ float2 ld_cluster_f2(uint32_t addr) {
-    float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+__device__ __forceinline__ float ld_cluster_f32(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
-    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v));
 }
-__device__ __forceinline__ uint32_t ld_cluster_u8(uint32_t addr) {
+__device__ __forceinline__ uint32_t ld_cluster_u32(uint32_t addr) {
     uint32_t v;
-    asm volatile("ld.shared::cluster.u8 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr));
     return v;
 }
+// The bit at home word h = (cta << 27) | slot, from any CTA of the cluster.
+__device__ __forceinline__ uint32_t ld_home_bit(uint32_t xs_base, uint32_t h) {
+    const uint32_t slot = h & kSlotMask;
+    return (ld_cluster_u32(map_rank(xs_base + (slot >> 5) * 4u, h >> kSlotBits)) >> (slot & 31u)) & 1u;
+}
 
-template <int CL>
-__global__ void __launch_bounds__(kResidThreads) resid_anneal_kernel(ResidArgs A) {
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Shared memory of the residual sweep's stage buffers.
+struct ResidStage {
+    unsigned long long* u;   // kChunkB Philox draws (53-bit)
+    float* rv;               // kChunkE gathered residuals
+    int32_t* row;            // kChunkB + 1 entry offsets (chunk-relative)
+    int32_t* nbp;            // kChunkB + 1 neighbour offsets (chunk-relative)
+    float* lin;              // kChunkB
+    float* q;                // kChunkB
+    uint8_t* xn;             // kChunkN neighbour bits
+};
+
+// Score, decide and (on accept) scatter bit k of the chunk with a group of G
+// lanes: lane l sums a * rw over entries l, l + G, ... as an fmaf chain, an
+// xor butterfly joins the lanes (the oracle mirrors this order).
+template <int CL, int G>
+__device__ __forceinline__ bool score_bit(int k, int gl, unsigned gmask, int leader, const ResidStage& S,
+                                          const uint4* ent, uint32_t rw_base, uint32_t* xs, int slot0, float lambda,
+                                          double T) {
+    constexpr int kShift = CL == 1 ? 0 : CL == 2 ? 1 : CL == 4 ? 2 : CL == 8 ? 3 : 4;
+    const int rs = S.row[k], re = S.row[k + 1], ns = S.nbp[k], ne = S.nbp[k + 1];
+    float acc = 0.0f;
+    for (int e = rs + gl; e < re; e += G) acc = fmaf(__uint_as_float(__ldg(&ent[e]).y), S.rv[e], acc);
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(gmask, acc, off));
+    const int slot = slot0 + k;
+    const uint32_t xi = (xs[slot >> 5] >> (slot & 31)) & 1u;
+    int unlike = 0;
+    for (int j = ns + gl; j < ne; j += G) unlike += S.xn[j] != xi ? 1 : 0;
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) unlike += __shfl_xor_sync(gmask, unlike, off);
+    int accept = 0;
+    if (gl == 0) {
+        const float delta = xi ? -1.0f : 1.0f;
+        const float t = __fadd_rn(S.lin[k], acc);
+        const float prior = __fmul_rn(lambda, float((ne - ns) - 2 * unlike));
+        const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), S.q[k]), prior);
+        accept = (dE <= 0.0f || double(S.u[k]) * 0x1.0p-53 < exp(-double(dE) / T)) ? 1 : 0;
+    }
+    accept = __shfl_sync(gmask, accept, leader);
+    if (accept) {
+        for (int e = rs + gl; e < re; e += G) {
+            const uint4 en = __ldg(&ent[e]);
+            const uint32_t ad = map_rank(rw_base + (en.x >> kShift) * 4u, en.x & (CL - 1));
+            const float wa = __uint_as_float(en.z);
+            st_cluster_f32(ad, xi ? __fsub_rn(S.rv[e], wa) : __fadd_rn(S.rv[e], wa));
+        }
+        if (gl == 0) atomicXor(&xs[slot >> 5], 1u << (slot & 31));
+    }
+    return accept != 0;
+}
+
+// One cluster anneals one branch. A colour class is worked through in chunks
+// of this CTA's slice (<= kChunkB bits, <= kChunkE entries, <= kChunkN
+// neighbour entries; the planner balances the slices and puts heavy bits
+// first); per chunk:
+//   1. every thread gathers into shared memory: the chunk's per-bit metadata,
+//      the bits' Philox draws (pure arithmetic that overlaps the loads), the
+//      entries' rw from the ray owners' shared memory and the neighbours'
+//      bits, while the next chunk's entries are prefetched into L2;
+//   2. heavy bits take a warp each, the others a kGroup-lane group: sum,
+//      score, decide; an accepted bit writes rw + (w a) delta straight back to
+//      the owners (no atomics: a class holds at most one bit of a ray) and
+//      flips its own bit;
+// and a cluster barrier closes the class.
+template <int CL, bool PHASES>
+__global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArgs A) {
     static_assert((CL & (CL - 1)) == 0 && CL <= 16, "cluster size: a power of two <= 16");
+    static_assert(kResidThreads % kGroup == 0 && 32 % kGroup == 0, "lane groups tile a warp");
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* rw = reinterpret_cast<float2*>(smem);                        // (w r, w) per owned ray
-    uint8_t* xs = smem + size_t(A.ray_slots) * sizeof(float2);         // owned bits
+    constexpr int kShift = CL == 1 ? 0 : CL == 2 ? 1 : CL == 4 ? 2 : CL == 8 ? 3 : 4;
+    constexpr int kGroups = kResidThreads / kGroup;
+    constexpr int kWarps = kResidThreads / 32;
+    ResidStage S;
+    S.u = reinterpret_cast<unsigned long long*>(smem);
+    float* rw = reinterpret_cast<float*>(S.u + kChunkB);                     // w r per owned ray
+    S.rv = rw + A.ray_slots;
+    S.row = reinterpret_cast<int32_t*>(S.rv + kChunkE);
+    S.nbp = S.row + (kChunkB + 1);
+    S.lin = reinterpret_cast<float*>(S.nbp + (kChunkB + 1));
+    S.q = S.lin + kChunkB;
+    S.xn = reinterpret_cast<uint8_t*>(S.q + kChunkB);
+    uint32_t* xs = reinterpret_cast<uint32_t*>(S.xn + kChunkN);             // owned bits, packed
+    __shared__ unsigned long long s_acc_count;
     cg::cluster_group cluster = cg::this_cluster();
     const uint32_t rank = cluster.block_rank();
     const int branch = int(blockIdx.x) / CL;
-    const int lane = int(threadIdx.x & 31u);
-    const int warp = int(threadIdx.x >> 5);
-    constexpr int kWarps = kResidThreads / 32;
-    constexpr int kShift = CL == 1 ? 0 : CL == 2 ? 1 : CL == 4 ? 2 : CL == 8 ? 3 : 4;
+    const int tid = int(threadIdx.x);
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int gl = tid % kGroup;
+    const int grp = tid / kGroup;
+    const unsigned gmask = (kGroup == 32 ? kFull : ((1u << kGroup) - 1u)) << (lane & ~(kGroup - 1));
     const uint64_t seed = A.seed0 + uint64_t(branch);
     const uint32_t rw_base = smem_addr(rw);
     const uint32_t xs_base = smem_addr(xs);
+    const int4* chunks = A.chunks + 2 * A.chunk_ptr[rank];
+    const int n_chunks = A.chunk_ptr[rank + 1] - A.chunk_ptr[rank];
 
-    for (int sl = int(threadIdx.x); sl < A.ray_slots; sl += kResidThreads) {
+    for (int sl = tid; sl < A.ray_slots; sl += kResidThreads) {
         const int b = (sl << kShift) + int(rank);
-        float2 v = make_float2(0.0f, 0.0f);
-        if (b < A.n_rays) {
-            v.x = float(A.w64[b] * (-A.d[b]));
-            v.y = A.wf[b];
-        }
-        rw[sl] = v;
+        rw[sl] = b < A.n_rays ? float(A.w64[b] * (-A.d[b])) : 0.0f;
     }
-    for (int sl = int(threadIdx.x); sl < A.bit_slots; sl += kResidThreads) xs[sl] = 0;
+    for (int sl = tid; sl < A.bit_words; sl += kResidThreads) xs[sl] = 0u;
+    if (tid == 0) s_acc_count = 0;
     cluster.sync();
 
+    unsigned long long my_accepts = 0;
+    long long ph_gather = 0, ph_score = 0, ph_bar = 0, ph_chunks = 0, t_ph = 0;
     for (int sweep = 0; sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
-            // fp64 refresh of the owned residuals: r_b = sum_{v on b, x_v} a - d_b
+            // fp64 refresh of the owned residuals: r_b = (sum over the ray's
+            // set bits of a, in ray order) - d_b
             float dmax = 0.0f;
-            for (int sl = warp; sl < A.ray_slots; sl += kWarps) {
+            for (int sl = tid; sl < A.ray_slots; sl += kResidThreads) {
                 const int b = (sl << kShift) + int(rank);
                 if (b >= A.n_rays) continue;
                 double acc = 0.0;
-                for (int k = A.rrow[b] + lane; k < A.rrow[b + 1]; k += 32) {
-                    const uint32_t h = A.rbit_home[k];
-                    if (ld_cluster_u8(map_rank(xs_base + (h & kSlotMask), h >> kSlotBits))) acc += double(A.ra[k]);
-                }
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) acc = acc + __shfl_xor_sync(kFull, acc, off);
-                if (lane == 0) {
-                    const float nv = float(A.w64[b] * (acc - A.d[b]));
-                    dmax = fmaxf(dmax, fabsf(nv - rw[sl].x));
-                    rw[sl].x = nv;
-                }
+                const int k1 = A.rrow[b + 1];
+                for (int k = A.rrow[b]; k < k1; ++k)
+                    if (ld_home_bit(xs_base, A.rbit_home[k])) acc += double(A.ra[k]);
+                const float nv = float(A.w64[b] * (acc - A.d[b]));
+                dmax = fmaxf(dmax, fabsf(nv - rw[sl]));
+                rw[sl] = nv;
             }
-            if (lane == 0 && dmax > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[branch]), __float_as_int(dmax));
+            if (dmax > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[branch]), __float_as_int(dmax));
             cluster.sync();
         }
         const double T = A.temp[sweep];
-        for (int c = 0; c < A.n_colours; ++c) {
-            const int cs = A.class_ptr[c], ce = A.class_ptr[c + 1];
-            const int chunk = (ce - cs + CL - 1) / CL;
-            const int b0 = cs + int(rank) * chunk;
-            const int b1 = min(b0 + chunk, ce);
-            const int slot0 = A.slot_base[c * CL + int(rank)];
-            for (int i = b0 + warp; i < b1; i += kWarps) {
-                const int rs = A.row[i], re = A.row[i + 1];
-                float acc = 0.0f;
-                for (int k = rs + lane; k < re; k += 32) {
-                    const int rb = A.ray[k];
-                    const float2 v = ld_cluster_f2(map_rank(rw_base + uint32_t(rb >> kShift) * 8u, uint32_t(rb & (CL - 1))));
-                    acc = fmaf(A.a[k], v.x, acc);
-                }
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, off));
-                const int slot = slot0 + (i - b0);
-                const uint32_t xi = xs[slot];
-                const int np0 = A.nbr_ptr[i], np1 = A.nbr_ptr[i + 1];
-                int unlike = 0;
-                for (int k = np0 + lane; k < np1; k += 32) {
-                    const uint32_t h = A.nbr_home[k];
-                    unlike += ld_cluster_u8(map_rank(xs_base + (h & kSlotMask), h >> kSlotBits)) != xi ? 1 : 0;
-                }
-                unlike = __reduce_add_sync(kFull, unlike);
-                const float delta = xi ? -1.0f : 1.0f;
-                int accept = 0;
-                if (lane == 0) {
-                    const float t = __fadd_rn(A.lin[i], acc);
-                    const float prior = __fmul_rn(A.lambda, float((np1 - np0) - 2 * unlike));
-                    const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), A.q[i]), prior);
-                    accept = metropolis(double(dE), T, seed, uint32_t(A.order[i]), uint32_t(sweep)) ? 1 : 0;
-                }
-                accept = __shfl_sync(kFull, accept, 0);
-                if (accept) {
-                    for (int k = rs + lane; k < re; k += 32) {
-                        const int rb = A.ray[k];
-                        const uint32_t ad = map_rank(rw_base + uint32_t(rb >> kShift) * 8u, uint32_t(rb & (CL - 1)));
-                        const float2 v = ld_cluster_f2(ad);
-                        const float upd = __fmul_rn(v.y, A.a[k]);
-                        st_cluster_f32(ad, xi ? __fsub_rn(v.x, upd) : __fadd_rn(v.x, upd));
-                    }
-                    if (lane == 0) xs[slot] = uint8_t(xi ^ 1u);
+        for (int ci = 0; ci < n_chunks; ++ci) {
+            const int4 c0 = chunks[2 * ci];       // b0, b1, slot of b0, last-of-class | heavy bits << 1
+            const int4 c1 = chunks[2 * ci + 1];   // e0, e1, n0, n1
+            const int nb = c0.y - c0.x;
+            if (PHASES) t_ph = clock64();
+            if (tid == 0) {   // the next chunk's entries into L2
+                const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
+                const int4 c1n = chunks[2 * nx + 1];
+                if (c1n.y > c1n.x) prefetch_l2(&A.ent[c1n.x], uint32_t(c1n.y - c1n.x) * 16u);
+            }
+            // 1. gather
+            for (int k = tid; k <= nb; k += kResidThreads) {
+                const int i = c0.x + k;
+                S.row[k] = A.row[i] - c1.x;
+                S.nbp[k] = A.nbr_ptr[i] - c1.z;
+                if (k < nb) {
+                    S.lin[k] = A.lin[i];
+                    S.q[k] = A.q[i];
+                    S.u[k] = draw_u53(seed, uint32_t(A.order[i]), uint32_t(sweep), 0u);
                 }
             }
-            cluster.sync();
+            for (int e0 = c1.x + tid; e0 < c1.y; e0 += 4 * kResidThreads) {
+                uint4 en[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = e0 + u * kResidThreads;
+                    en[u] = e < c1.y ? __ldg(&A.ent[e]) : make_uint4(0u, 0u, 0u, 0u);
+                }
+                float rv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    rv[u] = e0 + u * kResidThreads < c1.y
+                                ? ld_cluster_f32(map_rank(rw_base + (en[u].x >> kShift) * 4u, en[u].x & (CL - 1)))
+                                : 0.0f;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = e0 + u * kResidThreads;
+                    if (e < c1.y) S.rv[e - c1.x] = rv[u];
+                }
+            }
+            for (int j = c1.z + tid; j < c1.w; j += kResidThreads)
+                S.xn[j - c1.z] = uint8_t(ld_home_bit(xs_base, A.nbr_home[j]));
+            __syncthreads();
+            if (PHASES) {
+                const long long t1 = clock64();
+                ph_gather += t1 - t_ph;
+                t_ph = t1;
+            }
+            // 2. score, decide, scatter
+            const uint4* ent = A.ent + c1.x;
+            const int nh = c0.w >> 1;
+            for (int k = warp; k < nh; k += kWarps)
+                my_accepts += (score_bit<CL, 32>(k, lane, kFull, 0, S, ent, rw_base, xs, c0.z, A.lambda, T) && lane == 0);
+            for (int k = nh + grp; k < nb; k += kGroups)
+                my_accepts += (score_bit<CL, kGroup>(k, gl, gmask, lane & ~(kGroup - 1), S, ent, rw_base, xs, c0.z,
+                                                     A.lambda, T) && gl == 0);
+            if (PHASES) {
+                __syncthreads();
+                const long long t1 = clock64();
+                ph_score += t1 - t_ph;
+                t_ph = t1;
+            }
+            if (c0.w & 1) cluster.sync();   // class done: its flips become visible cluster-wide
+            else __syncthreads();           // stage buffers are reused by the next chunk
+            if (PHASES) {
+                ph_bar += clock64() - t_ph;
+                ++ph_chunks;
+            }
         }
     }
-    // branches out, original bit order
-    for (int c = 0; c < A.n_colours; ++c) {
-        const int cs = A.class_ptr[c], ce = A.class_ptr[c + 1];
-        const int chunk = (ce - cs + CL - 1) / CL;
-        const int b0 = cs + int(rank) * chunk;
-        const int b1 = min(b0 + chunk, ce);
-        const int slot0 = A.slot_base[c * CL + int(rank)];
-        for (int i = b0 + int(threadIdx.x); i < b1; i += kResidThreads)
-            A.x_out[size_t(branch) * size_t(A.n) + size_t(A.order[i])] = xs[slot0 + (i - b0)];
+    if (PHASES && tid == 0) {
+        unsigned long long* ph = A.phase + 4 * size_t(blockIdx.x);
+        ph[0] = ph_gather; ph[1] = ph_score; ph[2] = ph_bar; ph[3] = ph_chunks;
     }
+    // branches out, original bit order
+    for (int ci = 0; ci < n_chunks; ++ci) {
+        const int4 c0 = chunks[2 * ci];
+        for (int k = tid; k < c0.y - c0.x; k += kResidThreads) {
+            const int slot = c0.z + k;
+            A.x_out[size_t(branch) * size_t(A.n) + size_t(A.order[c0.x + k])] = uint8_t((xs[slot >> 5] >> (slot & 31)) & 1u);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) my_accepts += __shfl_xor_sync(kFull, my_accepts, off);
+    if (lane == 0 && my_accepts) atomicAdd(&s_acc_count, my_accepts);
+    __syncthreads();
+    if (tid == 0 && s_acc_count) atomicAdd(&A.accepts[branch], s_acc_count);
     cluster.sync();   // no CTA leaves while a peer may still read its shared memory
+}
+
+// ---- residual form, all branches in lockstep ------------------------------------------
+//
+// Every CTA of a co-resident (cooperative) grid takes a balanced slice of
+// each colour class; a warp scores one bit for 16 branches at once: lane l
+// serves branch l % 16 and entries of parity l / 16, so one coalesced 64-byte
+// load of rw[ray][16 branches] feeds 16 branches. Residuals and bits live in
+// global memory (L2-resident: 4.8 MB of residuals and 1.2 MB of bit words for
+// the benchmark pyramid at 16 branches); a bounded grid barrier closes each
+// class. Branch b of a bit sums h = fmaf chain over its even entries + fmaf
+// chain over its odd entries (the oracle's "lockstep" order).
+
+constexpr int kLockThreads = 1024;
+constexpr int kLockE = 2048;   // staged entries per chunk
+constexpr int kLockB = 256;    // staged bits per chunk
+constexpr int kLockN = 1536;   // staged neighbour entries per chunk
+constexpr int kSeg = 16;       // entries per segment: one warp, one batch of loads
+constexpr int kLockSegs = kLockE / kSeg + kLockB;   // segments a chunk can hold
+constexpr int kLockMaxNG = 4;  // branch groups of 16 one launch serves (64 branches)
+constexpr unsigned kSpinLimit = 1u << 24;   // polls of a grid barrier before it reports a timeout
+
+struct ResidLockArgs {
+    int n;
+    int n_rays;
+    int sweeps;
+    int refresh;
+    int R;              // branches
+    int NG;             // groups of 16 branches
+    float lambda;
+    uint64_t seed0;
+    const int4* chunks;         // per CTA: 2 x int4 per chunk {b0, b1, -, last} {e0, e1, n0, n1}
+    const int32_t* chunk_ptr;   // gridDim + 1
+    const uint4* ent;           // {ray, a, w a, 0} per bit-ray entry, sweep order
+    const uint4* meta;          // per bit, 2 x uint4: {row start, rays, nbr start, nbrs} {lin, q, input index, 0}
+    const int32_t* nbr;         // sweep-order index of each neighbour
+    const int32_t* order;
+    const double* d;
+    const double* w64;
+    const int32_t* rrow;
+    const int32_t* rbit;        // sweep-order bit of each ray-major entry
+    const float* ra;
+    const double* temp;
+    float* rw;                  // n_rays x (16 NG): weighted residuals of every branch
+    uint32_t* xb;               // n x NG: bit words, branch 16 g + l at bit l of word g
+    unsigned* bar;              // grid barrier counter (zero at launch)
+    int* err;                   // 1: a barrier timed out
+    uint8_t* x_out;
+    float* drift;
+    unsigned long long* accepts;
+    unsigned long long* phase;  // PHASES builds: per CTA {stage wait, items, barrier, chunks} clock64 sums
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Grid barrier of a cooperative launch: arrive, then poll the counter until
+// every CTA of barrier round `round` has arrived. A poll limit turns a lost
+// CTA into an error flag instead of a hang; every CTA then leaves its loops.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned round) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned target = round * gridDim.x;
+        red_release_gpu(bar, 1u);
+        unsigned spins = 0;
+        int ok = 1;
+        while (ld_acquire_gpu(bar) < target) {
+            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(20);
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+struct LockStage {
+    uint4* ent;      // kLockE
+    uint4* meta;     // 2 kLockB
+    int32_t* nbr;    // kLockN
+};
+
+// Stage a chunk's entries, bit records and neighbour lists (async copies).
+__device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0, const int4 c1, const LockStage& S) {
+    for (int e = c1.x + int(threadIdx.x); e < c1.y; e += kLockThreads) cp_async16(&S.ent[e - c1.x], &A.ent[e]);
+    for (int k = 2 * c0.x + int(threadIdx.x); k < 2 * c0.y; k += kLockThreads) cp_async16(&S.meta[k - 2 * c0.x], &A.meta[k]);
+    for (int j = c1.z + int(threadIdx.x); j < c1.w; j += kLockThreads) cp_async4(&S.nbr[j - c1.z], &A.nbr[j]);
+}
+
+// Every CTA of a cooperative grid works its chunk list (a balanced slice of
+// each colour class); the next chunk's structure is staged in shared memory
+// while the current one runs. Per chunk:
+//   A. a warp sums one 16-entry segment of one bit for 16 branches: lane l
+//      serves branch l % 16 and the segment's entries of parity l / 16, so one
+//      coalesced 64-byte load of rw[ray][16 branches] feeds 16 branches and
+//      each lane issues its eight loads at once; segment sum = the even-entry
+//      fmaf chain + the odd-entry chain;
+//   B. a warp per bit adds its segments in order, counts unlike neighbours,
+//      decides, and scatters w a delta with fire-and-forget reductions (a
+//      class touches a residual at most once: the result is deterministic).
+// A bounded grid barrier closes each class.
+template <bool PHASES>
+__global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLockArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = int(threadIdx.x);
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    constexpr int kWarps = kLockThreads / 32;
+    const int br = lane & 15;           // branch in the group
+    const int half = lane >> 4;         // entry parity
+    const int P = int(gridDim.x);
+    const int p = int(blockIdx.x);
+    const int RP = 16 * A.NG;           // residual row pitch (floats)
+    constexpr size_t kStageBytes = size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
+    float* hseg = reinterpret_cast<float*>(smem + 2 * kStageBytes);   // kLockSegs x NG x 16 segment sums
+    auto stage = [&](int b) {
+        LockStage L;
+        unsigned char* q = smem + size_t(b) * kStageBytes;
+        L.ent = reinterpret_cast<uint4*>(q);
+        L.meta = reinterpret_cast<uint4*>(q + size_t(kLockE) * 16);
+        L.nbr = reinterpret_cast<int32_t*>(q + size_t(kLockE) * 16 + size_t(kLockB) * 32);
+        return L;
+    };
+    const int4* chunks = A.chunks + 2 * A.chunk_ptr[p];
+    const int n_chunks = A.chunk_ptr[p + 1] - A.chunk_ptr[p];
+    unsigned round = 0;
+    unsigned long long my_accepts = 0;
+    __shared__ unsigned long long s_acc_count;
+    if (tid == 0) s_acc_count = 0;
+    // x = 0: rw_b = w_b (-d_b) for every branch
+    for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n_rays) * RP; k += size_t(P) * kLockThreads) {
+        const int b = int(k / RP);
+        A.rw[k] = float(A.w64[b] * (-A.d[b]));
+    }
+    for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
+    if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0));
+    cp_async_commit();
+    bool ok = grid_barrier(A.bar, A.err, ++round);
+    int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
+    long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0;
+    for (int sweep = 0; ok && sweep < A.sweeps; ++sweep) {
+        if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
+            // fp64 refresh: thread per (ray, branch), bits of the ray in order
+            for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n_rays) * RP; k += size_t(P) * kLockThreads) {
+                const int b = int(k / RP), j = int(k % RP);
+                if (j >= A.R) continue;
+                const int g = j >> 4, l = j & 15;
+                double acc = 0.0;
+                for (int e = A.rrow[b]; e < A.rrow[b + 1]; ++e)
+                    if ((__ldcg(&A.xb[size_t(A.rbit[e]) * A.NG + g]) >> l) & 1u) acc += double(A.ra[e]);
+                const float nv = float(A.w64[b] * (acc - A.d[b]));
+                const float dv = fabsf(nv - __ldcg(&A.rw[k]));
+                if (dv > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[j]), __float_as_int(dv));
+                __stcg(&A.rw[k], nv);
+            }
+            ok = grid_barrier(A.bar, A.err, ++round);
+            if (!ok) break;
+        }
+        const double T = A.temp[sweep];
+        for (int ci = 0; ci < n_chunks; ++ci, ++gci) {
+            const int4 c0 = chunks[2 * ci], c1 = chunks[2 * ci + 1];
+            // stage the next chunk (wrapping into the next sweep), then wait for this one
+            const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
+            if (PHASES) t_ph = clock64();
+            lock_stage(A, chunks[2 * nx], chunks[2 * nx + 1], stage((gci + 1) & 1));
+            cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();
+            if (PHASES) {
+                const long long t1 = clock64();
+                ph_wait += t1 - t_ph;
+                t_ph = t1;
+            }
+            const LockStage St = stage(gci & 1);
+            const int nb = c0.y - c0.x;
+            const int nseg = c0.z;                       // segments of the chunk
+            // A. segment sums
+            for (int it = warp; it < nseg * A.NG; it += kWarps) {
+                const int sg = it / A.NG, g = it % A.NG;
+                // the bit of segment sg: meta word 7 is the bit's first segment in the chunk
+                int lo = 0, hi = nb - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (int(St.meta[2 * mid + 1].w) <= sg) lo = mid; else hi = mid - 1;
+                }
+                const uint4 m0 = St.meta[2 * lo];
+                const int seg_in_bit = sg - int(St.meta[2 * lo + 1].w);
+                const int rs = int(m0.x) - c1.x + seg_in_bit * kSeg;
+                const int re = min(int(m0.x) - c1.x + int(m0.y), rs + kSeg);
+                float av[kSeg / 2], rv[kSeg / 2];
+#pragma unroll
+                for (int u = 0; u < kSeg / 2; ++u) {
+                    const int e = rs + half + 2 * u;
+                    if (e < re) {
+                        const uint4 en = St.ent[e];
+                        av[u] = __uint_as_float(en.y);
+                        rv[u] = __ldcg(&A.rw[size_t(en.x) * RP + 16 * g + br]);
+                    } else {
+                        av[u] = 0.0f;
+                        rv[u] = 0.0f;
+                    }
+                }
+                float acc = 0.0f;
+#pragma unroll
+                for (int u = 0; u < kSeg / 2; ++u)
+                    if (rs + half + 2 * u < re) acc = fmaf(av[u], rv[u], acc);
+                const float other = __shfl_xor_sync(kFull, acc, 16);
+                if (half == 0) hseg[(sg * A.NG + g) * 16 + br] = __fadd_rn(acc, other);
+            }
+            __syncthreads();
+            // B. decide and scatter, a warp per (bit, group)
+            for (int it = warp; it < nb * A.NG; it += kWarps) {
+                const int k = it / A.NG, g = it % A.NG;
+                const int branch = 16 * g + br;
+                const bool live = branch < A.R && half == 0;
+                const uint4 m0 = St.meta[2 * k], m1 = St.meta[2 * k + 1];
+                const int i = c0.x + k;
+                const uint64_t u53 = live ? draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u) : 0ull;
+                const uint32_t xw = __ldcg(&A.xb[size_t(i) * A.NG + g]);
+                const uint32_t xi = (xw >> br) & 1u;
+                const int ns = int(m0.z) - c1.z, ne = ns + int(m0.w);
+                int unlike = 0;
+                for (int j0 = ns; j0 < ne; j0 += 8) {
+                    uint32_t nw[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) nw[u] = j0 + u < ne ? __ldcg(&A.xb[size_t(St.nbr[j0 + u]) * A.NG + g]) : 0u;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (j0 + u < ne) unlike += ((nw[u] >> br) & 1u) != xi ? 1 : 0;
+                }
+                int flip = 0;
+                if (live) {
+                    const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
+                    const int s0 = int(m1.w);
+                    float h = 0.0f;
+                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * A.NG + g) * 16 + br]);
+                    const float delta = xi ? -1.0f : 1.0f;
+                    const float t = __fadd_rn(__uint_as_float(m1.x), h);
+                    const float prior = __fmul_rn(A.lambda, float((ne - ns) - 2 * unlike));
+                    const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), __uint_as_float(m1.y)), prior);
+                    flip = (dE <= 0.0f || double(u53) * 0x1.0p-53 < exp(-double(dE) / T)) ? 1 : 0;
+                }
+                const unsigned amask = __ballot_sync(kFull, flip) & 0xFFFFu;
+                if (amask) {
+                    if ((amask >> br) & 1u) {
+                        const int rs = int(m0.x) - c1.x, re = rs + int(m0.y);
+                        for (int e = rs + half; e < re; e += 2) {
+                            const uint4 en = St.ent[e];
+                            const float wa = __uint_as_float(en.z);
+                            atomicAdd(&A.rw[size_t(en.x) * RP + 16 * g + br], xi ? -wa : wa);
+                        }
+                    }
+                    if (lane == 0) {
+                        __stcg(&A.xb[size_t(i) * A.NG + g], xw ^ amask);
+                        my_accepts += unsigned(__popc(amask));
+                    }
+                }
+            }
+            if (PHASES) {
+                __syncthreads();
+                const long long t1 = clock64();
+                ph_items += t1 - t_ph;
+                t_ph = t1;
+            }
+            if (c0.w & 1) {
+                ok = grid_barrier(A.bar, A.err, ++round);
+                if (!ok) break;
+            } else {
+                __syncthreads();
+            }
+            if (PHASES) {
+                ph_bar += clock64() - t_ph;
+                ++ph_n;
+            }
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (PHASES && tid == 0) {
+        unsigned long long* ph = A.phase + 4 * size_t(blockIdx.x);
+        ph[0] = ph_wait; ph[1] = ph_items; ph[2] = ph_bar; ph[3] = ph_n;
+    }
+    if (ok) {
+        // branches out, original bit order
+        for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.R; k += size_t(P) * kLockThreads) {
+            const int i = int(k % A.n), b = int(k / A.n);
+            A.x_out[size_t(b) * A.n + A.order[i]] = uint8_t((__ldcg(&A.xb[size_t(i) * A.NG + (b >> 4)]) >> (b & 15)) & 1u);
+        }
+    }
+    if (lane == 0 && my_accepts) atomicAdd(&s_acc_count, my_accepts);
+    __syncthreads();
+    if (tid == 0 && s_acc_count) atomicAdd(&A.accepts[0], s_acc_count);
 }
 
 // binary_energy (src/ising_recon.hpp:65-79) of K states in fp64, one CTA per
@@ -460,14 +890,25 @@ qb_status launch_ising_energies(const IsingPlan& p, const uint8_t* x, int K, lon
     return QB_OK;
 }
 
-size_t resid_smem_bytes(const ResidualPlan& p) {
-    return size_t(p.ray_slots) * sizeof(float2) + size_t(p.bit_slots);
+size_t resid_stage_bytes() {
+    return size_t(kChunkB) * 8 + size_t(kChunkE) * 4 + size_t(kChunkB + 1) * 8 + size_t(kChunkB) * 8 + size_t(kChunkN);
 }
+
+size_t resid_smem_bytes(const ResidualPlan& p) {
+    const size_t words = (size_t(p.bit_slots) + 31) / 32;
+    return resid_stage_bytes() + size_t(p.ray_slots) * 4 + words * 4;
+}
+
+int resid_chunk_bits() { return kChunkB; }
+int resid_group_lanes() { return kGroup; }
+int resid_heavy_entries() { return kHeavy; }
+int resid_chunk_entries() { return kChunkE; }
+int resid_chunk_nbrs() { return kChunkN; }
 
 namespace {
 template <int CL>
 qb_status resid_launch_cl(const ResidArgs& A, int R, size_t smem, cudaStream_t st, bool check_only) {
-    auto kern = resid_anneal_kernel<CL>;
+    auto kern = A.phase ? resid_anneal_kernel<CL, true> : resid_anneal_kernel<CL, false>;
     QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     if (CL > 8) QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg{};
@@ -485,6 +926,9 @@ qb_status resid_launch_cl(const ResidArgs& A, int R, size_t smem, cudaStream_t s
     int clusters = 0;
     QB_CUDA(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
     if (clusters < 1) return fail(QB_ENOTSUP, "residual sweep: a cluster of this size does not fit on the device");
+    if (std::getenv("QB_DEBUG"))
+        std::fprintf(stderr, "[qublar] residual sweep: cluster %d x %d threads, %zu B shared, %d clusters co-resident, grid %d\n",
+                     CL, kResidThreads, smem, clusters, R * CL);
     if (check_only) return QB_OK;
     QB_CUDA(cudaLaunchKernelEx(&cfg, kern, A));
     QB_CUDA(cudaGetLastError());
@@ -497,18 +941,16 @@ qb_status launch_resid_anneal(const ResidualPlan& p, const SolveBuffers& b, int 
     ResidArgs A{};
     A.n = p.n;
     A.n_rays = p.n_rays;
-    A.n_colours = p.col.n_colours();
     A.sweeps = sweeps;
     A.refresh = refresh;
     A.ray_slots = p.ray_slots;
-    A.bit_slots = p.bit_slots;
+    A.bit_words = (p.bit_slots + 31) / 32;
     A.lambda = float(p.lambda);
     A.seed0 = seed0;
-    A.class_ptr = p.d_class_ptr.as<int32_t>();
-    A.slot_base = p.d_slot_base.as<int32_t>();
+    A.chunks = p.d_chunks.as<int4>();
+    A.chunk_ptr = p.d_chunk_ptr.as<int32_t>();
     A.row = p.d_row.as<int32_t>();
-    A.ray = p.d_ray.as<int32_t>();
-    A.a = p.d_a.as<float>();
+    A.ent = p.d_ent.as<uint4>();
     A.lin = p.d_lin.as<float>();
     A.q = p.d_q.as<float>();
     A.nbr_ptr = p.d_nbr_ptr.as<int32_t>();
@@ -516,20 +958,42 @@ qb_status launch_resid_anneal(const ResidualPlan& p, const SolveBuffers& b, int 
     A.order = p.d_order.as<int32_t>();
     A.d = p.d_d.as<double>();
     A.w64 = p.d_w64.as<double>();
-    A.wf = p.d_wf.as<float>();
     A.rrow = p.d_rrow.as<int32_t>();
     A.rbit_home = p.d_rbit.as<uint32_t>();
     A.ra = p.d_ra.as<float>();
     A.temp = b.temp;
     A.x_out = b.x;
     A.drift = b.drift;
+    A.accepts = b.accepts;
     const size_t smem = resid_smem_bytes(p);
+    // QB_PHASE_TIMES: per-CTA clock64 sums of the gather, score and barrier
+    // phases, printed to stderr after the launch (diagnostics; same work)
+    DevBuf phase;
+    const bool phases = std::getenv("QB_PHASE_TIMES") != nullptr;
+    if (phases) {
+        qb_status s = phase.alloc(size_t(R) * size_t(p.CL) * 32);
+        if (s != QB_OK) return s;
+        QB_CUDA(cudaMemsetAsync(phase.p, 0, phase.bytes, st));
+        A.phase = phase.as<unsigned long long>();
+    }
+    qb_status s;
     switch (p.CL) {
-        case 4: return resid_launch_cl<4>(A, R, smem, st, false);
-        case 8: return resid_launch_cl<8>(A, R, smem, st, false);
-        case 16: return resid_launch_cl<16>(A, R, smem, st, false);
+        case 4: s = resid_launch_cl<4>(A, R, smem, st, false); break;
+        case 8: s = resid_launch_cl<8>(A, R, smem, st, false); break;
+        case 16: s = resid_launch_cl<16>(A, R, smem, st, false); break;
         default: return fail(QB_EINVAL, "residual sweep: cluster size must be 4, 8 or 16");
     }
+    if (s == QB_OK && phases) {
+        std::vector<unsigned long long> h(size_t(R) * size_t(p.CL) * 4);
+        QB_CUDA(cudaMemcpyAsync(h.data(), phase.p, phase.bytes, cudaMemcpyDeviceToHost, st));
+        QB_CUDA(cudaStreamSynchronize(st));
+        double g = 0, sc = 0, br = 0, ch = 0;
+        const size_t ctas = size_t(R) * size_t(p.CL);
+        for (size_t c = 0; c < ctas; ++c) { g += h[4 * c]; sc += h[4 * c + 1]; br += h[4 * c + 2]; ch += h[4 * c + 3]; }
+        std::fprintf(stderr, "[qublar] phases per CTA: chunks %.0f, cycles per chunk: gather %.0f, score %.0f, barrier %.0f\n",
+                     ch / ctas, g / ch, sc / ch, br / ch);
+    }
+    return s;
 }
 
 qb_status resid_check_fit(const ResidualPlan& p) {
@@ -542,6 +1006,97 @@ qb_status resid_check_fit(const ResidualPlan& p) {
         case 16: return resid_launch_cl<16>(A, 1, smem, nullptr, true);
         default: return fail(QB_EINVAL, "residual sweep: cluster size must be 4, 8 or 16");
     }
+}
+
+size_t resid_lockstep_smem() {
+    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + size_t(kLockSegs) * kLockMaxNG * 16 * 4;
+}
+int resid_lockstep_max_branches() { return 16 * kLockMaxNG; }
+int resid_lockstep_segment() { return kSeg; }
+int resid_lockstep_chunk_segments() { return kLockSegs; }
+int resid_lockstep_chunk_bits() { return kLockB; }
+int resid_lockstep_chunk_entries() { return kLockE; }
+int resid_lockstep_chunk_nbrs() { return kLockN; }
+
+int resid_lockstep_grid() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    if (cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(resid_lockstep_smem())) != cudaSuccess ||
+        cudaFuncSetAttribute(resid_lockstep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(resid_lockstep_smem())) != cudaSuccess)
+        return 0;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resid_lockstep_kernel<false>, kLockThreads,
+                                                      resid_lockstep_smem()) != cudaSuccess)
+        return 0;
+    return per_sm >= 1 ? sms : 0;
+}
+
+size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
+    const int NG = (R + 15) / 16;
+    return size_t(p.n_rays) * 16 * NG * 4 + size_t(p.n) * NG * 4 + 64;
+}
+
+qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, int R, int sweeps, int refresh,
+                                uint64_t seed0, cudaStream_t st) {
+    ResidLockArgs A{};
+    A.n = p.n;
+    A.n_rays = p.n_rays;
+    A.sweeps = sweeps;
+    A.refresh = refresh;
+    A.R = R;
+    A.NG = (R + 15) / 16;
+    A.lambda = float(p.lambda);
+    A.seed0 = seed0;
+    A.chunks = p.d_chunks.as<int4>();
+    A.chunk_ptr = p.d_chunk_ptr.as<int32_t>();
+    A.ent = p.d_ent.as<uint4>();
+    A.meta = p.d_meta.as<uint4>();
+    A.nbr = p.d_nbr_new.as<int32_t>();
+    A.order = p.d_order.as<int32_t>();
+    A.d = p.d_d.as<double>();
+    A.w64 = p.d_w64.as<double>();
+    A.rrow = p.d_rrow.as<int32_t>();
+    A.rbit = p.d_rbit_new.as<int32_t>();
+    A.ra = p.d_ra.as<float>();
+    A.temp = b.temp;
+    char* sc = static_cast<char*>(b.scratch);
+    A.rw = reinterpret_cast<float*>(sc);
+    sc += size_t(p.n_rays) * 16 * A.NG * 4;
+    A.xb = reinterpret_cast<uint32_t*>(sc);
+    sc += size_t(p.n) * A.NG * 4;
+    A.bar = reinterpret_cast<unsigned*>(sc);
+    A.err = reinterpret_cast<int*>(sc + 16);
+    A.x_out = b.x;
+    A.drift = b.drift;
+    A.accepts = b.accepts;
+    QB_CUDA(cudaMemsetAsync(sc, 0, 64, st));
+    const int grid = p.lock_grid;
+    if (grid < 1) return fail(QB_ENOTSUP, "residual lockstep sweep: no co-resident grid");
+    DevBuf phase;
+    const bool phases = std::getenv("QB_PHASE_TIMES") != nullptr;
+    if (phases) {
+        qb_status s = phase.alloc(size_t(grid) * 32);
+        if (s != QB_OK) return s;
+        QB_CUDA(cudaMemsetAsync(phase.p, 0, phase.bytes, st));
+        A.phase = phase.as<unsigned long long>();
+    }
+    void* kern = phases ? reinterpret_cast<void*>(resid_lockstep_kernel<true>)
+                        : reinterpret_cast<void*>(resid_lockstep_kernel<false>);
+    void* args[] = {&A};
+    QB_CUDA(cudaLaunchCooperativeKernel(kern, dim3(unsigned(grid)), dim3(kLockThreads), args, resid_lockstep_smem(), st));
+    if (phases) {
+        std::vector<unsigned long long> h(size_t(grid) * 4);
+        QB_CUDA(cudaMemcpyAsync(h.data(), phase.p, phase.bytes, cudaMemcpyDeviceToHost, st));
+        QB_CUDA(cudaStreamSynchronize(st));
+        double w = 0, it = 0, br = 0, ch = 0;
+        for (int c = 0; c < grid; ++c) { w += h[4 * c]; it += h[4 * c + 1]; br += h[4 * c + 2]; ch += h[4 * c + 3]; }
+        std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: stage wait %.0f, items %.0f, barrier %.0f\n",
+                     ch / grid, w / ch, it / ch, br / ch);
+    }
+    return QB_OK;
 }
 
 qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st) {

@@ -126,13 +126,14 @@ struct qb_tomo {
 extern "C" void qb_tomo_params_default(qb_tomo_params* p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
-    // A Khufu-proportioned pyramid (height / half base = 139 / 115) at 3/4
-    // scale: 86.25 m half base, 104.25 m high, voxelised to 1.5 m cubes.
+    // A Khufu-proportioned pyramid (height / half base = 139 / 115): 87 m
+    // half base, 105.16 m high, voxelised to 1.5 m cubes; the first 306,328
+    // cells (x fastest, from the base up) are the bits, the apex is rock.
     p->target_bits = 306328;
     p->target_rays = 75594;
     p->voxel = 1.5;
-    p->half_base = 86.25;
-    p->height = 104.25;
+    p->half_base = 87.0;
+    p->height = 87.0 * 139.0 / 115.0;
     // Three detectors in galleries 2 m under the base, near the rim, each
     // looking inward across the pyramid at low elevation (zenith 50-88
     // degrees, +-70 degrees of azimuth around the axis): long chords. With
@@ -158,6 +159,7 @@ extern "C" void qb_tomo_params_default(qb_tomo_params* p) {
     p->exposure = 2.0e9;
     p->min_open = 30.0;
     p->sub_rays = 4;
+    p->room_radius = 12.0;   // every ray of a detector fans out of its room
     p->lambda = 2.0;
     p->kappa = std::log(999.0);   // prior void fraction 1e-3
     p->seed = 20260929ull;
@@ -194,6 +196,14 @@ extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out)
         const double wz = p->half_base * (1.0 - q[2] / p->height);
         if (q[2] < p->height && std::fabs(q[0]) <= wz && std::fabs(q[1]) <= wz) {
             rock[size_t(c)] = 1;
+            // detector rooms are surveyed, not inferred: cells within
+            // room_radius of a detector carry no bit (check_ising.cu:179-199)
+            bool room = false;
+            for (int k = 0; k < p->n_detectors; ++k) {
+                const double dx = q[0] - p->det[3 * k], dy = q[1] - p->det[3 * k + 1], dz = q[2] - p->det[3 * k + 2];
+                room |= dx * dx + dy * dy + dz * dz < p->room_radius * p->room_radius;
+            }
+            if (room) continue;
             if (std::fabs(q[0] - p->void_center[0]) <= hv && std::fabs(q[1] - p->void_center[1]) <= hv &&
                 std::fabs(q[2] - p->void_center[2]) <= hv)
                 is_void[size_t(c)] = 1;

@@ -233,6 +233,7 @@ def small_tomo_params(scale: float = 0.2, bins: int = 24, **overrides) -> TomoPa
               n_theta=bins, n_phi=bins, void_side=base.void_side * scale,
               void_center=[base.void_center[0] * scale, base.void_center[1] * scale, base.void_center[2] * scale],
               det=[base.det[i] * scale if i % 3 != 2 else base.det[i] for i in range(12)],
+              room_radius=base.room_radius * scale,
               exposure=base.exposure * bins * bins / (base.n_theta * base.n_phi) * 0.03)
     kw.update(overrides)
     return tomo_params(**kw)

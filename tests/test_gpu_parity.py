@@ -101,7 +101,7 @@ def test_residual_small_bit_exact():
     temps = O.temperatures(s.t_hot, s.t_cold, s.anneal_sweeps, s.hold_sweeps)
     drift_max = 0.0
     for k in range(R):
-        x, drift = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, k + 1)
+        x, drift = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, k + 1, mode=P.info().variant)
         assert (X[k] == x).all(), k
         drift_max = max(drift_max, drift)
         e = O.binary_energy(a, X[k])
@@ -173,7 +173,7 @@ def test_branch_fractions_call_shape():
     frac, X = branch_fractions(P, s, 4, 16, keep=True, seed_offset=10)
     order, _ = P.colouring()
     temps = O.temperatures(50.0, 1.0, 20, 5)
-    x, _ = O.resid_anneal_coloured(a, order, temps, 10, 2 + 1 + 10)
+    x, _ = O.resid_anneal_coloured(a, order, temps, 10, 2 + 1 + 10, mode=P.info().variant)
     assert (X[2] == x).all()
     assert (frac == O.fractions(X)).all()
 
@@ -198,5 +198,5 @@ def test_benchmark_pyramid_full_size_properties():
     assert r.info().max_drift < 1e-2 * float(np.abs(a["w"] * a["d"]).max())
     order, _ = P.colouring()
     temps = O.temperatures(s.t_hot, s.t_cold, s.anneal_sweeps, s.hold_sweeps)
-    x0, _ = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, 1)
+    x0, _ = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, 1, mode=P.info().variant)
     assert (X[0] == x0).all()
