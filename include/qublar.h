@@ -209,6 +209,31 @@ qb_status qb_result_marginals(qb_result* r, float* p);
 qb_status qb_result_tristate(qb_result* r, float lo, float hi, uint8_t* bits);
 void qb_result_destroy(qb_result* r);
 
+/* Size of the static device scratch of qb_solve_residual_noalloc: held by
+ * every GPU that loads the library, from its first use until the process
+ * exits (8 MiB: the 306,328-bit, 75,594-ray pyramid at 16 branches needs
+ * about 6.1 MB). */
+#define QB_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/* A residual solve that allocates nothing, for callers that must not call
+ * cudaMalloc/cudaFree while they run: a host that owns all device memory
+ * through its own pool, a plugin host that forbids allocation calls (they
+ * synchronise the device), a loop that allocated everything at start-up.
+ * This entry point has no counterpart in the reference. It runs the lockstep
+ * sweep of qb_solve for one block of at most 64 branches and writes the
+ * branches (n_branches x n bytes, 0/1, input bit order) into x_out, a device
+ * buffer the caller owns; the branches equal qb_solve's for the same
+ * arguments. Its per-solve scratch lives in one static device array of
+ * QB_NOALLOC_SCRATCH_BYTES; problems that need more return QB_ENOMEM with the
+ * size. The first call on a device looks up that array's device address;
+ * make it before any stream capture. Calls share the array: calls whose work
+ * overlaps on the GPU race, so serialise them. The problem must come from
+ * qb_problem_create_residual with the lockstep plan (qb_problem_info.variant
+ * == QB_RESID_LOCKSTEP). Returns once the work is queued on `stream`
+ * (cudaStream_t, NULL = legacy default stream). */
+qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
+                                    uint64_t seed_offset, uint8_t* x_out, void* stream);
+
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
 qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);

@@ -17,6 +17,7 @@ STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4:
                 5: "QB_ECUDA", 6: "QB_ENOTSUP", 7: "QB_ECANCELLED", 8: "QB_EBUSY"}
 KIND_ISING = 1
 KIND_RESIDUAL = 2
+NOALLOC_SCRATCH_BYTES = 8 << 20
 RESID_LOCKSTEP = 1
 RESID_CLUSTER = 2
 
@@ -96,6 +97,7 @@ SIGNATURES = {
     "qb_result_destroy": (None, [_P]),
     "qb_energies_ising": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_energies_residual": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P]),
     "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),

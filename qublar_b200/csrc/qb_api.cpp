@@ -45,10 +45,12 @@ void free_async(DevBuf& b, cudaStream_t st) {
     b.bytes = 0;
 }
 
+}  // namespace
+
 // The temperature of every sweep by the reference's expression
 // (ising_recon.hpp:129-131, ising_weighted.hpp:255-257); `volatile` keeps the
 // double rounding of gising::temperatures (ising_gpu.cuh:114-124).
-std::vector<double> temperatures(const qb_schedule& s) {
+std::vector<double> qb::temperatures(const qb_schedule& s) {
     const int total = s.anneal_sweeps + s.hold_sweeps;
     std::vector<double> t(size_t(total), 0.0);
     for (int sweep = 0; sweep < total; ++sweep) {
@@ -58,6 +60,8 @@ std::vector<double> temperatures(const qb_schedule& s) {
     }
     return t;
 }
+
+namespace {
 
 // Slices per class the host-only planner assumes for the lockstep sweep (the
 // SM count of a B200); the order inside a class does not change results.

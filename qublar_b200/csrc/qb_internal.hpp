@@ -50,6 +50,9 @@ qb_status upload_vec(DevBuf& dst, const std::vector<T>& v, cudaStream_t st) {
     return upload(dst, v.data(), v.size() * sizeof(T), st);
 }
 
+// The temperature of every sweep of a schedule (host, double).
+std::vector<double> temperatures(const qb_schedule& s);
+
 // ---- colouring ----------------------------------------------------------------
 
 // A sweep order: bits grouped by colour class. order[k] is the original index

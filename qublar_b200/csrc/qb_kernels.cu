@@ -30,6 +30,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "qb_kernels.hpp"
@@ -1138,4 +1140,134 @@ qb_status launch_i64_to_f64(const long long* e, int R, double* out, cudaStream_t
     return QB_OK;
 }
 
+
+// ---- residual solve without allocation ------------------------------------------------
+//
+// Some callers must not allocate device memory on their hot path: a host
+// framework that owns every byte of device memory through its own pool, a
+// plugin whose host forbids cudaMalloc/cudaFree while it runs (they
+// synchronise the device and can stall other work), or a latency-bound loop
+// that allocated once at start-up. qb_solve_residual_noalloc serves them: it
+// runs the lockstep residual sweep with its per-solve scratch (the branches'
+// residuals and bit words, the grid-barrier counter, the temperature table,
+// the drift and accept tallies) in one static device array that the library
+// carries, and writes the branches into a device buffer the caller owns.
+//
+// The array costs every GPU that loads the library QB_NOALLOC_SCRATCH_BYTES of
+// device memory until the process exits. Calls share it and it keeps the last
+// call's contents, so the entry point clears what must start at zero (the
+// barrier counter, the error flag, the tallies) and the kernel writes the
+// rest before reading it. Two calls whose work overlaps on the GPU (other
+// streams, other host threads) race on the array: serialise them.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoAllocDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocDevices] = {};
+
+// The array's device address on the current device. In host code the name
+// g_noalloc_scratch is a host-side stand-in, not a device address: the first
+// call on a device looks the address up with cudaGetSymbolAddress and keeps it.
+qb_status noalloc_scratch(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= kNoAllocDevices) return fail(QB_ENOTSUP, "qb_solve_residual_noalloc: device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* addr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+        g_noalloc_addr[dev] = addr;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    return QB_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+}  // namespace qb
+
+extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
+                                               uint64_t seed_offset, uint8_t* x_out, void* stream) {
+    using namespace qb;
+    if (!p || !s || !x_out) return fail(QB_EINVAL, "qb_solve_residual_noalloc: null argument");
+    if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_solve_residual_noalloc: residual problems only");
+    const ResidualPlan& P = p->resid;
+    if (P.variant != QB_RESID_LOCKSTEP || P.lock_grid < 1)
+        return fail(QB_ENOTSUP, "qb_solve_residual_noalloc: the problem is not planned for the lockstep sweep");
+    const int R = int(n_branches);
+    if (n_branches < 1 || R > 16 * kLockMaxNG)
+        return fail(QB_EINVAL, "qb_solve_residual_noalloc: n_branches must be in [1, 64]");
+    if (s->anneal_sweeps < 0 || s->hold_sweeps < 0 || s->anneal_sweeps + s->hold_sweeps < 1 || !(s->t_hot > 0.0) ||
+        !(s->t_cold > 0.0) || s->refresh_sweeps < 0)
+        return fail(QB_EINVAL, "qb_solve_residual_noalloc: bad schedule");
+    const int sweeps = s->anneal_sweeps + s->hold_sweeps;
+    const int NG = (R + 15) / 16;
+    // scratch layout: residuals | bit words | barrier counter + error flag |
+    // temperatures | drift | accepts
+    const size_t off_xb = align256(size_t(P.n_rays) * 16 * NG * 4);
+    const size_t off_bar = off_xb + align256(size_t(P.n) * NG * 4);
+    const size_t off_temp = off_bar + 256;
+    const size_t off_drift = off_temp + align256(size_t(sweeps) * 8);
+    const size_t off_acc = off_drift + align256(size_t(R) * 4);
+    const size_t need = off_acc + 256;
+    if (need > QB_NOALLOC_SCRATCH_BYTES) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg,
+                      "qb_solve_residual_noalloc: %zu bytes of scratch needed, the static scratch holds %zu "
+                      "(fewer rays, bits, branches or sweeps; or use qb_solve)",
+                      need, size_t(QB_NOALLOC_SCRATCH_BYTES));
+        return fail(QB_ENOMEM, msg);
+    }
+    QB_CUDA(cudaSetDevice(p->device));
+    unsigned char* base = nullptr;
+    qb_status st = noalloc_scratch(p->device, &base);
+    if (st != QB_OK) return st;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const std::vector<double> temp = temperatures(*s);
+    QB_CUDA(cudaMemcpyAsync(base + off_temp, temp.data(), temp.size() * 8, cudaMemcpyHostToDevice, cs));
+    QB_CUDA(cudaMemsetAsync(base + off_bar, 0, 256, cs));
+    QB_CUDA(cudaMemsetAsync(base + off_drift, 0, size_t(R) * 4, cs));
+    QB_CUDA(cudaMemsetAsync(base + off_acc, 0, 8, cs));
+    ResidLockArgs A{};
+    A.n = P.n;
+    A.n_rays = P.n_rays;
+    A.sweeps = sweeps;
+    A.refresh = s->refresh_sweeps;
+    A.R = R;
+    A.NG = NG;
+    A.lambda = float(P.lambda);
+    A.seed0 = 1 + seed_offset;
+    A.chunks = P.d_chunks.as<int4>();
+    A.chunk_ptr = P.d_chunk_ptr.as<int32_t>();
+    A.ent = P.d_ent.as<uint4>();
+    A.meta = P.d_meta.as<uint4>();
+    A.nbr = P.d_nbr_new.as<int32_t>();
+    A.order = P.d_order.as<int32_t>();
+    A.d = P.d_d.as<double>();
+    A.w64 = P.d_w64.as<double>();
+    A.rrow = P.d_rrow.as<int32_t>();
+    A.rbit = P.d_rbit_new.as<int32_t>();
+    A.ra = P.d_ra.as<float>();
+    A.temp = reinterpret_cast<const double*>(base + off_temp);
+    A.rw = reinterpret_cast<float*>(base);
+    A.xb = reinterpret_cast<uint32_t*>(base + off_xb);
+    A.bar = reinterpret_cast<unsigned*>(base + off_bar);
+    A.err = reinterpret_cast<int*>(base + off_bar + 16);
+    A.x_out = x_out;
+    A.drift = reinterpret_cast<float*>(base + off_drift);
+    A.accepts = reinterpret_cast<unsigned long long*>(base + off_acc);
+    A.phase = nullptr;
+    QB_CUDA(cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(resid_lockstep_smem())));
+    void* args[] = {&A};
+    QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resid_lockstep_kernel<false>), dim3(unsigned(P.lock_grid)),
+                                        dim3(kLockThreads), args, resid_lockstep_smem(), cs));
+    return QB_OK;
+}
+
+namespace qb {
 }  // namespace qb
