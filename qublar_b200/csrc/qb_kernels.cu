@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -504,7 +505,6 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Grid barrier of a cooperative launch: arrive, then poll the counter until
 // every CTA of barrier round `round` has arrived. A poll limit turns a lost
@@ -523,7 +523,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned r
                 ok = 0;
                 break;
             }
-            __nanosleep(20);
         }
         s_ok = ok;
     }
@@ -570,6 +569,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     const int RP = 16 * A.NG;           // residual row pitch (floats)
     constexpr size_t kStageBytes = size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
     float* hseg = reinterpret_cast<float*>(smem + 2 * kStageBytes);   // kLockSegs x NG x 16 segment sums
+    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * kLockMaxNG * 16);   // kLockB x NG bit words
+    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_xw + size_t(kLockB) * kLockMaxNG);          // kLockB x NG x 16 unlike counts
     auto stage = [&](int b) {
         LockStage L;
         unsigned char* q = smem + size_t(b) * kStageBytes;
@@ -594,7 +595,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     cp_async_commit();
     bool ok = grid_barrier(A.bar, A.err, ++round);
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
-    long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0;
+    long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0, ph_a = 0, ph_b = 0, t_a = 0;
     for (int sweep = 0; ok && sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
             // fp64 refresh: thread per (ray, branch), bits of the ray in order
@@ -619,9 +620,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             // stage the next chunk (wrapping into the next sweep), then wait for this one
             const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
             if (PHASES) t_ph = clock64();
-            lock_stage(A, chunks[2 * nx], chunks[2 * nx + 1], stage((gci + 1) & 1));
-            cp_async_commit();
-            cp_async_wait1();
+            // this chunk was staged during the previous chunk's barrier
+            asm volatile("cp.async.wait_all;" ::: "memory");
             __syncthreads();
             if (PHASES) {
                 const long long t1 = clock64();
@@ -631,8 +631,29 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             const LockStage St = stage(gci & 1);
             const int nb = c0.y - c0.x;
             const int nseg = c0.z;                       // segments of the chunk
-            // A. segment sums
-            for (int it = warp; it < nseg * A.NG; it += kWarps) {
+            if (PHASES) t_a = clock64();
+            // A. segment sums, and per (bit, group) the bit word and the
+            // unlike-neighbour counts, in one round of loads
+            const int nseg_items = nseg * A.NG;
+            for (int it = warp; it < nseg_items + nb * A.NG; it += kWarps) {
+                if (it >= nseg_items) {
+                    const int k = (it - nseg_items) / A.NG, g = (it - nseg_items) % A.NG;
+                    const uint4 m0 = St.meta[2 * k];
+                    const int ns = int(m0.z) - c1.z, nn = int(m0.w);
+                    const uint32_t xw = __ldcg(&A.xb[size_t(c0.x + k) * A.NG + g]);
+                    int unlike = 0;
+                    for (int j0 = 0; j0 < nn; j0 += 32) {
+                        const uint32_t w = j0 + lane < nn ? __ldcg(&A.xb[size_t(St.nbr[ns + j0 + lane]) * A.NG + g]) : 0u;
+                        const int m = min(32, nn - j0);
+                        for (int u = 0; u < m; ++u) {
+                            const uint32_t wu = __shfl_sync(kFull, w, u);
+                            unlike += ((wu ^ xw) >> br) & 1u;
+                        }
+                    }
+                    if (half == 0) s_unl[(k * A.NG + g) * 16 + br] = uint8_t(unlike);
+                    if (lane == 0) s_xw[k * A.NG + g] = xw;
+                    continue;
+                }
                 const int sg = it / A.NG, g = it % A.NG;
                 // the bit of segment sg: meta word 7 is the bit's first segment in the chunk
                 int lo = 0, hi = nb - 1;
@@ -665,6 +686,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (half == 0) hseg[(sg * A.NG + g) * 16 + br] = __fadd_rn(acc, other);
             }
             __syncthreads();
+            if (PHASES) {
+                const long long t1 = clock64();
+                ph_a += t1 - t_a;
+                t_a = t1;
+            }
             // B. decide and scatter, a warp per (bit, group)
             for (int it = warp; it < nb * A.NG; it += kWarps) {
                 const int k = it / A.NG, g = it % A.NG;
@@ -672,19 +698,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 const bool live = branch < A.R && half == 0;
                 const uint4 m0 = St.meta[2 * k], m1 = St.meta[2 * k + 1];
                 const int i = c0.x + k;
-                const uint64_t u53 = live ? draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u) : 0ull;
-                const uint32_t xw = __ldcg(&A.xb[size_t(i) * A.NG + g]);
+                const int ns = 0, ne = int(m0.w);
+                const uint32_t xw = s_xw[k * A.NG + g];
                 const uint32_t xi = (xw >> br) & 1u;
-                const int ns = int(m0.z) - c1.z, ne = ns + int(m0.w);
-                int unlike = 0;
-                for (int j0 = ns; j0 < ne; j0 += 8) {
-                    uint32_t nw[8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) nw[u] = j0 + u < ne ? __ldcg(&A.xb[size_t(St.nbr[j0 + u]) * A.NG + g]) : 0u;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (j0 + u < ne) unlike += ((nw[u] >> br) & 1u) != xi ? 1 : 0;
-                }
+                const int unlike = s_unl[(k * A.NG + g) * 16 + br];
+                const uint64_t u53 = live ? draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u) : 0ull;
                 int flip = 0;
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
@@ -713,8 +731,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     }
                 }
             }
+            __syncthreads();   // the other buffer is free: stage the next chunk under the barrier
+            if (PHASES) ph_b += clock64() - t_a;
+            lock_stage(A, chunks[2 * nx], chunks[2 * nx + 1], stage((gci + 1) & 1));
+            cp_async_commit();
             if (PHASES) {
-                __syncthreads();
                 const long long t1 = clock64();
                 ph_items += t1 - t_ph;
                 t_ph = t1;
@@ -733,8 +754,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     if (PHASES && tid == 0) {
-        unsigned long long* ph = A.phase + 4 * size_t(blockIdx.x);
-        ph[0] = ph_wait; ph[1] = ph_items; ph[2] = ph_bar; ph[3] = ph_n;
+        unsigned long long* ph = A.phase + 8 * size_t(blockIdx.x);
+        ph[0] = ph_wait; ph[1] = ph_items; ph[2] = ph_bar; ph[3] = ph_n; ph[4] = ph_a; ph[5] = ph_b;
     }
     if (ok) {
         // branches out, original bit order
@@ -1011,7 +1032,8 @@ qb_status resid_check_fit(const ResidualPlan& p) {
 }
 
 size_t resid_lockstep_smem() {
-    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + size_t(kLockSegs) * kLockMaxNG * 16 * 4;
+    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + size_t(kLockSegs) * kLockMaxNG * 16 * 4 +
+           size_t(kLockB) * kLockMaxNG * (4 + 16);
 }
 int resid_lockstep_max_branches() { return 16 * kLockMaxNG; }
 int resid_lockstep_segment() { return kSeg; }
@@ -1080,7 +1102,7 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     DevBuf phase;
     const bool phases = std::getenv("QB_PHASE_TIMES") != nullptr;
     if (phases) {
-        qb_status s = phase.alloc(size_t(grid) * 32);
+        qb_status s = phase.alloc(size_t(grid) * 64);
         if (s != QB_OK) return s;
         QB_CUDA(cudaMemsetAsync(phase.p, 0, phase.bytes, st));
         A.phase = phase.as<unsigned long long>();
@@ -1090,13 +1112,17 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     void* args[] = {&A};
     QB_CUDA(cudaLaunchCooperativeKernel(kern, dim3(unsigned(grid)), dim3(kLockThreads), args, resid_lockstep_smem(), st));
     if (phases) {
-        std::vector<unsigned long long> h(size_t(grid) * 4);
+        std::vector<unsigned long long> h(size_t(grid) * 8);
         QB_CUDA(cudaMemcpyAsync(h.data(), phase.p, phase.bytes, cudaMemcpyDeviceToHost, st));
         QB_CUDA(cudaStreamSynchronize(st));
-        double w = 0, it = 0, br = 0, ch = 0;
-        for (int c = 0; c < grid; ++c) { w += h[4 * c]; it += h[4 * c + 1]; br += h[4 * c + 2]; ch += h[4 * c + 3]; }
-        std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: stage wait %.0f, items %.0f, barrier %.0f\n",
-                     ch / grid, w / ch, it / ch, br / ch);
+        double w = 0, it = 0, br = 0, ch = 0, pa = 0, pb = 0, itmax = 0;
+        for (int c = 0; c < grid; ++c) {
+            w += h[8 * c]; it += h[8 * c + 1]; br += h[8 * c + 2]; ch += h[8 * c + 3]; pa += h[8 * c + 4]; pb += h[8 * c + 5];
+            itmax = std::max(itmax, double(h[8 * c + 1]) / std::max(1.0, double(h[8 * c + 3])));
+        }
+        std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: stage wait %.0f, items %.0f "
+                     "(A %.0f, B %.0f; slowest CTA's mean %.0f), barrier %.0f\n",
+                     ch / grid, w / ch, it / ch, pa / ch, pb / ch, itmax, br / ch);
     }
     return QB_OK;
 }
