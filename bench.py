@@ -37,9 +37,12 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "muon-tomography pyramid: 306,328 bits, 75,594 rays, 16 branches, T 50->1 (200 sweeps) + 50 at T=1"
 METRIC = "spin-flip attempts/s"
 BRANCHES = 16
-# DRAM bytes per launch of resid_anneal_kernel from the committed ncu
-# capture (profiles/resid_anneal_pyramid.md); None until one exists.
-NCU_TRAFFIC_PER_LAUNCH = None
+# DRAM bytes (read + write) per sweep of resid_lockstep_kernel from the
+# committed ncu capture of a 10-sweep launch on the same pyramid and 16
+# branches (profiles/resid_lockstep_pyramid.md): 1.924 GB + 6.3 MB over 10
+# sweeps. The bit->ray structure streams from DRAM once per sweep, so the
+# traffic of a full launch is this figure times its sweeps.
+NCU_TRAFFIC_PER_SWEEP = (1.924285e9 + 6.321408e6) / 10
 
 
 def log(*a):
@@ -109,20 +112,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(a, R, sweeps, refresh):
-    """Bytes one resid_anneal_kernel launch must move (per-sweep figure of
-    the residual form x sweeps): every branch streams the bit->ray CSR (ray
-    id + a, 8 B per entry; one branch per cluster, so R replica tiles), reads
-    and writes its residual state once (rays x 2 x 4 B), reads its bits
-    (1/8 B each, twice) and their prior neighbour lists (4 B per entry); each
-    fp64 refresh streams the ray-major CSR (8 B per entry) once per branch."""
+def algorithmic_bytes(a, R, sweeps, refresh, accepted):
+    """Bytes one launch of the lockstep residual sweep must move: the residual
+    form's per-sweep figure with a replica tile of 16 branches (one stream
+    of the bit->ray CSR -- ray id + a, 8 B per entry -- serves 16 branches),
+    each branch's residuals read and written once per sweep (rays x 2 x 4 B),
+    its bits read and written (2 x 1/8 B each), the prior's neighbour lists
+    once per tile (4 B per entry), plus every accepted flip's residual
+    read-modify-write (entries of the bit x 2 x 4 B, from the device's
+    accept count, at the mean entries per bit) and the fp64 refreshes
+    (ray-major CSR, 8 B per entry, once per tile)."""
     nnz = int(a["ray"].size)
     n = int(a["row_ptr"].size - 1)
     rays = int(a["d"].size)
     nbr = int(a["nbr"].size)
-    per_sweep = nnz * 8 * R + R * (rays * 2 * 4 + n * 2 / 8 + nbr * 4)
+    tiles = (R + 15) // 16
+    per_sweep = nnz * 8 * tiles + R * (rays * 2 * 4 + n * 2 / 8) + nbr * 4 * tiles
     refreshes = (sweeps - 1) // refresh if refresh > 0 else 0
-    return per_sweep * sweeps + refreshes * R * nnz * 8
+    return per_sweep * sweeps + refreshes * tiles * nnz * 8 + accepted * (nnz / n) * 2 * 4
 
 
 def cpu_baseline(a, sched, threads, branches):
@@ -251,6 +258,7 @@ def main():
     total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     infos = [r.info() for r in results]
     anneal_ms = statistics.mean(i.anneal_ms for i in infos)
+    accepted = statistics.mean(i.accepted for i in infos)
     launches = sum(i.launches for i in infos)
     drift = max(i.max_drift for i in infos)
     for r in results:
@@ -288,8 +296,11 @@ def main():
     e2e_value = world * attempts_step / e2e_mean
 
     hbm, peak_kind = peaks()
-    alg = algorithmic_bytes(a, BRANCHES, sched.sweeps, sched.refresh_sweeps)
+    alg = algorithmic_bytes(a, BRANCHES, sched.sweeps, sched.refresh_sweeps, accepted)
     achieved = alg / (anneal_ms / 1e3) / 1e9
+    traffic = None
+    if NCU_TRAFFIC_PER_SWEEP is not None:
+        traffic = NCU_TRAFFIC_PER_SWEEP * sched.sweeps
     line = {
         "metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -302,8 +313,8 @@ def main():
                 "s_per_step": e2e_mean},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": peak_kind, "traffic": NCU_TRAFFIC_PER_LAUNCH, "kernel": "resid_anneal_kernel",
-                     "kernel_ms": anneal_ms, "algorithmic_bytes": alg},
+                     "peak_kind": peak_kind, "traffic": traffic, "kernel": "resid_lockstep_kernel",
+                     "kernel_ms": anneal_ms, "algorithmic_bytes": alg, "accepted_flips": accepted},
         "max_residual_drift": drift,
         "clocks": clocks,
     }

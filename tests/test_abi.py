@@ -1,0 +1,222 @@
+"""The C ABI and the host logic, on the CPU (no device needed).
+
+* the library loads and exports every function include/*.h declares;
+* malformed inputs are refused before any device call, with the reference
+  loader's reasons (parse_rudy, ising_weighted.hpp:89-133);
+* the planner's colour classes are valid (no two interacting bits in a class)
+  and cover every bit once;
+* the C++ adapter compiles against stand-in types with the reference's member
+  names and fails cleanly without a device;
+* branches spread over two ranks (gloo) give the single-process fractions.
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+import qublar_b200 as qb
+from qublar_b200 import synth
+from qublar_b200._abi import IsingDesc, QBError, check, lib, ptr
+from qublar_b200.dist import branch_range, fractions_from_counts
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INCLUDE = os.path.join(ROOT, "include")
+
+
+def declared_functions():
+    names = set()
+    for h in os.listdir(INCLUDE):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(INCLUDE, h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(qb_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_function():
+    names = declared_functions()
+    assert len(names) > 25
+    L = lib()
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    L = lib()
+    assert L.qb_abi_version() == 1
+    for s in range(9):
+        assert L.qb_status_string(s)
+    assert L.qb_status_string(0) == b"ok"
+
+
+def _ising_status(n, eu, ev, ew):
+    eu, ev, ew = (np.ascontiguousarray(x, np.int32) for x in (eu, ev, ew))
+    d = IsingDesc(n, eu.size, ptr(eu), ptr(ev), ptr(ew))
+    h = C.c_void_p()
+    return lib().qb_problem_create_ising(C.byref(d), None, C.byref(h)), lib().qb_last_error().decode()
+
+
+@pytest.mark.parametrize("case,why", [
+    ((3, [0], [0], [1]), "self-loop"),
+    ((3, [0, 1], [1, 0], [1, 1]), "duplicate edge"),
+    ((3, [0], [3], [1]), "out of range"),
+    ((0, [], [], []), "n must be positive"),
+])
+def test_ising_refusals(case, why):
+    st, msg = _ising_status(*case)
+    assert st == 1 and why in msg   # QB_EINVAL
+
+
+def _resid_status(arr):
+    d = synth.residual_desc(arr)
+    h = C.c_void_p()
+    return lib().qb_problem_create_residual(C.byref(d), None, C.byref(h)), lib().qb_last_error().decode()
+
+
+def test_residual_refusals():
+    a = synth.tiny6()
+    b = dict(a)
+    b["ray"] = a["ray"].copy()
+    b["ray"][1] = b["ray"][0]   # a bit lists a ray twice (bit 0 has several rays)
+    assert a["row_ptr"][1] >= 2
+    st, msg = _resid_status(b)
+    assert st == 1 and "twice" in msg
+    c = dict(a)
+    c["nbr"] = a["nbr"].copy()
+    c["nbr"][0] = 3   # bit 0 lists 3, 3 does not list 0
+    st, msg = _resid_status(c)
+    assert st == 1 and "symmetric" in msg
+    e = dict(a)
+    e["ray"] = a["ray"].copy()
+    e["ray"][0] = 99
+    st, msg = _resid_status(e)
+    assert st == 1 and "out of range" in msg
+
+
+def test_solve_rejects_null_and_bad_schedule():
+    L = lib()
+    out = C.c_void_p()
+    s = qb.Schedule().to_c()
+    assert L.qb_solve(None, C.byref(s), 4, 0, None, C.byref(out)) == 1
+
+
+def _colour(kind, desc, n):
+    order = np.empty(n, np.int32)
+    cptr = np.empty(n + 1, np.int32)
+    nc = C.c_int32()
+    fn = lib().qb_colour_ising if kind == "ising" else lib().qb_colour_residual
+    check(fn(C.byref(desc), ptr(order), ptr(cptr), C.byref(nc)))
+    return order, cptr[: nc.value + 1]
+
+
+@pytest.mark.parametrize("gen", [lambda: synth.random_complete(16, 1000, 1), lambda: synth.random_sparse(300, 3000, 42, 0),
+                                 lambda: synth.erdos_renyi(800, 0.06, 1), lambda: synth.torus_pm1(32, 5),
+                                 lambda: synth.random_regular(500, 7, 3)])
+def test_graph_colouring_is_valid(gen):
+    n, eu, ev, ew = gen()
+    d = IsingDesc(n, eu.size, ptr(eu), ptr(ev), ptr(ew))
+    order, cptr = _colour("ising", d, n)
+    assert sorted(order.tolist()) == list(range(n))
+    colour = np.empty(n, np.int64)
+    for c in range(cptr.size - 1):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    assert (colour[eu] != colour[ev]).all()
+
+
+def test_residual_colouring_is_valid():
+    a = synth.tomography(synth.small_tomo_params())
+    n = a["row_ptr"].size - 1
+    d = synth.residual_desc(a)
+    order, cptr = _colour("residual", d, n)
+    assert sorted(order.tolist()) == list(range(n))
+    colour = np.empty(n, np.int64)
+    for c in range(cptr.size - 1):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    # no ray holds two bits of one class
+    bit_of_entry = np.repeat(np.arange(n), np.diff(a["row_ptr"]))
+    pairs = np.unique(np.stack([a["ray"], colour[bit_of_entry]], 1), axis=0)
+    assert pairs.shape[0] == a["ray"].size
+    # no prior bond inside a class
+    src = np.repeat(np.arange(n), np.diff(a["nbr_ptr"]))
+    assert (colour[src] != colour[a["nbr"]]).all()
+    # a class count near the longest ray (the clique bound)
+    assert cptr.size - 1 >= np.bincount(a["ray"]).max()
+
+
+def test_benchmark_pyramid_sizes():
+    a = synth.tomography()
+    assert a["row_ptr"].size - 1 == 306328 and a["d"].size == 75594
+    assert 140 < a["ray"].size / a["d"].size < 160
+
+
+def test_adapter_compiles_and_fails_cleanly_without_a_device(tmp_path):
+    exe = tmp_path / "adapter_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-I" + INCLUDE, os.path.join(ROOT, "tests", "adapter_check.cpp"),
+           "-L" + os.path.join(ROOT, "qublar_b200"), "-lqublar_b200", "-Wl,-rpath," + os.path.join(ROOT, "qublar_b200"),
+           "-o", str(exe)]
+    subprocess.run(cmd, check=True)
+    if qb.device_count() > 0:
+        pytest.skip("a device is visible: the GPU test covers the adapter")
+    write_adapter_inputs(tmp_path)
+    r = subprocess.run([str(exe), str(tmp_path), "cpu"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "exception" in r.stdout
+
+
+def write_adapter_inputs(d):
+    a = synth.tomography(synth.small_tomo_params(0.12, 12))
+    for k in ("d", "w", "row_ptr", "ray", "a", "nbr_ptr", "nbr"):
+        a[k].tofile(os.path.join(d, k + ".bin"))
+    np.array([a["lambda"], a["kappa"]], np.float64).tofile(os.path.join(d, "prior.bin"))
+    n, eu, ev, ew = synth.random_sparse(300, 3000, 7, 1000)
+    eu.tofile(os.path.join(d, "eu.bin"))
+    ev.tofile(os.path.join(d, "ev.bin"))
+    ew.tofile(os.path.join(d, "ew.bin"))
+    np.array([n], np.int32).tofile(os.path.join(d, "gn.bin"))
+    return a, (n, eu, ev, ew)
+
+
+def test_branch_range_covers_branches():
+    for R in (1, 5, 16, 64):
+        for W in (1, 2, 3, 8):
+            rs = [branch_range(R, W, r) for r in range(W)]
+            assert rs[0][0] == 0 and rs[-1][1] == R
+            assert all(rs[k][1] == rs[k + 1][0] for k in range(W - 1))
+
+
+def _gloo_worker(rank, world, port, X, out_path):
+    import torch.distributed as dist
+    from qublar_b200.dist import allreduce_counts
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    b0, b1 = branch_range(X.shape[0], world, rank)
+    counts = allreduce_counts(X[b0:b1])
+    if rank == 0:
+        np.save(out_path, fractions_from_counts(counts, X.shape[0]))
+    dist.destroy_process_group()
+
+
+def test_two_ranks_give_single_process_fractions(tmp_path):
+    """Branches split over two gloo ranks: the summed counts give the same
+    fractions as one process (the float division of branch_fractions)."""
+    import socket
+
+    import torch.multiprocessing as mp
+    rng = np.random.default_rng(5)
+    X = (rng.random((13, 1000)) < 0.3).astype(np.uint8)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "frac.npy")
+    mp.spawn(_gloo_worker, args=(2, port, X, out), nprocs=2, join=True)
+    got = np.load(out)
+    want = fractions_from_counts(X.sum(0), X.shape[0])
+    assert (got == want).all()
+    from oracle import oracle as O
+    assert (got == O.fractions(X)).all()

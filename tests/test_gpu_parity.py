@@ -200,3 +200,32 @@ def test_benchmark_pyramid_full_size_properties():
     temps = O.temperatures(s.t_hot, s.t_cold, s.anneal_sweeps, s.hold_sweeps)
     x0, _ = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, 1, mode=P.info().variant)
     assert (X[0] == x0).all()
+
+
+def test_cpp_adapter_matches_the_python_path(tmp_path):
+    """include/qublar_adapter.hpp, driven with stand-ins for the reference's
+    types: branch_fractions, wising::anneal and run_batch give the results of
+    the same calls through the Python binding (one library underneath)."""
+    import subprocess
+
+    from tests.test_abi import INCLUDE, ROOT, write_adapter_inputs
+    exe = tmp_path / "adapter_check"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I" + INCLUDE, os.path.join(ROOT, "tests", "adapter_check.cpp"),
+                    "-L" + os.path.join(ROOT, "qublar_b200"), "-lqublar_b200",
+                    "-Wl,-rpath," + os.path.join(ROOT, "qublar_b200"), "-o", str(exe)], check=True)
+    a, (n, eu, ev, ew) = write_adapter_inputs(tmp_path)
+    r = subprocess.run([str(exe), str(tmp_path), "gpu"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    P = ResidualProblem.from_arrays(a)
+    frac, X = branch_fractions(P, Schedule(50.0, 1.0, 40, 10, 50), 4, keep=True, seed_offset=5)
+    assert (np.fromfile(tmp_path / "frac.bin", np.float32) == frac).all()
+    assert (np.fromfile(tmp_path / "branches.bin", np.uint8).reshape(4, -1) == X).all()
+    G = IsingProblem(n, eu, ev, ew)
+    b = Budget(5.0, 1e-3, 100, 10)
+    from qublar_b200 import anneal, run_batch
+    ro = anneal(G, b, 3)
+    assert (np.fromfile(tmp_path / "anneal_x.bin", np.uint8) == ro.x).all()
+    assert int(np.fromfile(tmp_path / "anneal_e.bin", np.int64)[0]) == ro.energy_tracked
+    bo = run_batch(G, b, 1, 4)
+    assert (np.fromfile(tmp_path / "batch_x.bin", np.uint8).reshape(4, -1) == bo.X).all()
+    assert (np.fromfile(tmp_path / "batch_e.bin", np.int64) == bo.energy).all()
