@@ -234,6 +234,70 @@ void qb_result_destroy(qb_result* r);
 qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
                                     uint64_t seed_offset, uint8_t* x_out, void* stream);
 
+/* ---- batches: many ising instances in one persistent launch ----------------
+ *
+ * The reference anneals one instance per launch (gising::run_batch,
+ * src/ising_gpu.cuh:396-458, driven per graph by tools/gpu_anneal.cu:139).
+ * qb_solve_batch packs many ising problems of uneven size, each with its own
+ * schedule, branch count and seeds, into work items (one instance x a group
+ * of replicas) that one persistent kernel drains largest first. Every branch
+ * is identical to what qb_solve returns for its problem with the same
+ * schedule and seeds, whatever the batch holds and whatever the launch shape. */
+typedef struct qb_batch qb_batch;
+
+typedef struct qb_batch_item {
+    qb_problem* problem;     /* an ising problem (qb_problem_create_ising), on the batch's device */
+    qb_schedule schedule;    /* this instance's schedule */
+    uint32_t n_branches;     /* branch b uses seed b + 1 + seed_offset */
+    uint64_t seed_offset;
+} qb_batch_item;
+
+/* Launch shape of the packed kernel; zeros take the defaults (512 threads,
+ * 96 KiB of state per CTA, groups of up to 32 replicas). */
+typedef struct qb_batch_config {
+    int32_t threads;         /* per CTA: a multiple of 32 in [32, 1024] */
+    int32_t smem_bytes;      /* shared memory for one item's state (n x group x 5 bytes) */
+    int32_t max_group;       /* replicas per work item: a power of two in [1, 32] */
+    int32_t ctas;            /* persistent CTAs; 0 = as many as fit the device */
+} qb_batch_config;
+
+/* Times candidate shapes on the batch itself with its schedules sampled at
+ * sample_sweeps evenly spaced sweeps (0 = 8) and returns the fastest. The
+ * answer is kept per process for batches of the same shape (instance count,
+ * total bits, total edges, total branches) and returned at once next time.
+ * Results do not depend on the shape. */
+qb_status qb_batch_autotune(const qb_batch_item* items, int32_t count, int32_t sample_sweeps, const qb_opts* opts,
+                            qb_batch_config* out);
+
+/* Queues the packed anneal on opts->stream and returns. cfg may be NULL. */
+qb_status qb_solve_batch(const qb_batch_item* items, int32_t count, const qb_batch_config* cfg, const qb_opts* opts,
+                         qb_batch** out);
+
+typedef struct qb_batch_info {
+    int32_t items;           /* instances */
+    int32_t work_items;      /* instance x replica-group units */
+    int32_t global_items;    /* units whose state did not fit shared memory */
+    int32_t threads;
+    int32_t smem_bytes;
+    int32_t max_group;
+    int32_t ctas;
+    int32_t launches;        /* kernels the batch launched */
+    int64_t attempts;        /* sum over instances of branches x sweeps x n */
+    float anneal_ms;         /* CUDA-event time of the packed anneal */
+    float total_ms;          /* ... of the whole batch (anneal + marginals) */
+} qb_batch_info;
+/* Waits for the batch. */
+qb_status qb_batch_info_get(qb_batch* b, qb_batch_info* info);
+/* Instance `item`'s branches (n_branches x n, 0/1, input bit order). Waits. */
+qb_status qb_batch_branches(qb_batch* b, int32_t item, uint8_t* x);
+/* Instance `item`'s tracked energies E = -cut (n_branches). */
+qb_status qb_batch_energies_i64(qb_batch* b, int32_t item, int64_t* e);
+/* Instance `item`'s maintained fields (n_branches x n). */
+qb_status qb_batch_fields_i64(qb_batch* b, int32_t item, int64_t* f);
+/* Instance `item`'s per-bit fraction of branches with x = 1. */
+qb_status qb_batch_marginals(qb_batch* b, int32_t item, float* p);
+void qb_batch_destroy(qb_batch* b);
+
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
 qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);

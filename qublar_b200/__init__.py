@@ -22,11 +22,12 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import (KIND_ISING, KIND_RESIDUAL, IsingDesc, Opts, ProblemInfo, QBError, ResidualDesc, ResultInfo,
-                   ScheduleC, check, lib, ptr)
+from ._abi import (KIND_ISING, KIND_RESIDUAL, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts, ProblemInfo,
+                   QBError, ResidualDesc, ResultInfo, ScheduleC, check, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "Result", "RunOut", "BatchOut",
-           "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib"]
+           "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
+           "Batch", "solve_batch", "autotune_batch"]
 
 
 @dataclass
@@ -239,6 +240,88 @@ class ResidualProblem(_Problem):
         e = np.empty(X.shape[0], dtype=np.float64)
         check(lib().qb_energies_residual(self._h, ptr(X), int(X.shape[0]), ptr(e)))
         return e
+
+
+# ---- batches: many ising instances in one persistent launch --------------------------------
+
+def _batch_items(items):
+    """items: (IsingProblem, Schedule, n_branches, seed_offset) tuples."""
+    arr = (BatchItem * len(items))()
+    for k, (prob, sched, R, off) in enumerate(items):
+        arr[k] = BatchItem(prob._h.value, sched.to_c(), int(R), int(off))
+    return arr
+
+
+class Batch:
+    """One qb_solve_batch: every instance's branches stay on the device."""
+
+    def __init__(self, handle, items):
+        self._h = C.c_void_p(handle)
+        self.items = list(items)
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().qb_batch_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> BatchInfo:
+        i = BatchInfo()
+        check(lib().qb_batch_info_get(self._h, C.byref(i)))
+        return i
+
+    def _shape(self, k):
+        prob, _, R, _ = self.items[k]
+        return int(R), prob.n
+
+    def branches(self, k: int) -> np.ndarray:
+        R, n = self._shape(k)
+        x = np.empty((R, n), dtype=np.uint8)
+        check(lib().qb_batch_branches(self._h, int(k), ptr(x)))
+        return x
+
+    def energies_tracked(self, k: int) -> np.ndarray:
+        R, _ = self._shape(k)
+        e = np.empty(R, dtype=np.int64)
+        check(lib().qb_batch_energies_i64(self._h, int(k), ptr(e)))
+        return e
+
+    def fields(self, k: int) -> np.ndarray:
+        R, n = self._shape(k)
+        f = np.empty((R, n), dtype=np.int64)
+        check(lib().qb_batch_fields_i64(self._h, int(k), ptr(f)))
+        return f
+
+    def marginals(self, k: int) -> np.ndarray:
+        _, n = self._shape(k)
+        p = np.empty(n, dtype=np.float32)
+        check(lib().qb_batch_marginals(self._h, int(k), ptr(p)))
+        return p
+
+
+def autotune_batch(items, sample_sweeps: int = 8, stream=None) -> BatchConfig:
+    """The fastest packed-kernel shape for this batch (qb_batch_autotune)."""
+    arr = _batch_items(items)
+    cfg = BatchConfig()
+    o = _opts(-1, stream)
+    check(lib().qb_batch_autotune(arr, len(items), int(sample_sweeps), C.byref(o), C.byref(cfg)))
+    return cfg
+
+
+def solve_batch(items, config: BatchConfig | None = None, stream=None) -> Batch:
+    """Anneal many ising instances in one persistent launch (qb_solve_batch).
+    items: (IsingProblem, Schedule, n_branches, seed_offset) tuples."""
+    arr = _batch_items(items)
+    out = C.c_void_p()
+    o = _opts(-1, stream)
+    cfg = C.byref(config) if config is not None else None
+    check(lib().qb_solve_batch(arr, len(items), cfg, C.byref(o), C.byref(out)))
+    return Batch(out.value, items)
 
 
 # ---- the reference's call shapes ------------------------------------------------------------

@@ -73,6 +73,21 @@ class TomoParams(C.Structure):
                 ("lambda_", C.c_double), ("kappa", C.c_double), ("seed", C.c_uint64)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("problem", C.c_void_p), ("schedule", ScheduleC), ("n_branches", C.c_uint32),
+                ("seed_offset", C.c_uint64)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("smem_bytes", C.c_int32), ("max_group", C.c_int32), ("ctas", C.c_int32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("items", C.c_int32), ("work_items", C.c_int32), ("global_items", C.c_int32),
+                ("threads", C.c_int32), ("smem_bytes", C.c_int32), ("max_group", C.c_int32), ("ctas", C.c_int32),
+                ("launches", C.c_int32), ("attempts", C.c_int64), ("anneal_ms", C.c_float), ("total_ms", C.c_float)]
+
+
 _P = C.c_void_p
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -98,6 +113,16 @@ SIGNATURES = {
     "qb_energies_ising": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_energies_residual": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P]),
+    "qb_batch_autotune": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.c_int32, C.POINTER(Opts),
+                                    C.POINTER(BatchConfig)]),
+    "qb_solve_batch": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.POINTER(BatchConfig), C.POINTER(Opts),
+                                 C.POINTER(_P)]),
+    "qb_batch_info_get": (C.c_int, [_P, C.POINTER(BatchInfo)]),
+    "qb_batch_branches": (C.c_int, [_P, C.c_int32, _P]),
+    "qb_batch_energies_i64": (C.c_int, [_P, C.c_int32, _P]),
+    "qb_batch_fields_i64": (C.c_int, [_P, C.c_int32, _P]),
+    "qb_batch_marginals": (C.c_int, [_P, C.c_int32, _P]),
+    "qb_batch_destroy": (None, [_P]),
     "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),

@@ -1,0 +1,266 @@
+// Packed integer Ising sweep: many instances and replica groups of uneven size
+// in one persistent launch.
+//
+// Each CTA takes the next work item from a device counter (items arrive
+// sorted by estimated cost, largest first), anneals its G replicas of one
+// instance over its sweep range, and takes another. The item's fields (int32)
+// and spins (int8) sit in the CTA's shared memory, laid out bit-major with the
+// replica fastest, so a warp covers 32 / G consecutive bits of a class for all
+// G replicas: neighbour updates of one accepted bit land in G consecutive
+// words, and the CSR row of a bit is read once for its G replicas. Items too
+// large for shared memory run in place on their global state.
+//
+// The decisions are those of the single-instance sweep (qb_kernels.cu): colour
+// classes in order, dE = -s_i f_i, accept if dE <= 0, else if u53 * 2^-53 <
+// exp(-dE / T) with u53 the Philox draw of (replica seed, original bit,
+// sweep). For |dE| <= 256 the comparison uses a per-sweep table of
+// ceil(exp(-k / T) * 2^53), which is the same test on the integer u53 (the
+// scaling by 2^53 is exact), so a replica's trajectory does not depend on the
+// item it falls in, the launch shape, or the other instances of the batch.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "qb_batch.hpp"
+#include "qb_philox.cuh"
+
+namespace qb {
+
+namespace {
+
+constexpr int kThrMax = 256;
+constexpr int kClassMax = 512;   // class boundaries kept in shared memory
+constexpr int kBatchThreadsMax = 1024;
+
+static_assert(sizeof(IsingItem) % 8 == 0, "IsingItem is copied as 8-byte words");
+
+__device__ __forceinline__ unsigned long long accept_threshold(int k, double T) {
+    const double p = exp(-double(k) / T);
+    return (unsigned long long)ceil(p * 0x1.0p53);
+}
+
+template <typename WT, bool GLOBAL>
+__device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* smem, unsigned long long* thr,
+                                           unsigned long long* e_sh, int* cls) {
+    const int n = it.n;
+    const int lg = it.log2g;
+    const int G = 1 << lg;
+    const int NG = n << lg;
+    const int tid = int(threadIdx.x);
+    const int bs = int(blockDim.x);
+    const int flags = it.flags;
+    const int32_t* __restrict__ class_ptr = it.class_ptr;
+    const int32_t* __restrict__ order = it.order;
+    const double* __restrict__ temp = it.temp;
+    const int n_colours = it.n_colours;
+    const int bound = it.bound;
+    const int sweep0 = it.sweep0, sweep1 = it.sweep1;
+    int32_t* f;
+    int8_t* s;
+    if (GLOBAL) {
+        f = it.f_state;
+        s = it.s_state;
+    } else {
+        f = reinterpret_cast<int32_t*>(smem);
+        s = reinterpret_cast<int8_t*>(smem + size_t(NG) * 4);
+    }
+    const bool init = (flags & kItemInit) != 0;
+    if (init) {
+        for (int p = tid; p < NG; p += bs) {
+            f[p] = it.f0[p >> lg];
+            s[p] = -1;
+        }
+    } else if (!GLOBAL) {
+        for (int p = tid; p < NG; p += bs) {
+            f[p] = it.f_state[p];
+            s[p] = it.s_state[p];
+        }
+    }
+    // class boundaries on chip (most instances have far fewer classes)
+    const bool cls_sh = n_colours <= kClassMax;
+    if (cls_sh)
+        for (int c = tid; c <= n_colours; c += bs) cls[c] = class_ptr[c];
+    if (tid < G) e_sh[tid] = 0ull;
+    __syncthreads();
+    // bs is a multiple of G, so this thread always serves replica r
+    const int r = tid & (G - 1);
+    const uint64_t seed = it.seed0 + uint64_t(r);
+    const bool table = bound <= kThrMax;
+    long long E = 0;
+    for (int sweep = sweep0; sweep < sweep1; ++sweep) {
+        const double T = temp[sweep];
+        if (table) {
+            for (int k = tid + 1; k <= bound; k += bs) thr[k] = accept_threshold(k, T);
+            __syncthreads();
+        }
+        for (int c = 0; c < n_colours; ++c) {
+            const int p0 = (cls_sh ? cls[c] : class_ptr[c]) << lg;
+            const int p1 = (cls_sh ? cls[c + 1] : class_ptr[c + 1]) << lg;
+            for (int p = p0 + tid; p < p1; p += bs) {
+                const int i = p >> lg;
+                const uint32_t oi = uint32_t(__ldg(order + i));   // issued before the state loads
+                const int si = s[p];
+                const int dE = -si * f[p];
+                bool acc = dE <= 0;
+                if (!acc) {
+                    const unsigned long long t = table ? thr[dE] : accept_threshold(dE, T);
+                    if (t >= (1ull << 53)) acc = true;
+                    else if (t != 0ull) acc = draw_u53(seed, oi, uint32_t(sweep), 0u) < t;
+                }
+                if (acc) {
+                    s[p] = int8_t(-si);
+                    E += dE;
+                    // f_j -= 2 w_ij s_i in wrap-around uint32 arithmetic (the final
+                    // field fits int32, a partial term may not)
+                    const uint32_t ms = si > 0 ? 0xFFFFFFFEu : 2u;
+                    // the CSR pointers are read from the shared descriptor here, at
+                    // the (rarer) accepted flip, to keep them out of the registers
+                    const int32_t* __restrict__ row = it.row;
+                    const int32_t* __restrict__ adj = it.adj;
+                    const WT* __restrict__ w = static_cast<const WT*>(it.w);
+                    int k = __ldg(row + i);
+                    const int k1 = __ldg(row + i + 1);
+                    // four neighbours per step: their loads issue before the atomics
+                    for (; k + 4 <= k1; k += 4) {
+                        int j[4];
+                        uint32_t d[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            j[q] = __ldg(adj + k + q);
+                            d[q] = uint32_t(int32_t(__ldg(w + k + q))) * ms;
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            atomicAdd(reinterpret_cast<unsigned int*>(&f[(j[q] << lg) + r]), d[q]);
+                    }
+                    for (; k < k1; ++k)
+                        atomicAdd(reinterpret_cast<unsigned int*>(&f[(__ldg(adj + k) << lg) + r]),
+                                  uint32_t(int32_t(__ldg(w + k))) * ms);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    atomicAdd(&e_sh[r], (unsigned long long)E);
+    __syncthreads();
+    if (tid < G) {
+        const long long prev = init ? 0ll : it.e_acc[tid];
+        it.e_acc[tid] = prev + (long long)e_sh[tid];
+    }
+    if (flags & kItemFinal) {
+        for (int p = tid; p < NG; p += bs) {
+            const int i = p >> lg;
+            const size_t o = size_t(p & (G - 1)) * size_t(n) + size_t(order[i]);
+            it.x_out[o] = s[p] > 0 ? 1u : 0u;
+            it.f_out[o] = f[p];
+        }
+    }
+    if (!GLOBAL && (flags & kItemKeep)) {
+        for (int p = tid; p < NG; p += bs) {
+            it.f_state[p] = f[p];
+            it.s_state[p] = s[p];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreadsMax) ising_batch_kernel(const IsingItem* __restrict__ items, int n_items,
+                                                                      int* counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ unsigned long long thr[kThrMax + 1];
+    __shared__ unsigned long long e_sh[kBatchMaxGroup];
+    __shared__ __align__(16) IsingItem it;
+    __shared__ int next;
+    __shared__ int cls[kClassMax + 1];
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int k = next;
+        if (k >= n_items) return;
+        constexpr int kWords = int(sizeof(IsingItem) / 8);
+        if (threadIdx.x < kWords)
+            reinterpret_cast<uint64_t*>(&it)[threadIdx.x] = reinterpret_cast<const uint64_t*>(items + k)[threadIdx.x];
+        __syncthreads();
+        const bool global = (it.flags & kItemGlobal) != 0;
+        if (it.wbytes == 1) {
+            if (global) ising_item<int8_t, true>(it, smem, thr, e_sh, cls);
+            else ising_item<int8_t, false>(it, smem, thr, e_sh, cls);
+        } else {
+            if (global) ising_item<int32_t, true>(it, smem, thr, e_sh, cls);
+            else ising_item<int32_t, false>(it, smem, thr, e_sh, cls);
+        }
+        __syncthreads();
+    }
+}
+
+// Per-bit fraction of branches with x = 1 for every instance of a batch: the
+// float division of branch_fractions (ising_recon.hpp:160-163) on exact counts.
+__global__ void batch_marginals_kernel(const uint8_t* __restrict__ x, const BatchInstDev* __restrict__ inst, int n_inst,
+                                       int64_t total, float* __restrict__ p) {
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x) {
+        int lo = 0, hi = n_inst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (inst[mid].p_off <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchInstDev d = inst[lo];
+        const int64_t i = g - d.p_off;
+        int cnt = 0;
+        for (int r = 0; r < d.R; ++r) cnt += x[d.x_off + int64_t(r) * d.n + i];
+        p[g] = float(cnt) / float(d.R);
+    }
+}
+
+}  // namespace
+
+qb_status launch_batch_marginals(const uint8_t* x, const BatchInstDev* inst, int n_inst, int64_t total, float* p,
+                                 cudaStream_t st) {
+    if (total <= 0) return QB_OK;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    batch_marginals_kernel<<<dim3(unsigned(blocks)), 256, 0, st>>>(x, inst, n_inst, total, p);
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+}
+
+int batch_max_smem() {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, ising_batch_kernel) != cudaSuccess) return 0;
+    return optin - int(fa.sharedSizeBytes);
+}
+
+qb_status batch_ctas(const BatchShape& sh, int* ctas) {
+    int dev = 0, sms = 0, occ = 0;
+    QB_CUDA(cudaGetDevice(&dev));
+    QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (sh.threads < 32 || sh.threads > kBatchThreadsMax || sh.threads % kBatchMaxGroup)
+        return fail(QB_EINVAL, "batch: threads must be a multiple of 32 in [32, 1024]");
+    QB_CUDA(cudaFuncSetAttribute(ising_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes));
+    QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ising_batch_kernel, sh.threads, size_t(sh.smem_bytes)));
+    if (occ < 1) return fail(QB_EREFUSED, "batch: the launch shape does not fit an SM");
+    *ctas = occ * sms;
+    return QB_OK;
+}
+
+qb_status launch_ising_batch(const IsingItem* d_items, int n_items, int* d_counter, const BatchShape& sh,
+                             cudaStream_t st) {
+    int ctas = sh.ctas;
+    if (ctas <= 0) {
+        qb_status s = batch_ctas(sh, &ctas);
+        if (s != QB_OK) return s;
+    } else {
+        QB_CUDA(cudaFuncSetAttribute(ising_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes));
+    }
+    if (n_items <= 0) return QB_OK;
+    if (ctas > n_items) ctas = n_items;
+    QB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+    ising_batch_kernel<<<dim3(unsigned(ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, n_items,
+                                                                                                      d_counter);
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+}
+
+}  // namespace qb

@@ -120,6 +120,26 @@ def random_regular(n: int, d: int, seed: int):
     return n, pairs[:, 0].astype(np.int32), pairs[:, 1].astype(np.int32), w
 
 
+def mixed_batch(count: int, seed: int = 2026, n_min: int = 200, n_max: int = 20000):
+    """The batching workload: `count` ising instances with N log-uniform in
+    [n_min, n_max], alternately 2D +-1 tori (L = round(sqrt(N)), so N = L^2)
+    and random d-regular graphs with d uniform in 3..50 (at most N - 1) and
+    +-1 weights. Returns a list of (kind, (n, eu, ev, ew))."""
+    s = SplitMix(seed)
+    lo, hi = np.log(n_min), np.log(n_max)
+    out = []
+    for k in range(count):
+        n = int(round(float(np.exp(lo + s.uniform() * (hi - lo)))))
+        sub = (int(seed) * 1000003 + k) & 0xFFFFFFFF
+        if k % 2 == 0:
+            L = max(3, int(round(np.sqrt(n))))
+            out.append(("torus", torus_pm1(L, sub)))
+        else:
+            d = min(3 + int(s.uniform() * 48), n - 1)
+            out.append(("regular", random_regular(n, d, sub)))
+    return out
+
+
 # ---- residual-form instances --------------------------------------------------------------------
 
 def exhaustive16():

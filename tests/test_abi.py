@@ -220,3 +220,25 @@ def test_two_ranks_give_single_process_fractions(tmp_path):
     assert (got == want).all()
     from oracle import oracle as O
     assert (got == O.fractions(X)).all()
+
+
+def test_batch_refuses_an_empty_item_list_before_any_device_call():
+    out = C.c_void_p()
+    st = lib().qb_solve_batch(None, 0, None, None, C.byref(out))
+    assert st == 1 and "at least one item" in lib().qb_last_error().decode()
+
+
+def test_mixed_batch_generator_shapes():
+    b = synth.mixed_batch(24, seed=5, n_min=200, n_max=20000)
+    kinds = [k for k, _ in b]
+    assert kinds[0::2] == ["torus"] * 12 and kinds[1::2] == ["regular"] * 12
+    for kind, (n, eu, ev, ew) in b:
+        assert 150 <= n <= 21000
+        assert set(np.unique(ew).tolist()) <= {-1, 1}
+        deg = np.bincount(np.concatenate([eu, ev]), minlength=n)
+        if kind == "torus":
+            assert (deg == 4).all()
+        else:
+            assert deg.max() <= 50
+        pairs = np.stack([np.minimum(eu, ev), np.maximum(eu, ev)], 1)
+        assert np.unique(pairs, axis=0).shape[0] == eu.size and (eu != ev).all()
