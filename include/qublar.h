@@ -114,12 +114,24 @@ typedef struct qb_schedule {
 } qb_schedule;
 
 /* Per-call options. stream: a cudaStream_t (NULL = the legacy default
- * stream); device: CUDA ordinal (-1 = current). */
+ * stream); device: CUDA ordinal (-1 = current); flags: QB_OPT_* below. */
 typedef struct qb_opts {
     void* stream;
     int32_t device;
     uint32_t flags;
 } qb_opts;
+
+/* qb_opts.flags of qb_problem_create_*:
+ *   QB_OPT_DEFER_UPLOAD  plan on the host now, copy the inputs, and take
+ *                        device memory only when the problem is first solved
+ *                        or admitted by a server (qb_problem_info.device_bytes
+ *                        reports what it will take);
+ *   QB_OPT_RESID_CLUSTER plan a residual problem for the cluster sweep (one
+ *                        thread-block cluster per branch, which runs beside
+ *                        other kernels) instead of the whole-device lockstep
+ *                        sweep. */
+#define QB_OPT_DEFER_UPLOAD 1u
+#define QB_OPT_RESID_CLUSTER 2u
 
 /* Upload an integer graph and plan it (colouring, field width).
  * Replaces gising::make_plan + DeviceGraph (src/ising_gpu.cuh:74-101, :278-336). */
@@ -297,6 +309,101 @@ qb_status qb_batch_fields_i64(qb_batch* b, int32_t item, int64_t* f);
 /* Instance `item`'s per-bit fraction of branches with x = 1. */
 qb_status qb_batch_marginals(qb_batch* b, int32_t item, float* p);
 void qb_batch_destroy(qb_batch* b);
+
+/* ---- serving: a persistent request loop with continuous batching ----------
+ *
+ * The reference has no server: each solve is a blocking call on stream 0
+ * (gising::run_batch, src/ising_gpu.cuh:396-458; branch_fractions,
+ * src/ising_recon.hpp:148-166). A qb_server owns one device and a worker
+ * thread. Requests (a problem, a schedule, branches, a seed offset) are
+ * admitted in arrival order while the device-memory budget and the active
+ * limit allow; a problem created with QB_OPT_DEFER_UPLOAD goes to the device
+ * only then, and leaves it when its request finishes.
+ *   - ising requests advance together in ticks: one launch of the packed
+ *     kernel (replayed from a CUDA graph) moves every admitted request forward
+ *     by a slice of its sweeps, its spins and fields staying on the device in
+ *     between; a request admitted while a tick runs joins the next tick;
+ *   - residual requests (planned with QB_OPT_RESID_CLUSTER) run as one
+ *     cluster launch each on a pool of streams, beside the ticks.
+ * A request's branches equal those of qb_solve on its own with the same
+ * schedule and seeds, whatever else the server runs. All calls are
+ * thread-safe. */
+typedef struct qb_server qb_server;
+
+typedef struct qb_server_config {
+    int32_t device;              /* CUDA ordinal (-1 = current) */
+    int64_t hbm_budget_bytes;    /* admission budget: problems + working memory + unreleased results (0 = 150 GB,
+                                    capped at 90% of the free memory at creation) */
+    int32_t max_active;          /* requests on the device at once (0 = 4096) */
+    int32_t residual_streams;    /* streams for residual requests (0 = 8) */
+    int32_t tick_target_us;      /* ising slices are sized so a tick item takes about this long (0 = 20000) */
+    int32_t use_graph;           /* 0: launch ticks directly; otherwise replay a captured CUDA graph */
+    qb_batch_config batch;       /* packed-kernel shape (zeros = defaults) */
+} qb_server_config;
+
+/* Request states reported by qb_server_poll. */
+#define QB_REQ_PENDING 0
+#define QB_REQ_RUNNING 1
+#define QB_REQ_DONE 2
+#define QB_REQ_FAILED 3
+#define QB_REQ_CANCELLED 4
+
+typedef struct qb_request_info {
+    int32_t state;               /* QB_REQ_* */
+    int32_t status;              /* qb_status of a failed request */
+    int32_t kind;                /* QB_KIND_* */
+    int32_t n;
+    int32_t n_branches;
+    int32_t sweeps;
+    int64_t attempts;            /* n_branches x sweeps x n */
+    int64_t device_bytes;        /* budget charged at admission */
+    double t_submit;             /* host steady-clock seconds */
+    double t_admit;
+    double t_done;
+} qb_request_info;
+
+typedef struct qb_server_stats {
+    int64_t submitted;
+    int64_t completed;
+    int64_t failed;
+    int64_t cancelled;
+    int64_t pending;
+    int64_t active;
+    int64_t ticks;
+    int64_t bytes_in_use;
+    int64_t peak_bytes;
+    int64_t budget_bytes;
+    int64_t attempts_done;
+} qb_server_stats;
+
+qb_status qb_server_create(const qb_server_config* cfg, qb_server** out);
+/* Queues a request and returns its id at once. The problem must stay alive
+ * until the request is finished or cancelled; one problem serves one request
+ * at a time. */
+qb_status qb_server_submit(qb_server* s, qb_problem* problem, const qb_schedule* sched, uint32_t n_branches,
+                           uint64_t seed_offset, uint64_t* id);
+/* Current state (QB_REQ_*) of a request. */
+qb_status qb_server_poll(qb_server* s, uint64_t id, int32_t* state);
+/* Waits until the request is finished (QB_OK), failed (its status), cancelled
+ * (QB_ECANCELLED) or timeout_ms passes (QB_ETIMEDOUT; timeout_ms < 0 waits
+ * without limit). */
+qb_status qb_server_wait(qb_server* s, uint64_t id, int32_t timeout_ms);
+/* Cancels a request that has not finished: a pending one leaves the queue, a
+ * running ising request leaves at the next tick, a running residual request
+ * finishes its launch and is then dropped. */
+qb_status qb_server_cancel(qb_server* s, uint64_t id);
+qb_status qb_server_request_info(qb_server* s, uint64_t id, qb_request_info* info);
+/* Results of a finished request (layouts as the qb_result getters). */
+qb_status qb_server_result_branches(qb_server* s, uint64_t id, uint8_t* x);
+qb_status qb_server_result_marginals(qb_server* s, uint64_t id, float* p);
+/* Ising: tracked energies (int64); residual: fp64 energies from scratch. */
+qb_status qb_server_result_energies_i64(qb_server* s, uint64_t id, int64_t* e);
+qb_status qb_server_result_energies_f64(qb_server* s, uint64_t id, double* e);
+/* Frees a finished request's results and returns their memory to the budget. */
+qb_status qb_server_release(qb_server* s, uint64_t id);
+qb_status qb_server_stats_get(qb_server* s, qb_server_stats* st);
+/* Cancels what is pending, waits for what runs, stops the worker. */
+void qb_server_destroy(qb_server* s);
 
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */

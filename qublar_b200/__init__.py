@@ -22,12 +22,14 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import (KIND_ISING, KIND_RESIDUAL, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts, ProblemInfo,
-                   QBError, ResidualDesc, ResultInfo, ScheduleC, check, lib, ptr)
+from ._abi import (KIND_ISING, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
+                   REQ_FAILED, REQ_PENDING, REQ_RUNNING, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts,
+                   ProblemInfo, QBError, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig, ServerStats,
+                   check, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
-           "Batch", "solve_batch", "autotune_batch"]
+           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER"]
 
 
 @dataclass
@@ -65,11 +67,11 @@ def device_count() -> int:
     return int(lib().qb_device_count())
 
 
-def _opts(device: int = -1, stream=None) -> Opts:
+def _opts(device: int = -1, stream=None, flags: int = 0) -> Opts:
     s = None
     if stream is not None:
         s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", stream))
-    return Opts(s, int(device), 0)
+    return Opts(s, int(device), int(flags))
 
 
 def _c32(a):
@@ -178,14 +180,14 @@ class IsingProblem(_Problem):
     """An integer Max-Cut / Ising instance on the device (WeightedGraph + DeviceGraph)."""
     kind = KIND_ISING
 
-    def __init__(self, n: int, eu, ev, ew, device: int = -1, stream=None):
+    def __init__(self, n: int, eu, ev, ew, device: int = -1, stream=None, flags: int = 0):
         super().__init__()
         self.n = int(n)
         self.eu, self.ev, self.ew = _c32(eu), _c32(ev), _c32(ew)
         self.m = int(self.eu.size)
         d = self.desc()
         h = C.c_void_p()
-        o = _opts(device, stream)
+        o = _opts(device, stream, flags)
         check(lib().qb_problem_create_ising(C.byref(d), C.byref(o), C.byref(h)))
         self._h = h
 
@@ -209,7 +211,7 @@ class ResidualProblem(_Problem):
     kind = KIND_RESIDUAL
 
     def __init__(self, d, w, row_ptr, ray, a, nbr_ptr, nbr, lam: float, kappa: float, field=None,
-                 device: int = -1, stream=None):
+                 device: int = -1, stream=None, flags: int = 0):
         super().__init__()
         self.d = np.ascontiguousarray(d, dtype=np.float64)
         self.w = np.ascontiguousarray(w, dtype=np.float64)
@@ -222,7 +224,7 @@ class ResidualProblem(_Problem):
         self.n_rays = int(self.d.size)
         d_ = self.desc()
         h = C.c_void_p()
-        o = _opts(device, stream)
+        o = _opts(device, stream, flags)
         check(lib().qb_problem_create_residual(C.byref(d_), C.byref(o), C.byref(h)))
         self._h = h
 
@@ -322,6 +324,92 @@ def solve_batch(items, config: BatchConfig | None = None, stream=None) -> Batch:
     cfg = C.byref(config) if config is not None else None
     check(lib().qb_solve_batch(arr, len(items), cfg, C.byref(o), C.byref(out)))
     return Batch(out.value, items)
+
+
+# ---- serving --------------------------------------------------------------------------------
+
+class Server:
+    """qb_server: a persistent request loop on one device (continuous batching).
+
+    Problems should be created with ``flags=OPT_DEFER_UPLOAD`` (device memory
+    taken at admission) and residual ones also with ``OPT_RESID_CLUSTER``."""
+
+    def __init__(self, budget_bytes: int = 0, max_active: int = 0, residual_streams: int = 0,
+                 tick_target_us: int = 0, use_graph: bool = True, batch: BatchConfig | None = None,
+                 device: int = -1):
+        cfg = ServerConfig(int(device), int(budget_bytes), int(max_active), int(residual_streams),
+                           int(tick_target_us), 1 if use_graph else 0, batch or BatchConfig())
+        h = C.c_void_p()
+        check(lib().qb_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._shape = {}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().qb_server_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, problem, schedule: Schedule, n_branches: int, seed_offset: int = 0) -> int:
+        rid = C.c_uint64()
+        s = schedule.to_c()
+        check(lib().qb_server_submit(self._h, problem._h, C.byref(s), int(n_branches), int(seed_offset),
+                                     C.byref(rid)))
+        self._shape[rid.value] = (int(n_branches), problem.n, problem.kind)
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        st = C.c_int32()
+        check(lib().qb_server_poll(self._h, int(rid), C.byref(st)))
+        return st.value
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> None:
+        check(lib().qb_server_wait(self._h, int(rid), int(timeout_ms)))
+
+    def cancel(self, rid: int) -> None:
+        check(lib().qb_server_cancel(self._h, int(rid)))
+
+    def info(self, rid: int) -> RequestInfo:
+        i = RequestInfo()
+        check(lib().qb_server_request_info(self._h, int(rid), C.byref(i)))
+        return i
+
+    def branches(self, rid: int) -> np.ndarray:
+        R, n, _ = self._shape[rid]
+        x = np.empty((R, n), dtype=np.uint8)
+        check(lib().qb_server_result_branches(self._h, int(rid), ptr(x)))
+        return x
+
+    def marginals(self, rid: int) -> np.ndarray:
+        _, n, _ = self._shape[rid]
+        p = np.empty(n, dtype=np.float32)
+        check(lib().qb_server_result_marginals(self._h, int(rid), ptr(p)))
+        return p
+
+    def energies(self, rid: int) -> np.ndarray:
+        """Tracked int64 energies (ising) or fp64 energies from scratch (residual)."""
+        R, _, kind = self._shape[rid]
+        if kind == KIND_ISING:
+            e = np.empty(R, dtype=np.int64)
+            check(lib().qb_server_result_energies_i64(self._h, int(rid), ptr(e)))
+        else:
+            e = np.empty(R, dtype=np.float64)
+            check(lib().qb_server_result_energies_f64(self._h, int(rid), ptr(e)))
+        return e
+
+    def release(self, rid: int) -> None:
+        check(lib().qb_server_release(self._h, int(rid)))
+        self._shape.pop(rid, None)
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().qb_server_stats_get(self._h, C.byref(st)))
+        return st
 
 
 # ---- the reference's call shapes ------------------------------------------------------------

@@ -18,6 +18,9 @@ STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4:
 KIND_ISING = 1
 KIND_RESIDUAL = 2
 NOALLOC_SCRATCH_BYTES = 8 << 20
+OPT_DEFER_UPLOAD = 1
+OPT_RESID_CLUSTER = 2
+REQ_PENDING, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 RESID_LOCKSTEP = 1
 RESID_CLUSTER = 2
 
@@ -88,6 +91,24 @@ class BatchInfo(C.Structure):
                 ("launches", C.c_int32), ("attempts", C.c_int64), ("anneal_ms", C.c_float), ("total_ms", C.c_float)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int32),
+                ("residual_streams", C.c_int32), ("tick_target_us", C.c_int32), ("use_graph", C.c_int32),
+                ("batch", BatchConfig)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("kind", C.c_int32), ("n", C.c_int32),
+                ("n_branches", C.c_int32), ("sweeps", C.c_int32), ("attempts", C.c_int64),
+                ("device_bytes", C.c_int64), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "completed", "failed", "cancelled", "pending", "active", "ticks",
+                                          "bytes_in_use", "peak_bytes", "budget_bytes", "attempts_done")]
+
+
 _P = C.c_void_p
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -123,6 +144,19 @@ SIGNATURES = {
     "qb_batch_fields_i64": (C.c_int, [_P, C.c_int32, _P]),
     "qb_batch_marginals": (C.c_int, [_P, C.c_int32, _P]),
     "qb_batch_destroy": (None, [_P]),
+    "qb_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),
+    "qb_server_submit": (C.c_int, [_P, _P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "qb_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int32)]),
+    "qb_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int32]),
+    "qb_server_cancel": (C.c_int, [_P, C.c_uint64]),
+    "qb_server_request_info": (C.c_int, [_P, C.c_uint64, C.POINTER(RequestInfo)]),
+    "qb_server_result_branches": (C.c_int, [_P, C.c_uint64, _P]),
+    "qb_server_result_marginals": (C.c_int, [_P, C.c_uint64, _P]),
+    "qb_server_result_energies_i64": (C.c_int, [_P, C.c_uint64, _P]),
+    "qb_server_result_energies_f64": (C.c_int, [_P, C.c_uint64, _P]),
+    "qb_server_release": (C.c_int, [_P, C.c_uint64]),
+    "qb_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "qb_server_destroy": (None, [_P]),
     "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),

@@ -36,6 +36,8 @@ qb_status alloc_async(DevBuf& b, size_t bytes, cudaStream_t st) {
     if (bytes == 0) return QB_OK;
     QB_CUDA(cudaMallocAsync(&b.p, bytes, st));
     b.bytes = bytes;
+    b.pooled = true;
+    b.pool_stream = st;
     return QB_OK;
 }
 
@@ -43,6 +45,7 @@ void free_async(DevBuf& b, cudaStream_t st) {
     if (b.p) cudaFreeAsync(b.p, st);
     b.p = nullptr;
     b.bytes = 0;
+    b.pooled = false;
 }
 
 }  // namespace
@@ -148,6 +151,12 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
     return QB_OK;
 }
 
+// Device bytes upload_ising will take.
+int64_t ising_device_bytes(const IsingPlan& P) {
+    return int64_t(P.row.size() + P.adj.size() + P.f0.size() + P.col.order.size() + P.col.class_ptr.size()) * 4 +
+           int64_t(P.wgt.size()) * P.weight_bytes + P.m * 12;
+}
+
 qb_status upload_ising(IsingPlan& P, const qb_ising_desc* g, cudaStream_t st, int64_t* bytes) {
     qb_status s;
     if ((s = upload_vec(P.d_row, P.row, st))) return s;
@@ -235,15 +244,16 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     // cluster size: the smallest whose shared memory holds one branch
     // (QB_RESID_CLUSTER overrides)
     int CL = env_int("QB_RESID_CLUSTER", 0);
-    const int candidates[2] = {8, 16};
-    for (int t = 0; t < 2 && CL == 0; ++t) {
+    const int candidates[5] = {1, 2, 4, 8, 16};
+    for (int t = 0; t < 5 && CL == 0; ++t) {
         const int c = candidates[t];
         const size_t bytes = size_t((nr + c - 1) / c) * 4 + size_t(n / c + nc + 64) / 8 + resid_stage_bytes();
         if (bytes <= size_t(112) * 1024) CL = c;
     }
     if (P.variant == QB_RESID_CLUSTER) {
         if (CL == 0) return fail(QB_ENOTSUP, "residual: the problem exceeds one cluster's shared memory");
-        if (CL != 4 && CL != 8 && CL != 16) return fail(QB_EINVAL, "residual: cluster size must be 4, 8 or 16");
+        if (CL != 1 && CL != 2 && CL != 4 && CL != 8 && CL != 16)
+            return fail(QB_EINVAL, "residual: cluster size must be 1, 2, 4, 8 or 16");
     }
     if (CL == 0) CL = 16;
     P.CL = CL;
@@ -382,6 +392,17 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     return QB_OK;
 }
 
+// Device bytes upload_residual will take.
+int64_t residual_device_bytes(const ResidualPlan& P) {
+    const int64_t n = P.n, nr = P.n_rays, nnz = P.nnz;
+    int64_t b = int64_t(P.h_ent.size() + P.h_row.size() + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
+                        P.h_nbr_home.size() + P.col.order.size() + P.col.class_ptr.size() + P.chunks.size() +
+                        P.chunk_ptr.size()) * 4;
+    b += 2 * ((nr + 1) * 4 + nnz * 8) + n * 8 + nr * 16 + (n + 1) * 4 + P.n_nbr * 4;
+    if (P.variant == QB_RESID_LOCKSTEP) b += int64_t(P.h_meta.size() + P.h_nbr_new.size()) * 4 + nnz * 4;
+    return b;
+}
+
 qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
@@ -464,16 +485,62 @@ qb_status download(qb_result* r, void* dst, const DevBuf& src, size_t bytes) {
 
 // ---- problems ------------------------------------------------------------------------------
 
+qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
+    if (p->uploaded) return QB_OK;
+    if (p->kind == QB_KIND_ISING ? p->host.eu.empty() && p->ising.m > 0 : p->host.row_ptr.empty())
+        return fail(QB_EINVAL, "problem: its device memory was released and its inputs are gone");
+    QB_CUDA(cudaSetDevice(p->device));
+    HostDesc& h = p->host;
+    qb_status s;
+    if (p->kind == QB_KIND_ISING) {
+        const qb_ising_desc d{p->ising.n, p->ising.m, h.eu.data(), h.ev.data(), h.ew.data()};
+        s = upload_ising(p->ising, &d, st, &p->device_bytes);
+    } else {
+        const qb_residual_desc d{p->resid.n, p->resid.n_rays, h.d.data(), h.w.data(), h.row_ptr.data(), h.ray.data(),
+                                 h.a.data(), h.nbr_ptr.data(), h.nbr.data(), h.lambda, h.kappa,
+                                 h.has_field ? h.field.data() : nullptr};
+        s = upload_residual(p->resid, &d, st, &p->device_bytes);
+    }
+    if (s != QB_OK) return s;
+    p->uploaded = true;
+    p->host = HostDesc();   // the device holds the problem now
+    return QB_OK;
+}
+
+void qb::problem_release_device(qb_problem* p) {
+    IsingPlan& I = p->ising;
+    DevBuf* ib[] = {&I.d_row, &I.d_adj, &I.d_w, &I.d_f0, &I.d_order, &I.d_class_ptr, &I.d_eu, &I.d_ev, &I.d_ew};
+    for (DevBuf* b : ib) b->release();
+    ResidualPlan& R = p->resid;
+    DevBuf* rb[] = {&R.d_row, &R.d_ent, &R.d_lin, &R.d_q, &R.d_nbr_ptr, &R.d_nbr_home, &R.d_order, &R.d_class_ptr,
+                    &R.d_chunks, &R.d_chunk_ptr, &R.d_d, &R.d_w64, &R.d_rrow, &R.d_rbit, &R.d_ra, &R.d_meta,
+                    &R.d_nbr_new, &R.d_rbit_new, &R.d_o_row, &R.d_o_ray, &R.d_o_a, &R.d_o_nbr_ptr, &R.d_o_nbr,
+                    &R.d_o_lin, &R.d_o_rrow, &R.d_o_rbit, &R.d_o_ra};
+    for (DevBuf* b : rb) b->release();
+    p->d_temp.release();
+    p->uploaded = false;
+}
+
 extern "C" qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb_opts* opts, qb_problem** out) {
     if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_ising: null argument");
     *out = nullptr;
     qb_problem* p = new (std::nothrow) qb_problem();
     if (!p) return fail(QB_ENOMEM, "qb_problem_create_ising: out of host memory");
     p->kind = QB_KIND_ISING;
+    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
     qb_status s = plan_ising(desc, p->ising);
     if (s == QB_OK && p->ising.w_min == 0) s = fail(QB_EREFUSED, "ising: all weights are zero");   // ising_gpu.cuh:94
     if (s == QB_OK) s = select_device(opts, &p->device);
-    if (s == QB_OK) s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
+    if (s == QB_OK && defer) {
+        const size_t m = size_t(desc->m);
+        p->host.eu.assign(desc->eu, desc->eu + m);
+        p->host.ev.assign(desc->ev, desc->ev + m);
+        p->host.ew.assign(desc->ew, desc->ew + m);
+        p->device_bytes = ising_device_bytes(p->ising);
+    } else if (s == QB_OK) {
+        s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
+        p->uploaded = s == QB_OK;
+    }
     if (s != QB_OK) {
         delete p;
         return s;
@@ -490,10 +557,31 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
     qb_problem* p = new (std::nothrow) qb_problem();
     if (!p) return fail(QB_ENOMEM, "qb_problem_create_residual: out of host memory");
     p->kind = QB_KIND_RESIDUAL;
+    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
+    const bool cluster = opts && (opts->flags & QB_OPT_RESID_CLUSTER);
     s = select_device(opts, &p->device);
-    if (s == QB_OK) s = plan_residual(desc, p->resid, resid_lockstep_grid());
+    if (s == QB_OK) s = plan_residual(desc, p->resid, cluster ? 0 : resid_lockstep_grid());
     if (s == QB_OK && p->resid.variant == QB_RESID_CLUSTER) s = resid_check_fit(p->resid);
-    if (s == QB_OK) s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
+    if (s == QB_OK && defer) {
+        HostDesc& h = p->host;
+        const int n = desc->n_vars, nr = desc->n_rays;
+        const size_t nnz = size_t(desc->row_ptr[n]), nn = size_t(desc->nbr_ptr[n]);
+        h.d.assign(desc->d, desc->d + nr);
+        h.w.assign(desc->w, desc->w + nr);
+        h.row_ptr.assign(desc->row_ptr, desc->row_ptr + n + 1);
+        h.ray.assign(desc->ray, desc->ray + nnz);
+        h.a.assign(desc->a, desc->a + nnz);
+        h.nbr_ptr.assign(desc->nbr_ptr, desc->nbr_ptr + n + 1);
+        h.nbr.assign(desc->nbr, desc->nbr + nn);
+        h.has_field = desc->field != nullptr;
+        if (h.has_field) h.field.assign(desc->field, desc->field + n);
+        h.lambda = desc->lambda;
+        h.kappa = desc->kappa;
+        p->device_bytes = residual_device_bytes(p->resid);
+    } else if (s == QB_OK) {
+        s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
+        p->uploaded = s == QB_OK;
+    }
     if (s != QB_OK) {
         delete p;
         return s;
@@ -593,6 +681,7 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
     if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_solve: n_branches must be in [1, 2^20]");
     QB_CUDA(cudaSetDevice(p->device));
     cudaStream_t st = stream_of(opts);
+    if ((s = problem_upload(p, st)) != QB_OK) return s;
     qb_result* r = new (std::nothrow) qb_result();
     if (!r) return fail(QB_ENOMEM, "qb_solve: out of host memory");
     r->prob = p;
@@ -769,6 +858,7 @@ extern "C" void qb_result_destroy(qb_result* r) {
 extern "C" qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e) {
     if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_ising: bad argument");
     if (p->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_energies_ising: ising problems only");
+    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_ising: the problem is not on the device");
     if (k == 0) return QB_OK;
     QB_CUDA(cudaSetDevice(p->device));
     DevBuf dx, de;
@@ -783,6 +873,7 @@ extern "C" qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, in
 extern "C" qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x, int32_t k, double* e) {
     if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_residual: bad argument");
     if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_energies_residual: residual problems only");
+    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_residual: the problem is not on the device");
     if (k == 0) return QB_OK;
     QB_CUDA(cudaSetDevice(p->device));
     DevBuf dx, de;

@@ -163,19 +163,22 @@ __device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* s
     }
 }
 
+// items are handed out by ctl[0]; their count is n_items, or ctl[1] when
+// n_items < 0 (a launch replayed from a graph reads it from device memory).
 __global__ void __launch_bounds__(kBatchThreadsMax) ising_batch_kernel(const IsingItem* __restrict__ items, int n_items,
-                                                                      int* counter) {
+                                                                      int* ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned long long thr[kThrMax + 1];
     __shared__ unsigned long long e_sh[kBatchMaxGroup];
     __shared__ __align__(16) IsingItem it;
     __shared__ int next;
     __shared__ int cls[kClassMax + 1];
+    const int total = n_items >= 0 ? n_items : ctl[1];
     for (;;) {
-        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) next = atomicAdd(ctl, 1);
         __syncthreads();
         const int k = next;
-        if (k >= n_items) return;
+        if (k >= total) return;
         constexpr int kWords = int(sizeof(IsingItem) / 8);
         if (threadIdx.x < kWords)
             reinterpret_cast<uint64_t*>(&it)[threadIdx.x] = reinterpret_cast<const uint64_t*>(items + k)[threadIdx.x];
@@ -212,6 +215,14 @@ __global__ void batch_marginals_kernel(const uint8_t* __restrict__ x, const Batc
 }
 
 }  // namespace
+
+qb_status launch_ising_batch_ctl(const IsingItem* d_items, int* d_ctl, const BatchShape& sh, cudaStream_t st) {
+    if (sh.ctas <= 0) return fail(QB_EINVAL, "batch: the launch needs its CTA count");
+    ising_batch_kernel<<<dim3(unsigned(sh.ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, -1,
+                                                                                                        d_ctl);
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+}
 
 qb_status launch_batch_marginals(const uint8_t* x, const BatchInstDev* inst, int n_inst, int64_t total, float* p,
                                  cudaStream_t st) {

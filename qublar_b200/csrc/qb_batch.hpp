@@ -64,6 +64,12 @@ qb_status batch_ctas(const BatchShape& sh, int* ctas);
 qb_status launch_ising_batch(const IsingItem* d_items, int n_items, int* d_counter, const BatchShape& sh,
                              cudaStream_t st);
 
+// The same kernel with its item count in device memory: ctl[0] must be 0 and
+// ctl[1] the item count when it starts (a launch a graph can replay).
+// sh.ctas must be set; the shared-memory attribute must have been set by
+// batch_ctas for this shape.
+qb_status launch_ising_batch_ctl(const IsingItem* d_items, int* d_ctl, const BatchShape& sh, cudaStream_t st);
+
 // Where one instance's outputs sit in the batch arenas.
 struct BatchInstDev {
     int64_t x_off;   // first byte of its R x n branches

@@ -153,6 +153,8 @@ qb_status prepare(const qb_batch_item* items, int32_t count, const qb_opts* opts
     b->total_bits = p_off;
     QB_CUDA(cudaSetDevice(b->device));
     qb_status s;
+    for (auto& I : b->inst)
+        if ((s = problem_upload(I.prob, b->stream)) != QB_OK) return s;
     if ((s = b->d_x.alloc(size_t(x_off)))) return s;
     if ((s = b->d_f.alloc(size_t(x_off) * 4))) return s;
     if ((s = b->d_e.alloc(size_t(e_off) * 8))) return s;

@@ -9,6 +9,18 @@ namespace qb {
 
 namespace {
 thread_local std::string g_last_error;
+thread_local bool g_async_on = false;
+thread_local cudaStream_t g_async_stream = nullptr;
+}
+
+AsyncAllocScope::AsyncAllocScope(cudaStream_t st) : prev(g_async_stream), prev_on(g_async_on) {
+    g_async_on = true;
+    g_async_stream = st;
+}
+
+AsyncAllocScope::~AsyncAllocScope() {
+    g_async_on = prev_on;
+    g_async_stream = prev;
 }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
@@ -29,7 +41,14 @@ qb_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 qb_status DevBuf::alloc(size_t n) {
     release();
     if (n == 0) return QB_OK;
-    cudaError_t e = cudaMalloc(&p, n);
+    cudaError_t e;
+    if (g_async_on) {
+        e = cudaMallocAsync(&p, n, g_async_stream);
+        pooled = e == cudaSuccess;
+        pool_stream = g_async_stream;
+    } else {
+        e = cudaMalloc(&p, n);
+    }
     if (e != cudaSuccess) {
         p = nullptr;
         return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);

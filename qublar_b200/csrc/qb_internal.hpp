@@ -26,15 +26,34 @@ qb_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 
 // ---- device buffer (RAII, library-owned) -------------------------------------
 
+// Allocations of a DevBuf are stream-ordered (cudaMallocAsync / cudaFreeAsync)
+// while an AsyncAllocScope is open on the allocating thread: a server thread
+// takes and returns request memory without the device-wide synchronisation of
+// cudaMalloc/cudaFree, so work on other streams keeps running.
+struct AsyncAllocScope {
+    explicit AsyncAllocScope(cudaStream_t st);
+    ~AsyncAllocScope();
+    AsyncAllocScope(const AsyncAllocScope&) = delete;
+    AsyncAllocScope& operator=(const AsyncAllocScope&) = delete;
+    cudaStream_t prev;
+    bool prev_on;
+};
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool pooled = false;              // from cudaMallocAsync: returned with cudaFreeAsync
+    cudaStream_t pool_stream = nullptr;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) cudaFreeAsync(p, pool_stream);
+            else cudaFree(p);
+        }
+        pooled = false;
         p = nullptr;
         bytes = 0;
     }
@@ -139,6 +158,17 @@ struct ResidualPlan {
     DevBuf d_o_rrow, d_o_rbit, d_o_ra;
 };
 
+// Host copies of a problem's input arrays, kept when its upload is deferred
+// (QB_OPT_DEFER_UPLOAD) so that the problem can go to the device later.
+struct HostDesc {
+    std::vector<int32_t> eu, ev, ew;                       // ising
+    std::vector<double> d, w, field;                       // residual
+    std::vector<int32_t> row_ptr, ray, nbr_ptr, nbr;
+    std::vector<float> a;
+    double lambda = 0.0, kappa = 0.0;
+    bool has_field = false;
+};
+
 }  // namespace qb
 
 struct qb_problem {
@@ -146,12 +176,21 @@ struct qb_problem {
     int device = 0;
     qb::IsingPlan ising;
     qb::ResidualPlan resid;
-    int64_t device_bytes = 0;
+    int64_t device_bytes = 0;     // device memory the problem holds (or will hold once uploaded)
+    bool uploaded = false;
+    qb::HostDesc host;            // filled while the upload is deferred
     // temperature table of the last schedule solved (reused while unchanged:
     // no pageable upload, hence no stream synchronisation, per solve)
     qb_schedule temp_sched{};
     qb::DevBuf d_temp;
 };
+
+namespace qb {
+// Upload of a problem created with QB_OPT_DEFER_UPLOAD (no-op when already on
+// the device), and the release of its device memory.
+qb_status problem_upload(qb_problem* p, cudaStream_t st);
+void problem_release_device(qb_problem* p);
+}  // namespace qb
 
 struct qb_result {
     qb_problem* prob = nullptr;

@@ -1001,10 +1001,12 @@ qb_status launch_resid_anneal(const ResidualPlan& p, const SolveBuffers& b, int 
     }
     qb_status s;
     switch (p.CL) {
+        case 1: s = resid_launch_cl<1>(A, R, smem, st, false); break;
+        case 2: s = resid_launch_cl<2>(A, R, smem, st, false); break;
         case 4: s = resid_launch_cl<4>(A, R, smem, st, false); break;
         case 8: s = resid_launch_cl<8>(A, R, smem, st, false); break;
         case 16: s = resid_launch_cl<16>(A, R, smem, st, false); break;
-        default: return fail(QB_EINVAL, "residual sweep: cluster size must be 4, 8 or 16");
+        default: return fail(QB_EINVAL, "residual sweep: cluster size must be 1, 2, 4, 8 or 16");
     }
     if (s == QB_OK && phases) {
         std::vector<unsigned long long> h(size_t(R) * size_t(p.CL) * 4);
@@ -1024,10 +1026,12 @@ qb_status resid_check_fit(const ResidualPlan& p) {
     const size_t smem = resid_smem_bytes(p);
     if (smem > size_t(227) * 1024) return fail(QB_ENOTSUP, "residual sweep: state exceeds the cluster's shared memory");
     switch (p.CL) {
+        case 1: return resid_launch_cl<1>(A, 1, smem, nullptr, true);
+        case 2: return resid_launch_cl<2>(A, 1, smem, nullptr, true);
         case 4: return resid_launch_cl<4>(A, 1, smem, nullptr, true);
         case 8: return resid_launch_cl<8>(A, 1, smem, nullptr, true);
         case 16: return resid_launch_cl<16>(A, 1, smem, nullptr, true);
-        default: return fail(QB_EINVAL, "residual sweep: cluster size must be 4, 8 or 16");
+        default: return fail(QB_EINVAL, "residual sweep: cluster size must be 1, 2, 4, 8 or 16");
     }
 }
 
@@ -1224,6 +1228,7 @@ extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_sch
     const ResidualPlan& P = p->resid;
     if (P.variant != QB_RESID_LOCKSTEP || P.lock_grid < 1)
         return fail(QB_ENOTSUP, "qb_solve_residual_noalloc: the problem is not planned for the lockstep sweep");
+    if (!p->uploaded) return fail(QB_EINVAL, "qb_solve_residual_noalloc: the problem is not on the device (deferred upload)");
     const int R = int(n_branches);
     if (n_branches < 1 || R > 16 * kLockMaxNG)
         return fail(QB_EINVAL, "qb_solve_residual_noalloc: n_branches must be in [1, 64]");

@@ -242,3 +242,13 @@ def test_mixed_batch_generator_shapes():
             assert deg.max() <= 50
         pairs = np.stack([np.minimum(eu, ev), np.maximum(eu, ev)], 1)
         assert np.unique(pairs, axis=0).shape[0] == eu.size and (eu != ev).all()
+
+
+def test_server_create_fails_cleanly_without_a_device():
+    if qb.device_count() > 0:
+        pytest.skip("a device is visible: the GPU tests cover the server")
+    h = C.c_void_p()
+    st = lib().qb_server_create(None, C.byref(h))
+    assert st != 0 and not h.value
+    rid = C.c_uint64()
+    assert lib().qb_server_submit(None, None, None, 1, 0, C.byref(rid)) == 1

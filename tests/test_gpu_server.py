@@ -1,0 +1,227 @@
+"""The serving loop (qb_server_*) on the GPU.
+
+Each result must be the same alone and in the mix: a request's branches equal
+qb_solve's for the same problem, schedule and seeds, bit for bit, whatever the
+server runs beside it (ising requests share ticks of the packed kernel,
+residual requests run as cluster launches beside them). Admission respects the
+device-memory budget, requests admitted while others run finish without
+waiting for them, cancellation and timeouts behave as declared.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, QBError, ResidualProblem, Schedule,
+                         Server, synth)
+from qublar_b200._abi import REQ_CANCELLED, REQ_DONE
+
+pytestmark = pytest.mark.gpu
+
+DEFER = OPT_DEFER_UPLOAD
+RESID = OPT_DEFER_UPLOAD | OPT_RESID_CLUSTER
+
+
+def _ising_cases():
+    gens = [g for _, g in synth.mixed_batch(6, seed=21, n_min=100, n_max=4000)]
+    gens.append(synth.random_sparse(500, 4000, 3, 1000))   # int32 weights
+    gens.append(synth.torus_pm1(150, 5))                    # 22,500 bits: global state in a 96 KiB CTA
+    out = []
+    for k, g in enumerate(gens):
+        P0 = IsingProblem(*g)
+        sched = P0.scaled_schedule(60 + 20 * (k % 3), 10)
+        out.append((g, sched, [8, 16, 32, 5][k % 4], 10 * k))
+        P0.close()
+    return out
+
+
+def _resid_cases():
+    small = synth.tomography(synth.small_tomo_params(0.12, 12))
+    mid = synth.tomography(synth.small_tomo_params(0.2, 24))
+    return [(small, Schedule(50.0, 1.0, 60, 20, 20), 8, 0), (mid, Schedule(50.0, 1.0, 40, 10, 25), 16, 3),
+            (synth.exhaustive16(), Schedule(5.0, 0.05, 100, 20, 10), 12, 7)]
+
+
+def _resid_problem(arr, flags):
+    return ResidualProblem.from_arrays(arr, flags=flags)
+
+
+def _alone(kind, data, sched, R, off):
+    P = IsingProblem(*data) if kind == "ising" else _resid_problem(data, OPT_RESID_CLUSTER)
+    r = P.solve(sched, R, off)
+    x = r.branches()
+    e = r.energies_tracked() if kind == "ising" else r.energies()
+    p = r.marginals()
+    r.close()
+    P.close()
+    return x, e, p
+
+
+@pytest.fixture(scope="module")
+def mix():
+    cases = [("ising",) + c for c in _ising_cases()] + [("resid",) + c for c in _resid_cases()]
+    S = Server()
+    probs, ids = [], []
+    for kind, data, sched, R, off in cases:
+        P = IsingProblem(*data, flags=DEFER) if kind == "ising" else _resid_problem(data, RESID)
+        probs.append(P)
+        ids.append(S.submit(P, sched, R, off))
+    for i in ids:
+        S.wait(i, 120000)
+    yield cases, S, ids
+    S.close()
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(mix):
+    cases, S, ids = mix
+    for (kind, data, sched, R, off), rid in zip(cases, ids):
+        assert S.poll(rid) == REQ_DONE
+        x, e, p = _alone(kind, data, sched, R, off)
+        assert (S.branches(rid) == x).all(), (kind, rid)
+        if kind == "ising":
+            assert (S.energies(rid) == e).all()
+        else:
+            np.testing.assert_allclose(S.energies(rid), e, rtol=1e-12)
+        assert (S.marginals(rid) == p).all()
+
+
+def test_served_residual_branch_matches_the_oracle(mix):
+    cases, S, ids = mix
+    kind, arr, sched, R, off = cases[-1]          # exhaustive16
+    P = _resid_problem(arr, OPT_RESID_CLUSTER)
+    order, _ = P.colouring()
+    temps = O.temperatures(sched.t_hot, sched.t_cold, sched.anneal_sweeps, sched.hold_sweeps)
+    X = S.branches(ids[-1])
+    for b in range(3):
+        x, _ = O.resid_anneal_coloured(arr, order, temps, sched.refresh_sweeps, b + 1 + off, mode=2)
+        assert (X[b] == x).all(), b
+
+
+def test_ising_energies_are_exact_from_scratch(mix):
+    cases, S, ids = mix
+    for (kind, data, sched, R, off), rid in zip(cases, ids):
+        if kind != "ising":
+            continue
+        g = O.Graph(*data)
+        X, E = S.branches(rid), S.energies(rid)
+        for r in range(R):
+            assert E[r] == g.energy_scratch(X[r])
+
+
+def test_budget_and_stats(mix):
+    cases, S, ids = mix
+    st = S.stats()
+    assert st.completed >= len(ids) and st.failed == 0
+    assert st.peak_bytes <= st.budget_bytes
+    assert st.ticks >= 1
+
+
+def test_admission_respects_a_small_budget():
+    """A budget that holds about two requests at a time: all finish, the peak
+    stays under the budget, and later requests are admitted only after
+    earlier ones free memory."""
+    gens = [synth.random_regular(3000, 10, s) for s in range(6)]
+    probs = [IsingProblem(*g, flags=DEFER) for g in gens]
+    need = probs[0].info().device_bytes + 3000 * 16 * 10 + 400 * 8
+    S = Server(budget_bytes=int(2.5 * need))
+    sched = Schedule(3.0, 0.05, 300, 0, 0)
+    ids = [S.submit(P, sched, 16, k) for k, P in enumerate(probs)]
+    for i in ids:
+        S.wait(i, 120000)
+    st = S.stats()
+    assert st.completed == 6 and st.peak_bytes <= st.budget_bytes
+    infos = [S.info(i) for i in ids]
+    done_first_two = min(infos[0].t_done, infos[1].t_done)
+    assert any(inf.t_admit >= done_first_two for inf in infos[2:])
+    for k, i in enumerate(ids):
+        x, e, _ = _alone("ising", gens[k], sched, 16, k)
+        assert (S.branches(i) == x).all()
+        S.release(i)
+    assert S.stats().bytes_in_use == 0
+    S.close()
+
+
+def test_request_larger_than_the_budget_fails():
+    P = IsingProblem(*synth.random_regular(2000, 8, 1), flags=DEFER)
+    S = Server(budget_bytes=4096)
+    rid = S.submit(P, Schedule(3.0, 0.05, 50, 0, 0), 8)
+    with pytest.raises(QBError) as ex:
+        S.wait(rid, 60000)
+    assert ex.value.status == 2   # QB_ENOMEM
+    S.close()
+
+
+def test_continuous_batching_a_late_small_request_finishes_first():
+    """A small ising request submitted while a long one runs joins the next
+    tick and finishes long before the long one."""
+    big = IsingProblem(*synth.torus_pm1(200, 9), flags=DEFER)
+    small = IsingProblem(*synth.random_regular(400, 6, 2), flags=DEFER)
+    S = Server(tick_target_us=2000)
+    a = S.submit(big, Schedule(3.0, 0.05, 4000, 0, 0), 32)
+    time.sleep(0.05)
+    b = S.submit(small, Schedule(3.0, 0.05, 100, 0, 0), 8)
+    S.wait(b, 60000)
+    assert S.poll(a) != REQ_DONE
+    S.wait(a, 300000)
+    ia, ib = S.info(a), S.info(b)
+    assert ib.t_done < ia.t_done and ib.t_admit < ia.t_done
+    assert S.stats().ticks > 2
+    S.close()
+
+
+def test_cancel_and_timeout():
+    P1 = IsingProblem(*synth.torus_pm1(200, 4), flags=DEFER)
+    P2 = IsingProblem(*synth.torus_pm1(60, 4), flags=DEFER)
+    S = Server(max_active=1, tick_target_us=2000)
+    a = S.submit(P1, Schedule(3.0, 0.05, 20000, 0, 0), 32)
+    b = S.submit(P2, Schedule(3.0, 0.05, 100, 0, 0), 8)   # waits behind a (max_active = 1)
+    with pytest.raises(QBError) as ex:
+        S.wait(a, 1)
+    assert ex.value.status == 4   # QB_ETIMEDOUT
+    S.cancel(a)
+    with pytest.raises(QBError) as ex:
+        S.wait(a, 120000)
+    assert ex.value.status == 7   # QB_ECANCELLED
+    assert S.poll(a) == REQ_CANCELLED
+    S.wait(b, 120000)
+    assert S.poll(b) == REQ_DONE
+    S.close()
+
+
+def test_graph_and_direct_ticks_agree():
+    g = synth.random_regular(1500, 12, 8)
+    sched = Schedule(3.0, 0.05, 200, 20, 0)
+    out = []
+    for use_graph in (True, False):
+        S = Server(use_graph=use_graph, tick_target_us=1000)
+        P = IsingProblem(*g, flags=DEFER)   # must outlive its request
+        rid = S.submit(P, sched, 16, 4)
+        S.wait(rid, 120000)
+        out.append(S.branches(rid))
+        assert S.stats().ticks > 1
+        S.close()
+    assert (out[0] == out[1]).all()
+
+
+def test_submissions_from_several_threads():
+    gens = [synth.random_regular(800 + 100 * k, 5 + k, k) for k in range(8)]
+    sched = Schedule(3.0, 0.05, 150, 0, 0)
+    S = Server()
+    ids = [None] * len(gens)
+
+    def client(k):
+        P = IsingProblem(*gens[k], flags=DEFER)
+        ids[k] = (S.submit(P, sched, 8, k), P)
+        S.wait(ids[k][0], 120000)
+
+    th = [threading.Thread(target=client, args=(k,)) for k in range(len(gens))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for k, (rid, _) in enumerate(ids):
+        x, _, _ = _alone("ising", gens[k], sched, 8, k)
+        assert (S.branches(rid) == x).all()
+    S.close()
