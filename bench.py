@@ -184,6 +184,307 @@ def run_reference(args):
     return 0
 
 
+# ---- batch: many Max-Cut instances in one persistent launch ----------------------------------
+
+BATCH_WORKLOAD = ("4096 Max-Cut instances, N log-uniform 200..20,000, alternately 2D +-1 tori and random "
+                  "d-regular graphs (d 3..50, +-1), 32 replicas each, 2000 sweeps (scaled schedule sigma -> "
+                  "0.1 w_min), one persistent launch")
+
+
+def _spawn_map(fn, items, procs=None):
+    """Builds inputs in spawned processes (before any CUDA call of this one)."""
+    import multiprocessing as mp
+    procs = procs or min(32, os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(fn, items, chunksize=max(1, len(items) // (4 * procs)))
+
+
+def _create_all(make, items, threads=16):
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(threads) as ex:   # planning runs in the library, outside the GIL
+        return list(ex.map(make, items))
+
+
+def batch_algorithmic_bytes(probs, R, sweeps, G):
+    """Bytes per launch by the Ising formula: the CSR (4 B column + weight
+    bytes per directed entry) streamed once per replica group of G per sweep,
+    every replica's state (int32 field + int8 spin) read and written once per
+    sweep. Accepted flips' field updates are not counted (a lower bound)."""
+    b = 0.0
+    for P in probs:
+        i = P.info()
+        b += sweeps * (i.nnz * (4 + i.weight_bytes) * ((R + G - 1) // G) + R * i.n * (2 * 4 + 2 * 1))
+    return b
+
+
+def run_batch(args):
+    from qublar_b200 import synth
+    specs = synth.mixed_batch_specs(args.instances)
+    t0 = time.perf_counter()
+    graphs = _spawn_map(synth.build_spec, specs)
+    log(f"[batch] built {len(graphs)} instances in {time.perf_counter() - t0:.1f} s")
+    import torch
+
+    from qublar_b200 import IsingProblem, autotune_batch, solve_batch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    R, S = 32, args.batch_sweeps
+    t0 = time.perf_counter()
+    probs = _create_all(lambda g: IsingProblem(*g), graphs)
+    log(f"[batch] planned and uploaded in {time.perf_counter() - t0:.1f} s")
+    items = [(P, P.scaled_schedule(S, 0), R, 0) for P in probs]
+    attempts = sum(R * S * P.n for P in probs)
+    cfg = autotune_batch(items, 8)
+    log(f"[batch] tuned shape: {cfg.threads} threads, {cfg.smem_bytes} B, groups of {cfg.max_group}")
+    for _ in range(args.warmup):
+        B = solve_batch(items, cfg, stream=stream)
+        B.info()
+        B.close()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.synchronize()
+    sampler.start()
+    infos = []
+    for _ in range(args.steps):
+        flush.zero_()
+        B = solve_batch(items, cfg, stream=stream)
+        infos.append(B.info())
+        B.close()
+    clocks = sampler.stop()
+    total_ms = statistics.mean(i.total_ms for i in infos)
+    anneal_ms = statistics.mean(i.anneal_ms for i in infos)
+    value = attempts / (total_ms / 1e3)
+    # plain form: one qb_solve per instance, on a size-stratified sample
+    order = sorted(range(len(probs)), key=lambda k: probs[k].n)
+    sample = [order[int(j)] for j in np.linspace(0, len(order) - 1, min(64, len(order)))]
+    p_att, p_ms = 0, 0.0
+    for k in sample:
+        P, sch, _, _ = items[k]
+        r = P.solve(sch, R, stream=stream)
+        inf = r.info()
+        p_att += inf.attempts
+        p_ms += inf.total_ms
+        r.close()
+    plain = p_att / (p_ms / 1e3)
+    # end to end: host graphs -> plan + upload -> packed solve -> every instance's fractions on the host
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    probs2 = _create_all(lambda g: IsingProblem(*g), graphs)
+    items2 = [(P, P.scaled_schedule(S, 0), R, 0) for P in probs2]
+    B = solve_batch(items2, cfg, stream=stream)
+    d2h = 0
+    for k in range(len(items2)):
+        d2h += B.marginals(k).nbytes
+    e2e_s = time.perf_counter() - t0
+    B.close()
+    h2d = sum(g[1].nbytes * 3 for g in graphs)
+    hbm, peak_kind = peaks()
+    alg = batch_algorithmic_bytes(probs, R, S, cfg.max_group)
+    achieved = alg / (anneal_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "instances": len(probs), "bits": int(sum(P.n for P in probs)),
+                   "replicas": R, "sweeps": S, "shape": {"threads": cfg.threads, "smem_bytes": cfg.smem_bytes,
+                                                         "max_group": cfg.max_group},
+                   "work_items": infos[0].work_items, "global_items": infos[0].global_items,
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": "1 GPU"},
+        "plain": {"value": plain, "unit": "attempts/s", "form": "one qb_solve per instance (CTA per replica)",
+                  "sample": f"{len(sample)} instances stratified by size"},
+        "vs_plain": value / plain,
+        "e2e": {"value": attempts / e2e_s, "unit": "attempts/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s},
+        "gpu_launches": sum(i.launches for i in infos),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": None, "kernel": "ising_batch_kernel",
+                     "kernel_ms": anneal_ms, "algorithmic_bytes": alg,
+                     "note": "CSR and state stay in L2 and shared memory; the sweep is issue-bound (Philox, "
+                             "shared-memory field updates), not DRAM-bound"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = batch_cpu_baseline(graphs, items, R, S)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch_cpu_baseline(graphs, items, R, S):
+    """The reference's wising::anneal (oracle/_ref) on the host's cores: the
+    instances nearest the mean size, all R replicas, the full schedule, until
+    about 1e9 attempts."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    mean_n = statistics.mean(g[0] for g in graphs)
+    order = sorted(range(len(graphs)), key=lambda k: abs(graphs[k][0] - mean_n))
+    att, wall, used = 0, 0.0, 0
+    for k in order:
+        n, eu, ev, ew = graphs[k]
+        sch = items[k][1]
+        if O.ref_available():
+            g = O.RefGraph(O.Graph(n, eu, ev, ew).rudy())
+            _, _, w = g.anneal_many(sch.t_hot, sch.t_cold, sch.anneal_sweeps, sch.hold_sweeps, 1, R, threads)
+            kind = "reference"
+        else:
+            g = O.Graph(n, eu, ev, ew)
+            t0 = time.perf_counter()
+            for r in range(R):
+                g.wising_anneal(sch.t_hot, sch.t_cold, sch.anneal_sweeps, sch.hold_sweeps, r + 1)
+            w = time.perf_counter() - t0
+            kind = "port"
+        att += R * S * n
+        wall += w
+        used += 1
+        if att >= 1e9:
+            break
+    return {"value": att / wall, "unit": "attempts/s", "cores": threads, "kind": kind,
+            "sample": f"{used} instances near the mean size (N ~ {mean_n:.0f}), {R} replicas, {S} sweeps, "
+                      f"{threads} threads, {wall:.1f} s"}
+
+
+# ---- serve: a Poisson request stream through the serving loop -----------------------------------
+
+SERVE_WORKLOAD = ("Poisson request stream: N log-uniform 1,000..300,000, half tomography-style pyramids, half "
+                  "sparse +-1 Max-Cut (d-regular, d 3..12), sweeps 500..5000, branches 8..32")
+
+
+def _serve_schedule(spec, P):
+    from qublar_b200 import Schedule
+    S = spec["sweeps"]
+    if spec["kind"] == "tomography":
+        hold = S // 5
+        return Schedule(50.0, 1.0, S - hold, hold, 50)
+    return P.scaled_schedule(S, 0)
+
+
+def _serve_run(probs, specs, scheds, rate, seed):
+    """Submits the stream (all at once when rate is None, else Poisson at
+    `rate` requests/s) to a fresh server; returns per-request latencies,
+    the makespan and the server's stats."""
+    from qublar_b200 import Server
+    S = Server()
+    rng = np.random.default_rng(seed)
+    gaps = np.zeros(len(probs)) if rate is None else rng.exponential(1.0 / rate, len(probs))
+    t0 = time.perf_counter()
+    due = t0
+    ids = []
+    for k, P in enumerate(probs):
+        due += gaps[k]
+        dt = due - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(S.submit(P, scheds[k], specs[k]["branches"], k))
+    for i in ids:
+        S.wait(i, -1)
+    infos = [S.info(i) for i in ids]
+    first = min(i.t_submit for i in infos)
+    last = max(i.t_done for i in infos)
+    lat = np.array([i.t_done - i.t_submit for i in infos])
+    stats = S.stats()
+    out = {"ids": ids, "server": S, "lat": lat, "makespan": last - first, "ticks": stats.ticks,
+           "peak_bytes": stats.peak_bytes}
+    return out
+
+
+def run_serve(args):
+    from qublar_b200 import synth
+    specs = synth.serve_specs(args.requests)
+    t0 = time.perf_counter()
+    data = _spawn_map(synth.build_request, specs)
+    log(f"[serve] built {len(data)} requests in {time.perf_counter() - t0:.1f} s")
+    import torch
+
+    from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, ResidualProblem)
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+
+    def make(k):
+        if specs[k]["kind"] == "tomography":
+            return ResidualProblem.from_arrays(data[k], flags=OPT_DEFER_UPLOAD | OPT_RESID_CLUSTER)
+        return IsingProblem(*data[k], flags=OPT_DEFER_UPLOAD)
+
+    t0 = time.perf_counter()
+    probs = _create_all(make, range(len(specs)))
+    log(f"[serve] planned in {time.perf_counter() - t0:.1f} s")
+    scheds = [_serve_schedule(sp, P) for sp, P in zip(specs, probs)]
+    attempts = [sp["branches"] * sch.sweeps * P.n for sp, sch, P in zip(specs, scheds, probs)]
+    total = float(sum(attempts))
+    # warm-up: a few small requests through a server
+    small = sorted(range(len(probs)), key=lambda k: attempts[k])[:max(3, args.warmup)]
+    for _ in range(1):
+        w = _serve_run([probs[k] for k in small], [specs[k] for k in small], [scheds[k] for k in small], None, 0)
+        w["server"].close()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    sat = _serve_run(probs, specs, scheds, None, 1)
+    clocks = sampler.stop()
+    value = total / sat["makespan"]
+    # check: served results equal the plain solve of the same plan (sampled)
+    mu = len(probs) / sat["makespan"]
+    S = sat["server"]
+    sample = [int(j) for j in np.linspace(0, len(probs) - 1, min(24, len(probs)))]
+    same = 0
+    e_rel = []
+    p_att, p_s = 0.0, 0.0
+    for k in sample:
+        x_served = S.branches(sat["ids"][k])
+        e_served = S.energies(sat["ids"][k])
+        # plain form: this request alone through qb_solve (lockstep sweep for the pyramids)
+        if specs[k]["kind"] == "tomography":
+            Q = ResidualProblem.from_arrays(data[k])
+        else:
+            Q = IsingProblem(*data[k])
+        r = Q.solve(scheds[k], specs[k]["branches"], k)
+        inf = r.info()
+        p_att += inf.attempts
+        p_s += inf.total_ms / 1e3
+        x_plain = r.branches()
+        e_plain = r.energies()
+        if specs[k]["kind"] != "tomography":
+            same += int((x_plain == x_served).all())
+        else:
+            same += 1 if abs(e_plain.mean() - e_served.mean()) <= 0.05 * abs(e_plain.mean()) + 1e-9 else 0
+        e_rel.append(float((e_served.mean() - e_plain.mean()) / max(1e-12, abs(e_plain.mean()))))
+        r.close()
+        Q.close()
+    plain = p_att / p_s
+    S.close()
+    lat_sat = sat["lat"]
+    rates = {}
+    for frac in (0.5, 0.8):
+        run = _serve_run(probs, specs, scheds, frac * mu, 2)
+        rates[f"{frac:.1f}x capacity"] = {"rate_per_s": frac * mu, "p50_s": float(np.percentile(run["lat"], 50)),
+                                          "p99_s": float(np.percentile(run["lat"], 99)),
+                                          "throughput": total / run["makespan"]}
+        run["server"].close()
+    hbm, peak_kind = peaks()
+    line = {
+        "metric": "spin-flip attempts/s; p50/p99 solve latency at equal energy, served vs plain", "value": value,
+        "unit": "attempts/s", "n_gpus": 1, "steps": 1, "warmup": len(small), "ms_per_step": sat["makespan"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed (int32 / f32)",
+        "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "requests": len(probs), "total_attempts": total,
+                   "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
+        "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
+                                  "p99_s": float(np.percentile(lat_sat, 99))}, **rates},
+        "plain": {"value": plain, "unit": "attempts/s",
+                  "form": "each request alone through qb_solve (lockstep sweep for pyramids, CTA per replica for "
+                          "Max-Cut)", "sample": f"{len(sample)} requests"},
+        "vs_plain": value / plain,
+        "equal_energy": {"checked": len(sample), "agree": same,
+                         "mean_rel_energy_diff": float(np.mean(e_rel)) if e_rel else None,
+                         "rule": "Max-Cut: identical branches; pyramids: mean energy within 5% (cluster vs "
+                                 "lockstep summation order)"},
+        "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "requests enter as host problems (deferred upload) and the server uploads them at "
+                        "admission inside the timed makespan"},
+        "server": {"ticks": sat["ticks"], "peak_bytes": sat["peak_bytes"]},
+        "peak_hbm_gbs": hbm, "peak_kind": peak_kind,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,7 +495,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps", type=int, default=250,
                     help="schedule length (default 250 = 200 + 50, the benchmark); shorter runs are for profiling only")
+    ap.add_argument("--workload", default="tomography", choices=["tomography", "batch", "serve"],
+                    help="tomography: the pyramid (default); batch: many Max-Cut instances in one persistent "
+                         "launch; serve: a Poisson request stream through the serving loop")
+    ap.add_argument("--instances", type=int, default=4096, help="batch: instances")
+    ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch: sweeps per instance")
+    ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
     args = ap.parse_args()
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
 

@@ -125,7 +125,9 @@ typedef struct qb_opts {
  *   QB_OPT_DEFER_UPLOAD  plan on the host now, copy the inputs, and take
  *                        device memory only when the problem is first solved
  *                        or admitted by a server (qb_problem_info.device_bytes
- *                        reports what it will take);
+ *                        reports what it will take); the host copies stay, so
+ *                        a server can release the device copy when a request
+ *                        finishes and the problem can be submitted again;
  *   QB_OPT_RESID_CLUSTER plan a residual problem for the cluster sweep (one
  *                        thread-block cluster per branch, which runs beside
  *                        other kernels) instead of the whole-device lockstep

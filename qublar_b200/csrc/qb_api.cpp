@@ -403,7 +403,8 @@ int64_t residual_device_bytes(const ResidualPlan& P) {
     return b;
 }
 
-qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes) {
+qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes,
+                          bool keep_host = false) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
     // ray-major CSR, bits ascending in input order inside a ray: the refresh
@@ -448,8 +449,9 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     int64_t tot = 0;
     for (const DevBuf* b : all) tot += int64_t(b->bytes);
     *bytes = tot;
-    // the plan's host copies are not needed after the upload
-    std::vector<uint32_t>().swap(P.h_ent);
+    // the plan's host copies are not needed after the upload (unless the
+    // problem may go to the device again)
+    if (!keep_host) std::vector<uint32_t>().swap(P.h_ent);
     return QB_OK;
 }
 
@@ -488,7 +490,7 @@ qb_status download(qb_result* r, void* dst, const DevBuf& src, size_t bytes) {
 qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
     if (p->uploaded) return QB_OK;
     if (p->kind == QB_KIND_ISING ? p->host.eu.empty() && p->ising.m > 0 : p->host.row_ptr.empty())
-        return fail(QB_EINVAL, "problem: its device memory was released and its inputs are gone");
+        return fail(QB_EINVAL, "problem: its device memory was released and it was not created with deferred upload");
     QB_CUDA(cudaSetDevice(p->device));
     HostDesc& h = p->host;
     qb_status s;
@@ -499,11 +501,10 @@ qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
         const qb_residual_desc d{p->resid.n, p->resid.n_rays, h.d.data(), h.w.data(), h.row_ptr.data(), h.ray.data(),
                                  h.a.data(), h.nbr_ptr.data(), h.nbr.data(), h.lambda, h.kappa,
                                  h.has_field ? h.field.data() : nullptr};
-        s = upload_residual(p->resid, &d, st, &p->device_bytes);
+        s = upload_residual(p->resid, &d, st, &p->device_bytes, true);
     }
     if (s != QB_OK) return s;
-    p->uploaded = true;
-    p->host = HostDesc();   // the device holds the problem now
+    p->uploaded = true;   // host copies stay: the problem can go to the device again after a release
     return QB_OK;
 }
 

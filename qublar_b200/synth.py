@@ -120,11 +120,11 @@ def random_regular(n: int, d: int, seed: int):
     return n, pairs[:, 0].astype(np.int32), pairs[:, 1].astype(np.int32), w
 
 
-def mixed_batch(count: int, seed: int = 2026, n_min: int = 200, n_max: int = 20000):
-    """The batching workload: `count` ising instances with N log-uniform in
-    [n_min, n_max], alternately 2D +-1 tori (L = round(sqrt(N)), so N = L^2)
-    and random d-regular graphs with d uniform in 3..50 (at most N - 1) and
-    +-1 weights. Returns a list of (kind, (n, eu, ev, ew))."""
+def mixed_batch_specs(count: int, seed: int = 2026, n_min: int = 200, n_max: int = 20000):
+    """The batching workload's instance list: `count` (kind, n, degree, seed)
+    with N log-uniform in [n_min, n_max], alternately 2D +-1 tori (L =
+    round(sqrt(N)), so N = L^2) and random d-regular graphs with d uniform in
+    3..50 (at most N - 1) and +-1 weights."""
     s = SplitMix(seed)
     lo, hi = np.log(n_min), np.log(n_max)
     out = []
@@ -133,11 +133,65 @@ def mixed_batch(count: int, seed: int = 2026, n_min: int = 200, n_max: int = 200
         sub = (int(seed) * 1000003 + k) & 0xFFFFFFFF
         if k % 2 == 0:
             L = max(3, int(round(np.sqrt(n))))
-            out.append(("torus", torus_pm1(L, sub)))
+            out.append(("torus", L * L, 4, sub))
         else:
-            d = min(3 + int(s.uniform() * 48), n - 1)
-            out.append(("regular", random_regular(n, d, sub)))
+            out.append(("regular", n, min(3 + int(s.uniform() * 48), n - 1), sub))
     return out
+
+
+def build_spec(spec):
+    """(n, eu, ev, ew) of one mixed_batch_specs entry."""
+    kind, n, d, sub = spec
+    if kind == "torus":
+        return torus_pm1(int(round(np.sqrt(n))), sub)
+    return random_regular(n, d, sub)
+
+
+def mixed_batch(count: int, seed: int = 2026, n_min: int = 200, n_max: int = 20000, threads: int = 1):
+    """The batching workload built: a list of (kind, (n, eu, ev, ew))."""
+    specs = mixed_batch_specs(count, seed, n_min, n_max)
+    if threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(threads) as ex:
+            graphs = list(ex.map(build_spec, specs))
+    else:
+        graphs = [build_spec(sp) for sp in specs]
+    return [(sp[0], g) for sp, g in zip(specs, graphs)]
+
+
+def serve_specs(count: int, seed: int = 77, n_min: int = 1000, n_max: int = 300000):
+    """The serving workload's request stream: `count` requests with N
+    log-uniform in [n_min, n_max], alternately tomography-style QUBOs (a
+    pyramid scaled to about N bits) and sparse +-1 Max-Cut graphs (random
+    d-regular, d uniform in 3..12), each with sweeps uniform in [500, 5000]
+    and branches uniform in [8, 32]. Returns dicts (data built by
+    build_request)."""
+    s = SplitMix(seed)
+    lo, hi = np.log(n_min), np.log(n_max)
+    out = []
+    for k in range(count):
+        n = int(round(float(np.exp(lo + s.uniform() * (hi - lo)))))
+        sweeps = 500 + int(s.uniform() * 4501)
+        branches = 8 + int(s.uniform() * 25)
+        d = 3 + int(s.uniform() * 10)
+        out.append({"kind": "tomography" if k % 2 == 0 else "maxcut", "n": n, "sweeps": sweeps,
+                    "branches": branches, "degree": d, "seed": (int(seed) * 7919 + k) & 0xFFFFFFFF})
+    return out
+
+
+def tomography_of_size(n_bits: int, seed: int = 20260929) -> dict:
+    """A pyramid of the benchmark's construction scaled to about n_bits bits
+    (the cell count grows as 312,000 x scale^3)."""
+    scale = (max(n_bits, 300) / 312000.0) ** (1.0 / 3.0)
+    bins = max(8, int(round(120 * scale)))
+    return tomography(small_tomo_params(scale, bins, seed=int(seed)))
+
+
+def build_request(spec):
+    """The QUBO of one serve_specs entry: residual arrays or (n, eu, ev, ew)."""
+    if spec["kind"] == "tomography":
+        return tomography_of_size(spec["n"], spec["seed"])
+    return random_regular(spec["n"], spec["degree"], spec["seed"])
 
 
 # ---- residual-form instances --------------------------------------------------------------------
