@@ -54,6 +54,7 @@ typedef enum qb_status {
 /* Problem kinds reported by qb_problem_info_get. */
 #define QB_KIND_ISING 1     /* integer-weighted Max-Cut / Ising, E = -cut */
 #define QB_KIND_RESIDUAL 2  /* residual-form QUBO (rays + 6-neighbour prior) */
+#define QB_KIND_QUBO 3      /* weighted QUBO with fp32 couplings and linear terms */
 
 /* Text of a status code (static storage). */
 const char* qb_status_string(qb_status s);
@@ -99,12 +100,31 @@ typedef struct qb_residual_desc {
     const double* field;    /* n_vars, or NULL */
 } qb_residual_desc;
 
+/* Weighted QUBO with real couplings, x in {0,1}:
+ *   E(x) = offset + sum_i h_i x_i + sum_e J_e x_{u_e} x_{v_e},
+ * the Model of src/check_ree_qubo.cu (offset, Qd, Qo; evaluated by
+ * qubo_energy, :158-163), which the reference anneals only through its
+ * pair-ray encoding into a BinaryProblem (to_engine, :172-192). Couplings and
+ * linear terms are fp32; edges are 0-based, u != v, no duplicates in either
+ * orientation; h may be NULL (all zero). */
+typedef struct qb_qubo_desc {
+    int32_t n;
+    int64_t m;
+    const int32_t* eu;
+    const int32_t* ev;
+    const float* ew;
+    const float* h;
+    double offset;
+} qb_qubo_desc;
+
 /* Geometric schedule: T(s) = t_hot (t_cold/t_hot)^min(1, s/max(1, A-1)) for
  * s < A, then t_cold for `hold_sweeps` more sweeps -- the expression of
  * ising_recon.hpp:129-131 and ising_weighted.hpp:255-257. Replaces
  * argos::Schedule (ising_recon.hpp:81-86) and wising::Budget (:227-232).
  * refresh_sweeps: residual instances recompute their fp32 residuals from
- * scratch in fp64 every this many sweeps (0 = at the start only). */
+ * scratch in fp64 every this many sweeps (0 = at the start only); weighted
+ * QUBO instances recompute their compensated fp32 local fields in fp64 every
+ * this many sweeps (0 = never). */
 typedef struct qb_schedule {
     double t_hot;
     double t_cold;
@@ -142,6 +162,12 @@ qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb_opts* opts
  * share a ray or a neighbour bond). Replaces passing a BinaryProblem to
  * branch_fractions (src/ising_recon.hpp:148). */
 qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts* opts, qb_problem** out);
+/* Plan a weighted QUBO for the compensated-field sweep: all replicas of a
+ * launch (up to 64) in lockstep on a cooperative grid, local fields carried
+ * as fp32 hi + lo sums, refreshed in fp64 every schedule.refresh_sweeps.
+ * Replaces annealing the pair-ray encoding of the Model through
+ * anneal_branch (src/check_ree_qubo.cu:172-192, src/ising_recon.hpp:121-144). */
+qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_opts* opts, qb_problem** out);
 void qb_problem_destroy(qb_problem* p);
 
 typedef struct qb_problem_info {
@@ -203,8 +229,10 @@ typedef struct qb_result_info {
     float anneal_ms;        /* CUDA-event time of the anneal kernels (on the solve's stream) */
     float total_ms;         /* CUDA-event time of the whole solve */
     int64_t attempts;       /* n_branches * sweeps * n */
-    double max_drift;       /* residual: max |fp32 residual - fp64 residual| seen at refreshes */
-    int64_t accepted;       /* residual: accepted flips over all branches and sweeps */
+    double max_drift;       /* residual: max |fp32 residual - fp64 residual| seen at refreshes;
+                               qubo: max |compensated fp32 field - fp64 field| seen at refreshes */
+    int64_t accepted;       /* residual, qubo: accepted flips over all branches and sweeps */
+    double max_energy_error;   /* qubo: max over branches of |offset + sum of accepted dE - fp64 energy from scratch| */
 } qb_result_info;
 /* Waits for the solve. */
 qb_status qb_result_info_get(qb_result* r, qb_result_info* info);
@@ -410,6 +438,9 @@ void qb_server_destroy(qb_server* s);
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
 qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);
+/* Device fp64 energies of k caller states for a weighted QUBO problem
+ * (qubo_energy, src/check_ree_qubo.cu:158-163). */
+qb_status qb_energies_qubo(const qb_problem* p, const uint8_t* x, int32_t k, double* e);
 /* Device fp64 energies of k caller states for a residual problem
  * (binary_energy, src/ising_recon.hpp:65-79). */
 qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x, int32_t k, double* e);

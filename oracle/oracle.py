@@ -63,6 +63,9 @@ def orc() -> C.CDLL:
             "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, C.c_int, P, P, P]),
             "orc_classify": (None, [P, I64, C.c_float, C.c_float, P]),
             "orc_fractions": (None, [P, C.c_int, I64, P]),
+            "orc_qubo_energy": (D, [C.c_int, I64, P, P, P, P, D, P]),
+            "orc_qubo_anneal_coloured": (D, [C.c_int, I64, P, P, P, P, P, P, C.c_int, P, C.c_int, C.c_int, U64, P,
+                                             P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -223,6 +226,35 @@ def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False, m
     orc().orc_resid_anneal_coloured(C.byref(d), _p(order), _p(temps), int(temps.size), int(refresh), seed, int(mode),
                                     _p(x), C.byref(drift), _p(tr))
     return (x, float(drift.value), tr) if trace else (x, float(drift.value))
+
+
+def qubo_energy(q: dict, x) -> float:
+    """qubo_energy (check_ree_qubo.cu:158-163) in fp64 for a weighted QUBO
+    given as {n, eu, ev, ew (float32), h (float32 or None), offset}."""
+    eu, ev = np.ascontiguousarray(q["eu"], np.int32), np.ascontiguousarray(q["ev"], np.int32)
+    ew = np.ascontiguousarray(q["ew"], np.float32)
+    h = None if q.get("h") is None else np.ascontiguousarray(q["h"], np.float32)
+    x = np.ascontiguousarray(x, np.uint8)
+    return float(orc().orc_qubo_energy(int(q["n"]), int(eu.size), _p(eu), _p(ev), _p(ew), _p(h),
+                                       float(q.get("offset", 0.0)), _p(x)))
+
+
+def qubo_anneal_coloured(q: dict, order, class_ptr, temps, refresh, seed):
+    """The GPU's compensated-field weighted-QUBO sweep for one replica:
+    returns (x, tracked sum of accepted dE, max fp32-vs-fp64 field drift)."""
+    eu, ev = np.ascontiguousarray(q["eu"], np.int32), np.ascontiguousarray(q["ev"], np.int32)
+    ew = np.ascontiguousarray(q["ew"], np.float32)
+    h = None if q.get("h") is None else np.ascontiguousarray(q["h"], np.float32)
+    order = np.ascontiguousarray(order, np.int32)
+    cptr = np.ascontiguousarray(class_ptr, np.int32)
+    temps = np.ascontiguousarray(temps, np.float64)
+    n = int(q["n"])
+    x = np.empty(n, np.uint8)
+    drift = C.c_float(0.0)
+    track = orc().orc_qubo_anneal_coloured(n, int(eu.size), _p(eu), _p(ev), _p(ew), _p(h), _p(order), _p(cptr),
+                                           int(cptr.size - 1), _p(temps), int(temps.size), int(refresh), int(seed),
+                                           _p(x), C.byref(drift))
+    return x, float(track), float(drift.value)
 
 
 def fractions(X) -> np.ndarray:

@@ -439,3 +439,98 @@ void orc_fractions(const uint8_t* X, int R, int64_t n, float* frac) {
         for (int64_t i = 0; i < n; ++i) frac[i] += X[(size_t)b * (size_t)n + (size_t)i];
     for (int64_t i = 0; i < n; ++i) frac[i] /= (float)R;
 }
+
+/* ---- weighted QUBO ------------------------------------------------------------------ */
+
+/* E(x) = offset + sum_i h_i x_i + sum_e J_e x_u x_v in fp64: qubo_energy of
+ * src/check_ree_qubo.cu:158-163 (offset + Qd over set bits + Qo over pairs of
+ * set bits), summed sequentially. h may be NULL. */
+double orc_qubo_energy(int n, int64_t m, const int32_t* eu, const int32_t* ev, const float* ew, const float* h,
+                       double offset, const uint8_t* x) {
+    double e = offset;
+    if (h)
+        for (int i = 0; i < n; ++i)
+            if (x[i]) e += (double)h[i];
+    for (int64_t k = 0; k < m; ++k)
+        if (x[eu[k]] && x[ev[k]]) e += (double)ew[k];
+    return e;
+}
+
+/* hi + lo += v with the fp32 rounding error carried in lo (TwoSum), the
+ * compensated update of the GPU sweep. */
+static void orc_two_sum(float* hi, float* lo, float v) {
+    const float s = *hi + v;
+    const float bp = s - *hi;
+    const float e = (*hi - (s - bp)) + (v - bp);
+    *hi = s;
+    *lo = *lo + e;
+}
+
+/* Mirror of the weighted-QUBO sweep of qublar_b200/csrc/qb_qubo.cu for one
+ * replica: bits in colour-class order (order[k] = original bit at sweep
+ * position k, classes class_ptr[0..nc]); a visit first adds the deltas of the
+ * neighbours that flipped at their latest visit (CSR built from the edge list
+ * in edge order, TwoSum into the fp32 pair hi + lo), every `refresh` sweeps
+ * (sweep > 0) recomputes the field in fp64 and records |fp32 - fp64|, then
+ * accepts if dE <= 0 or u53 * 2^-53 < exp(-dE / T). Returns the tracked sum of
+ * accepted dE in fp64. */
+double orc_qubo_anneal_coloured(int n, int64_t m, const int32_t* eu, const int32_t* ev, const float* ew,
+                                const float* h, const int32_t* order, const int32_t* class_ptr, int nc,
+                                const double* temps, int sweeps, int refresh, uint64_t seed, uint8_t* x_out,
+                                float* drift_out) {
+    int64_t* row = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+    for (int64_t e = 0; e < m; ++e) { row[eu[e] + 1]++; row[ev[e] + 1]++; }
+    for (int i = 0; i < n; ++i) row[i + 1] += row[i];
+    int32_t* col = (int32_t*)malloc(sizeof(int32_t) * (size_t)(2 * m + 1));
+    float* w = (float*)malloc(sizeof(float) * (size_t)(2 * m + 1));
+    int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    for (int i = 0; i < n; ++i) fill[i] = row[i];
+    for (int64_t e = 0; e < m; ++e) {
+        col[fill[eu[e]]] = ev[e]; w[fill[eu[e]]++] = ew[e];
+        col[fill[ev[e]]] = eu[e]; w[fill[ev[e]]++] = ew[e];
+    }
+    uint8_t* x = (uint8_t*)calloc((size_t)n, 1);
+    uint8_t* f = (uint8_t*)calloc((size_t)n, 1);
+    float* hi = (float*)malloc(sizeof(float) * (size_t)n);
+    float* lo = (float*)calloc((size_t)n, sizeof(float));
+    for (int i = 0; i < n; ++i) hi[i] = h ? h[i] : 0.0f;
+    double track = 0.0;
+    float drift = 0.0f;
+    for (int sweep = 0; sweep < sweeps; ++sweep) {
+        const double T = temps[sweep];
+        const int fresh = refresh > 0 && sweep > 0 && sweep % refresh == 0;
+        for (int c = 0; c < nc; ++c)
+            for (int k = class_ptr[c]; k < class_ptr[c + 1]; ++k) {
+                const int i = order[k];
+                float H = hi[i], L = lo[i];
+                double a = fresh ? (double)(h ? h[i] : 0.0f) : 0.0;
+                for (int64_t e = row[i]; e < row[i + 1]; ++e) {
+                    const int j = col[e];
+                    if (f[j]) orc_two_sum(&H, &L, x[j] ? w[e] : -w[e]);
+                    if (fresh && x[j]) a += (double)w[e];
+                }
+                if (fresh) {
+                    const float d = (float)fabs((double)(H + L) - a);
+                    if (d > drift) drift = d;
+                    H = (float)a;
+                    L = (float)(a - (double)H);
+                }
+                const float Lf = H + L;
+                const float dE = x[i] ? -Lf : Lf;
+                const int acc = dE <= 0.0f ||
+                                (double)orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u) * 0x1.0p-53 <
+                                    exp(-(double)dE / T);
+                f[i] = (uint8_t)acc;
+                if (acc) {
+                    x[i] ^= 1u;
+                    track += (double)dE;
+                }
+                hi[i] = H;
+                lo[i] = L;
+            }
+    }
+    memcpy(x_out, x, (size_t)n);
+    if (drift_out) *drift_out = drift;
+    free(row); free(col); free(w); free(fill); free(x); free(f); free(hi); free(lo);
+    return track;
+}

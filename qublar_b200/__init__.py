@@ -22,12 +22,12 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import (KIND_ISING, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
+from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
                    REQ_FAILED, REQ_PENDING, REQ_RUNNING, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts,
-                   ProblemInfo, QBError, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig, ServerStats,
+                   ProblemInfo, QBError, QuboDesc, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig, ServerStats,
                    check, lib, ptr)
 
-__all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "Result", "RunOut", "BatchOut",
+__all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
            "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER"]
 
@@ -241,6 +241,37 @@ class ResidualProblem(_Problem):
         X = np.ascontiguousarray(X, dtype=np.uint8).reshape(-1, self.n)
         e = np.empty(X.shape[0], dtype=np.float64)
         check(lib().qb_energies_residual(self._h, ptr(X), int(X.shape[0]), ptr(e)))
+        return e
+
+
+class QuboProblem(_Problem):
+    """A weighted QUBO with fp32 couplings and linear terms (the Model of
+    check_ree_qubo.cu), annealed with compensated fp32 local fields."""
+    kind = KIND_QUBO
+
+    def __init__(self, n: int, eu, ev, ew, h=None, offset: float = 0.0, device: int = -1, stream=None,
+                 flags: int = 0):
+        super().__init__()
+        self.n = int(n)
+        self.eu, self.ev = _c32(eu), _c32(ev)
+        self.ew = np.ascontiguousarray(ew, dtype=np.float32)
+        self.h = None if h is None else np.ascontiguousarray(h, dtype=np.float32)
+        self.offset = float(offset)
+        self.m = int(self.eu.size)
+        d = QuboDesc(self.n, self.m, ptr(self.eu), ptr(self.ev), ptr(self.ew), ptr(self.h), self.offset)
+        h_ = C.c_void_p()
+        o = _opts(device, stream, flags)
+        check(lib().qb_problem_create_qubo(C.byref(d), C.byref(o), C.byref(h_)))
+        self._h = h_
+
+    @classmethod
+    def from_dict(cls, q: dict, **kw) -> "QuboProblem":
+        return cls(q["n"], q["eu"], q["ev"], q["ew"], q.get("h"), q.get("offset", 0.0), **kw)
+
+    def energies(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.uint8).reshape(-1, self.n)
+        e = np.empty(X.shape[0], dtype=np.float64)
+        check(lib().qb_energies_qubo(self._h, ptr(X), int(X.shape[0]), ptr(e)))
         return e
 
 

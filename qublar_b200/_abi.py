@@ -17,6 +17,7 @@ STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4:
                 5: "QB_ECUDA", 6: "QB_ENOTSUP", 7: "QB_ECANCELLED", 8: "QB_EBUSY"}
 KIND_ISING = 1
 KIND_RESIDUAL = 2
+KIND_QUBO = 3
 NOALLOC_SCRATCH_BYTES = 8 << 20
 OPT_DEFER_UPLOAD = 1
 OPT_RESID_CLUSTER = 2
@@ -36,6 +37,11 @@ class QBError(RuntimeError):
 
 class IsingDesc(C.Structure):
     _fields_ = [("n", C.c_int32), ("m", C.c_int64), ("eu", C.c_void_p), ("ev", C.c_void_p), ("ew", C.c_void_p)]
+
+
+class QuboDesc(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m", C.c_int64), ("eu", C.c_void_p), ("ev", C.c_void_p), ("ew", C.c_void_p),
+                ("h", C.c_void_p), ("offset", C.c_double)]
 
 
 class ResidualDesc(C.Structure):
@@ -63,7 +69,7 @@ class ProblemInfo(C.Structure):
 class ResultInfo(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_branches", C.c_int32), ("sweeps", C.c_int32), ("launches", C.c_int32),
                 ("anneal_ms", C.c_float), ("total_ms", C.c_float), ("attempts", C.c_int64),
-                ("max_drift", C.c_double), ("accepted", C.c_int64)]
+                ("max_drift", C.c_double), ("accepted", C.c_int64), ("max_energy_error", C.c_double)]
 
 
 class TomoParams(C.Structure):
@@ -118,6 +124,7 @@ SIGNATURES = {
     "qb_device_count": (C.c_int32, []),
     "qb_problem_create_ising": (C.c_int, [C.POINTER(IsingDesc), C.POINTER(Opts), C.POINTER(_P)]),
     "qb_problem_create_residual": (C.c_int, [C.POINTER(ResidualDesc), C.POINTER(Opts), C.POINTER(_P)]),
+    "qb_problem_create_qubo": (C.c_int, [C.POINTER(QuboDesc), C.POINTER(Opts), C.POINTER(_P)]),
     "qb_problem_destroy": (None, [_P]),
     "qb_problem_info_get": (C.c_int, [_P, C.POINTER(ProblemInfo)]),
     "qb_problem_colouring": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32)]),
@@ -133,6 +140,7 @@ SIGNATURES = {
     "qb_result_destroy": (None, [_P]),
     "qb_energies_ising": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_energies_residual": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "qb_energies_qubo": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P]),
     "qb_batch_autotune": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.c_int32, C.POINTER(Opts),
                                     C.POINTER(BatchConfig)]),

@@ -10,6 +10,7 @@
 
 #include "qb_internal.hpp"
 #include "qb_kernels.hpp"
+#include "qb_qubo.hpp"
 
 using namespace qb;
 
@@ -178,6 +179,91 @@ qb_status upload_ising(IsingPlan& P, const qb_ising_desc* g, cudaStream_t st, in
     QB_CUDA(cudaStreamSynchronize(st));
     *bytes = int64_t(P.d_row.bytes + P.d_adj.bytes + P.d_w.bytes + P.d_f0.bytes + P.d_order.bytes +
                      P.d_class_ptr.bytes + P.d_eu.bytes + P.d_ev.bytes + P.d_ew.bytes);
+    return QB_OK;
+}
+
+// ---- weighted qubo planning ---------------------------------------------------------------
+
+qb_status plan_qubo(const qb_qubo_desc* g, QuboPlan& P) {
+    const int n = g->n;
+    const int64_t m = g->m;
+    if (n <= 0) return fail(QB_EINVAL, "qubo: n must be positive");
+    if (m < 0) return fail(QB_EINVAL, "qubo: m must be non-negative");
+    if (m > 0 && (!g->eu || !g->ev || !g->ew)) return fail(QB_EINVAL, "qubo: null edge arrays");
+    if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "qubo: more than 2^30 edges");
+    if (!std::isfinite(g->offset)) return fail(QB_EINVAL, "qubo: offset must be finite");
+    std::vector<uint64_t> key(static_cast<size_t>(m));
+    for (int64_t e = 0; e < m; ++e) {
+        const int32_t u = g->eu[e], v = g->ev[e];
+        if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "qubo: vertex index out of range");
+        if (u == v) return fail(QB_EINVAL, "qubo: self-loop (put diagonal terms in h)");
+        if (!std::isfinite(g->ew[e])) return fail(QB_EINVAL, "qubo: coupling is not finite");
+        key[size_t(e)] = (uint64_t(std::min(u, v)) << 32) | uint64_t(std::max(u, v));
+    }
+    std::sort(key.begin(), key.end());
+    for (size_t k = 1; k < key.size(); ++k)
+        if (key[k] == key[k - 1]) return fail(QB_EINVAL, "qubo: duplicate edge");
+    if (g->h)
+        for (int i = 0; i < n; ++i)
+            if (!std::isfinite(g->h[i])) return fail(QB_EINVAL, "qubo: linear term is not finite");
+    P.n = n;
+    P.m = m;
+    P.nnz = 2 * m;
+    P.offset = g->offset;
+    // symmetric CSR, edge order per vertex
+    std::vector<int64_t> row(size_t(n) + 1, 0);
+    for (int64_t e = 0; e < m; ++e) { row[size_t(g->eu[e]) + 1]++; row[size_t(g->ev[e]) + 1]++; }
+    for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
+    std::vector<int32_t> col(size_t(2 * m));
+    std::vector<float> w(size_t(2 * m));
+    std::vector<int64_t> fill(row.begin(), row.end() - 1);
+    for (int64_t e = 0; e < m; ++e) {
+        const int32_t a = g->eu[e], b = g->ev[e];
+        col[size_t(fill[size_t(a)])] = b; w[size_t(fill[size_t(a)]++)] = g->ew[e];
+        col[size_t(fill[size_t(b)])] = a; w[size_t(fill[size_t(b)]++)] = g->ew[e];
+    }
+    P.col = colour_graph(n, row, col);
+    const Colouring& C = P.col;
+    P.row.assign(size_t(n) + 1, 0);
+    P.adj.resize(size_t(2 * m));
+    P.J.resize(size_t(2 * m));
+    P.h.assign(size_t(n), 0.0f);
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        int32_t pos = P.row[size_t(k)];
+        for (int64_t e = row[size_t(i)]; e < row[size_t(i) + 1]; ++e) {
+            P.adj[size_t(pos)] = C.inverse[size_t(col[size_t(e)])];
+            P.J[size_t(pos)] = w[size_t(e)];
+            ++pos;
+        }
+        P.row[size_t(k) + 1] = pos;
+        P.h[size_t(k)] = g->h ? g->h[i] : 0.0f;
+    }
+    return QB_OK;
+}
+
+int64_t qubo_device_bytes(const QuboPlan& P) {
+    return int64_t(P.row.size() + P.adj.size() + P.J.size() + P.h.size() + P.col.order.size() +
+                   P.col.class_ptr.size()) * 4 + P.m * 12 + int64_t(P.n) * 4;
+}
+
+qb_status upload_qubo(QuboPlan& P, const qb_qubo_desc* g, cudaStream_t st, int64_t* bytes) {
+    qb_status s;
+    if ((s = upload_vec(P.d_row, P.row, st))) return s;
+    if ((s = upload_vec(P.d_adj, P.adj, st))) return s;
+    if ((s = upload_vec(P.d_J, P.J, st))) return s;
+    if ((s = upload_vec(P.d_h, P.h, st))) return s;
+    if ((s = upload_vec(P.d_order, P.col.order, st))) return s;
+    if ((s = upload_vec(P.d_class_ptr, P.col.class_ptr, st))) return s;
+    if ((s = upload(P.d_eu, g->eu, size_t(P.m) * 4, st))) return s;
+    if ((s = upload(P.d_ev, g->ev, size_t(P.m) * 4, st))) return s;
+    if ((s = upload(P.d_ew, g->ew, size_t(P.m) * 4, st))) return s;
+    std::vector<float> ho(size_t(P.n), 0.0f);
+    if (g->h) std::memcpy(ho.data(), g->h, size_t(P.n) * 4);
+    if ((s = upload_vec(P.d_ho, ho, st))) return s;
+    QB_CUDA(cudaStreamSynchronize(st));   // `ho` is a local
+    *bytes = int64_t(P.d_row.bytes + P.d_adj.bytes + P.d_J.bytes + P.d_h.bytes + P.d_order.bytes +
+                     P.d_class_ptr.bytes + P.d_eu.bytes + P.d_ev.bytes + P.d_ew.bytes + P.d_ho.bytes);
     return QB_OK;
 }
 
@@ -470,6 +556,11 @@ qb_status wait(qb_result* r) {
         QB_CUDA(cudaStreamSynchronize(r->stream));
         r->synced = true;
     }
+    if (r->d_err) {
+        int e = 0;
+        QB_CUDA(cudaMemcpy(&e, r->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) return fail(QB_ETIMEDOUT, "a grid barrier of the sweep timed out: the results are not valid");
+    }
     return QB_OK;
 }
 
@@ -480,7 +571,7 @@ qb_status download(qb_result* r, void* dst, const DevBuf& src, size_t bytes) {
     QB_CUDA(cudaMemcpyAsync(dst, src.p, bytes, cudaMemcpyDeviceToHost, r->stream));
     QB_CUDA(cudaStreamSynchronize(r->stream));
     r->synced = true;
-    return QB_OK;
+    return wait(r);
 }
 
 }  // namespace
@@ -489,7 +580,10 @@ qb_status download(qb_result* r, void* dst, const DevBuf& src, size_t bytes) {
 
 qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
     if (p->uploaded) return QB_OK;
-    if (p->kind == QB_KIND_ISING ? p->host.eu.empty() && p->ising.m > 0 : p->host.row_ptr.empty())
+    const bool gone = p->kind == QB_KIND_ISING   ? p->host.eu.empty() && p->ising.m > 0
+                      : p->kind == QB_KIND_QUBO ? p->host.eu.empty() && p->qubo.m > 0
+                                                : p->host.row_ptr.empty();
+    if (gone)
         return fail(QB_EINVAL, "problem: its device memory was released and it was not created with deferred upload");
     QB_CUDA(cudaSetDevice(p->device));
     HostDesc& h = p->host;
@@ -497,6 +591,10 @@ qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
     if (p->kind == QB_KIND_ISING) {
         const qb_ising_desc d{p->ising.n, p->ising.m, h.eu.data(), h.ev.data(), h.ew.data()};
         s = upload_ising(p->ising, &d, st, &p->device_bytes);
+    } else if (p->kind == QB_KIND_QUBO) {
+        const qb_qubo_desc d{p->qubo.n, p->qubo.m, h.eu.data(), h.ev.data(), h.wf.data(),
+                             h.hf.empty() ? nullptr : h.hf.data(), h.offset};
+        s = upload_qubo(p->qubo, &d, st, &p->device_bytes);
     } else {
         const qb_residual_desc d{p->resid.n, p->resid.n_rays, h.d.data(), h.w.data(), h.row_ptr.data(), h.ray.data(),
                                  h.a.data(), h.nbr_ptr.data(), h.nbr.data(), h.lambda, h.kappa,
@@ -518,6 +616,9 @@ void qb::problem_release_device(qb_problem* p) {
                     &R.d_nbr_new, &R.d_rbit_new, &R.d_o_row, &R.d_o_ray, &R.d_o_a, &R.d_o_nbr_ptr, &R.d_o_nbr,
                     &R.d_o_lin, &R.d_o_rrow, &R.d_o_rbit, &R.d_o_ra};
     for (DevBuf* b : rb) b->release();
+    QuboPlan& Q = p->qubo;
+    DevBuf* qbf[] = {&Q.d_row, &Q.d_adj, &Q.d_J, &Q.d_h, &Q.d_order, &Q.d_class_ptr, &Q.d_eu, &Q.d_ev, &Q.d_ew, &Q.d_ho};
+    for (DevBuf* b : qbf) b->release();
     p->d_temp.release();
     p->uploaded = false;
 }
@@ -591,6 +692,36 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
     return QB_OK;
 }
 
+extern "C" qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_opts* opts, qb_problem** out) {
+    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_qubo: null argument");
+    *out = nullptr;
+    qb_problem* p = new (std::nothrow) qb_problem();
+    if (!p) return fail(QB_ENOMEM, "qb_problem_create_qubo: out of host memory");
+    p->kind = QB_KIND_QUBO;
+    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
+    qb_status s = plan_qubo(desc, p->qubo);
+    if (s == QB_OK) s = select_device(opts, &p->device);
+    if (s == QB_OK && defer) {
+        const size_t m = size_t(desc->m);
+        HostDesc& h = p->host;
+        h.eu.assign(desc->eu, desc->eu + m);
+        h.ev.assign(desc->ev, desc->ev + m);
+        h.wf.assign(desc->ew, desc->ew + m);
+        if (desc->h) h.hf.assign(desc->h, desc->h + desc->n);
+        h.offset = desc->offset;
+        p->device_bytes = qubo_device_bytes(p->qubo);
+    } else if (s == QB_OK) {
+        s = upload_qubo(p->qubo, desc, stream_of(opts), &p->device_bytes);
+        p->uploaded = s == QB_OK;
+    }
+    if (s != QB_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return QB_OK;
+}
+
 extern "C" void qb_problem_destroy(qb_problem* p) {
     if (!p) return;
     cudaSetDevice(p->device);
@@ -602,7 +733,7 @@ extern "C" qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* i
     std::memset(info, 0, sizeof(*info));
     info->kind = p->kind;
     info->device_bytes = p->device_bytes;
-    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->resid.col;
+    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->kind == QB_KIND_QUBO ? p->qubo.col : p->resid.col;
     info->n_colours = C.n_colours();
     for (int k = 0; k < C.n_colours(); ++k)
         info->max_class = std::max(info->max_class, C.class_ptr[size_t(k) + 1] - C.class_ptr[size_t(k)]);
@@ -615,6 +746,11 @@ extern "C" qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* i
         info->sigma = P.sigma;
         info->w_min = double(P.w_min);
         info->field_bound = P.B;
+    } else if (p->kind == QB_KIND_QUBO) {
+        info->n = p->qubo.n;
+        info->nnz = p->qubo.nnz;
+        info->field_bytes = 8;    // fp32 hi + lo
+        info->weight_bytes = 4;
     } else {
         const ResidualPlan& P = p->resid;
         info->n = P.n;
@@ -629,7 +765,7 @@ extern "C" qb_status qb_problem_info_get(const qb_problem* p, qb_problem_info* i
 
 extern "C" qb_status qb_problem_colouring(const qb_problem* p, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
     if (!p) return fail(QB_EINVAL, "qb_problem_colouring: null problem");
-    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->resid.col;
+    const Colouring& C = p->kind == QB_KIND_ISING ? p->ising.col : p->kind == QB_KIND_QUBO ? p->qubo.col : p->resid.col;
     if (order) std::memcpy(order, C.order.data(), C.order.size() * sizeof(int32_t));
     if (class_ptr) std::memcpy(class_ptr, C.class_ptr.data(), C.class_ptr.size() * sizeof(int32_t));
     if (n_colours) *n_colours = C.n_colours();
@@ -691,7 +827,7 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
     r->R = int(n_branches);
     r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
     const int R = r->R;
-    const int n = p->kind == QB_KIND_ISING ? p->ising.n : p->resid.n;
+    const int n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
     r->n = n;
     const uint64_t seed0 = 1 + seed_offset;   // branch b: seed b + 1 + offset (ising_recon.hpp:157)
     auto bail = [&](qb_status e) {
@@ -733,6 +869,36 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
         if ((s = launch_ising_energies(P, b.x, R, r->d_e_scr.as<long long>(), st))) return bail(s);
         if ((s = launch_i64_to_f64(r->d_e_scr.as<long long>(), R, b.e_f64, st))) return bail(s);
         r->launches = 3;
+    } else if (p->kind == QB_KIND_QUBO) {
+        const QuboPlan& P = p->qubo;
+        if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
+        if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
+        if ((s = alloc_async(r->d_e_track, size_t(R) * 8, st))) return bail(s);
+        if ((s = alloc_async(r->d_scratch, qubo_scratch(P), st))) return bail(s);
+        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
+            cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess ||
+            cudaMemsetAsync(r->d_e_track.p, 0, size_t(R) * 8, st) != cudaSuccess ||
+            cudaMemsetAsync(r->d_scratch.p, 0, 64, st) != cudaSuccess)
+            return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+        r->d_err = reinterpret_cast<const int*>(static_cast<const char*>(r->d_scratch.p) + 16);
+        const int RB = qubo_max_branches();
+        cudaEventRecord(r->ev0, st);
+        int anneal_launches = 0;
+        for (int b0 = 0; b0 < R && s == QB_OK; b0 += RB, ++anneal_launches) {
+            QuboBuffers qbuf;
+            qbuf.x = b.x + size_t(b0) * size_t(n);
+            qbuf.temp = b.temp;
+            qbuf.drift = r->d_drift.as<float>() + b0;
+            qbuf.e_track = r->d_e_track.as<double>() + b0;
+            qbuf.accepts = r->d_accepts.as<unsigned long long>() + b0;
+            qbuf.scratch = r->d_scratch.p;
+            s = launch_qubo_lockstep(P, qbuf, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
+                                     seed0 + uint64_t(b0), st);
+        }
+        if (s != QB_OK) return bail(s);
+        cudaEventRecord(r->ev1, st);
+        if ((s = launch_qubo_energies(P, b.x, R, b.e_f64, st))) return bail(s);
+        r->launches = anneal_launches + 1;
     } else {
         const ResidualPlan& P = p->resid;
         if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
@@ -746,6 +912,8 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
         if (P.variant == QB_RESID_LOCKSTEP) {
             if ((s = alloc_async(r->d_scratch, resid_lockstep_scratch(P, RB), st))) return bail(s);
             b.scratch = r->d_scratch.p;
+            QB_CUDA(cudaMemsetAsync(r->d_scratch.p, 0, 64, st));   // control block, timeout flag included
+            r->d_err = reinterpret_cast<const int*>(static_cast<const char*>(r->d_scratch.p) + 16);
         }
         cudaEventRecord(r->ev0, st);
         int anneal_launches = 0;
@@ -787,7 +955,14 @@ extern "C" qb_status qb_result_info_get(qb_result* r, qb_result_info* info) {
     info->attempts = int64_t(r->R) * int64_t(r->sweeps) * int64_t(r->n);
     QB_CUDA(cudaEventElapsedTime(&info->anneal_ms, r->ev0, r->ev1));
     QB_CUDA(cudaEventElapsedTime(&info->total_ms, r->ev0, r->ev2));
-    if (r->prob->kind == QB_KIND_RESIDUAL) {
+    if (r->prob->kind == QB_KIND_QUBO) {
+        std::vector<double> et(static_cast<size_t>(r->R)), ef(static_cast<size_t>(r->R));
+        QB_CUDA(cudaMemcpy(et.data(), r->d_e_track.p, et.size() * 8, cudaMemcpyDeviceToHost));
+        QB_CUDA(cudaMemcpy(ef.data(), r->d_e_f64.p, ef.size() * 8, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < et.size(); ++k)
+            info->max_energy_error = std::max(info->max_energy_error, std::fabs(r->prob->qubo.offset + et[k] - ef[k]));
+    }
+    if (r->prob->kind == QB_KIND_RESIDUAL || r->prob->kind == QB_KIND_QUBO) {
         std::vector<float> dr(static_cast<size_t>(r->R));
         QB_CUDA(cudaMemcpy(dr.data(), r->d_drift.p, dr.size() * sizeof(float), cudaMemcpyDeviceToHost));
         for (float v : dr) info->max_drift = std::max(info->max_drift, double(v));
@@ -846,7 +1021,8 @@ extern "C" void qb_result_destroy(qb_result* r) {
     if (!r) return;
     cudaSetDevice(r->device);
     cudaStream_t st = r->stream;
-    DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift, &r->d_accepts, &r->d_scratch};
+    DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift,
+                     &r->d_accepts, &r->d_e_track, &r->d_scratch};
     for (DevBuf* b : all) free_async(*b, st);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
@@ -867,6 +1043,21 @@ extern "C" qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, in
     if ((s = upload(dx, x, size_t(k) * size_t(p->ising.n), nullptr))) return s;
     if ((s = de.alloc(size_t(k) * 8))) return s;
     if ((s = launch_ising_energies(p->ising, dx.as<uint8_t>(), k, de.as<long long>(), nullptr))) return s;
+    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+    return QB_OK;
+}
+
+extern "C" qb_status qb_energies_qubo(const qb_problem* p, const uint8_t* x, int32_t k, double* e) {
+    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_qubo: bad argument");
+    if (p->kind != QB_KIND_QUBO) return fail(QB_EINVAL, "qb_energies_qubo: weighted qubo problems only");
+    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_qubo: the problem is not on the device");
+    if (k == 0) return QB_OK;
+    QB_CUDA(cudaSetDevice(p->device));
+    DevBuf dx, de;
+    qb_status s;
+    if ((s = upload(dx, x, size_t(k) * size_t(p->qubo.n), nullptr))) return s;
+    if ((s = de.alloc(size_t(k) * 8))) return s;
+    if ((s = launch_qubo_energies(p->qubo, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
     QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
     return QB_OK;
 }

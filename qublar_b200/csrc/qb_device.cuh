@@ -1,0 +1,44 @@
+// Device helpers shared by the cooperative-grid sweeps: acquire/release
+// global accesses and the bounded grid barrier.
+#pragma once
+
+#include <cstdint>
+
+namespace qb {
+
+constexpr unsigned kSpinLimit = 1u << 24;   // polls of a grid barrier before it reports a timeout
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier of a cooperative launch: arrive, then poll the counter until
+// every CTA of barrier round `round` has arrived. A poll limit turns a lost
+// CTA into an error flag instead of a hang; every CTA then leaves its loops.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned round) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned target = round * gridDim.x;
+        red_release_gpu(bar, 1u);
+        unsigned spins = 0;
+        int ok = 1;
+        while (ld_acquire_gpu(bar) < target) {
+            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+}  // namespace qb

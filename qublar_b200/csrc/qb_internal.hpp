@@ -158,10 +158,29 @@ struct ResidualPlan {
     DevBuf d_o_rrow, d_o_rbit, d_o_ra;
 };
 
+// Weighted QUBO E(x) = offset + sum_i h_i x_i + sum_e J_e x_u x_v with fp32
+// couplings and linear terms, planned for the compensated lockstep sweep.
+struct QuboPlan {
+    int n = 0;
+    int64_t m = 0;
+    int64_t nnz = 0;          // 2m
+    double offset = 0.0;
+    Colouring col;
+    // sweep order: neighbours of the bit at position p are adj[row[p] ..
+    // row[p+1]) as sweep positions, in the order of the symmetric CSR built
+    // from the edge list (edge order per vertex)
+    std::vector<int32_t> row, adj;
+    std::vector<float> J, h;
+    DevBuf d_row, d_adj, d_J, d_h, d_order, d_class_ptr;
+    DevBuf d_eu, d_ev, d_ew, d_ho;   // edge list and h as given (fp64 evaluator)
+};
+
 // Host copies of a problem's input arrays, kept when its upload is deferred
 // (QB_OPT_DEFER_UPLOAD) so that the problem can go to the device later.
 struct HostDesc {
-    std::vector<int32_t> eu, ev, ew;                       // ising
+    std::vector<int32_t> eu, ev, ew;                       // ising (eu, ev also qubo)
+    std::vector<float> wf, hf;                             // qubo couplings and linear terms
+    double offset = 0.0;
     std::vector<double> d, w, field;                       // residual
     std::vector<int32_t> row_ptr, ray, nbr_ptr, nbr;
     std::vector<float> a;
@@ -176,6 +195,7 @@ struct qb_problem {
     int device = 0;
     qb::IsingPlan ising;
     qb::ResidualPlan resid;
+    qb::QuboPlan qubo;
     int64_t device_bytes = 0;     // device memory the problem holds (or will hold once uploaded)
     bool uploaded = false;
     qb::HostDesc host;            // filled while the upload is deferred
@@ -209,7 +229,9 @@ struct qb_result {
     qb::DevBuf d_p;          // n marginals
     qb::DevBuf d_temp;       // sweeps temperatures
     qb::DevBuf d_drift;      // R floats
-    qb::DevBuf d_accepts;    // R accepted-flip counts (residual)
+    qb::DevBuf d_accepts;    // R accepted-flip counts (residual, qubo)
+    qb::DevBuf d_e_track;    // R tracked energies minus offset (qubo)
     qb::DevBuf d_scratch;    // per-branch state that does not fit on chip
+    const int* d_err = nullptr;   // timeout flag of a cooperative sweep (inside d_scratch), or null
     bool synced = false;
 };

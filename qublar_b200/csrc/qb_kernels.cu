@@ -35,6 +35,7 @@
 #include <mutex>
 #include <vector>
 
+#include "qb_device.cuh"
 #include "qb_kernels.hpp"
 #include "qb_philox.cuh"
 
@@ -457,7 +458,6 @@ constexpr int kLockN = 1536;   // staged neighbour entries per chunk
 constexpr int kSeg = 16;       // entries per segment: one warp, one batch of loads
 constexpr int kLockSegs = kLockE / kSeg + kLockB;   // segments a chunk can hold
 constexpr int kLockMaxNG = 4;  // branch groups of 16 one launch serves (64 branches)
-constexpr unsigned kSpinLimit = 1u << 24;   // polls of a grid barrier before it reports a timeout
 
 struct ResidLockArgs {
     int n;
@@ -490,14 +490,6 @@ struct ResidLockArgs {
     unsigned long long* phase;  // PHASES builds: per CTA {stage wait, items, barrier, chunks} clock64 sums
 };
 
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
@@ -505,30 +497,6 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-// Grid barrier of a cooperative launch: arrive, then poll the counter until
-// every CTA of barrier round `round` has arrived. A poll limit turns a lost
-// CTA into an error flag instead of a hang; every CTA then leaves its loops.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned round) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned target = round * gridDim.x;
-        red_release_gpu(bar, 1u);
-        unsigned spins = 0;
-        int ok = 1;
-        while (ld_acquire_gpu(bar) < target) {
-            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
-                atomicExch(err, 1);
-                ok = 0;
-                break;
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 struct LockStage {
     uint4* ent;      // kLockE
@@ -1067,6 +1035,7 @@ size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
     return size_t(p.n_rays) * 16 * NG * 4 + size_t(p.n) * NG * 4 + 64;
 }
 
+
 qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, int R, int sweeps, int refresh,
                                 uint64_t seed0, cudaStream_t st) {
     ResidLockArgs A{};
@@ -1090,17 +1059,18 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     A.rbit = p.d_rbit_new.as<int32_t>();
     A.ra = p.d_ra.as<float>();
     A.temp = b.temp;
+    // scratch: control block (barrier counter, timeout flag at +16), residuals, bit words
     char* sc = static_cast<char*>(b.scratch);
-    A.rw = reinterpret_cast<float*>(sc);
-    sc += size_t(p.n_rays) * 16 * A.NG * 4;
-    A.xb = reinterpret_cast<uint32_t*>(sc);
-    sc += size_t(p.n) * A.NG * 4;
     A.bar = reinterpret_cast<unsigned*>(sc);
     A.err = reinterpret_cast<int*>(sc + 16);
+    A.rw = reinterpret_cast<float*>(sc + 64);
+    A.xb = reinterpret_cast<uint32_t*>(sc + 64 + size_t(p.n_rays) * 16 * A.NG * 4);
     A.x_out = b.x;
     A.drift = b.drift;
     A.accepts = b.accepts;
-    QB_CUDA(cudaMemsetAsync(sc, 0, 64, st));
+    // the barrier counter restarts per launch; the timeout flag (+16) is
+    // zeroed once per solve by the caller, so a timeout of any launch shows
+    QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));
     const int grid = p.lock_grid;
     if (grid < 1) return fail(QB_ENOTSUP, "residual lockstep sweep: no co-resident grid");
     DevBuf phase;

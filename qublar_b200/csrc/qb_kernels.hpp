@@ -57,6 +57,8 @@ int resid_lockstep_chunk_segments();
 int resid_lockstep_segment();        // entries per segment (the summation order)
 int resid_lockstep_max_branches();   // branches one lockstep solve serves
 size_t resid_lockstep_scratch(const ResidualPlan& p, int R);
+// The scratch starts with a 64-byte control block: the barrier counter, then
+// (at +16) the timeout flag, which the caller zeroes once per solve.
 qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, int R, int sweeps, int refresh,
                                 uint64_t seed0, cudaStream_t st);
 qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st);

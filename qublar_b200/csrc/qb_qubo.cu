@@ -1,0 +1,290 @@
+// Weighted QUBO sweep with compensated fp32 local fields (the general real
+// QUBO E(x) = offset + sum_i h_i x_i + sum_{i<j} J_ij x_i x_j, x in {0,1},
+// of qubo_energy, src/check_ree_qubo.cu:158-163, which the reference anneals
+// only through its pair-ray encoding into anneal_branch, :172-192).
+//
+// All replicas (up to 64 per launch) of one problem run in lockstep on a
+// cooperative grid. A warp visits one bit for every replica: lane l serves
+// replicas l and l + 32. The state lives in global memory, L2-resident:
+//   xw[i]  -- 64-bit word, bit r = x_i of replica r;
+//   fw[i]  -- 64-bit word, bit r = "replica r flipped x_i at its latest visit";
+//   L[i][r] -- the local field L_i = h_i + sum_j J_ij x_j as an unevaluated
+//             sum hi + lo of two fp32 numbers.
+// Incremental fields, deterministically: when bit i is visited, every
+// neighbour j has been visited exactly once since i's previous visit (colour
+// classes in a fixed order, no two bits of a class coupled), so fw[j] names
+// exactly the changes i has not seen. The visit adds their deltas +-J_ij to
+// L_i in CSR order with the TwoSum error carried in lo (compensated
+// summation), scores dE = (1 - 2 x_i)(hi + lo), decides, and publishes its
+// own flips in fw[i]. Pushing deltas with atomics instead would make fp32
+// results depend on arrival order; pulling them keeps every bit reproducible.
+// Every `refresh` sweeps a visit also recomputes L_i from scratch in fp64,
+// records |fp32 - fp64| (the drift) and restarts hi + lo from it. The final
+// energies are recomputed in fp64 from scratch by a separate kernel.
+// Acceptance: dE <= 0, else u53 * 2^-53 < exp(-dE / T) in double, u53 the
+// Philox draw of (replica seed, original bit, sweep).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "qb_device.cuh"
+#include "qb_internal.hpp"
+#include "qb_philox.cuh"
+#include "qb_qubo.hpp"
+
+namespace qb {
+
+namespace {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int kQThreads = 512;
+
+struct QuboArgs {
+    int n;
+    int n_colours;
+    int sweeps;
+    int refresh;
+    int R;
+    uint64_t seed0;
+    const int32_t* class_ptr;
+    const int32_t* row;
+    const int32_t* adj;
+    const float* J;
+    const float* h;
+    const int32_t* order;
+    const double* temp;
+    float* Lhi;                    // n x 64
+    float* Llo;                    // n x 64
+    unsigned long long* xw;        // n
+    unsigned long long* fw;        // n
+    unsigned* bar;
+    int* err;
+    uint8_t* x_out;                // R x n, original order
+    float* drift;                  // R
+    double* e_track;               // R: sum of accepted dE (E - offset)
+    unsigned long long* accepts;   // R
+};
+
+// hi + lo += v, the rounding error of the fp32 add carried into lo (Knuth's
+// TwoSum; no fused operations).
+__device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float v) {
+    const float s = __fadd_rn(hi, v);
+    const float bp = __fsub_rn(s, hi);
+    const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(v, bp));
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+
+__global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A) {
+    const int lane = int(threadIdx.x & 31u);
+    const int wpc = int(blockDim.x >> 5);
+    const int gw = int(blockIdx.x) * wpc + int(threadIdx.x >> 5);
+    const int tw = int(gridDim.x) * wpc;
+    const int r0 = lane, r1 = lane + 32;
+    const bool has0 = r0 < A.R, has1 = r1 < A.R;
+    const uint64_t seed_a = A.seed0 + uint64_t(r0), seed_b = A.seed0 + uint64_t(r1);
+    float eh0 = 0.0f, el0 = 0.0f, eh1 = 0.0f, el1 = 0.0f;
+    unsigned long long acc_a = 0, acc_b = 0;
+    float dr0 = 0.0f, dr1 = 0.0f;
+    unsigned round = 0;
+
+    for (int j = gw; j < A.n; j += tw) {
+        const float hj = A.h[j];
+        const size_t base = size_t(j) * 64;
+        A.Lhi[base + r0] = hj;
+        A.Lhi[base + r1] = hj;
+        A.Llo[base + r0] = 0.0f;
+        A.Llo[base + r1] = 0.0f;
+        if (lane == 0) {
+            A.xw[j] = 0ull;
+            A.fw[j] = 0ull;
+        }
+    }
+    bool ok = grid_barrier(A.bar, A.err, ++round);
+    for (int sweep = 0; sweep < A.sweeps && ok; ++sweep) {
+        const double T = A.temp[sweep];
+        const bool refresh = A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0;
+        for (int c = 0; c < A.n_colours && ok; ++c) {
+            const int c1 = A.class_ptr[c + 1];
+            for (int j = A.class_ptr[c] + gw; j < c1; j += tw) {
+                const size_t base = size_t(j) * 64;
+                float hi0 = __ldcg(A.Lhi + base + r0), lo0 = __ldcg(A.Llo + base + r0);
+                float hi1 = __ldcg(A.Lhi + base + r1), lo1 = __ldcg(A.Llo + base + r1);
+                double a0 = 0.0, a1 = 0.0;
+                if (refresh) a0 = a1 = double(__ldg(A.h + j));
+                const int k0 = __ldg(A.row + j), k1 = __ldg(A.row + j + 1);
+                for (int kb = k0; kb < k1; kb += 32) {
+                    // lane q fetches neighbour kb + q, then the warp walks them in order
+                    const int k = kb + lane;
+                    float Jk = 0.0f;
+                    unsigned long long f = 0ull, x = 0ull;
+                    if (k < k1) {
+                        const int nb = __ldg(A.adj + k);
+                        Jk = __ldg(A.J + k);
+                        f = __ldcg(A.fw + nb);
+                        if (f != 0ull || refresh) x = __ldcg(A.xw + nb);
+                    }
+                    // neighbours to walk in CSR order: those some replica flipped
+                    // (every one on a refresh sweep)
+                    unsigned todo = __ballot_sync(kFullMask, k < k1 && (f != 0ull || refresh));
+                    while (todo) {
+                        const int q = __ffs(todo) - 1;
+                        todo &= todo - 1u;
+                        const unsigned long long fq = __shfl_sync(kFullMask, f, q);
+                        const unsigned long long xq = __shfl_sync(kFullMask, x, q);
+                        const float Jq = __shfl_sync(kFullMask, Jk, q);
+                        if ((fq >> r0) & 1ull) two_sum_acc(hi0, lo0, ((xq >> r0) & 1ull) ? Jq : -Jq);
+                        if ((fq >> r1) & 1ull) two_sum_acc(hi1, lo1, ((xq >> r1) & 1ull) ? Jq : -Jq);
+                        if (refresh) {
+                            if ((xq >> r0) & 1ull) a0 += double(Jq);
+                            if ((xq >> r1) & 1ull) a1 += double(Jq);
+                        }
+                    }
+                }
+                if (refresh) {
+                    if (has0) dr0 = fmaxf(dr0, float(fabs(double(__fadd_rn(hi0, lo0)) - a0)));
+                    if (has1) dr1 = fmaxf(dr1, float(fabs(double(__fadd_rn(hi1, lo1)) - a1)));
+                    hi0 = float(a0);
+                    lo0 = float(a0 - double(hi0));
+                    hi1 = float(a1);
+                    lo1 = float(a1 - double(hi1));
+                }
+                const unsigned long long xj = __ldcg(A.xw + j);
+                const bool b0 = (xj >> r0) & 1ull, b1 = (xj >> r1) & 1ull;
+                const float L0 = __fadd_rn(hi0, lo0), L1 = __fadd_rn(hi1, lo1);
+                const float dE0 = b0 ? -L0 : L0, dE1 = b1 ? -L1 : L1;
+                const uint32_t oj = uint32_t(__ldg(A.order + j));
+                bool acc0 = false, acc1 = false;
+                if (has0)
+                    acc0 = dE0 <= 0.0f ||
+                           double(draw_u53(seed_a, oj, uint32_t(sweep), 0u)) * 0x1.0p-53 < exp(-double(dE0) / T);
+                if (has1)
+                    acc1 = dE1 <= 0.0f ||
+                           double(draw_u53(seed_b, oj, uint32_t(sweep), 0u)) * 0x1.0p-53 < exp(-double(dE1) / T);
+                const unsigned m0 = __ballot_sync(kFullMask, acc0), m1 = __ballot_sync(kFullMask, acc1);
+                const unsigned long long mask = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
+                if (lane == 0) {
+                    A.fw[j] = mask;
+                    A.xw[j] = xj ^ mask;
+                }
+                if (acc0) {
+                    two_sum_acc(eh0, el0, dE0);
+                    ++acc_a;
+                }
+                if (acc1) {
+                    two_sum_acc(eh1, el1, dE1);
+                    ++acc_b;
+                }
+                A.Lhi[base + r0] = hi0;
+                A.Llo[base + r0] = lo0;
+                A.Lhi[base + r1] = hi1;
+                A.Llo[base + r1] = lo1;
+            }
+            ok = grid_barrier(A.bar, A.err, ++round);
+        }
+    }
+    if (ok) {
+        for (int j = gw; j < A.n; j += tw) {
+            const unsigned long long xj = __ldcg(A.xw + j);
+            const size_t o = size_t(__ldg(A.order + j));
+            if (has0) A.x_out[size_t(r0) * size_t(A.n) + o] = uint8_t((xj >> r0) & 1ull);
+            if (has1) A.x_out[size_t(r1) * size_t(A.n) + o] = uint8_t((xj >> r1) & 1ull);
+        }
+    }
+    if (has0) {
+        if (dr0 > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[r0]), __float_as_int(dr0));
+        if (acc_a) atomicAdd(&A.accepts[r0], acc_a);
+        atomicAdd(&A.e_track[r0], double(eh0) + double(el0));
+    }
+    if (has1) {
+        if (dr1 > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[r1]), __float_as_int(dr1));
+        if (acc_b) atomicAdd(&A.accepts[r1], acc_b);
+        atomicAdd(&A.e_track[r1], double(eh1) + double(el1));
+    }
+}
+
+// E(x) = offset + sum_i h_i x_i + sum_e J_e x_u x_v in fp64 from scratch
+// (qubo_energy, src/check_ree_qubo.cu:158-163), one CTA per state, a fixed
+// reduction shape.
+__global__ void qubo_energy_kernel(const int32_t* eu, const int32_t* ev, const float* ew, int64_t m, const float* h,
+                                   int n, double offset, const uint8_t* X, double* e) {
+    __shared__ double red[256 / 32];
+    const uint8_t* x = X + size_t(blockIdx.x) * size_t(n);
+    double acc = 0.0;
+    for (int i = int(threadIdx.x); i < n; i += int(blockDim.x))
+        if (x[i]) acc += double(h[i]);
+    for (int64_t k = threadIdx.x; k < m; k += blockDim.x)
+        if (x[eu[k]] && x[ev[k]]) acc += double(ew[k]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+    if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = offset;
+        for (int q = 0; q < int(blockDim.x >> 5); ++q) t += red[q];
+        e[blockIdx.x] = t;
+    }
+}
+
+}  // namespace
+
+int qubo_lockstep_grid() {
+    int dev = 0, sms = 0, occ = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, qubo_lockstep_kernel, kQThreads, 0) != cudaSuccess) return 0;
+    return occ * sms;
+}
+
+int qubo_max_branches() { return 64; }
+
+size_t qubo_scratch(const QuboPlan& p) { return 64 + size_t(p.n) * 64 * 4 * 2 + size_t(p.n) * 16; }
+
+qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, int sweeps, int refresh, uint64_t seed0,
+                               cudaStream_t st) {
+    if (R < 1 || R > 64) return fail(QB_EINVAL, "qubo sweep: 1 to 64 replicas per launch");
+    const int grid = qubo_lockstep_grid();
+    if (grid < 1) return fail(QB_ENOTSUP, "qubo sweep: no co-resident grid on this device");
+    QuboArgs A{};
+    A.n = p.n;
+    A.n_colours = p.col.n_colours();
+    A.sweeps = sweeps;
+    A.refresh = refresh;
+    A.R = R;
+    A.seed0 = seed0;
+    A.class_ptr = p.d_class_ptr.as<int32_t>();
+    A.row = p.d_row.as<int32_t>();
+    A.adj = p.d_adj.as<int32_t>();
+    A.J = p.d_J.as<float>();
+    A.h = p.d_h.as<float>();
+    A.order = p.d_order.as<int32_t>();
+    A.temp = b.temp;
+    // scratch: control block (barrier counter, timeout flag at +16), fields, words
+    char* sc = static_cast<char*>(b.scratch);
+    A.bar = reinterpret_cast<unsigned*>(sc);
+    A.err = reinterpret_cast<int*>(sc + 16);
+    A.Lhi = reinterpret_cast<float*>(sc + 64);
+    A.Llo = A.Lhi + size_t(p.n) * 64;
+    A.xw = reinterpret_cast<unsigned long long*>(A.Llo + size_t(p.n) * 64);
+    A.fw = A.xw + p.n;
+    A.x_out = b.x;
+    A.drift = b.drift;
+    A.e_track = b.e_track;
+    A.accepts = b.accepts;
+    QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));   // the timeout flag is zeroed once per solve by the caller
+    void* args[] = {&A};
+    QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(qubo_lockstep_kernel), dim3(unsigned(grid)),
+                                        dim3(kQThreads), args, 0, st));
+    return QB_OK;
+}
+
+qb_status launch_qubo_energies(const QuboPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st) {
+    if (K == 0) return QB_OK;
+    qubo_energy_kernel<<<dim3(unsigned(K)), 256, 0, st>>>(p.d_eu.as<int32_t>(), p.d_ev.as<int32_t>(), p.d_ew.as<float>(),
+                                                        p.m, p.d_ho.as<float>(), p.n, p.offset, x, e);
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+}
+
+}  // namespace qb

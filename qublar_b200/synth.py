@@ -194,6 +194,80 @@ def build_request(spec):
     return random_regular(spec["n"], spec["degree"], spec["seed"])
 
 
+def lattice_qubo(L: int = 58, n_total: int = 200000, degree: float = 20.0, seed: int = 4242):
+    """The precision workload: a weighted QUBO on a periodic L^3 lattice (6
+    neighbours per site) plus n_total - L^3 extra sites, with random
+    long-range edges (uniform endpoints over all sites, no self-loops or
+    repeats) added until the average degree reaches `degree`; couplings and
+    linear terms N(0, 1) in fp32. Returns {n, eu, ev, ew, h, offset}."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    n_lat = L ** 3
+    n = max(int(n_total), n_lat)
+    idx = np.arange(n_lat).reshape(L, L, L)
+    parts = [np.stack([idx.ravel(), np.roll(idx, -1, axis=a).ravel()], 1) for a in range(3)]
+    lat = np.concatenate(parts)
+    lat = np.unique(np.sort(lat, axis=1), axis=0)
+    lat = lat[lat[:, 0] != lat[:, 1]]
+    m_target = int(round(n * degree / 2))
+    have = {int(a) * n + int(b) for a, b in lat}
+    extra = []
+    need = m_target - len(lat)
+    while need > 0:
+        cand = rng.integers(0, n, size=(int(need * 1.1) + 16, 2))
+        cand = cand[cand[:, 0] != cand[:, 1]]
+        cand = np.sort(cand, axis=1)
+        keys = cand[:, 0].astype(np.int64) * n + cand[:, 1]
+        keys, first = np.unique(keys, return_index=True)
+        for kk in keys.tolist():
+            if need == 0:
+                break
+            if kk not in have:
+                have.add(kk)
+                extra.append(kk)
+                need -= 1
+    ex = np.array(extra, dtype=np.int64)
+    eu = np.concatenate([lat[:, 0], ex // n]).astype(np.int32)
+    ev = np.concatenate([lat[:, 1], ex % n]).astype(np.int32)
+    ew = rng.standard_normal(eu.size).astype(np.float32)
+    h = rng.standard_normal(n).astype(np.float32)
+    return {"n": n, "eu": eu, "ev": ev, "ew": ew, "h": h, "offset": 0.0}
+
+
+def random_qubo(n: int, m: int, seed: int, scale: float = 1.0):
+    """A small weighted QUBO: m distinct random pairs, N(0, scale) couplings and
+    linear terms in fp32."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    keys = set()
+    eu, ev = [], []
+    while len(eu) < m:
+        a, b = (int(v) for v in rng.integers(0, n, size=2))
+        if a == b:
+            continue
+        k = (min(a, b), max(a, b))
+        if k in keys:
+            continue
+        keys.add(k)
+        eu.append(k[0])
+        ev.append(k[1])
+    return {"n": n, "eu": np.array(eu, np.int32), "ev": np.array(ev, np.int32),
+            "ew": (rng.standard_normal(m) * scale).astype(np.float32),
+            "h": (rng.standard_normal(n) * scale).astype(np.float32), "offset": 0.0}
+
+
+def qubo_pair_ray(q: dict) -> dict:
+    """The reference's pair-ray encoding of a weighted QUBO into a
+    BinaryProblem (to_engine, src/check_ree_qubo.cu:172-192): one ray per
+    coupling with d = 0, w = 1, a = sqrt|J| on u and sign(J) sqrt|J| on v, and
+    the field h corrected by -a^2/2 per ray end (a rounded to fp32)."""
+    n = int(q["n"])
+    eu, ev, ew = q["eu"], q["ev"], q["ew"]
+    h = q["h"] if q.get("h") is not None else np.zeros(n, np.float32)
+    pairs = [(int(eu[k]), int(ev[k])) for k in range(len(eu))]
+    Qd = np.asarray(h, np.float64)
+    Qo_vals = np.asarray(ew, np.float64)
+    return qubo_to_residual(n, Qd, pairs, Qo_vals)
+
+
 # ---- residual-form instances --------------------------------------------------------------------
 
 def exhaustive16():

@@ -1,0 +1,80 @@
+"""The weighted-QUBO sweep (compensated fp32 local fields, fp64 refresh) on
+the GPU, through the C ABI.
+
+Bit-exact: every branch equals the oracle's mirror of the sweep (same colour
+order, same CSR order of the pulled deltas, same TwoSum rounding, same Philox
+draws), and so does each branch's maximum field drift. fp64: final energies
+equal qubo_energy (check_ree_qubo.cu:158-163) to 1e-12 relative; the tracked
+energy (offset + sum of accepted fp32 dE) differs from it by < 1e-3 absolute
+on N(0,1) couplings. Statistical: final energies agree with the reference's
+own annealer run on the pair-ray encoding of the same QUBO (anneal_branch,
+ising_recon.hpp:121-144), Welch z < 4.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qublar_b200 import QuboProblem, Schedule, synth
+
+pytestmark = pytest.mark.gpu
+
+E_RTOL = 1e-12
+
+
+def _check(q, R, sched, offset=0):
+    P = QuboProblem.from_dict(q)
+    r = P.solve(sched, R, offset)
+    X, E, info = r.branches(), r.energies(), r.info()
+    order, cptr = P.colouring()
+    temps = O.temperatures(sched.t_hot, sched.t_cold, sched.anneal_sweeps, sched.hold_sweeps)
+    drifts = []
+    for b in range(R):
+        x, track, drift = O.qubo_anneal_coloured(q, order, cptr, temps, sched.refresh_sweeps, b + 1 + offset)
+        assert (X[b] == x).all(), b
+        drifts.append(drift)
+        e = O.qubo_energy(q, X[b])
+        assert abs(E[b] - e) <= E_RTOL * max(1.0, abs(e))
+    assert info.max_drift == pytest.approx(max(drifts), rel=0, abs=0)
+    assert info.max_energy_error < 1e-3
+    assert info.accepted > 0
+    return P, X, E
+
+
+def test_random_qubo_bit_exact():
+    _check(synth.random_qubo(300, 1500, 3), 16, Schedule(3.0, 0.05, 150, 20, 32))
+
+
+def test_two_launches_and_offsets_bit_exact():
+    q = synth.random_qubo(200, 900, 8)
+    q["offset"] = -3.5
+    _check(q, 70, Schedule(2.0, 0.1, 60, 10, 16), offset=5)   # 64 + 6 replicas
+
+
+def test_small_lattice_with_long_range_edges_bit_exact():
+    q = synth.lattice_qubo(L=10, n_total=1200, degree=20.0, seed=3)
+    _check(q, 32, Schedule(3.0, 0.05, 100, 10, 64))
+
+
+def test_device_energies_equal_the_oracle():
+    q = synth.random_qubo(150, 700, 13)
+    P = QuboProblem.from_dict(q)
+    X = (np.random.default_rng(1).random((50, 150)) < 0.5).astype(np.uint8)
+    e = P.energies(X)
+    for k in range(50):
+        ref = O.qubo_energy(q, X[k])
+        assert abs(e[k] - ref) <= E_RTOL * max(1.0, abs(ref))
+
+
+def test_final_energies_agree_with_the_reference_annealer():
+    if not O.ref_available():
+        pytest.skip("the compiled reference is not built")
+    q = synth.random_qubo(120, 600, 21)
+    sched = Schedule(3.0, 0.05, 200, 20, 64)
+    P = QuboProblem.from_dict(q)
+    r = P.solve(sched, 48)
+    e_gpu = r.energies()
+    rp = O.RefProblem(synth.qubo_pair_ray(q))
+    e_ref = np.array([O.qubo_energy(q, rp.anneal_branch(sched.t_hot, sched.t_cold, sched.anneal_sweeps,
+                                                         sched.hold_sweeps, s + 1)) for s in range(48)])
+    se = np.sqrt(e_gpu.var(ddof=1) / e_gpu.size + e_ref.var(ddof=1) / e_ref.size) + 1e-12
+    assert abs(e_gpu.mean() - e_ref.mean()) / se < 4.0

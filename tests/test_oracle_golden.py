@@ -185,3 +185,42 @@ def test_golden_reference_runs_present():
     G = np.load(os.path.join(GOLD, "ref_runs.npz"))
     assert G["er800_energy"].shape == (64,)
     assert G["tomo_small_frac"].shape[0] == int(G["tomo_small_n"])
+
+
+# ---- weighted QUBO ------------------------------------------------------------------
+
+def test_qubo_energy_restates_qubo_energy():
+    """orc_qubo_energy = offset + sum_i h_i x_i + sum_e J_e x_u x_v
+    (check_ree_qubo.cu:158-163) on random states, against a direct sum."""
+    q = synth.random_qubo(60, 200, 11)
+    q["offset"] = 1.25
+    rng = np.random.default_rng(2)
+    for _ in range(20):
+        x = (rng.random(60) < 0.5).astype(np.uint8)
+        want = q["offset"] + float(np.sum(q["h"].astype(np.float64) * x))
+        want += sum(float(q["ew"][k]) for k in range(200) if x[q["eu"][k]] and x[q["ev"][k]])
+        assert abs(O.qubo_energy(q, x) - want) <= 1e-12 * max(1.0, abs(want))
+
+
+def test_pair_ray_encoding_matches_the_qubo_within_the_fp32_bound():
+    """The reference anneals a weighted QUBO through its pair-ray
+    BinaryProblem (to_engine, check_ree_qubo.cu:172-192): its binary_energy
+    equals qubo_energy up to the fp32 rounding of a = sqrt|J| (KL-005)."""
+    q = synth.random_qubo(40, 150, 5)
+    arr = synth.qubo_pair_ray(q)
+    rng = np.random.default_rng(9)
+    bound = sum(abs(float(v)) for v in q["ew"]) * 2.0 ** -22 + 1e-9
+    for _ in range(20):
+        x = (rng.random(40) < 0.5).astype(np.uint8)
+        assert abs(O.binary_energy(arr, x) - O.qubo_energy(q, x)) <= bound
+
+
+def test_qubo_oracle_tracks_its_energy_and_drifts_little():
+    q = synth.random_qubo(200, 1200, 7)
+    order = np.arange(200, dtype=np.int32)   # any order with singleton classes is a valid sweep
+    cptr = np.arange(201, dtype=np.int32)
+    temps = O.temperatures(3.0, 0.05, 150, 20)
+    for seed in (1, 2):
+        x, track, drift = O.qubo_anneal_coloured(q, order, cptr, temps, 16, seed)
+        assert abs(track - O.qubo_energy(q, x)) < 1e-4
+        assert 0.0 <= drift < 1e-4
