@@ -344,6 +344,7 @@ def batch_cpu_baseline(graphs, items, R, S):
 
 # ---- serve: a Poisson request stream through the serving loop -----------------------------------
 
+SERVE_LOCKSTEP_BITS = 40000
 SERVE_WORKLOAD = ("Poisson request stream: N log-uniform 1,000..300,000, half tomography-style pyramids, half "
                   "sparse +-1 Max-Cut (d-regular, d 3..12), sweeps 500..5000, branches 8..32")
 
@@ -398,8 +399,11 @@ def run_serve(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
 
     def make(k):
+        # pyramids of 40,000 bits and more take the whole-device lockstep sweep
+        # (run exclusively); smaller ones one cluster per branch beside the rest
         if specs[k]["kind"] == "tomography":
-            return ResidualProblem.from_arrays(data[k], flags=OPT_DEFER_UPLOAD | OPT_RESID_CLUSTER)
+            fl = OPT_DEFER_UPLOAD | (0 if specs[k]["n"] >= SERVE_LOCKSTEP_BITS else OPT_RESID_CLUSTER)
+            return ResidualProblem.from_arrays(data[k], flags=fl)
         return IsingProblem(*data[k], flags=OPT_DEFER_UPLOAD)
 
     t0 = time.perf_counter()
@@ -463,6 +467,8 @@ def run_serve(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed (int32 / f32)",
         "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "requests": len(probs), "total_attempts": total,
+                   "policy": f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: whole-device lockstep sweep, run alone; "
+                             "smaller pyramids: one cluster per branch; Max-Cut: ticks of the packed kernel",
                    "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
         "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
                                   "p99_s": float(np.percentile(lat_sat, 99))}, **rates},
@@ -485,6 +491,173 @@ def run_serve(args):
     return 0
 
 
+# ---- qubo: the weighted fp32 lattice QUBO --------------------------------------------------------
+
+QUBO_WORKLOAD = ("weighted QUBO on a 58^3 periodic lattice + 4,888 extra sites with random long-range edges "
+                 "(N = 200,000, average degree 20), J and h ~ N(0,1) fp32, 64 replicas, 5000 sweeps T 3 -> 0.05, "
+                 "compensated fp32 fields with an fp64 refresh every 64 sweeps")
+
+
+def qubo_algorithmic_bytes(info, n, m, R, sweeps, refresh, accepted):
+    """Bytes per launch by the weighted formula: the CSR (4 B column + 4 B
+    coupling per directed entry) once per sweep for all 64 replicas, every
+    replica's compensated field (8 B) read and written and its bit words once
+    per sweep, each accepted flip's delta applied to its neighbours' fields
+    (d x 2 x 8 B), and the fp64 refreshes' extra CSR pass."""
+    nnz = 2 * m
+    d = nnz / n
+    tiles = (R + 63) // 64
+    per_sweep = nnz * 8 * tiles + R * n * (2 * 8 + 2 / 8)
+    refreshes = (sweeps - 1) // refresh if refresh > 0 else 0
+    return per_sweep * sweeps + accepted * d * 2 * 8 + refreshes * nnz * 8 * tiles
+
+
+def run_qubo(args):
+    from qublar_b200 import synth
+    t0 = time.perf_counter()
+    q = synth.lattice_qubo()
+    log(f"[qubo] built in {time.perf_counter() - t0:.1f} s")
+    import torch
+
+    from qublar_b200 import QuboProblem, Schedule
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    R, S = 64, 5000
+    sched = Schedule(3.0, 0.05, S - S // 10, S // 10, 64)
+    P = QuboProblem.from_dict(q, stream=stream)
+    n, m = int(q["n"]), int(q["eu"].size)
+    attempts = R * S * n
+    for _ in range(args.warmup):
+        r = P.solve(sched, R, stream=stream)
+        r.info()
+        r.close()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.synchronize()
+    sampler.start()
+    infos, energies = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        r = P.solve(sched, R, stream=stream)
+        infos.append(r.info())
+        energies.append(r.energies())
+        r.close()
+    clocks = sampler.stop()
+    total_ms = statistics.mean(i.total_ms for i in infos)
+    anneal_ms = statistics.mean(i.anneal_ms for i in infos)
+    value = attempts / (total_ms / 1e3)
+    # end to end: host arrays -> plan + upload -> solve -> fractions back
+    torch.cuda.synchronize()
+    e2e = []
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        Q = QuboProblem.from_dict(q, stream=stream)
+        r = Q.solve(sched, R, stream=stream)
+        p = r.marginals()
+        e2e.append(time.perf_counter() - t0)
+        r.close()
+        Q.close()
+    h2d = int(q["eu"].nbytes + q["ev"].nbytes + q["ew"].nbytes + q["h"].nbytes)
+    hbm, peak_kind = peaks()
+    acc = statistics.mean(i.accepted for i in infos)
+    alg = qubo_algorithmic_bytes(infos[0], n, m, R, S, sched.refresh_sweeps, acc)
+    achieved = alg / (anneal_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (compensated) + f64 refresh", "data": "synthetic",
+        "config": {"workload": QUBO_WORKLOAD, "bits": n, "edges": m, "replicas": R, "sweeps": S,
+                   "colours": int(P.info().n_colours), "refresh_sweeps": sched.refresh_sweeps,
+                   "l2": "flushed (256 MB write) before every timed step; state 106 MB", "parallelism": "1 GPU"},
+        "precision": {"max_field_drift": max(i.max_drift for i in infos),
+                      "max_energy_error": max(i.max_energy_error for i in infos),
+                      "mean_final_energy": float(np.mean(energies[-1])),
+                      "note": "drift: |compensated fp32 field - fp64 field| at refreshes; energy error: |offset + "
+                              "sum of accepted fp32 dE - fp64 energy from scratch|"},
+        "e2e": {"value": attempts / statistics.mean(e2e), "unit": "attempts/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": n * 4, "s_per_step": statistics.mean(e2e)},
+        "gpu_launches": sum(i.launches for i in infos),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": None, "kernel": "qubo_lockstep_kernel",
+                     "kernel_ms": anneal_ms, "algorithmic_bytes": alg, "accepted_flips": acc},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = qubo_cpu_baseline(q, sched)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def qubo_cpu_baseline(q, sched):
+    """The reference's anneal_branch on the pair-ray encoding of the same
+    QUBO (check_ree_qubo.cu:172-192, oracle/_ref) on the host's cores: 16
+    branches of a 40-sweep sample of the schedule (one ray per coupling)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    from qublar_b200 import synth
+    threads = os.cpu_count() or 1
+    arr = synth.qubo_pair_ray(q)
+    n = int(q["n"])
+    hold = 4
+    branches = min(16, threads)
+    if O.ref_available():
+        rp = O.RefProblem(arr)
+        _, _, wall = rp.branch_fractions(sched.t_hot, sched.t_cold, 40 - hold, hold, branches, threads, 0, keep=False)
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda b: O.anneal_branch(arr, sched.t_hot, sched.t_cold, 40 - hold, hold, b + 1),
+                        range(branches)))
+        wall = time.perf_counter() - t0
+        kind = "port"
+    return {"value": branches * 40 * n / wall, "unit": "attempts/s", "cores": threads, "kind": kind,
+            "sample": f"{branches} branches x 40 sweeps of the pair-ray encoding (one ray per coupling), "
+                      f"{threads} threads, {wall:.1f} s"}
+
+
+# ---- maxcut: the 800-node Erdos-Renyi graph ------------------------------------------------------
+
+def run_maxcut(args):
+    import torch
+
+    from qublar_b200 import Budget, IsingProblem, synth
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    n, eu, ev, ew = synth.erdos_renyi(800, 0.06, 1)
+    R, S = 16, 1000
+    sched = Budget(3.0, 0.05, S, 0, 0)
+    P = IsingProblem(n, eu, ev, ew, stream=stream)
+    for _ in range(args.warmup):
+        P.solve(sched, R, stream=stream).info()
+    infos, cuts = [], []
+    for _ in range(args.steps):
+        r = P.solve(sched, R, stream=stream)
+        infos.append(r.info())
+        cuts.append(-r.energies_tracked())
+        r.close()
+    total_ms = statistics.mean(i.total_ms for i in infos)
+    value = R * S * n / (total_ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "Max-Cut on ER(800, 0.06), w = +1, 16 replicas, 1000 sweeps T 3 -> 0.05",
+                       "edges": int(eu.size), "parallelism": "1 GPU"},
+            "best_cut": int(max(c.max() for c in cuts)), "mean_cut": float(np.mean(cuts[-1])),
+            "gpu_launches": sum(i.launches for i in infos)}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        if O.ref_available():
+            g = O.RefGraph(O.Graph(n, eu, ev, ew).rudy())
+            _, _, wall = g.anneal_many(3.0, 0.05, S, 0, 1, R, threads)
+            line["cpu_baseline"] = {"value": R * S * n / wall, "unit": "attempts/s", "cores": threads,
+                                    "kind": "reference", "sample": f"all {R} replicas, {threads} threads"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -495,9 +668,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps", type=int, default=250,
                     help="schedule length (default 250 = 200 + 50, the benchmark); shorter runs are for profiling only")
-    ap.add_argument("--workload", default="tomography", choices=["tomography", "batch", "serve"],
+    ap.add_argument("--workload", default="tomography", choices=["tomography", "batch", "serve", "qubo", "maxcut"],
                     help="tomography: the pyramid (default); batch: many Max-Cut instances in one persistent "
-                         "launch; serve: a Poisson request stream through the serving loop")
+                         "launch; serve: a Poisson request stream through the serving loop; qubo: the weighted "
+                         "fp32 lattice QUBO; maxcut: the 800-node ER graph")
     ap.add_argument("--instances", type=int, default=4096, help="batch: instances")
     ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch: sweeps per instance")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
@@ -506,6 +680,10 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "qubo":
+        return run_qubo(args)
+    if args.workload == "maxcut":
+        return run_maxcut(args)
     if args.impl == "reference":
         return run_reference(args)
 

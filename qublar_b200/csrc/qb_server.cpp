@@ -23,6 +23,7 @@
 #include "qb_batch.hpp"
 #include "qb_internal.hpp"
 #include "qb_kernels.hpp"
+#include "qb_qubo.hpp"
 
 using namespace qb;
 
@@ -73,8 +74,9 @@ struct Request {
     int64_t charge_work = 0;      // problem + working memory: returned when the request finishes
     int64_t charge_results = 0;   // results: returned when the client releases them
     bool cancel = false;
+    bool exclusive = false;       // a cooperative whole-device sweep: runs with nothing beside it
     // device memory (stream-ordered allocations)
-    DevBuf d_x, d_f, d_e, d_p, d_temp, d_state, d_drift, d_accepts, d_ef64;
+    DevBuf d_x, d_f, d_e, d_p, d_temp, d_state, d_drift, d_accepts, d_ef64, d_etrack;
     // ising progress
     std::vector<Group> groups;
     int cursor = 0;       // next sweep
@@ -115,6 +117,7 @@ struct qb_server {
     cudaGraphNode_t copy_node = nullptr;
     std::vector<Request*> running_ising;
     std::vector<Request*> running_resid;
+    Request* exclusive_run = nullptr;
     bool tick_inflight = false;
     std::vector<std::pair<Request*, int>> tick_members;   // request, sweep end of its slice
     std::string fatal;
@@ -148,6 +151,7 @@ void drop_work(qb_server* S, Request* r) {
     r->d_temp.release();
     r->d_drift.release();
     r->d_accepts.release();
+    r->d_etrack.release();
     if (r->done_ev) {
         cudaEventDestroy(r->done_ev);
         r->done_ev = nullptr;
@@ -169,7 +173,11 @@ int64_t ising_work_bytes(const qb_problem* p, int R, int sweeps) {
 }
 int64_t ising_result_bytes(int n, int R) { return int64_t(n) * R * 5 + int64_t(R) * 8 + int64_t(n) * 4; }
 int64_t resid_work_bytes(const qb_problem* p, int R, int sweeps) {
-    return p->device_bytes + int64_t(sweeps) * 8 + int64_t(R) * 12;
+    int64_t b = p->device_bytes + int64_t(sweeps) * 8 + int64_t(R) * 12;
+    if (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP)
+        b += int64_t(resid_lockstep_scratch(p->resid, std::min(R, resid_lockstep_max_branches())));
+    if (p->kind == QB_KIND_QUBO) b += int64_t(qubo_scratch(p->qubo)) + int64_t(R) * 8;
+    return b;
 }
 int64_t resid_result_bytes(int n, int R) { return int64_t(n) * R + int64_t(R) * 8 + int64_t(n) * 4; }
 
@@ -259,8 +267,74 @@ qb_status launch_resid(qb_server* S, Request* r) {
     return QB_OK;
 }
 
+// A whole-device cooperative sweep (lockstep residual or weighted QUBO), run
+// when nothing else runs on the device; its scratch lives in d_state.
+qb_status launch_exclusive(qb_server* S, Request* r) {
+    qb_status s;
+    const bool qubo = r->kind == QB_KIND_QUBO;
+    {
+        AsyncAllocScope scope(S->upload_stream);
+        if ((s = problem_upload(r->prob, S->upload_stream)) != QB_OK) return s;
+        const std::vector<double> temp = temperatures(r->sched);
+        if ((s = upload_vec(r->d_temp, temp, S->upload_stream))) return s;
+        const size_t scratch = qubo ? qubo_scratch(r->prob->qubo)
+                                    : resid_lockstep_scratch(r->prob->resid, std::min(r->R, resid_lockstep_max_branches()));
+        if ((s = r->d_state.alloc(scratch))) return s;
+        if ((s = r->d_x.alloc(size_t(r->R) * size_t(r->n)))) return s;
+        if ((s = r->d_drift.alloc(size_t(r->R) * 4))) return s;
+        if ((s = r->d_accepts.alloc(size_t(r->R) * 8))) return s;
+        if ((s = r->d_ef64.alloc(size_t(r->R) * 8))) return s;
+        if ((s = r->d_p.alloc(size_t(r->n) * 4))) return s;
+        if (qubo && (s = r->d_etrack.alloc(size_t(r->R) * 8))) return s;
+        QB_CUDA(cudaMemsetAsync(r->d_drift.p, 0, r->d_drift.bytes, S->upload_stream));
+        QB_CUDA(cudaMemsetAsync(r->d_accepts.p, 0, r->d_accepts.bytes, S->upload_stream));
+        if (qubo) QB_CUDA(cudaMemsetAsync(r->d_etrack.p, 0, r->d_etrack.bytes, S->upload_stream));
+        QB_CUDA(cudaMemsetAsync(r->d_state.p, 0, 64, S->upload_stream));   // barrier counter and timeout flag
+        QB_CUDA(cudaStreamSynchronize(S->upload_stream));   // `temp` is a local
+    }
+    cudaStream_t st = S->tick_stream;
+    uint8_t* x = r->d_x.as<uint8_t>();
+    if (qubo) {
+        const int RB = qubo_max_branches();
+        for (int b0 = 0; b0 < r->R; b0 += RB) {
+            QuboBuffers qb;
+            qb.x = x + size_t(b0) * size_t(r->n);
+            qb.temp = r->d_temp.as<double>();
+            qb.drift = r->d_drift.as<float>() + b0;
+            qb.e_track = r->d_etrack.as<double>() + b0;
+            qb.accepts = r->d_accepts.as<unsigned long long>() + b0;
+            qb.scratch = r->d_state.p;
+            if ((s = launch_qubo_lockstep(r->prob->qubo, qb, std::min(RB, r->R - b0), r->sweeps,
+                                          r->sched.refresh_sweeps, r->seed0 + uint64_t(b0), st)))
+                return s;
+        }
+        if ((s = launch_qubo_energies(r->prob->qubo, x, r->R, r->d_ef64.as<double>(), st))) return s;
+    } else {
+        const ResidualPlan& P = r->prob->resid;
+        const int RB = resid_lockstep_max_branches();
+        for (int b0 = 0; b0 < r->R; b0 += RB) {
+            SolveBuffers b;
+            b.x = x + size_t(b0) * size_t(r->n);
+            b.temp = r->d_temp.as<double>();
+            b.drift = r->d_drift.as<float>() + b0;
+            b.accepts = r->d_accepts.as<unsigned long long>() + b0;
+            b.scratch = r->d_state.p;
+            if ((s = launch_resid_lockstep(P, b, std::min(RB, r->R - b0), r->sweeps, r->sched.refresh_sweeps,
+                                           r->seed0 + uint64_t(b0), st)))
+                return s;
+        }
+        if ((s = launch_resid_energies(P, x, r->R, r->d_ef64.as<double>(), st))) return s;
+    }
+    if ((s = launch_marginals(x, r->R, r->n, r->d_p.as<float>(), st))) return s;
+    QB_CUDA(cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming));
+    QB_CUDA(cudaEventRecord(r->done_ev, st));
+    return QB_OK;
+}
+
 // Admits pending requests in arrival order while the budget and the active
-// limit allow (a request larger than the whole budget fails).
+// limit allow (a request larger than the whole budget fails). An exclusive
+// request waits at the head until the device is idle and holds back those
+// behind it while it runs.
 void admit_pending(qb_server* S) {
     for (;;) {
         Request* r = nullptr;
@@ -285,6 +359,8 @@ void admit_pending(qb_server* S) {
                 continue;
             }
             if (S->bytes_in_use + need > S->budget || S->active >= S->cfg.max_active) return;
+            if (S->exclusive_run) return;
+            if (q->exclusive && (S->tick_inflight || !S->running_ising.empty() || !S->running_resid.empty())) return;
             S->pending.pop_front();
             S->bytes_in_use += need;
             S->peak_bytes = std::max(S->peak_bytes, S->bytes_in_use);
@@ -293,7 +369,9 @@ void admit_pending(qb_server* S) {
             q->t_admit = now_s();
             r = q;
         }
-        const qb_status s = r->kind == QB_KIND_ISING ? admit_ising(S, r) : launch_resid(S, r);
+        const qb_status s = r->exclusive ? launch_exclusive(S, r)
+                            : r->kind == QB_KIND_ISING ? admit_ising(S, r)
+                                                       : launch_resid(S, r);
         if (s != QB_OK) {
             const std::string msg = qb_last_error();
             drop_work(S, r);
@@ -304,7 +382,8 @@ void admit_pending(qb_server* S) {
             finish_locked(S, r, QB_REQ_FAILED, s, msg);
             continue;
         }
-        if (r->kind == QB_KIND_ISING) S->running_ising.push_back(r);
+        if (r->exclusive) S->exclusive_run = r;
+        else if (r->kind == QB_KIND_ISING) S->running_ising.push_back(r);
         else S->running_resid.push_back(r);
     }
 }
@@ -511,6 +590,40 @@ void poll_resid(qb_server* S) {
     S->running_resid.swap(keep);
 }
 
+void poll_exclusive(qb_server* S) {
+    Request* r = S->exclusive_run;
+    if (!r) return;
+    cudaError_t e = cudaEventQuery(r->done_ev);
+    if (e == cudaErrorNotReady) return;
+    int timed_out = 0;
+    if (e == cudaSuccess) {
+        const cudaError_t c = cudaMemcpy(&timed_out, static_cast<const char*>(r->d_state.p) + 16, sizeof(int),
+                                         cudaMemcpyDeviceToHost);
+        if (c != cudaSuccess) e = c;
+    }
+    std::string msg;
+    if (e != cudaSuccess) {
+        cuda_fail(e, "exclusive request", __FILE__, __LINE__);
+        msg = qb_last_error();
+        S->fatal = msg;
+    }
+    S->exclusive_run = nullptr;
+    const bool cancelled = r->cancel;
+    drop_work(S, r);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (e != cudaSuccess || timed_out || cancelled) {
+        drop_results(r);
+        S->bytes_in_use -= r->charge_results;
+        r->charge_results = 0;
+        if (e != cudaSuccess) finish_locked(S, r, QB_REQ_FAILED, QB_ECUDA, msg);
+        else if (timed_out)
+            finish_locked(S, r, QB_REQ_FAILED, QB_ETIMEDOUT, "a grid barrier of the sweep timed out: no results");
+        else finish_locked(S, r, QB_REQ_CANCELLED, QB_ECANCELLED, "cancelled while running");
+    } else {
+        finish_locked(S, r, QB_REQ_DONE, QB_OK, "");
+    }
+}
+
 // Cancelled ising requests leave between ticks.
 void reap_cancelled_ising(qb_server* S) {
     std::vector<Request*> keep;
@@ -534,6 +647,7 @@ void worker_main(qb_server* S) {
     for (;;) {
         poll_resid(S);
         poll_tick(S);
+        poll_exclusive(S);
         if (!S->tick_inflight) reap_cancelled_ising(S);
         admit_pending(S);
         if (!S->tick_inflight && !S->running_ising.empty() && S->fatal.empty()) {
@@ -543,7 +657,7 @@ void worker_main(qb_server* S) {
             }
         }
         std::unique_lock<std::mutex> lk(S->mu);
-        const bool busy = S->tick_inflight || !S->running_resid.empty();
+        const bool busy = S->tick_inflight || !S->running_resid.empty() || S->exclusive_run != nullptr;
         if (S->stop && !busy && S->running_ising.empty()) break;
         if (busy) S->cv_work.wait_for(lk, std::chrono::microseconds(50), [&] { return S->kick; });
         else S->cv_work.wait(lk, [&] { return S->kick || S->stop; });
@@ -621,15 +735,15 @@ extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_sche
         !(sch->t_hot > 0.0) || !(sch->t_cold > 0.0) || !std::isfinite(sch->t_hot) || !std::isfinite(sch->t_cold) ||
         sch->refresh_sweeps < 0)
         return fail(QB_EINVAL, "qb_server_submit: bad schedule");
-    if (p->kind == QB_KIND_RESIDUAL && p->resid.variant != QB_RESID_CLUSTER)
-        return fail(QB_ENOTSUP, "qb_server_submit: residual problems must be planned with QB_OPT_RESID_CLUSTER");
+
     std::unique_ptr<Request> r(new (std::nothrow) Request());
     if (!r) return fail(QB_ENOMEM, "qb_server_submit: out of host memory");
     r->prob = p;
     r->sched = *sch;
     r->kind = p->kind;
     r->R = int(n_branches);
-    r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->resid.n;
+    r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
+    r->exclusive = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
     r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
     r->seed0 = 1 + seed_offset;
     if (p->kind == QB_KIND_ISING) {
@@ -729,7 +843,7 @@ qb_status result_copy(qb_server* S, uint64_t id, void* dst, const char* what, in
                 if (r->kind != QB_KIND_ISING) return fail(QB_EINVAL, std::string(what) + ": ising requests only");
                 src = r->d_e.p; bytes = size_t(r->R) * 8; break;
             default:
-                if (r->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, std::string(what) + ": residual requests only");
+                if (r->kind == QB_KIND_ISING) return fail(QB_EINVAL, std::string(what) + ": residual or qubo requests only");
                 src = r->d_ef64.p; bytes = size_t(r->R) * 8; break;
         }
         if (!src) return fail(QB_EINVAL, std::string(what) + ": the results were released");

@@ -14,8 +14,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, QBError, ResidualProblem, Schedule,
-                         Server, synth)
+from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, QBError, QuboProblem, ResidualProblem,
+                         Schedule, Server, synth)
 from qublar_b200._abi import REQ_CANCELLED, REQ_DONE
 
 pytestmark = pytest.mark.gpu
@@ -203,6 +203,36 @@ def test_graph_and_direct_ticks_agree():
         assert S.stats().ticks > 1
         S.close()
     assert (out[0] == out[1]).all()
+
+
+def test_exclusive_requests_beside_ticks_are_the_same_alone():
+    """A lockstep-planned pyramid and a weighted QUBO run as whole-device
+    sweeps with nothing beside them; ising requests submitted around them
+    still finish, and every result equals its solve alone."""
+    pyr = synth.tomography(synth.small_tomo_params(0.2, 24))
+    q = synth.random_qubo(400, 2500, 17)
+    g1, g2 = synth.random_regular(2000, 8, 5), synth.torus_pm1(40, 2)
+    sp, sq, si = Schedule(50.0, 1.0, 60, 15, 25), Schedule(3.0, 0.05, 120, 10, 32), Schedule(3.0, 0.05, 200, 0, 0)
+    P1 = IsingProblem(*g1, flags=DEFER)
+    Pp = ResidualProblem.from_arrays(pyr, flags=DEFER)       # lockstep plan: exclusive
+    Pq = QuboProblem.from_dict(q, flags=DEFER)                # exclusive
+    P2 = IsingProblem(*g2, flags=DEFER)
+    S = Server()
+    ids = [S.submit(P1, si, 16, 1), S.submit(Pp, sp, 20, 2), S.submit(Pq, sq, 40, 3), S.submit(P2, si, 8, 4)]
+    for i in ids:
+        S.wait(i, 120000)
+    infos = [S.info(i) for i in ids]
+    # nothing overlaps an exclusive request
+    for k in (1, 2):
+        for j in range(4):
+            if j != k:
+                assert infos[j].t_done <= infos[k].t_admit or infos[j].t_admit >= infos[k].t_done
+    alone = [IsingProblem(*g1).solve(si, 16, 1), ResidualProblem.from_arrays(pyr).solve(sp, 20, 2),
+             QuboProblem.from_dict(q).solve(sq, 40, 3), IsingProblem(*g2).solve(si, 8, 4)]
+    for rid, r in zip(ids, alone):
+        assert (S.branches(rid) == r.branches()).all()
+    np.testing.assert_allclose(S.energies(ids[2]), alone[2].energies(), rtol=1e-12)
+    S.close()
 
 
 def test_submissions_from_several_threads():
