@@ -234,8 +234,13 @@ def run_batch(args):
     log(f"[batch] planned and uploaded in {time.perf_counter() - t0:.1f} s")
     items = [(P, P.scaled_schedule(S, 0), R, 0) for P in probs]
     attempts = sum(R * S * P.n for P in probs)
-    cfg = autotune_batch(items, 8)
-    log(f"[batch] tuned shape: {cfg.threads} threads, {cfg.smem_bytes} B, groups of {cfg.max_group}")
+    if args.shape:
+        from qublar_b200._abi import BatchConfig
+        t_, s_, g_ = (int(v) for v in args.shape.split(","))
+        cfg = BatchConfig(t_, s_, g_, 0)
+    else:
+        cfg = autotune_batch(items, 8)
+    log(f"[batch] shape: {cfg.threads} threads, {cfg.smem_bytes} B, groups of {cfg.max_group}")
     for _ in range(args.warmup):
         B = solve_batch(items, cfg, stream=stream)
         B.info()
@@ -254,6 +259,10 @@ def run_batch(args):
     total_ms = statistics.mean(i.total_ms for i in infos)
     anneal_ms = statistics.mean(i.anneal_ms for i in infos)
     value = attempts / (total_ms / 1e3)
+    if args.kernel_only:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "attempts/s", "kernel_ms": anneal_ms,
+                          "config": {"instances": len(probs), "sweeps": S, "work_items": infos[0].work_items}}))
+        return 0
     # plain form: one qb_solve per instance, on a size-stratified sample
     order = sorted(range(len(probs)), key=lambda k: probs[k].n)
     sample = [order[int(j)] for j in np.linspace(0, len(order) - 1, min(64, len(order)))]
@@ -493,6 +502,11 @@ def run_serve(args):
 
 # ---- qubo: the weighted fp32 lattice QUBO --------------------------------------------------------
 
+# DRAM bytes (read + write) per sweep of qubo_lockstep_kernel from the
+# committed ncu capture of a 100-sweep launch on the same 200,000-bit QUBO with
+# 64 replicas (profiles/qubo_lockstep_lattice.md): the replicas' compensated
+# fields stream once per sweep, so a full launch moves this times its sweeps.
+QUBO_NCU_TRAFFIC_PER_SWEEP = (13.331829e9 + 10.152890e9) / 100
 QUBO_WORKLOAD = ("weighted QUBO on a 58^3 periodic lattice + 4,888 extra sites with random long-range edges "
                  "(N = 200,000, average degree 20), J and h ~ N(0,1) fp32, 64 replicas, 5000 sweeps T 3 -> 0.05, "
                  "compensated fp32 fields with an fp64 refresh every 64 sweeps")
@@ -522,7 +536,7 @@ def run_qubo(args):
     from qublar_b200 import QuboProblem, Schedule
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     stream = torch.cuda.current_stream()
-    R, S = 64, 5000
+    R, S = 64, args.qubo_sweeps
     sched = Schedule(3.0, 0.05, S - S // 10, S // 10, 64)
     P = QuboProblem.from_dict(q, stream=stream)
     n, m = int(q["n"]), int(q["eu"].size)
@@ -546,6 +560,10 @@ def run_qubo(args):
     total_ms = statistics.mean(i.total_ms for i in infos)
     anneal_ms = statistics.mean(i.anneal_ms for i in infos)
     value = attempts / (total_ms / 1e3)
+    if args.kernel_only:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "attempts/s", "kernel_ms": anneal_ms,
+                          "config": {"bits": n, "replicas": R, "sweeps": S}}))
+        return 0
     # end to end: host arrays -> plan + upload -> solve -> fractions back
     torch.cuda.synchronize()
     e2e = []
@@ -578,7 +596,7 @@ def run_qubo(args):
                 "d2h_bytes_per_step": n * 4, "s_per_step": statistics.mean(e2e)},
         "gpu_launches": sum(i.launches for i in infos),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": peak_kind, "traffic": None, "kernel": "qubo_lockstep_kernel",
+                     "peak_kind": peak_kind, "traffic": QUBO_NCU_TRAFFIC_PER_SWEEP * S, "kernel": "qubo_lockstep_kernel",
                      "kernel_ms": anneal_ms, "algorithmic_bytes": alg, "accepted_flips": acc},
         "clocks": clocks,
     }
@@ -675,6 +693,11 @@ def main():
     ap.add_argument("--instances", type=int, default=4096, help="batch: instances")
     ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch: sweeps per instance")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
+    ap.add_argument("--shape", default=None,
+                    help="batch: fixed packed-kernel shape 'threads,smem_bytes,max_group' instead of autotuning")
+    ap.add_argument("--qubo-sweeps", type=int, default=5000, help="qubo: sweeps (shorter runs are for profiling)")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="batch/qubo: time the kernel only (no plain-form, end-to-end or CPU legs; for profiling)")
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)
