@@ -1,6 +1,10 @@
 // The C ABI (include/qublar.h): validation, planning, upload, solve, results.
 #include <algorithm>
 #include <climits>
+#include <functional>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -346,24 +350,29 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     P.ray_slots = (nr + CL - 1) / CL;
     const int S = P.variant == QB_RESID_LOCKSTEP ? P.lock_grid : CL;   // slices per class
     const int heavy = resid_heavy_entries();
-    // balanced slices
-    std::vector<int32_t> slice_ptr(size_t(nc) * size_t(S + 1), 0);   // per class: CL + 1 offsets
+    // balanced slices: per class, longest-processing-time first onto the
+    // least-loaded slice (a min-heap of loads); classes are independent
+    std::vector<int32_t> slice_ptr(size_t(nc) * size_t(S + 1), 0);   // per class: S + 1 offsets
+#pragma omp parallel
     {
-        std::vector<int32_t> mem, slot_of;
+        std::vector<int32_t> mem;
         std::vector<std::vector<int32_t>> slices(static_cast<size_t>(S));
-        std::vector<int64_t> load(static_cast<size_t>(S));
+        std::vector<std::pair<int64_t, int>> heap;
+#pragma omp for schedule(dynamic, 1)
         for (int c = 0; c < nc; ++c) {
             const int cs = C.class_ptr[size_t(c)], ce = C.class_ptr[size_t(c) + 1];
             mem.assign(C.order.begin() + cs, C.order.begin() + ce);
             std::stable_sort(mem.begin(), mem.end(), [&](int a, int b) { return deg(a) > deg(b); });
             for (auto& v : slices) v.clear();
-            std::fill(load.begin(), load.end(), 0);
+            heap.clear();
+            for (int t = 0; t < S; ++t) heap.emplace_back(0, t);   // (load, slice): smallest first
+            std::make_heap(heap.begin(), heap.end(), std::greater<std::pair<int64_t, int>>());
             for (int i : mem) {
-                int t = 0;
-                for (int u = 1; u < S; ++u)
-                    if (load[size_t(u)] < load[size_t(t)]) t = u;
-                slices[size_t(t)].push_back(i);
-                load[size_t(t)] += deg(i) + 8;
+                std::pop_heap(heap.begin(), heap.end(), std::greater<std::pair<int64_t, int>>());
+                auto& top = heap.back();
+                slices[size_t(top.second)].push_back(i);
+                top.first += deg(i) + 8;
+                std::push_heap(heap.begin(), heap.end(), std::greater<std::pair<int64_t, int>>());
             }
             int pos = cs;
             for (int t = 0; t < S; ++t) {
@@ -377,8 +386,8 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
             }
             slice_ptr[size_t(c) * (S + 1) + size_t(S)] = pos;
         }
-        for (int k = 0; k < n; ++k) C.inverse[size_t(C.order[size_t(k)])] = k;
     }
+    for (int k = 0; k < n; ++k) C.inverse[size_t(C.order[size_t(k)])] = k;
     const bool lock = P.variant == QB_RESID_LOCKSTEP;
     // homes (cluster variant): bit k of slice t of class c -> (t << 27) |
     // running slot of CTA t
@@ -396,14 +405,20 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         }
     P.bit_slots = *std::max_element(used.begin(), used.end());
     if (!lock && P.bit_slots >= (1 << 27)) return fail(QB_EREFUSED, "residual: too many bits per CTA");
-    // sweep-order arrays
+    // sweep-order arrays: offsets first, then every bit's entries in parallel
     P.h_row.assign(size_t(n) + 1, 0);
-    P.h_ent.assign(size_t(P.nnz) * 4, 0u);
-    P.h_lin.assign(size_t(n), 0.0f);
-    P.h_q.assign(size_t(n), 0.0f);
     P.h_nbr_ptr.assign(size_t(n) + 1, 0);
-    P.h_nbr_home.assign(size_t(P.n_nbr), 0u);
-    P.h_nbr_new.assign(size_t(P.n_nbr), 0);
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        P.h_row[size_t(k) + 1] = P.h_row[size_t(k)] + (d->row_ptr[i + 1] - d->row_ptr[i]);
+        P.h_nbr_ptr[size_t(k) + 1] = P.h_nbr_ptr[size_t(k)] + (d->nbr_ptr[i + 1] - d->nbr_ptr[i]);
+    }
+    P.h_ent.resize(size_t(P.nnz) * 4);
+    P.h_lin.resize(size_t(n));
+    P.h_q.resize(size_t(n));
+    P.h_nbr_home.resize(size_t(P.n_nbr));
+    P.h_nbr_new.resize(size_t(P.n_nbr));
+#pragma omp parallel for schedule(static, 1024)
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
         int32_t pos = P.h_row[size_t(k)];
@@ -411,13 +426,14 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
             const float a = d->a[e];
             const float wa = float(d->w[d->ray[e]]) * a;   // the fp32 scatter increment
-            P.h_ent[size_t(pos) * 4 + 0] = uint32_t(d->ray[e]);
-            std::memcpy(&P.h_ent[size_t(pos) * 4 + 1], &a, 4);
-            std::memcpy(&P.h_ent[size_t(pos) * 4 + 2], &wa, 4);
+            uint32_t* en = &P.h_ent[size_t(pos) * 4];
+            en[0] = uint32_t(d->ray[e]);
+            std::memcpy(&en[1], &a, 4);
+            std::memcpy(&en[2], &wa, 4);
+            en[3] = 0u;
             qd += 0.5 * d->w[d->ray[e]] * double(a) * double(a);
             ++pos;
         }
-        P.h_row[size_t(k) + 1] = pos;
         P.h_q[size_t(k)] = float(qd);
         P.h_lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
         int32_t np = P.h_nbr_ptr[size_t(k)];
@@ -425,10 +441,10 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
             P.h_nbr_new[size_t(np)] = C.inverse[size_t(d->nbr[e])];
             P.h_nbr_home[size_t(np++)] = P.bit_home[size_t(C.inverse[size_t(d->nbr[e])])];
         }
-        P.h_nbr_ptr[size_t(k) + 1] = np;
     }
     if (lock) {
         P.h_meta.assign(size_t(n) * 8, 0u);
+#pragma omp parallel for schedule(static, 4096)
         for (int k = 0; k < n; ++k) {
             uint32_t* m = &P.h_meta[size_t(k) * 8];
             m[0] = uint32_t(P.h_row[size_t(k)]);
@@ -495,21 +511,56 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     const Colouring& C = P.col;
     // ray-major CSR, bits ascending in input order inside a ray: the refresh
     // (bits by home) and the energy verifier (bits by input index)
+    // counting sort by ray, split over threads by contiguous bit ranges: each
+    // thread counts its bits per ray, the counts are prefix-summed across
+    // threads, and each thread fills its own offsets (ascending bits per ray)
     std::vector<int32_t> rrow(size_t(nr) + 1, 0);
-    for (int64_t e = 0; e < P.nnz; ++e) rrow[size_t(d->ray[e]) + 1]++;
-    for (int b = 0; b < nr; ++b) rrow[size_t(b) + 1] += rrow[size_t(b)];
-    std::vector<int32_t> rfill(rrow.begin(), rrow.end() - 1), rbit_o(static_cast<size_t>(P.nnz));
+    std::vector<int32_t> rbit_o(static_cast<size_t>(P.nnz));
     std::vector<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
     std::vector<int32_t> rbit_n(static_cast<size_t>(P.nnz));
     std::vector<float> ra(static_cast<size_t>(P.nnz));
-    for (int i = 0; i < n; ++i)
-        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
-            const int32_t k = rfill[size_t(d->ray[e])]++;
-            rbit_o[size_t(k)] = i;
-            rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
-            rbit_n[size_t(k)] = C.inverse[size_t(i)];
-            ra[size_t(k)] = d->a[e];
+    {
+        int T = 1;
+#ifdef _OPENMP
+        T = std::max(1, std::min(omp_get_max_threads(), 32));
+#endif
+        std::vector<std::vector<int32_t>> cnt(static_cast<size_t>(T));
+        auto bits_of = [&](int t, int* i0, int* i1) {
+            *i0 = int(int64_t(n) * t / T);
+            *i1 = int(int64_t(n) * (t + 1) / T);
+        };
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            int i0, i1;
+            bits_of(t, &i0, &i1);
+            auto& c = cnt[size_t(t)];
+            c.assign(size_t(nr), 0);
+            for (int e = d->row_ptr[i0]; e < d->row_ptr[i1]; ++e) c[size_t(d->ray[e])]++;
         }
+        for (int b = 0; b < nr; ++b) {
+            int32_t run = rrow[size_t(b)];
+            for (int t = 0; t < T; ++t) {
+                const int32_t v = cnt[size_t(t)][size_t(b)];
+                cnt[size_t(t)][size_t(b)] = run;   // this thread's first slot on ray b
+                run += v;
+            }
+            rrow[size_t(b) + 1] = run;
+        }
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            int i0, i1;
+            bits_of(t, &i0, &i1);
+            auto& fill = cnt[size_t(t)];
+            for (int i = i0; i < i1; ++i)
+                for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
+                    const int32_t k = fill[size_t(d->ray[e])]++;
+                    rbit_o[size_t(k)] = i;
+                    rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
+                    rbit_n[size_t(k)] = C.inverse[size_t(i)];
+                    ra[size_t(k)] = d->a[e];
+                }
+        }
+    }
     std::vector<double> o_lin(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) o_lin[size_t(i)] = d->field ? d->field[i] : d->kappa;
     qb_status s;
