@@ -79,6 +79,20 @@ typedef struct qb_ising_desc {
     const int32_t* ew;
 } qb_ising_desc;
 
+/* A graph read from rudy / G-set text: the input format of the reference's
+ * integer engine. qb_parse_rudy replaces parse_rudy
+ * (src/ising_weighted.hpp:83-149): header "n m", then m lines "u v [w]",
+ * 1-based, w = +1 when absent; it refuses what parse_rudy refuses, with the
+ * same reason in qb_last_error (bad header, a token that is not an integer, a
+ * weight outside int32, a trailing token, a vertex out of range, a self-loop,
+ * an edge count that differs from the header, a duplicate edge).
+ * qb_graph_desc points a descriptor at the graph's arrays (valid until
+ * qb_graph_destroy) for qb_problem_create_ising. Host only. */
+typedef struct qb_graph qb_graph;
+qb_status qb_parse_rudy(const char* text, size_t size, qb_graph** out);
+qb_status qb_graph_desc(const qb_graph* g, qb_ising_desc* desc);
+void qb_graph_destroy(qb_graph* g);
+
 /* Residual-form QUBO; replaces argos::BinaryProblem (src/engine.hpp:30-49):
  *   E(x) = 1/2 sum_b w_b (sum_v a_bv x_v - d_b)^2
  *        + lambda sum_<uv> [x_u != x_v] + sum_v lin_v x_v,

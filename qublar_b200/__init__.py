@@ -29,7 +29,7 @@ from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_R
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
-           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER"]
+           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "parse_rudy"]
 
 
 @dataclass
@@ -273,6 +273,23 @@ class QuboProblem(_Problem):
         e = np.empty(X.shape[0], dtype=np.float64)
         check(lib().qb_energies_qubo(self._h, ptr(X), int(X.shape[0]), ptr(e)))
         return e
+
+
+def parse_rudy(text):
+    """(n, eu, ev, ew) of rudy / G-set text (parse_rudy, ising_weighted.hpp:83-149),
+    0-based; raises QBError with the reference's refusal reason."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    h = C.c_void_p()
+    check(lib().qb_parse_rudy(data, len(data), C.byref(h)))
+    try:
+        d = IsingDesc()
+        check(lib().qb_graph_desc(h, C.byref(d)))
+        m = int(d.m)
+        arr = lambda p_: np.ctypeslib.as_array(C.cast(p_, C.POINTER(C.c_int32)), shape=(m,)).copy() if m else \
+            np.zeros(0, np.int32)
+        return int(d.n), arr(d.eu), arr(d.ev), arr(d.ew)
+    finally:
+        lib().qb_graph_destroy(h)
 
 
 # ---- batches: many ising instances in one persistent launch --------------------------------

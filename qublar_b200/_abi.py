@@ -165,6 +165,9 @@ SIGNATURES = {
     "qb_server_release": (C.c_int, [_P, C.c_uint64]),
     "qb_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "qb_server_destroy": (None, [_P]),
+    "qb_parse_rudy": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(_P)]),
+    "qb_graph_desc": (C.c_int, [_P, C.POINTER(IsingDesc)]),
+    "qb_graph_destroy": (None, [_P]),
     "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),

@@ -87,22 +87,29 @@ Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32
     std::vector<int32_t> vis(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
     std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) { return conf[size_t(a)] > conf[size_t(b)]; });
+    int top = -1;   // highest colour given so far: words above (top >> 6) + 1 are empty
     for (int i : vis) {
         for (;;) {
-            forbid.assign(size_t(words), 0);
+            const int nw = std::min(words, ((top + 1) >> 6) + 1);   // words that can hold a used colour, plus the next
+            forbid.assign(size_t(nw), 0);
             for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
                 const uint64_t* u = &used[size_t(ray[k]) * size_t(words)];
-                for (int q = 0; q < words; ++q) forbid[size_t(q)] |= u[q];
+                for (int q = 0; q < nw; ++q) forbid[size_t(q)] |= u[q];
             }
             for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
                 const int cj = c.colour[size_t(nbr[k])];
-                if (cj >= 0 && cj < 64 * words) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
+                if (cj >= 0 && cj < 64 * nw) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
             }
             int cc = -1;
-            for (int q = 0; q < words && cc < 0; ++q)
+            for (int q = 0; q < nw && cc < 0; ++q)
                 if (~forbid[size_t(q)]) cc = 64 * q + __builtin_ctzll(~forbid[size_t(q)]);
-            if (cc < 0) { grow(words * 2); continue; }
+            if (cc < 0) {
+                if (nw == words) grow(words * 2);
+                top = std::max(top, 64 * nw - 1);   // widen the scan to the next word
+                continue;
+            }
             c.colour[size_t(i)] = cc;
+            top = std::max(top, cc);
             for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
                 used[size_t(ray[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
             break;

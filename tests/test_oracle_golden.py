@@ -224,3 +224,62 @@ def test_qubo_oracle_tracks_its_energy_and_drifts_little():
         x, track, drift = O.qubo_anneal_coloured(q, order, cptr, temps, 16, seed)
         assert abs(track - O.qubo_energy(q, x)) < 1e-4
         assert 0.0 <= drift < 1e-4
+
+
+# ---- rudy / G-set reader ---------------------------------------------------------------
+
+RUDY_CASES = [
+    "3 2\n1 2\n2 3 -5\n",                 # missing weight = +1
+    "  4 3\n\n1 2 7\n3 4\n\n2 3 -1\n",   # blank lines
+    "3 2\r\n1 2 1\r\n2 3 1\r\n",         # CR LF
+    "3 1\n1 2 1.5\n",                    # real weight
+    "3 1\n1 2 1 9\n",                    # trailing token
+    "3 1\n1 4\n",                        # out of range
+    "3 1\n0 2\n",                        # out of range (0-based)
+    "3 1\n2 2\n",                        # self-loop
+    "3 2\n1 2\n",                        # count mismatch
+    "3 2\n1 2\n2 1\n",                   # duplicate, reversed
+    "x 2\n",                             # bad n
+    "3\n1 2\n",                          # m missing on the header line
+    "3 1\n1\n",                          # missing v
+    "3 1\n1 a\n",                        # bad v
+    "3 1\n1 2 3000000000\n",             # weight beyond int32
+    "3 1\n1 2 +4\n",                     # explicit sign
+    "3 0\n",                             # no edges
+]
+
+
+@pytest.mark.parametrize("text", RUDY_CASES)
+def test_rudy_reader_matches_the_reference_loader(text):
+    """qb_parse_rudy accepts and refuses what parse_rudy (ising_weighted.hpp:83-149,
+    compiled from the reference) does, with the same reason; accepted graphs
+    give the same cut on random states."""
+    if not O.ref_available():
+        pytest.skip("the compiled reference is not built")
+    from qublar_b200 import QBError, parse_rudy
+    ref_err, ours_err = None, None
+    try:
+        rg = O.RefGraph(text.encode())
+    except ValueError as e:
+        ref_err = str(e)
+    try:
+        n, eu, ev, ew = parse_rudy(text)
+    except QBError as e:
+        ours_err = e.message
+    assert ours_err == ref_err
+    if ref_err is None:
+        assert n == rg.n and eu.size == rg.m
+        g = O.Graph(n, eu, ev, ew)
+        rng = np.random.default_rng(1)
+        for _ in range(8):
+            x = (rng.random(n) < 0.5).astype(np.uint8)
+            assert g.cut(x) == rg.cut(x)
+
+
+def test_rudy_reader_round_trips_generated_graphs():
+    from qublar_b200 import parse_rudy
+    for gen in (synth.random_sparse(300, 2000, 3, 1000), synth.erdos_renyi(200, 0.1, 2)):
+        n, eu, ev, ew = gen
+        text = O.Graph(n, eu, ev, ew).rudy()
+        n2, eu2, ev2, ew2 = parse_rudy(text)
+        assert n2 == n and (eu2 == eu).all() and (ev2 == ev).all() and (ew2 == ew).all()
