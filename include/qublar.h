@@ -449,6 +449,50 @@ qb_status qb_server_stats_get(qb_server* s, qb_server_stats* st);
 /* Cancels what is pending, waits for what runs, stops the worker. */
 void qb_server_destroy(qb_server* s);
 
+/* ---- provable-rock freezing --------------------------------------------------
+ *
+ * freeze_provable_rock (src/ising_recon.hpp:168-235) on the device: every bit
+ * whose 0 -> 1 flip costs at least `margin` whatever the other bits do
+ * (bound: sum_b w_b a (a/2 - d_b) + lin + lambda (#frozen - #free
+ * neighbours)) is fixed at 0, repeated to a fixpoint; the reduced problem
+ * keeps the other bits (in order) with the bonds to frozen rock folded into
+ * their field. The frozen set and the reduced problem equal the reference's
+ * (the fixpoint does not depend on the visiting order when lambda >= 0, which
+ * is required); `rounds` counts the device's parallel rounds. The reduced
+ * problem's arrays live in the handle (valid until qb_freeze_destroy); pass
+ * them to qb_problem_create_residual and map results back through `kept`
+ * (reduced bit -> original bit; every other bit is 0). */
+typedef struct qb_freeze qb_freeze;
+qb_status qb_freeze_rock(const qb_residual_desc* desc, double margin, const qb_opts* opts, qb_freeze** out);
+qb_status qb_freeze_info(const qb_freeze* f, int32_t* n_kept, int32_t* rounds);
+qb_status qb_freeze_kept(const qb_freeze* f, int32_t* kept);
+qb_status qb_freeze_reduced(const qb_freeze* f, qb_residual_desc* reduced);
+void qb_freeze_destroy(qb_freeze* f);
+
+/* ---- exact local posterior of a region ------------------------------------
+ *
+ * qb_roi_qubo: the conditional QUBO of the region roi[0..n_roi) of a
+ * residual-form problem, every other bit held at x_bar (roi_qubo,
+ * src/ising_recon.hpp:240-300): E(x_R) - E(0_R) = sum_i h_i x_i +
+ * sum_{i<j} J_ij x_i x_j, h of n_roi and J of n_roi x n_roi (upper triangle
+ * used), equal to the reference's bit for bit. Host only.
+ * qb_enumerate_qubo: every one of the 2^n states (n <= 34) of a dense QUBO
+ * on the device, at temperature T: log Z, the exact marginals p(x_i = 1)
+ * (into marginals[n]), the mean energy and the ground state (bit i of x_min =
+ * x_i; the first found on ties). The reference exports the region's QUBO for
+ * other tools; here it is enumerated. */
+typedef struct qb_enum_result {
+    double log_z;
+    double e_min;
+    uint64_t x_min;
+    double mean_energy;
+    uint64_t states;
+} qb_enum_result;
+qb_status qb_roi_qubo(const qb_residual_desc* p, const int32_t* roi, int32_t n_roi, const uint8_t* x_bar, double* h,
+                      double* J);
+qb_status qb_enumerate_qubo(int32_t n, const double* h, const double* J, double T, const qb_opts* opts,
+                            qb_enum_result* out, double* marginals);
+
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
 qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);

@@ -98,6 +98,8 @@ def ref() -> C.CDLL:
             "ref_anneal_branch": (None, [P, D, D, C.c_int, C.c_int, U64, P]),
             "ref_branch_fractions": (D, [P, D, D, C.c_int, C.c_int, C.c_int, C.c_uint, U64, P, P]),
             "ref_anneal_branch_trace": (None, [P, D, D, C.c_int, C.c_int, U64, P, P]),
+            "ref_freeze": (C.c_int, [P, D, P, P, P, P, P]),
+            "ref_roi_qubo": (None, [P, P, C.c_int, P, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -346,3 +348,24 @@ class RefProblem:
         tr = np.empty(anneal + hold, np.float64)
         ref().ref_anneal_branch_trace(self.h, t_hot, t_cold, anneal, hold, seed, _p(x), _p(tr))
         return x, tr
+
+    def freeze(self, margin):
+        """freeze_provable_rock: (kept, reduced field, reduced nbr_ptr, reduced nbr, rounds)."""
+        n = self.n
+        nn = int(self.arr["nbr"].size)
+        kept = np.empty(n, np.int32)
+        field = np.empty(n, np.float64)
+        nptr = np.empty(n + 1, np.int32)
+        nbr = np.empty(max(nn, 1), np.int32)
+        rounds = C.c_int(0)
+        k = ref().ref_freeze(self.h, float(margin), _p(kept), _p(field), _p(nptr), _p(nbr), C.byref(rounds))
+        return kept[:k].copy(), field[:k].copy(), nptr[:k + 1].copy(), nbr[:int(nptr[k])].copy(), rounds.value
+
+    def roi_qubo(self, roi, x_bar):
+        """roi_qubo: (h, J) of the region with the rest held at x_bar."""
+        roi = np.ascontiguousarray(roi, np.int32)
+        x_bar = np.ascontiguousarray(x_bar, np.uint8)
+        h = np.empty(roi.size, np.float64)
+        J = np.empty(roi.size * roi.size, np.float64)
+        ref().ref_roi_qubo(self.h, _p(roi), int(roi.size), _p(x_bar), _p(h), _p(J))
+        return h, J.reshape(roi.size, roi.size)

@@ -203,4 +203,28 @@ void ref_anneal_branch_trace(void* h, double t_hot, double t_cold, int anneal, i
     std::memcpy(xo, x.data(), x.size());
 }
 
+// freeze_provable_rock (ising_recon.hpp:187-234): returns the kept count and
+// fills kept (reduced -> original), the reduced field and neighbour CSR.
+int ref_freeze(void* h, double margin, int32_t* kept, double* field, int32_t* nbr_ptr, int32_t* nbr, int* rounds) {
+    const auto* p = static_cast<argos::BinaryProblem*>(h);
+    const argos::FreezeResult fr = argos::freeze_provable_rock(*p, margin);
+    const int nk = int(fr.kept.size());
+    std::memcpy(kept, fr.kept.data(), size_t(nk) * 4);
+    std::memcpy(field, fr.reduced.field.data(), size_t(nk) * 8);
+    std::memcpy(nbr_ptr, fr.reduced.nbr_ptr.data(), size_t(nk + 1) * 4);
+    std::memcpy(nbr, fr.reduced.nbr.data(), fr.reduced.nbr.size() * 4);
+    *rounds = fr.rounds;
+    return nk;
+}
+
+// roi_qubo (ising_recon.hpp:251-300): h (n) and J (n x n, upper triangle) of
+// the region `roi` with the rest held at x_bar.
+void ref_roi_qubo(void* h, const int32_t* roi, int n_roi, const uint8_t* x_bar, double* h_out, double* J_out) {
+    const auto* p = static_cast<argos::BinaryProblem*>(h);
+    const argos::RoiQubo q = argos::roi_qubo(*p, std::vector<int>(roi, roi + n_roi),
+                                             std::vector<uint8_t>(x_bar, x_bar + p->n_vars()));
+    std::memcpy(h_out, q.h.data(), size_t(n_roi) * 8);
+    std::memcpy(J_out, q.J.data(), size_t(n_roi) * size_t(n_roi) * 8);
+}
+
 }  // extern "C"

@@ -29,7 +29,8 @@ from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_R
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
-           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "parse_rudy"]
+           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "parse_rudy",
+           "freeze_rock", "roi_qubo", "enumerate_qubo"]
 
 
 @dataclass
@@ -290,6 +291,68 @@ def parse_rudy(text):
         return int(d.n), arr(d.eu), arr(d.ev), arr(d.ew)
     finally:
         lib().qb_graph_destroy(h)
+
+
+def freeze_rock(arrays: dict, margin: float, device: int = -1):
+    """freeze_provable_rock (ising_recon.hpp:168-235) on the device: returns
+    (reduced residual arrays, kept = reduced bit -> original bit, rounds)."""
+    from .synth import residual_desc
+    d = residual_desc(arrays)
+    h = C.c_void_p()
+    o = _opts(device, None)
+    check(lib().qb_freeze_rock(C.byref(d), float(margin), C.byref(o), C.byref(h)))
+    try:
+        nk, rounds = C.c_int32(), C.c_int32()
+        check(lib().qb_freeze_info(h, C.byref(nk), C.byref(rounds)))
+        kept = np.empty(nk.value, np.int32)
+        check(lib().qb_freeze_kept(h, ptr(kept)))
+        r = ResidualDesc()
+        check(lib().qb_freeze_reduced(h, C.byref(r)))
+
+        def arr(p_, count, ct, dt):
+            if count == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(C.cast(p_, C.POINTER(ct)), shape=(count,)).astype(dt, copy=True)
+
+        n = nk.value
+        nnz = int(arr(r.row_ptr, n + 1, C.c_int32, np.int32)[-1])
+        nptr = arr(r.nbr_ptr, n + 1, C.c_int32, np.int32)
+        red = {"d": arr(r.d, r.n_rays, C.c_double, np.float64), "w": arr(r.w, r.n_rays, C.c_double, np.float64),
+               "row_ptr": arr(r.row_ptr, n + 1, C.c_int32, np.int32), "ray": arr(r.ray, nnz, C.c_int32, np.int32),
+               "a": arr(r.a, nnz, C.c_float, np.float32), "nbr_ptr": nptr,
+               "nbr": arr(r.nbr, int(nptr[-1]), C.c_int32, np.int32), "lambda": float(r.lambda_),
+               "kappa": float(r.kappa), "field": arr(r.field, n, C.c_double, np.float64)}
+        return red, kept, rounds.value
+    finally:
+        lib().qb_freeze_destroy(h)
+
+
+def roi_qubo(arrays: dict, roi, x_bar):
+    """(h, J) of the region `roi` with the other bits held at x_bar
+    (roi_qubo, ising_recon.hpp:240-300); J is n x n, upper triangle used."""
+    from .synth import residual_desc
+    d = residual_desc(arrays)
+    roi = np.ascontiguousarray(roi, np.int32)
+    x_bar = np.ascontiguousarray(x_bar, np.uint8)
+    h = np.empty(roi.size, np.float64)
+    J = np.empty((roi.size, roi.size), np.float64)
+    check(lib().qb_roi_qubo(C.byref(d), ptr(roi), int(roi.size), ptr(x_bar), ptr(h), ptr(J)))
+    return h, J
+
+
+def enumerate_qubo(h, J, T: float = 1.0, device: int = -1):
+    """All 2^n states of E(x) = h.x + sum_{i<j} J_ij x_i x_j on the device:
+    returns (marginals p(x_i = 1), log Z, mean energy, e_min, x_min as 0/1)."""
+    from ._abi import EnumResult
+    h = np.ascontiguousarray(h, np.float64)
+    J = np.ascontiguousarray(J, np.float64)
+    n = int(h.size)
+    p = np.empty(n, np.float64)
+    res = EnumResult()
+    o = _opts(device, None)
+    check(lib().qb_enumerate_qubo(n, ptr(h), ptr(J), float(T), C.byref(o), C.byref(res), ptr(p)))
+    x_min = np.array([(res.x_min >> i) & 1 for i in range(n)], np.uint8)
+    return p, res.log_z, res.mean_energy, res.e_min, x_min
 
 
 # ---- batches: many ising instances in one persistent launch --------------------------------

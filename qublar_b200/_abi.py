@@ -115,6 +115,11 @@ class ServerStats(C.Structure):
                                           "bytes_in_use", "peak_bytes", "budget_bytes", "attempts_done")]
 
 
+class EnumResult(C.Structure):
+    _fields_ = [("log_z", C.c_double), ("e_min", C.c_double), ("x_min", C.c_uint64), ("mean_energy", C.c_double),
+                ("states", C.c_uint64)]
+
+
 _P = C.c_void_p
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -168,6 +173,13 @@ SIGNATURES = {
     "qb_parse_rudy": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(_P)]),
     "qb_graph_desc": (C.c_int, [_P, C.POINTER(IsingDesc)]),
     "qb_graph_destroy": (None, [_P]),
+    "qb_freeze_rock": (C.c_int, [C.POINTER(ResidualDesc), C.c_double, C.POINTER(Opts), C.POINTER(_P)]),
+    "qb_freeze_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "qb_freeze_kept": (C.c_int, [_P, _P]),
+    "qb_freeze_reduced": (C.c_int, [_P, C.POINTER(ResidualDesc)]),
+    "qb_freeze_destroy": (None, [_P]),
+    "qb_roi_qubo": (C.c_int, [C.POINTER(ResidualDesc), _P, C.c_int32, _P, _P, _P]),
+    "qb_enumerate_qubo": (C.c_int, [C.c_int32, _P, _P, C.c_double, C.POINTER(Opts), C.POINTER(EnumResult), _P]),
     "qb_colour_ising": (C.c_int, [C.POINTER(IsingDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),

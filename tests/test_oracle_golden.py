@@ -283,3 +283,30 @@ def test_rudy_reader_round_trips_generated_graphs():
         text = O.Graph(n, eu, ev, ew).rudy()
         n2, eu2, ev2, ew2 = parse_rudy(text)
         assert n2 == n and (eu2 == eu).all() and (ev2 == ev).all() and (ew2 == ew).all()
+
+
+# ---- region-of-interest QUBO -----------------------------------------------------------
+
+def test_roi_qubo_equals_the_reference_and_the_full_energy():
+    """qb_roi_qubo equals roi_qubo (ising_recon.hpp:240-300, compiled from the
+    reference) bit for bit, and E(x) - E(0_R) of the full problem equals the
+    region's QUBO on random states (the reference driver's own check,
+    check_ising.cu:540-560)."""
+    from qublar_b200 import roi_qubo
+    a = synth.tomography(synth.small_tomo_params(0.2, 24))
+    n = a["row_ptr"].size - 1
+    rng = np.random.default_rng(4)
+    x_bar = (rng.random(n) < 0.1).astype(np.uint8)
+    roi = np.sort(rng.choice(n, 14, replace=False)).astype(np.int32)
+    h, J = roi_qubo(a, roi, x_bar)
+    if O.ref_available():
+        rh, rJ = O.RefProblem(a).roi_qubo(roi, x_bar)
+        assert (h == rh).all() and (np.triu(J, 1) == np.triu(rJ, 1)).all()
+    xf = x_bar.copy()
+    xf[roi] = 0
+    e0 = O.binary_energy(a, xf)
+    for _ in range(8):
+        xr = (rng.random(roi.size) < 0.5).astype(np.uint8)
+        xf[roi] = xr
+        eq = float(h @ xr + xr @ np.triu(J, 1) @ xr)
+        assert abs((O.binary_energy(a, xf) - e0) - eq) < 1e-6 * max(1.0, abs(e0))
