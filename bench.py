@@ -42,7 +42,7 @@ BRANCHES = 16
 # branches (profiles/resid_lockstep_pyramid.md): 1.924 GB + 6.3 MB over 10
 # sweeps. The bit->ray structure streams from DRAM once per sweep, so the
 # traffic of a full launch is this figure times its sweeps.
-NCU_TRAFFIC_PER_SWEEP = (1.924285e9 + 6.321408e6) / 10
+NCU_TRAFFIC_PER_SWEEP = (1.931776e9 + 5.473536e6) / 10
 
 
 def log(*a):
