@@ -78,15 +78,24 @@ struct IsingArgs {
     const double* temp;
     int32_t* f_scratch;   // R x n (global-state variant)
     int8_t* s_scratch;    // R x n
+    int wide;             // rows long enough that a warp per accepted flip pays for a second barrier
     uint8_t* x_out;       // R x n
     int32_t* f_out;       // R x n
     long long* e_out;     // R
 };
 
+// Accepted bits of a class listed for the warp-wide neighbour update, used
+// when some bit has at least kWideRow neighbours (a second barrier per class
+// then pays for itself).
+constexpr int kAccList = 1024;
+constexpr int kWideRow = 24;
+
 template <typename WT, bool SMEM>
 __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ long long red[kIsingThreads / 32];
+    __shared__ int2 acc_list[kAccList];   // (bit, -2 s_i mod 2^32) of the class's accepted flips
+    __shared__ int acc_count[2];          // per class parity
     const int rep = int(blockIdx.x);
     const int n = A.n;
     int32_t* f;
@@ -102,29 +111,51 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
         f[i] = A.f0[i];
         s[i] = -1;
     }
+    if (threadIdx.x < 2) acc_count[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t seed = A.seed0 + uint64_t(rep);
     const WT* w = static_cast<const WT*>(A.w);
+    const int lane = int(threadIdx.x & 31u), warp = int(threadIdx.x >> 5), n_warps = int(blockDim.x >> 5);
     long long E = 0;
+    int parity = 0;
     for (int sweep = 0; sweep < A.sweeps; ++sweep) {
         const double T = A.temp[sweep];
-        for (int c = 0; c < A.n_colours; ++c) {
+        for (int c = 0; c < A.n_colours; ++c, parity ^= 1) {
             const int c1 = A.class_ptr[c + 1];
+            // 1. decide every bit of the class; with wide rows, list the
+            // accepted flips, else update their neighbours at once
             for (int i = A.class_ptr[c] + int(threadIdx.x); i < c1; i += blockDim.x) {
                 const int si = s[i];
                 const long long dE = -(long long)si * (long long)f[i];
                 if (metropolis(double(dE), T, seed, uint32_t(A.order[i]), uint32_t(sweep))) {
                     s[i] = int8_t(-si);
                     E += dE;
-                    const int r1 = A.row[i + 1];
                     // f_j -= 2 w_ij s_i, in wrap-around uint32 arithmetic: the
                     // final field fits int32 (|f| <= field bound), the term may not
                     const uint32_t ms = si > 0 ? 0xFFFFFFFEu : 2u;   // -2 s_i mod 2^32
-                    for (int k = A.row[i]; k < r1; ++k)
-                        atomicAdd(reinterpret_cast<unsigned int*>(&f[A.adj[k]]), uint32_t(int32_t(w[k])) * ms);
+                    const int slot = A.wide ? atomicAdd(&acc_count[parity], 1) : kAccList;
+                    if (slot < kAccList) {
+                        acc_list[slot] = make_int2(i, int(ms));
+                    } else {   // narrow rows or a full list: update the neighbours here
+                        const int r1 = A.row[i + 1];
+                        for (int k = A.row[i]; k < r1; ++k)
+                            atomicAdd(reinterpret_cast<unsigned int*>(&f[A.adj[k]]), uint32_t(int32_t(w[k])) * ms);
+                    }
                 }
             }
             __syncthreads();
+            if (!A.wide) continue;
+            // 2. a warp per accepted flip, its lanes over the bit's neighbours
+            // (integer sums: the order of the atomics does not matter)
+            const int na = min(acc_count[parity], kAccList);
+            for (int q = warp; q < na; q += n_warps) {
+                const int2 e = acc_list[q];
+                const int r1 = A.row[e.x + 1];
+                for (int k = A.row[e.x] + lane; k < r1; k += 32)
+                    atomicAdd(reinterpret_cast<unsigned int*>(&f[A.adj[k]]), uint32_t(int32_t(w[k])) * uint32_t(e.y));
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) acc_count[parity] = 0;   // reused two classes later, after two barriers
         }
     }
     for (int i = int(threadIdx.x); i < n; i += blockDim.x) {
@@ -875,6 +906,9 @@ qb_status launch_ising_anneal(const IsingPlan& p, const SolveBuffers& b, int R, 
     A.x_out = b.x;
     A.f_out = b.f;
     A.e_out = b.e_i64;
+    int max_deg = 0;
+    for (int i = 0; i < p.n; ++i) max_deg = std::max(max_deg, p.row[size_t(i) + 1] - p.row[size_t(i)]);
+    A.wide = max_deg >= kWideRow ? 1 : 0;
     const size_t smem = ising_smem_bytes(p);
     if (smem == 0) {
         if (!b.scratch) return fail(QB_EINVAL, "ising sweep: global state needs scratch");
