@@ -252,3 +252,26 @@ def test_server_create_fails_cleanly_without_a_device():
     assert st != 0 and not h.value
     rid = C.c_uint64()
     assert lib().qb_server_submit(None, None, None, 1, 0, C.byref(rid)) == 1
+
+
+def _qubo_status(n, eu, ev, ew, h=None):
+    from qublar_b200._abi import QuboDesc
+    eu, ev = (np.ascontiguousarray(x, np.int32) for x in (eu, ev))
+    ew = np.ascontiguousarray(ew, np.float32)
+    hh = None if h is None else np.ascontiguousarray(h, np.float32)
+    d = QuboDesc(n, eu.size, ptr(eu), ptr(ev), ptr(ew), ptr(hh), 0.0)
+    out = C.c_void_p()
+    return lib().qb_problem_create_qubo(C.byref(d), None, C.byref(out)), lib().qb_last_error().decode()
+
+
+@pytest.mark.parametrize("case,why", [
+    ((3, [0], [0], [1.0]), "self-loop"),
+    ((3, [0, 1], [1, 0], [1.0, 2.0]), "duplicate edge"),
+    ((3, [0], [5], [1.0]), "out of range"),
+    ((3, [0], [1], [float("nan")]), "not finite"),
+    ((3, [0], [1], [1.0], [0.0, float("inf"), 0.0]), "linear term is not finite"),
+    ((0, [], [], []), "n must be positive"),
+])
+def test_qubo_refusals(case, why):
+    st, msg = _qubo_status(*case)
+    assert st == 1 and why in msg
