@@ -383,6 +383,8 @@ typedef struct qb_server_config {
     int32_t tick_target_us;      /* ising slices are sized so a tick item takes about this long (0 = 20000) */
     int32_t use_graph;           /* 0: launch ticks directly; otherwise replay a captured CUDA graph */
     qb_batch_config batch;       /* packed-kernel shape (zeros = defaults) */
+    int32_t max_pending;         /* requests waiting for admission at most; a submit beyond returns QB_EBUSY
+                                    (0 = no limit) */
 } qb_server_config;
 
 /* Request states reported by qb_server_poll. */
@@ -421,9 +423,9 @@ typedef struct qb_server_stats {
 } qb_server_stats;
 
 qb_status qb_server_create(const qb_server_config* cfg, qb_server** out);
-/* Queues a request and returns its id at once. The problem must stay alive
- * until the request is finished or cancelled; one problem serves one request
- * at a time. */
+/* Queues a request and returns its id at once (QB_EBUSY when max_pending
+ * requests already wait). The problem must stay alive until the request is
+ * finished or cancelled; one problem serves one request at a time. */
 qb_status qb_server_submit(qb_server* s, qb_problem* problem, const qb_schedule* sched, uint32_t n_branches,
                            uint64_t seed_offset, uint64_t* id);
 /* Current state (QB_REQ_*) of a request. */

@@ -447,9 +447,9 @@ class Server:
 
     def __init__(self, budget_bytes: int = 0, max_active: int = 0, residual_streams: int = 0,
                  tick_target_us: int = 0, use_graph: bool = True, batch: BatchConfig | None = None,
-                 device: int = -1):
+                 device: int = -1, max_pending: int = 0):
         cfg = ServerConfig(int(device), int(budget_bytes), int(max_active), int(residual_streams),
-                           int(tick_target_us), 1 if use_graph else 0, batch or BatchConfig())
+                           int(tick_target_us), 1 if use_graph else 0, batch or BatchConfig(), int(max_pending))
         h = C.c_void_p()
         check(lib().qb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -121,6 +122,8 @@ struct qb_server {
     bool tick_inflight = false;
     std::vector<std::pair<Request*, int>> tick_members;   // request, sweep end of its slice
     std::string fatal;
+    int64_t admissions = 0;
+    int64_t fail_admission = 0;   // QB_SERVER_FAIL_ADMIT=k: the k-th admission fails (host-side fault injection)
 };
 
 namespace {
@@ -369,7 +372,10 @@ void admit_pending(qb_server* S) {
             q->t_admit = now_s();
             r = q;
         }
-        const qb_status s = r->exclusive ? launch_exclusive(S, r)
+        ++S->admissions;
+        const qb_status s = S->admissions == S->fail_admission
+                                ? fail(QB_ENOMEM, "injected admission failure (QB_SERVER_FAIL_ADMIT)")
+                            : r->exclusive ? launch_exclusive(S, r)
                             : r->kind == QB_KIND_ISING ? admit_ising(S, r)
                                                        : launch_resid(S, r);
         if (s != QB_OK) {
@@ -683,7 +689,7 @@ extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** o
     if (c.residual_streams == 0) c.residual_streams = kDefaultResidStreams;
     if (c.tick_target_us == 0) c.tick_target_us = kDefaultTickUs;
     if (c.hbm_budget_bytes < 0 || c.max_active < 0 || c.residual_streams < 0 || c.residual_streams > 64 ||
-        c.tick_target_us < 0)
+        c.tick_target_us < 0 || c.max_pending < 0)
         return fail(QB_EINVAL, "qb_server_create: negative or out-of-range setting");
     if (c.batch.threads == 0) c.batch.threads = 512;
     if (c.batch.smem_bytes == 0) c.batch.smem_bytes = 96 * 1024;
@@ -720,6 +726,7 @@ extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** o
     }
     QB_CUDA(cudaEventCreateWithFlags(&S->upload_ev, cudaEventDisableTiming));
     QB_CUDA(cudaEventCreateWithFlags(&S->tick_ev, cudaEventDisableTiming));
+    if (const char* fa = std::getenv("QB_SERVER_FAIL_ADMIT")) S->fail_admission = std::atoll(fa);
     qb_server* raw = S.release();
     raw->worker = std::thread(worker_main, raw);
     *out = raw;
@@ -756,6 +763,8 @@ extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_sche
     r->t_submit = now_s();
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stop) return fail(QB_EINVAL, "qb_server_submit: the server is stopping");
+    if (S->cfg.max_pending > 0 && int64_t(S->pending.size()) >= S->cfg.max_pending)
+        return fail(QB_EBUSY, "qb_server_submit: the queue is full");
     for (auto& kv : S->reqs)
         if (kv.second->prob == p && (kv.second->state == QB_REQ_PENDING || kv.second->state == QB_REQ_RUNNING))
             return fail(QB_EBUSY, "qb_server_submit: the problem already has a request in flight");

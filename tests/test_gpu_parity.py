@@ -229,3 +229,35 @@ def test_cpp_adapter_matches_the_python_path(tmp_path):
     bo = run_batch(G, b, 1, 4)
     assert (np.fromfile(tmp_path / "batch_x.bin", np.uint8).reshape(4, -1) == bo.X).all()
     assert (np.fromfile(tmp_path / "batch_e.bin", np.int64) == bo.energy).all()
+
+
+def test_empty_pyramid_shows_no_false_voids():
+    """The reference's empty-pyramid control (check_ising.cu:322-361): with no
+    void in the rock, the posterior labels no bit NotThere."""
+    a = synth.tomography(synth.small_tomo_params(0.2, 24, void_side=0.0))
+    P = ResidualProblem.from_arrays(a)
+    p = P.solve(Schedule(), 32).marginals()
+    assert int((classify(p) == 1).sum()) == 0
+
+
+def test_freezing_keeps_the_void_map_within_seed_spread():
+    """The reference's freezing check (check_ising.cu:444-505): the NotThere set
+    of the frozen problem stays within the seed-to-seed Jaccard spread of the
+    full problem's."""
+    from qublar_b200 import freeze_rock
+    a = synth.tomography(synth.small_tomo_params(0.3, 36))
+    n = a["row_ptr"].size - 1
+    sched = Schedule()
+    P = ResidualProblem.from_arrays(a)
+    ref = set(np.flatnonzero(classify(P.solve(sched, 32).marginals()) == 1).tolist())
+    other = set(np.flatnonzero(classify(P.solve(sched, 32, 1000).marginals()) == 1).tolist())
+    red, kept, _ = freeze_rock(a, 10.0)
+    pr = ResidualProblem.from_arrays(red).solve(sched, 32).marginals()
+    got = set(kept[classify(pr) == 1].tolist())
+
+    def jaccard(x, y):
+        u = len(x | y)
+        return len(x & y) / u if u else 1.0
+
+    assert kept.size < n
+    assert jaccard(got, ref) >= jaccard(other, ref) - 0.15

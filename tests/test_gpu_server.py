@@ -255,3 +255,45 @@ def test_submissions_from_several_threads():
         x, _, _ = _alone("ising", gens[k], sched, 8, k)
         assert (S.branches(rid) == x).all()
     S.close()
+
+
+def test_queue_overflow_is_refused():
+    P = [IsingProblem(*synth.torus_pm1(60 + 2 * k, k), flags=DEFER) for k in range(4)]
+    S = Server(max_active=1, max_pending=2, tick_target_us=2000)
+    a = S.submit(P[0], Schedule(3.0, 0.05, 20000, 0, 0), 32)
+    time.sleep(0.05)                                   # a is admitted; the queue is empty
+    b = S.submit(P[1], Schedule(3.0, 0.05, 100, 0, 0), 8)
+    c = S.submit(P[2], Schedule(3.0, 0.05, 100, 0, 0), 8)
+    with pytest.raises(QBError) as ex:
+        S.submit(P[3], Schedule(3.0, 0.05, 100, 0, 0), 8)
+    assert ex.value.status == 8   # QB_EBUSY
+    S.cancel(a)
+    for i in (b, c):
+        S.wait(i, 120000)
+    S.close()
+
+
+def test_an_injected_admission_failure_fails_only_its_request(monkeypatch):
+    """Host-side fault injection: the second admission fails with QB_ENOMEM;
+    the other requests finish and all memory returns to the budget."""
+    monkeypatch.setenv("QB_SERVER_FAIL_ADMIT", "2")
+    S = Server()
+    monkeypatch.delenv("QB_SERVER_FAIL_ADMIT")
+    gens = [synth.random_regular(500, 6, k) for k in range(3)]
+    P = [IsingProblem(*g, flags=DEFER) for g in gens]
+    sched = Schedule(3.0, 0.05, 100, 0, 0)
+    ids = []
+    for k in range(3):
+        ids.append(S.submit(P[k], sched, 8, k))
+        S.wait(ids[-1], 120000) if k != 1 else None
+        time.sleep(0.02)
+    with pytest.raises(QBError) as ex:
+        S.wait(ids[1], 120000)
+    assert ex.value.status == 2 and "injected" in ex.value.message
+    for k in (0, 2):
+        x, _, _ = _alone("ising", gens[k], sched, 8, k)
+        assert (S.branches(ids[k]) == x).all()
+        S.release(ids[k])
+    S.release(ids[1])
+    assert S.stats().bytes_in_use == 0 and S.stats().failed == 1
+    S.close()
