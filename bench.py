@@ -354,17 +354,31 @@ def batch_cpu_baseline(graphs, items, R, S):
 # ---- serve: a Poisson request stream through the serving loop -----------------------------------
 
 SERVE_LOCKSTEP_BITS = 40000
+SERVE_QUBO_MAXCUT_BITS = 50000
 SERVE_WORKLOAD = ("Poisson request stream: N log-uniform 1,000..300,000, half tomography-style pyramids, half "
                   "sparse +-1 Max-Cut (d-regular, d 3..12), sweeps 500..5000, branches 8..32")
 
 
-def _serve_schedule(spec, P):
-    from qublar_b200 import Schedule
+def _serve_schedule(spec, P, data):
+    from qublar_b200 import Budget, Schedule
     S = spec["sweeps"]
     if spec["kind"] == "tomography":
         hold = S // 5
         return Schedule(50.0, 1.0, S - hold, hold, 50)
-    return P.scaled_schedule(S, 0)
+    if hasattr(P, "scaled_schedule"):
+        return P.scaled_schedule(S, 0)
+    # a Max-Cut graph served as the equal QUBO: the integer form's scaled
+    # schedule (T_hot = sqrt(2 sum w^2 / n), T_cold = w_min / 10)
+    n, _, _, ew = data
+    a = np.abs(np.asarray(ew, np.float64))
+    nz = a[a > 0]
+    return Budget(float(np.sqrt(2.0 * np.sum(a * a) / n)), 0.1 * float(nz.min() if nz.size else 0.0), S, 0, 0)
+
+
+def _serve_path(P, spec):
+    if spec["kind"] != "tomography":
+        return "maxcut exclusive qubo" if spec["n"] >= SERVE_QUBO_MAXCUT_BITS else "maxcut ticks"
+    return "pyramid exclusive lockstep" if P.info().variant == 1 else "pyramid cluster"
 
 
 def _serve_run(probs, specs, scheds, rate, seed):
@@ -391,8 +405,16 @@ def _serve_run(probs, specs, scheds, rate, seed):
     last = max(i.t_done for i in infos)
     lat = np.array([i.t_done - i.t_submit for i in infos])
     stats = S.stats()
+    # where the time went: service (admission to done) and queueing, by path
+    paths = {}
+    for P, sp, inf in zip(probs, specs, infos):
+        d = paths.setdefault(_serve_path(P, sp), {"requests": 0, "attempts": 0.0, "service_s": 0.0, "queue_s": 0.0})
+        d["requests"] += 1
+        d["attempts"] += float(inf.attempts)
+        d["service_s"] += inf.t_done - inf.t_admit
+        d["queue_s"] += inf.t_admit - inf.t_submit
     out = {"ids": ids, "server": S, "lat": lat, "makespan": last - first, "ticks": stats.ticks,
-           "peak_bytes": stats.peak_bytes}
+           "peak_bytes": stats.peak_bytes, "paths": paths}
     return out
 
 
@@ -404,21 +426,30 @@ def run_serve(args):
     log(f"[serve] built {len(data)} requests in {time.perf_counter() - t0:.1f} s")
     import torch
 
-    from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, ResidualProblem)
+    from qublar_b200 import (OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, IsingProblem, QuboProblem, ResidualProblem)
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
 
-    def make(k):
+    def make(k, served=True):
         # pyramids of 40,000 bits and more take the whole-device lockstep sweep
-        # (run exclusively); smaller ones one cluster per branch beside the rest
-        if specs[k]["kind"] == "tomography":
-            fl = OPT_DEFER_UPLOAD | (0 if specs[k]["n"] >= SERVE_LOCKSTEP_BITS else OPT_RESID_CLUSTER)
+        # (run exclusively); smaller ones one cluster per branch beside the rest.
+        # Max-Cut graphs of 50,000 bits and more run as the equal weighted QUBO
+        # on the whole-device sweep (identical branches); smaller ones in ticks.
+        # The plain form (served=False) is the same problem solved alone; its
+        # pyramids always take the lockstep sweep, qb_solve's default plan.
+        sp = specs[k]
+        fl = OPT_DEFER_UPLOAD if served else 0
+        if sp["kind"] == "tomography":
+            if served and sp["n"] < SERVE_LOCKSTEP_BITS:
+                fl |= OPT_RESID_CLUSTER
             return ResidualProblem.from_arrays(data[k], flags=fl)
-        return IsingProblem(*data[k], flags=OPT_DEFER_UPLOAD)
+        if sp["n"] >= SERVE_QUBO_MAXCUT_BITS:
+            return QuboProblem.from_dict(synth.maxcut_qubo(*data[k]), flags=fl)
+        return IsingProblem(*data[k], flags=fl)
 
     t0 = time.perf_counter()
     probs = _create_all(make, range(len(specs)))
     log(f"[serve] planned in {time.perf_counter() - t0:.1f} s")
-    scheds = [_serve_schedule(sp, P) for sp, P in zip(specs, probs)]
+    scheds = [_serve_schedule(sp, P, data[k]) for k, (sp, P) in enumerate(zip(specs, probs))]
     attempts = [sp["branches"] * sch.sweeps * P.n for sp, sch, P in zip(specs, scheds, probs)]
     total = float(sum(attempts))
     # warm-up: a few small requests through a server
@@ -441,11 +472,8 @@ def run_serve(args):
     for k in sample:
         x_served = S.branches(sat["ids"][k])
         e_served = S.energies(sat["ids"][k])
-        # plain form: this request alone through qb_solve (lockstep sweep for the pyramids)
-        if specs[k]["kind"] == "tomography":
-            Q = ResidualProblem.from_arrays(data[k])
-        else:
-            Q = IsingProblem(*data[k])
+        # plain form: this request alone through qb_solve
+        Q = make(k, served=False)
         r = Q.solve(scheds[k], specs[k]["branches"], k)
         inf = r.info()
         p_att += inf.attempts
@@ -477,13 +505,16 @@ def run_serve(args):
         "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "requests": len(probs), "total_attempts": total,
                    "policy": f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: whole-device lockstep sweep, run alone; "
-                             "smaller pyramids: one cluster per branch; Max-Cut: ticks of the packed kernel",
+                             "smaller pyramids: one cluster per branch; Max-Cut >= "
+                             f"{SERVE_QUBO_MAXCUT_BITS} bits: the equal weighted QUBO on the whole-device sweep, run "
+                             "alone; smaller Max-Cut: ticks of the packed kernel",
                    "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
         "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
                                   "p99_s": float(np.percentile(lat_sat, 99))}, **rates},
         "plain": {"value": plain, "unit": "attempts/s",
-                  "form": "each request alone through qb_solve (lockstep sweep for pyramids, CTA per replica for "
-                          "Max-Cut)", "sample": f"{len(sample)} requests"},
+                  "form": "each request alone through qb_solve (lockstep sweep for pyramids, the whole-device "
+                          f"QUBO sweep for Max-Cut >= {SERVE_QUBO_MAXCUT_BITS} bits, CTA per replica below)",
+                  "sample": f"{len(sample)} requests"},
         "vs_plain": value / plain,
         "equal_energy": {"checked": len(sample), "agree": same,
                          "mean_rel_energy_diff": float(np.mean(e_rel)) if e_rel else None,
@@ -492,7 +523,7 @@ def run_serve(args):
         "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "requests enter as host problems (deferred upload) and the server uploads them at "
                         "admission inside the timed makespan"},
-        "server": {"ticks": sat["ticks"], "peak_bytes": sat["peak_bytes"]},
+        "server": {"ticks": sat["ticks"], "peak_bytes": sat["peak_bytes"], "paths_saturated": sat["paths"]},
         "peak_hbm_gbs": hbm, "peak_kind": peak_kind,
         "clocks": clocks,
     }

@@ -22,6 +22,7 @@
 #include <cstdint>
 
 #include "qb_batch.hpp"
+#include "qb_device.cuh"
 #include "qb_philox.cuh"
 
 namespace qb {
@@ -249,7 +250,7 @@ qb_status batch_ctas(const BatchShape& sh, int* ctas) {
     QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (sh.threads < 32 || sh.threads > kBatchThreadsMax || sh.threads % kBatchMaxGroup)
         return fail(QB_EINVAL, "batch: threads must be a multiple of 32 in [32, 1024]");
-    QB_CUDA(cudaFuncSetAttribute(ising_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes));
+    QB_CUDA(allow_max_smem(ising_batch_kernel));
     QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ising_batch_kernel, sh.threads, size_t(sh.smem_bytes)));
     if (occ < 1) return fail(QB_EREFUSED, "batch: the launch shape does not fit an SM");
     *ctas = occ * sms;
@@ -263,7 +264,7 @@ qb_status launch_ising_batch(const IsingItem* d_items, int n_items, int* d_count
         qb_status s = batch_ctas(sh, &ctas);
         if (s != QB_OK) return s;
     } else {
-        QB_CUDA(cudaFuncSetAttribute(ising_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes));
+        QB_CUDA(allow_max_smem(ising_batch_kernel));
     }
     if (n_items <= 0) return QB_OK;
     if (ctas > n_items) ctas = n_items;

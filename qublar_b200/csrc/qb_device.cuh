@@ -2,6 +2,8 @@
 // global accesses and the bounded grid barrier.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 namespace qb {
@@ -66,6 +68,22 @@ __device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned roun
     }
     __syncthreads();
     return s_ok2 != 0;
+}
+
+// Raises a kernel's dynamic shared-memory limit to the device maximum (the
+// opt-in per-block size less the kernel's static shared memory). Every launcher
+// sets the same value, so planning threads that check occupancy while others
+// launch all see one limit; the launch itself passes the bytes it needs.
+template <typename K>
+inline cudaError_t allow_max_smem(K* kern) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(fa.sharedSizeBytes));
+    return e;
 }
 
 }  // namespace qb

@@ -918,10 +918,10 @@ qb_status launch_ising_anneal(const IsingPlan& p, const SolveBuffers& b, int R, 
     const dim3 grid(static_cast<unsigned>(R)), block(kIsingThreads);
     if (smem) {
         if (p.weight_bytes == 1) {
-            QB_CUDA(cudaFuncSetAttribute(ising_anneal_kernel<int8_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            QB_CUDA(allow_max_smem(ising_anneal_kernel<int8_t, true>));
             ising_anneal_kernel<int8_t, true><<<grid, block, smem, st>>>(A);
         } else {
-            QB_CUDA(cudaFuncSetAttribute(ising_anneal_kernel<int32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            QB_CUDA(allow_max_smem(ising_anneal_kernel<int32_t, true>));
             ising_anneal_kernel<int32_t, true><<<grid, block, smem, st>>>(A);
         }
     } else {
@@ -963,7 +963,7 @@ namespace {
 template <int CL>
 qb_status resid_launch_cl(const ResidArgs& A, int R, size_t smem, cudaStream_t st, bool check_only) {
     auto kern = A.phase ? resid_anneal_kernel<CL, true> : resid_anneal_kernel<CL, false>;
-    QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    QB_CUDA(allow_max_smem(kern));
     if (CL > 8) QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(unsigned(R * CL));

@@ -233,6 +233,27 @@ def lattice_qubo(L: int = 58, n_total: int = 200000, degree: float = 20.0, seed:
     return {"n": n, "eu": eu, "ev": ev, "ew": ew, "h": h, "offset": 0.0}
 
 
+def maxcut_qubo(n: int, eu, ev, ew) -> dict:
+    """A Max-Cut graph as the weighted QUBO with the same energy: E = -sum_e
+    w_e [x_u != x_v] = sum_i h_i x_i + sum_e 2 w_e x_u x_v with h_i = -sum_j
+    w_ij. With integer weights whose field sums stay below 2^24 every fp32
+    field is exact, so the compensated-field sweep makes the integer sweep's
+    decisions."""
+    eu = np.asarray(eu, np.int32)
+    ev = np.asarray(ev, np.int32)
+    w = np.asarray(ew, np.int64)
+    h = np.zeros(n, np.int64)
+    np.add.at(h, eu, -w)
+    np.add.at(h, ev, -w)
+    absum = np.zeros(n, np.int64)
+    np.add.at(absum, eu, np.abs(w))
+    np.add.at(absum, ev, np.abs(w))
+    if absum.max(initial=0) * 2 >= (1 << 24):
+        raise ValueError("field sums reach 2^24: fp32 fields would not be exact")
+    return {"n": int(n), "eu": eu, "ev": ev, "ew": (2 * w).astype(np.float32), "h": h.astype(np.float32),
+            "offset": 0.0}
+
+
 def random_qubo(n: int, m: int, seed: int, scale: float = 1.0):
     """A small weighted QUBO: m distinct random pairs, N(0, scale) couplings and
     linear terms in fp32."""

@@ -78,3 +78,22 @@ def test_final_energies_agree_with_the_reference_annealer():
                                                          sched.hold_sweeps, s + 1)) for s in range(48)])
     se = np.sqrt(e_gpu.var(ddof=1) / e_gpu.size + e_ref.var(ddof=1) / e_ref.size) + 1e-12
     assert abs(e_gpu.mean() - e_ref.mean()) / se < 4.0
+
+
+@pytest.mark.parametrize("gen", [lambda: synth.random_regular(3000, 6, 5), lambda: synth.torus_pm1(40, 3),
+                                 lambda: synth.random_sparse(2000, 9000, 7, 50)],
+                         ids=["regular6", "torus40", "sparse_w50"])
+def test_maxcut_through_the_qubo_sweep_equals_the_ising_sweep(gen):
+    """A Max-Cut graph as a weighted QUBO (h = -sum w, J = 2 w): with exact
+    fp32 fields the compensated sweep makes the integer sweep's decisions, so
+    the branches are identical and the energies equal -cut."""
+    from qublar_b200 import IsingProblem
+    n, eu, ev, ew = gen()
+    I = IsingProblem(n, eu, ev, ew)
+    sched = I.scaled_schedule(150, 10)
+    ri = I.solve(sched, 40, 2)
+    Q = QuboProblem.from_dict(synth.maxcut_qubo(n, eu, ev, ew))
+    rq = Q.solve(sched, 40, 2)
+    assert (rq.branches() == ri.branches()).all()
+    assert (rq.energies() == ri.energies_tracked().astype(np.float64)).all()
+    assert rq.info().max_energy_error == 0.0

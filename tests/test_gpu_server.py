@@ -297,3 +297,32 @@ def test_an_injected_admission_failure_fails_only_its_request(monkeypatch):
     S.release(ids[1])
     assert S.stats().bytes_in_use == 0 and S.stats().failed == 1
     S.close()
+
+
+def test_problems_planned_and_solved_from_many_threads():
+    """Cluster-planned pyramids of different sizes created from 8 threads while
+    other threads solve integer problems: every plan's fit check sees the same
+    kernel limits (no thread sees another's shared-memory setting), and every
+    solve equals the same solve made alone."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from qublar_b200._abi import RESID_CLUSTER
+    arrs = [synth.tomography(synth.small_tomo_params(0.08 + 0.02 * (k % 6), 10 + 2 * (k % 6))) for k in range(24)]
+    graphs = [synth.torus_pm1(20 + 10 * k, k) for k in range(8)]
+
+    def solve(g):
+        P = IsingProblem(*g)
+        r = P.solve(P.scaled_schedule(40, 5), 8, 0)
+        x = r.branches()
+        r.close()
+        P.close()
+        return x
+
+    alone = [solve(g) for g in graphs]
+    with ThreadPoolExecutor(8) as ex:
+        fut_x = [ex.submit(solve, g) for g in graphs]
+        probs = list(ex.map(lambda a: ResidualProblem.from_arrays(a, flags=RESID), arrs))
+        xs = [f.result() for f in fut_x]
+    assert all(P.info().variant == RESID_CLUSTER for P in probs)
+    for a, b in zip(alone, xs):
+        assert (a == b).all()
