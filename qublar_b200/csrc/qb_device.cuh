@@ -70,6 +70,24 @@ __device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned roun
     return s_ok2 != 0;
 }
 
+// The Metropolis test of an uphill move, u53 * 2^-53 < exp(-dE / T) with the
+// quotient and the exp in fp64, settled in fp32 when the two sides are far
+// apart. p = __expf(-dE * inv_T) (inv_T = fp32 1/T) is within a relative
+// 3e-5 of exp(-dE / T) wherever it is a normal number: the argument's
+// roundings cost |x| * 2e-7 with |x| < 88, and __expf's documented error is
+// 2 + 1.173 |x| ulp. u = hi * 2^-32 (hi = the draw's top 32 bits) is at most
+// 2^-32 below u53 * 2^-53. So u + 2^-32 < 0.999 p proves acceptance and
+// u > 1.001 p proves rejection (also after p underflows: a draw of 2^-32 or
+// more exceeds exp(-87)); a zero draw, non-finite values and the narrow band
+// between take the fp64 test. The outcome is always the fp64 test's.
+__device__ __forceinline__ bool uphill_accept(uint64_t u53, double dE, double T, float inv_T) {
+    const float u = __uint2float_rn(uint32_t(u53 >> 21)) * 0x1p-32f;
+    const float p = __expf(-(float(dE) * inv_T));
+    if (u + 0x1p-32f < 0.999f * p) return true;
+    if (u > 1.001f * p) return false;
+    return double(u53) * 0x1.0p-53 < exp(-dE / T);
+}
+
 // Raises a kernel's dynamic shared-memory limit to the device maximum (the
 // opt-in per-block size less the kernel's static shared memory). Every launcher
 // sets the same value, so planning threads that check occupancy while others

@@ -56,10 +56,10 @@ constexpr int kChunkN = 6144;   // stage neighbour entries per chunk
 constexpr uint32_t kSlotBits = 27;
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
 
-__device__ __forceinline__ bool metropolis(double dE, double T, uint64_t seed, uint32_t bit, uint32_t sweep) {
+__device__ __forceinline__ bool metropolis(double dE, double T, float inv_T, uint64_t seed, uint32_t bit,
+                                           uint32_t sweep) {
     if (dE <= 0.0) return true;
-    const uint64_t u53 = draw_u53(seed, bit, sweep, 0u);
-    return double(u53) * 0x1.0p-53 < exp(-dE / T);
+    return uphill_accept(draw_u53(seed, bit, sweep, 0u), dE, T, inv_T);
 }
 
 // ---- integer Ising ----------------------------------------------------------------
@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
     int parity = 0;
     for (int sweep = 0; sweep < A.sweeps; ++sweep) {
         const double T = A.temp[sweep];
+        const float inv_T = float(1.0 / T);
         for (int c = 0; c < A.n_colours; ++c, parity ^= 1) {
             const int c1 = A.class_ptr[c + 1];
             // 1. decide every bit of the class; with wide rows, list the
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
             for (int i = A.class_ptr[c] + int(threadIdx.x); i < c1; i += blockDim.x) {
                 const int si = s[i];
                 const long long dE = -(long long)si * (long long)f[i];
-                if (metropolis(double(dE), T, seed, uint32_t(A.order[i]), uint32_t(sweep))) {
+                if (metropolis(double(dE), T, inv_T, seed, uint32_t(A.order[i]), uint32_t(sweep))) {
                     s[i] = int8_t(-si);
                     E += dE;
                     // f_j -= 2 w_ij s_i, in wrap-around uint32 arithmetic: the
@@ -270,7 +271,7 @@ struct ResidStage {
 template <int CL, int G>
 __device__ __forceinline__ bool score_bit(int k, int gl, unsigned gmask, int leader, const ResidStage& S,
                                           const uint4* ent, uint32_t rw_base, uint32_t* xs, int slot0, float lambda,
-                                          double T) {
+                                          double T, float inv_T) {
     constexpr int kShift = CL == 1 ? 0 : CL == 2 ? 1 : CL == 4 ? 2 : CL == 8 ? 3 : 4;
     const int rs = S.row[k], re = S.row[k + 1], ns = S.nbp[k], ne = S.nbp[k + 1];
     float acc = 0.0f;
@@ -289,7 +290,7 @@ __device__ __forceinline__ bool score_bit(int k, int gl, unsigned gmask, int lea
         const float t = __fadd_rn(S.lin[k], acc);
         const float prior = __fmul_rn(lambda, float((ne - ns) - 2 * unlike));
         const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), S.q[k]), prior);
-        accept = (dE <= 0.0f || double(S.u[k]) * 0x1.0p-53 < exp(-double(dE) / T)) ? 1 : 0;
+        accept = (dE <= 0.0f || uphill_accept(S.u[k], double(dE), T, inv_T)) ? 1 : 0;
     }
     accept = __shfl_sync(gmask, accept, leader);
     if (accept) {
@@ -381,6 +382,7 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
             cluster.sync();
         }
         const double T = A.temp[sweep];
+        const float inv_T = float(1.0 / T);
         for (int ci = 0; ci < n_chunks; ++ci) {
             const int4 c0 = chunks[2 * ci];       // b0, b1, slot of b0, last-of-class | heavy bits << 1
             const int4 c1 = chunks[2 * ci + 1];   // e0, e1, n0, n1
@@ -433,10 +435,10 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
             const uint4* ent = A.ent + c1.x;
             const int nh = c0.w >> 1;
             for (int k = warp; k < nh; k += kWarps)
-                my_accepts += (score_bit<CL, 32>(k, lane, kFull, 0, S, ent, rw_base, xs, c0.z, A.lambda, T) && lane == 0);
+                my_accepts += (score_bit<CL, 32>(k, lane, kFull, 0, S, ent, rw_base, xs, c0.z, A.lambda, T, inv_T) && lane == 0);
             for (int k = nh + grp; k < nb; k += kGroups)
                 my_accepts += (score_bit<CL, kGroup>(k, gl, gmask, lane & ~(kGroup - 1), S, ent, rw_base, xs, c0.z,
-                                                     A.lambda, T) && gl == 0);
+                                                     A.lambda, T, inv_T) && gl == 0);
             if (PHASES) {
                 __syncthreads();
                 const long long t1 = clock64();
@@ -632,6 +634,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             if (!ok) break;
         }
         const double T = A.temp[sweep];
+        const float inv_T = float(1.0 / T);
         for (int ci = 0; ci < n_chunks; ++ci, ++gci) {
             const int4 c0 = cur0, c1 = cur1;
             // stage the next chunk (wrapping into the next sweep), then wait for this one;
@@ -734,7 +737,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
                     const float prior = __fmul_rn(A.lambda, float((ne - ns) - 2 * unlike));
                     const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), __uint_as_float(m1.y)), prior);
-                    flip = (dE <= 0.0f || double(u53) * 0x1.0p-53 < exp(-double(dE) / T)) ? 1 : 0;
+                    flip = (dE <= 0.0f || uphill_accept(u53, double(dE), T, inv_T)) ? 1 : 0;
                 }
                 const unsigned amask = __ballot_sync(kFull, flip) & 0xFFFFu;
                 if (amask) {

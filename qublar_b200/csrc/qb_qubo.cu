@@ -22,7 +22,8 @@
 // records |fp32 - fp64| (the drift) and restarts hi + lo from it. The final
 // energies are recomputed in fp64 from scratch by a separate kernel.
 // Acceptance: dE <= 0, else u53 * 2^-53 < exp(-dE / T) in double, u53 the
-// Philox draw of (replica seed, original bit, sweep).
+// Philox draw of (replica seed, original bit, sweep); uphill_accept settles
+// most draws in fp32 with the same outcome.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -65,6 +66,19 @@ struct QuboArgs {
     unsigned long long* accepts;   // R
 };
 
+// 32 x 32 bit transpose across the warp: lane p returns the word whose bit q
+// is bit p of lane q's w (five rounds of block swaps between lanes l, l ^ j).
+__device__ __forceinline__ unsigned warp_transpose32(unsigned w, int lane) {
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const unsigned L = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu : j == 2 ? 0x33333333u
+                                                                                                  : 0x55555555u;
+        const unsigned o = __shfl_xor_sync(kFullMask, w, j);
+        w = (lane & j) ? ((w & ~L) | ((o & ~L) >> j)) : ((w & L) | ((o & L) << j));
+    }
+    return w;
+}
+
 // hi + lo += v, the rounding error of the fp32 add carried into lo (Knuth's
 // TwoSum; no fused operations).
 __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float v) {
@@ -103,6 +117,7 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
     bool ok = grid_barrier(A.bar, A.err, ++round);
     for (int sweep = 0; sweep < A.sweeps && ok; ++sweep) {
         const double T = A.temp[sweep];
+        const float inv_T = float(1.0 / T);
         const bool refresh = A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0;
         for (int c = 0; c < A.n_colours && ok; ++c) {
             const int c1 = A.class_ptr[c + 1];
@@ -124,9 +139,31 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                         f = __ldcg(A.fw + nb);
                         if (f != 0ull || refresh) x = __ldcg(A.xw + nb);
                     }
-                    // neighbours to walk in CSR order: those some replica flipped
-                    // (every one on a refresh sweep)
-                    unsigned todo = __ballot_sync(kFullMask, k < k1 && (f != 0ull || refresh));
+                    if (!refresh) {
+                        // each lane walks, in CSR order, the neighbours that one of its two
+                        // replicas flipped: bit q of F0 (F1) = neighbour kb + q flipped in
+                        // replica r0 (r1), so the warp iterates over the busiest lane's
+                        // flips instead of every neighbour that any replica flipped
+                        if (__ballot_sync(kFullMask, f != 0ull) == 0u) continue;
+                        const unsigned F0 = warp_transpose32(uint32_t(f), lane);
+                        const unsigned F1 = warp_transpose32(uint32_t(f >> 32), lane);
+                        const unsigned xlo = uint32_t(x), xhi = uint32_t(x >> 32);
+                        unsigned todo = F0 | F1;
+                        while (__any_sync(kFullMask, todo != 0u)) {
+                            const unsigned bit = todo & (0u - todo);
+                            const int q = bit ? __ffs(bit) - 1 : 0;
+                            todo ^= bit;
+                            const float Jq = __shfl_sync(kFullMask, Jk, q);
+                            const unsigned xl = __shfl_sync(kFullMask, xlo, q);
+                            const unsigned xh = __shfl_sync(kFullMask, xhi, q);
+                            if (F0 & bit) two_sum_acc(hi0, lo0, ((xl >> lane) & 1u) ? Jq : -Jq);
+                            if (F1 & bit) two_sum_acc(hi1, lo1, ((xh >> lane) & 1u) ? Jq : -Jq);
+                        }
+                        continue;
+                    }
+                    // refresh sweep: walk every neighbour in CSR order (the fp64 sum needs
+                    // every x), applying the flips' deltas as above
+                    unsigned todo = __ballot_sync(kFullMask, k < k1);
                     while (todo) {
                         const int q = __ffs(todo) - 1;
                         todo &= todo - 1u;
@@ -156,11 +193,9 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                 const uint32_t oj = uint32_t(__ldg(A.order + j));
                 bool acc0 = false, acc1 = false;
                 if (has0)
-                    acc0 = dE0 <= 0.0f ||
-                           double(draw_u53(seed_a, oj, uint32_t(sweep), 0u)) * 0x1.0p-53 < exp(-double(dE0) / T);
+                    acc0 = dE0 <= 0.0f || uphill_accept(draw_u53(seed_a, oj, uint32_t(sweep), 0u), double(dE0), T, inv_T);
                 if (has1)
-                    acc1 = dE1 <= 0.0f ||
-                           double(draw_u53(seed_b, oj, uint32_t(sweep), 0u)) * 0x1.0p-53 < exp(-double(dE1) / T);
+                    acc1 = dE1 <= 0.0f || uphill_accept(draw_u53(seed_b, oj, uint32_t(sweep), 0u), double(dE1), T, inv_T);
                 const unsigned m0 = __ballot_sync(kFullMask, acc0), m1 = __ballot_sync(kFullMask, acc1);
                 const unsigned long long mask = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
                 if (lane == 0) {
