@@ -1,5 +1,7 @@
 // The C ABI (include/qublar.h): validation, planning, upload, solve, results.
 #include <algorithm>
+#include <cstdio>
+#include <chrono>
 #include <climits>
 #include <functional>
 #ifdef _OPENMP
@@ -287,23 +289,50 @@ qb_status check_residual(const qb_residual_desc* d) {
     const int64_t nnz = d->row_ptr[n];
     if (nnz > 0 && (!d->ray || !d->a)) return fail(QB_EINVAL, "residual: null ray or a");
     if (d->nbr_ptr[n] > 0 && !d->nbr) return fail(QB_EINVAL, "residual: null nbr");
-    std::vector<int32_t> stamp(size_t(std::max(d->n_rays, 1)), -1);
-    for (int i = 0; i < n; ++i) {
-        for (int k = d->row_ptr[i]; k < d->row_ptr[i + 1]; ++k) {
-            const int b = d->ray[k];
-            if (b < 0 || b >= d->n_rays) return fail(QB_EINVAL, "residual: ray index out of range");
-            if (stamp[size_t(b)] == i) return fail(QB_EINVAL, "residual: a bit lists a ray twice");
-            stamp[size_t(b)] = i;
-            if (!std::isfinite(d->a[k])) return fail(QB_EINVAL, "residual: non-finite a");
+    // Bits are checked in parallel; the reported failure is the one of the
+    // lowest failing bit (its first failing entry), as a sequential scan finds.
+    static const char* const kWhy[] = {nullptr, "residual: ray index out of range",
+                                       "residual: a bit lists a ray twice", "residual: non-finite a",
+                                       "residual: neighbour index out of range",
+                                       "residual: the neighbour lists are not symmetric"};
+    int first_bad = n, why = 0;
+#pragma omp parallel
+    {
+        std::vector<int32_t> stamp(size_t(std::max(d->n_rays, 1)), -1);
+        int my_bad = n, my_why = 0;
+#pragma omp for schedule(static, 2048)
+        for (int i = 0; i < n; ++i) {
+            if (i > my_bad) continue;
+            int w = 0;
+            for (int k = d->row_ptr[i]; k < d->row_ptr[i + 1] && !w; ++k) {
+                const int b = d->ray[k];
+                if (b < 0 || b >= d->n_rays) w = 1;
+                else if (stamp[size_t(b)] == i) w = 2;
+                else if (!std::isfinite(d->a[k])) w = 3;
+                else stamp[size_t(b)] = i;
+            }
+            for (int k = d->nbr_ptr[i]; k < d->nbr_ptr[i + 1] && !w; ++k) {
+                const int j = d->nbr[k];
+                if (j < 0 || j >= n || j == i) {
+                    w = 4;
+                } else {
+                    bool back = false;
+                    for (int q = d->nbr_ptr[j]; q < d->nbr_ptr[j + 1]; ++q) back |= d->nbr[q] == i;
+                    if (!back) w = 5;
+                }
+            }
+            if (w && i < my_bad) {
+                my_bad = i;
+                my_why = w;
+            }
         }
-        for (int k = d->nbr_ptr[i]; k < d->nbr_ptr[i + 1]; ++k) {
-            const int j = d->nbr[k];
-            if (j < 0 || j >= n || j == i) return fail(QB_EINVAL, "residual: neighbour index out of range");
-            bool back = false;
-            for (int q = d->nbr_ptr[j]; q < d->nbr_ptr[j + 1]; ++q) back |= d->nbr[q] == i;
-            if (!back) return fail(QB_EINVAL, "residual: the neighbour lists are not symmetric");
+#pragma omp critical
+        if (my_bad < first_bad) {
+            first_bad = my_bad;
+            why = my_why;
         }
     }
+    if (why) return fail(QB_EINVAL, kWhy[why]);
     for (int b = 0; b < d->n_rays; ++b)
         if (!std::isfinite(d->d[b]) || !std::isfinite(d->w[b])) return fail(QB_EINVAL, "residual: non-finite d or w");
     return QB_OK;
@@ -322,7 +351,14 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     P.nnz = d->row_ptr[n];
     P.n_nbr = d->nbr_ptr[n];
     P.lambda = d->lambda;
+    const bool times = std::getenv("QB_PLAN_TIMES") != nullptr;
+    std::vector<std::pair<const char*, std::chrono::steady_clock::time_point>> marks;
+    auto mark = [&](const char* what) {
+        if (times) marks.emplace_back(what, std::chrono::steady_clock::now());
+    };
+    mark("start");
     P.col = colour_residual(n, nr, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
+    mark("colour");
     Colouring& C = P.col;
     const int nc = C.n_colours();
     auto deg = [&](int i) { return d->row_ptr[i + 1] - d->row_ptr[i]; };
@@ -388,6 +424,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         }
     }
     for (int k = 0; k < n; ++k) C.inverse[size_t(C.order[size_t(k)])] = k;
+    mark("slices");
     const bool lock = P.variant == QB_RESID_LOCKSTEP;
     // homes (cluster variant): bit k of slice t of class c -> (t << 27) |
     // running slot of CTA t
@@ -456,6 +493,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
             m[6] = uint32_t(C.order[size_t(k)]);
         }
     }
+    mark("arrays");
     // chunk table of every CTA (see ResidualPlan)
     const int kB = lock ? resid_lockstep_chunk_bits() : resid_chunk_bits();
     const int kE = lock ? resid_lockstep_chunk_entries() : resid_chunk_entries();
@@ -491,6 +529,10 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         }
         P.chunk_ptr[size_t(t) + 1] = int32_t(P.chunks.size() / 8);
     }
+    mark("chunks");
+    for (size_t k = 1; k < marks.size(); ++k)
+        std::fprintf(stderr, "[qb plan]   %s %.1f ms\n", marks[k].first,
+                     std::chrono::duration<double, std::milli>(marks[k].second - marks[k - 1].second).count());
     return QB_OK;
 }
 
@@ -500,7 +542,7 @@ int64_t residual_device_bytes(const ResidualPlan& P) {
     int64_t b = int64_t(P.h_ent.size() + P.h_row.size() + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
                         P.h_nbr_home.size() + P.col.order.size() + P.col.class_ptr.size() + P.chunks.size() +
                         P.chunk_ptr.size()) * 4;
-    b += 2 * ((nr + 1) * 4 + nnz * 8) + n * 8 + nr * 16 + (n + 1) * 4 + P.n_nbr * 4;
+    b += (nr + 1) * 4 + nnz * 12 + n * 8 + nr * 16 + (n + 1) * 4 + P.n_nbr * 4;   // ray-major CSR (two bit orders)
     if (P.variant == QB_RESID_LOCKSTEP) b += int64_t(P.h_meta.size() + P.h_nbr_new.size()) * 4 + nnz * 4;
     return b;
 }
@@ -515,10 +557,10 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     // thread counts its bits per ray, the counts are prefix-summed across
     // threads, and each thread fills its own offsets (ascending bits per ray)
     std::vector<int32_t> rrow(size_t(nr) + 1, 0);
-    std::vector<int32_t> rbit_o(static_cast<size_t>(P.nnz));
-    std::vector<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
-    std::vector<int32_t> rbit_n(static_cast<size_t>(P.nnz));
-    std::vector<float> ra(static_cast<size_t>(P.nnz));
+    RawVec<int32_t> rbit_o(static_cast<size_t>(P.nnz));
+    RawVec<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
+    RawVec<int32_t> rbit_n(static_cast<size_t>(P.nnz));
+    RawVec<float> ra(static_cast<size_t>(P.nnz));
     {
         int T = 1;
 #ifdef _OPENMP
@@ -569,7 +611,7 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     QB_UP(d_nbr_ptr, P.h_nbr_ptr); QB_UP(d_nbr_home, P.h_nbr_home); QB_UP(d_order, C.order);
     QB_UP(d_class_ptr, C.class_ptr); QB_UP(d_chunks, P.chunks); QB_UP(d_chunk_ptr, P.chunk_ptr);
     QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra);
-    QB_UP(d_o_rrow, rrow); QB_UP(d_o_rbit, rbit_o); QB_UP(d_o_ra, ra); QB_UP(d_o_lin, o_lin);
+    QB_UP(d_o_rbit, rbit_o); QB_UP(d_o_lin, o_lin);
     if (P.variant == QB_RESID_LOCKSTEP) {
         QB_UP(d_meta, P.h_meta); QB_UP(d_nbr_new, P.h_nbr_new); QB_UP(d_rbit_new, rbit_n);
     }
@@ -581,14 +623,14 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     QB_CUDA(cudaStreamSynchronize(st));   // the host vectors above are locals
     const DevBuf* all[] = {&P.d_row, &P.d_ent, &P.d_lin, &P.d_q, &P.d_nbr_ptr, &P.d_nbr_home, &P.d_order,
                            &P.d_class_ptr, &P.d_chunks, &P.d_chunk_ptr, &P.d_d, &P.d_w64, &P.d_rrow, &P.d_rbit,
-                           &P.d_ra, &P.d_o_rrow, &P.d_o_rbit, &P.d_o_ra, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin,
+                           &P.d_ra, &P.d_o_rbit, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin,
                            &P.d_meta, &P.d_nbr_new, &P.d_rbit_new};
     int64_t tot = 0;
     for (const DevBuf* b : all) tot += int64_t(b->bytes);
     *bytes = tot;
     // the plan's host copies are not needed after the upload (unless the
     // problem may go to the device again)
-    if (!keep_host) std::vector<uint32_t>().swap(P.h_ent);
+    if (!keep_host) RawVec<uint32_t>().swap(P.h_ent);
     return QB_OK;
 }
 
@@ -665,7 +707,7 @@ void qb::problem_release_device(qb_problem* p) {
     DevBuf* rb[] = {&R.d_row, &R.d_ent, &R.d_lin, &R.d_q, &R.d_nbr_ptr, &R.d_nbr_home, &R.d_order, &R.d_class_ptr,
                     &R.d_chunks, &R.d_chunk_ptr, &R.d_d, &R.d_w64, &R.d_rrow, &R.d_rbit, &R.d_ra, &R.d_meta,
                     &R.d_nbr_new, &R.d_rbit_new, &R.d_o_row, &R.d_o_ray, &R.d_o_a, &R.d_o_nbr_ptr, &R.d_o_nbr,
-                    &R.d_o_lin, &R.d_o_rrow, &R.d_o_rbit, &R.d_o_ra};
+                    &R.d_o_lin, &R.d_o_rbit};
     for (DevBuf* b : rb) b->release();
     QuboPlan& Q = p->qubo;
     DevBuf* qbf[] = {&Q.d_row, &Q.d_adj, &Q.d_J, &Q.d_h, &Q.d_order, &Q.d_class_ptr, &Q.d_eu, &Q.d_ev, &Q.d_ew, &Q.d_ho};
@@ -705,6 +747,13 @@ extern "C" qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb
 extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts* opts, qb_problem** out) {
     if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_residual: null argument");
     *out = nullptr;
+    // QB_PLAN_TIMES=1 prints the host check, plan and upload times to stderr
+    const bool times = std::getenv("QB_PLAN_TIMES") != nullptr;
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    const auto t0 = now();
     qb_status s = check_residual(desc);
     if (s != QB_OK) return s;
     qb_problem* p = new (std::nothrow) qb_problem();
@@ -713,8 +762,10 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
     const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
     const bool cluster = opts && (opts->flags & QB_OPT_RESID_CLUSTER);
     s = select_device(opts, &p->device);
+    const auto t1 = now();
     if (s == QB_OK) s = plan_residual(desc, p->resid, cluster ? 0 : resid_lockstep_grid());
     if (s == QB_OK && p->resid.variant == QB_RESID_CLUSTER) s = resid_check_fit(p->resid);
+    const auto t2 = now();
     if (s == QB_OK && defer) {
         HostDesc& h = p->host;
         const int n = desc->n_vars, nr = desc->n_rays;
@@ -735,6 +786,9 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
         s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
         p->uploaded = s == QB_OK;
     }
+    if (times)
+        std::fprintf(stderr, "[qb plan] check %.1f ms, plan %.1f ms, upload %.1f ms\n", ms(t0, t1), ms(t1, t2),
+                     ms(t2, now()));
     if (s != QB_OK) {
         delete p;
         return s;

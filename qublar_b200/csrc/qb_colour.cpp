@@ -7,11 +7,16 @@
 // be updated at once because no two of them share a coupling (Ising) or a ray
 // or a prior bond (residual form): the dE each one sees is exact.
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 
 #include "qb_internal.hpp"
 
 namespace qb {
+
+namespace {
+constexpr int kColourWords = 8;   // 64-colour words per ray row at the start: one cache line
+}  // namespace
 
 void finish_colouring(Colouring& c, int n) {
     int nc = 0;
@@ -60,60 +65,94 @@ Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32
                           const int32_t* nbr_ptr, const int32_t* nbr) {
     Colouring c;
     c.colour.assign(size_t(n), -1);
-    // Per-ray bitset of the colours already on the ray. Grown in 64-colour
-    // words when a bit runs out of free colours.
-    int words = 4;
-    std::vector<uint64_t> used(size_t(n_rays) * size_t(words), 0);
-    std::vector<uint64_t> forbid;
-    auto grow = [&](int new_words) {
-        std::vector<uint64_t> g(size_t(n_rays) * size_t(new_words), 0);
-        for (int b = 0; b < n_rays; ++b)
-            std::memcpy(&g[size_t(b) * size_t(new_words)], &used[size_t(b) * size_t(words)],
-                        sizeof(uint64_t) * size_t(words));
-        used.swap(g);
-        words = new_words;
+    // Per-ray bitset of the colours already on the ray: `words` 64-colour
+    // words per ray, one 64-byte cache line at the start (512 colours), grown
+    // when a bit runs out of free colours. The rows start on a cache line.
+    int words = kColourWords;
+    std::vector<uint64_t> store;
+    uint64_t* used = nullptr;
+    auto alloc_rows = [&](int w) {
+        std::vector<uint64_t> g(size_t(std::max(n_rays, 1)) * size_t(w) + 8, 0);
+        uint64_t* base = g.data();
+        while (reinterpret_cast<uintptr_t>(base) % 64) ++base;
+        if (used)
+            for (int b = 0; b < n_rays; ++b)
+                std::memcpy(base + size_t(b) * size_t(w), used + size_t(b) * size_t(words), sizeof(uint64_t) * size_t(words));
+        store.swap(g);
+        used = base;
+        words = w;
     };
+    alloc_rows(kColourWords);
     // Visit bits by their conflict degree counted with multiplicity (the sum
-    // of the lengths of their rays), largest first (Welsh-Powell order): long
-    // conflict lists get the low colours, which keeps the class count near
-    // the longest ray (340 classes on the 306,328-bit pyramid whose longest
-    // ray crosses 288 bits; ordering by ray count gives 349).
+    // of the lengths of their rays), largest first (Welsh-Powell order), ties
+    // by index: long conflict lists get the low colours, which keeps the class
+    // count near the longest ray (340 classes on the 306,328-bit pyramid whose
+    // longest ray crosses 288 bits; ordering by ray count gives 349).
     std::vector<int32_t> raylen(static_cast<size_t>(std::max(n_rays, 1)), 0);
     for (int i = 0; i < n; ++i)
         for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) raylen[size_t(ray[k])]++;
     std::vector<int64_t> conf(static_cast<size_t>(n), 0);
-    for (int i = 0; i < n; ++i)
-        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) conf[size_t(i)] += raylen[size_t(ray[k])];
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        int64_t s = 0;
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) s += raylen[size_t(ray[k])];
+        conf[size_t(i)] = s;
+    }
+    // stable counting sort by decreasing conflict degree
+    int64_t cmax = 0;
+    for (int i = 0; i < n; ++i) cmax = std::max(cmax, conf[size_t(i)]);
     std::vector<int32_t> vis(static_cast<size_t>(n));
-    for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
-    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) { return conf[size_t(a)] > conf[size_t(b)]; });
-    int top = -1;   // highest colour given so far: words above (top >> 6) + 1 are empty
-    for (int i : vis) {
-        for (;;) {
-            const int nw = std::min(words, ((top + 1) >> 6) + 1);   // words that can hold a used colour, plus the next
-            forbid.assign(size_t(nw), 0);
+    if (cmax <= int64_t(16) * n + (1 << 20)) {
+        std::vector<int32_t> start(size_t(cmax) + 2, 0);
+        for (int i = 0; i < n; ++i) start[size_t(cmax - conf[size_t(i)]) + 1]++;
+        for (int64_t v = 0; v <= cmax; ++v) start[size_t(v) + 1] += start[size_t(v)];
+        for (int i = 0; i < n; ++i) vis[size_t(start[size_t(cmax - conf[size_t(i)])]++)] = i;
+    } else {
+        for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
+        std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) { return conf[size_t(a)] > conf[size_t(b)]; });
+    }
+    // First fit: the lowest colour on none of the bit's rays and on none of its
+    // prior neighbours.
+    std::vector<uint64_t> forbid;
+    for (size_t v = 0; v < vis.size(); ++v) {
+        const int i = vis[v];
+        if (v + 2 < vis.size()) {   // the rows of the bit after next into cache (they are random rays)
+            const int i2 = vis[v + 2];
+            for (int k = row_ptr[i2]; k < row_ptr[i2 + 1]; ++k)
+                __builtin_prefetch(used + size_t(ray[k]) * size_t(words), 1);
+        }
+        int cc = -1;
+        if (words == kColourWords) {
+            uint64_t f[kColourWords] = {};
             for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
-                const uint64_t* u = &used[size_t(ray[k]) * size_t(words)];
-                for (int q = 0; q < nw; ++q) forbid[size_t(q)] |= u[q];
+                const uint64_t* u = used + size_t(ray[k]) * kColourWords;
+                for (int q = 0; q < kColourWords; ++q) f[q] |= u[q];
             }
             for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
                 const int cj = c.colour[size_t(nbr[k])];
-                if (cj >= 0 && cj < 64 * nw) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
+                if (cj >= 0) f[cj >> 6] |= uint64_t(1) << (cj & 63);
             }
-            int cc = -1;
-            for (int q = 0; q < nw && cc < 0; ++q)
-                if (~forbid[size_t(q)]) cc = 64 * q + __builtin_ctzll(~forbid[size_t(q)]);
-            if (cc < 0) {
-                if (nw == words) grow(words * 2);
-                top = std::max(top, 64 * nw - 1);   // widen the scan to the next word
-                continue;
-            }
-            c.colour[size_t(i)] = cc;
-            top = std::max(top, cc);
-            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
-                used[size_t(ray[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
-            break;
+            for (int q = 0; q < kColourWords && cc < 0; ++q)
+                if (~f[q]) cc = 64 * q + __builtin_ctzll(~f[q]);
+            if (cc < 0) alloc_rows(2 * kColourWords);   // all 512 taken: continue with wider rows
         }
+        while (cc < 0) {
+            forbid.assign(size_t(words), 0);
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+                const uint64_t* u = used + size_t(ray[k]) * size_t(words);
+                for (int q = 0; q < words; ++q) forbid[size_t(q)] |= u[q];
+            }
+            for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
+                const int cj = c.colour[size_t(nbr[k])];
+                if (cj >= 0) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
+            }
+            for (int q = 0; q < words && cc < 0; ++q)
+                if (~forbid[size_t(q)]) cc = 64 * q + __builtin_ctzll(~forbid[size_t(q)]);
+            if (cc < 0) alloc_rows(words * 2);
+        }
+        c.colour[size_t(i)] = cc;
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+            used[size_t(ray[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
     }
     finish_colouring(c, n);
     return c;

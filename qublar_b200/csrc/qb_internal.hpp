@@ -5,7 +5,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "qublar.h"
@@ -64,10 +68,35 @@ struct DevBuf {
 
 qb_status upload(DevBuf& dst, const void* src, size_t bytes, cudaStream_t st);
 
-template <typename T>
-qb_status upload_vec(DevBuf& dst, const std::vector<T>& v, cudaStream_t st) {
+template <typename T, typename A>
+qb_status upload_vec(DevBuf& dst, const std::vector<T, A>& v, cudaStream_t st) {
     return upload(dst, v.data(), v.size() * sizeof(T), st);
 }
+
+// An allocator whose value-initialisation leaves elements uninitialised, for
+// large host tables that a parallel loop fills right after sizing: the
+// single-threaded zero fill is skipped and the filling threads touch the
+// pages first.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using RawVec = std::vector<T, NoInitAlloc<T>>;
 
 // The temperature of every sweep of a schedule (host, double).
 std::vector<double> temperatures(const qb_schedule& s);
@@ -146,7 +175,8 @@ struct ResidualPlan {
     std::vector<uint32_t> h_meta;     // lockstep: per bit 8 words {row start, rays, nbr start, nbrs, lin, q, index, 0}
     // host copies of the sweep-order arrays (h_ent is released after upload)
     std::vector<int32_t> h_row, h_nbr_ptr;
-    std::vector<uint32_t> h_ent, h_nbr_home;
+    RawVec<uint32_t> h_ent;
+    std::vector<uint32_t> h_nbr_home;
     std::vector<float> h_lin, h_q;
     // device arrays in sweep order
     DevBuf d_row, d_ent, d_lin, d_q, d_nbr_ptr, d_nbr_home, d_order, d_class_ptr, d_chunks, d_chunk_ptr;
@@ -155,7 +185,7 @@ struct ResidualPlan {
     DevBuf d_meta, d_nbr_new, d_rbit_new;   // lockstep tables
     // energy verifier (original order)
     DevBuf d_o_row, d_o_ray, d_o_a, d_o_nbr_ptr, d_o_nbr, d_o_lin;
-    DevBuf d_o_rrow, d_o_rbit, d_o_ra;
+    DevBuf d_o_rbit;                  // ray-major bits in input order (offsets and a: d_rrow, d_ra)
 };
 
 // Weighted QUBO E(x) = offset + sum_i h_i x_i + sum_e J_e x_u x_v with fp32

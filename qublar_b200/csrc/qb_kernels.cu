@@ -1181,9 +1181,9 @@ qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, 
     A.lambda = p.lambda;
     A.d = p.d_d.as<double>();
     A.w = p.d_w64.as<double>();
-    A.rrow = p.d_o_rrow.as<int32_t>();
+    A.rrow = p.d_rrow.as<int32_t>();   // the ray-major offsets and a are shared with the refresh
     A.rbit = p.d_o_rbit.as<int32_t>();
-    A.ra = p.d_o_ra.as<float>();
+    A.ra = p.d_ra.as<float>();
     A.lin = p.d_o_lin.as<double>();
     A.nbr_ptr = p.d_o_nbr_ptr.as<int32_t>();
     A.nbr = p.d_o_nbr.as<int32_t>();
