@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "qb_build.hpp"
 #include "qb_internal.hpp"
 #include "qb_kernels.hpp"
 #include "qb_qubo.hpp"
@@ -357,7 +358,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         if (times) marks.emplace_back(what, std::chrono::steady_clock::now());
     };
     mark("start");
-    P.col = colour_residual(n, nr, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
+    P.col = colour_residual(n, nr, &P.max_ray_len, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
     mark("colour");
     Colouring& C = P.col;
     const int nc = C.n_colours();
@@ -442,7 +443,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         }
     P.bit_slots = *std::max_element(used.begin(), used.end());
     if (!lock && P.bit_slots >= (1 << 27)) return fail(QB_EREFUSED, "residual: too many bits per CTA");
-    // sweep-order arrays: offsets first, then every bit's entries in parallel
+    // sweep-order per-bit arrays (the entry table itself is assembled at upload)
     P.h_row.assign(size_t(n) + 1, 0);
     P.h_nbr_ptr.assign(size_t(n) + 1, 0);
     for (int k = 0; k < n; ++k) {
@@ -450,7 +451,6 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         P.h_row[size_t(k) + 1] = P.h_row[size_t(k)] + (d->row_ptr[i + 1] - d->row_ptr[i]);
         P.h_nbr_ptr[size_t(k) + 1] = P.h_nbr_ptr[size_t(k)] + (d->nbr_ptr[i + 1] - d->nbr_ptr[i]);
     }
-    P.h_ent.resize(size_t(P.nnz) * 4);
     P.h_lin.resize(size_t(n));
     P.h_q.resize(size_t(n));
     P.h_nbr_home.resize(size_t(P.n_nbr));
@@ -458,18 +458,10 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
 #pragma omp parallel for schedule(static, 1024)
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
-        int32_t pos = P.h_row[size_t(k)];
         double qd = 0.0;
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
             const float a = d->a[e];
-            const float wa = float(d->w[d->ray[e]]) * a;   // the fp32 scatter increment
-            uint32_t* en = &P.h_ent[size_t(pos) * 4];
-            en[0] = uint32_t(d->ray[e]);
-            std::memcpy(&en[1], &a, 4);
-            std::memcpy(&en[2], &wa, 4);
-            en[3] = 0u;
             qd += 0.5 * d->w[d->ray[e]] * double(a) * double(a);
-            ++pos;
         }
         P.h_q[size_t(k)] = float(qd);
         P.h_lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
@@ -539,7 +531,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
 // Device bytes upload_residual will take.
 int64_t residual_device_bytes(const ResidualPlan& P) {
     const int64_t n = P.n, nr = P.n_rays, nnz = P.nnz;
-    int64_t b = int64_t(P.h_ent.size() + P.h_row.size() + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
+    int64_t b = int64_t(P.nnz * 4 + int64_t(P.h_row.size()) + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
                         P.h_nbr_home.size() + P.col.order.size() + P.col.class_ptr.size() + P.chunks.size() +
                         P.chunk_ptr.size()) * 4;
     b += (nr + 1) * 4 + nnz * 12 + n * 8 + nr * 16 + (n + 1) * 4 + P.n_nbr * 4;   // ray-major CSR (two bit orders)
@@ -547,80 +539,158 @@ int64_t residual_device_bytes(const ResidualPlan& P) {
     return b;
 }
 
-qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes,
-                          bool keep_host = false) {
+// The sweep-order entry table and the ray-major CSR on the host: the same
+// arrays as the device assembly (qb_build.cu), for rays too long for its sort.
+static void host_build_residual(const ResidualPlan& P, const qb_residual_desc* d, RawVec<uint32_t>& ent,
+                                std::vector<int32_t>& rrow, RawVec<int32_t>& rbit_o, RawVec<uint32_t>& rbit_h,
+                                RawVec<int32_t>& rbit_n, RawVec<float>& ra) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
-    // ray-major CSR, bits ascending in input order inside a ray: the refresh
-    // (bits by home) and the energy verifier (bits by input index)
-    // counting sort by ray, split over threads by contiguous bit ranges: each
-    // thread counts its bits per ray, the counts are prefix-summed across
-    // threads, and each thread fills its own offsets (ascending bits per ray)
-    std::vector<int32_t> rrow(size_t(nr) + 1, 0);
-    RawVec<int32_t> rbit_o(static_cast<size_t>(P.nnz));
-    RawVec<uint32_t> rbit_h(static_cast<size_t>(P.nnz));
-    RawVec<int32_t> rbit_n(static_cast<size_t>(P.nnz));
-    RawVec<float> ra(static_cast<size_t>(P.nnz));
-    {
-        int T = 1;
+    ent.resize(size_t(P.nnz) * 4);
+#pragma omp parallel for schedule(static, 1024)
+    for (int k = 0; k < n; ++k) {
+        const int i = C.order[size_t(k)];
+        int32_t pos = P.h_row[size_t(k)];
+        for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e, ++pos) {
+            const float a = d->a[e];
+            const float wa = float(d->w[d->ray[e]]) * a;   // the fp32 scatter increment
+            uint32_t* en = &ent[size_t(pos) * 4];
+            en[0] = uint32_t(d->ray[e]);
+            std::memcpy(&en[1], &a, 4);
+            std::memcpy(&en[2], &wa, 4);
+            en[3] = 0u;
+        }
+    }
+    // ray-major CSR, bits ascending in input order inside a ray: a counting
+    // sort by ray split over threads by contiguous bit ranges (each thread
+    // counts its bits per ray, the counts are prefix-summed across threads,
+    // and each thread fills its own slots)
+    rrow.assign(size_t(nr) + 1, 0);
+    rbit_o.resize(size_t(P.nnz));
+    rbit_h.resize(size_t(P.nnz));
+    rbit_n.resize(size_t(P.nnz));
+    ra.resize(size_t(P.nnz));
+    int T = 1;
 #ifdef _OPENMP
-        T = std::max(1, std::min(omp_get_max_threads(), 32));
+    T = std::max(1, std::min(omp_get_max_threads(), 32));
 #endif
-        std::vector<std::vector<int32_t>> cnt(static_cast<size_t>(T));
-        auto bits_of = [&](int t, int* i0, int* i1) {
-            *i0 = int(int64_t(n) * t / T);
-            *i1 = int(int64_t(n) * (t + 1) / T);
-        };
+    std::vector<std::vector<int32_t>> cnt(static_cast<size_t>(T));
+    auto bits_of = [&](int t, int* i0, int* i1) {
+        *i0 = int(int64_t(n) * t / T);
+        *i1 = int(int64_t(n) * (t + 1) / T);
+    };
 #pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        int i0, i1;
+        bits_of(t, &i0, &i1);
+        auto& c = cnt[size_t(t)];
+        c.assign(size_t(nr), 0);
+        for (int e = d->row_ptr[i0]; e < d->row_ptr[i1]; ++e) c[size_t(d->ray[e])]++;
+    }
+    for (int b = 0; b < nr; ++b) {
+        int32_t run = rrow[size_t(b)];
         for (int t = 0; t < T; ++t) {
-            int i0, i1;
-            bits_of(t, &i0, &i1);
-            auto& c = cnt[size_t(t)];
-            c.assign(size_t(nr), 0);
-            for (int e = d->row_ptr[i0]; e < d->row_ptr[i1]; ++e) c[size_t(d->ray[e])]++;
+            const int32_t v = cnt[size_t(t)][size_t(b)];
+            cnt[size_t(t)][size_t(b)] = run;   // this thread's first slot on ray b
+            run += v;
         }
-        for (int b = 0; b < nr; ++b) {
-            int32_t run = rrow[size_t(b)];
-            for (int t = 0; t < T; ++t) {
-                const int32_t v = cnt[size_t(t)][size_t(b)];
-                cnt[size_t(t)][size_t(b)] = run;   // this thread's first slot on ray b
-                run += v;
+        rrow[size_t(b) + 1] = run;
+    }
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        int i0, i1;
+        bits_of(t, &i0, &i1);
+        auto& fill = cnt[size_t(t)];
+        for (int i = i0; i < i1; ++i)
+            for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
+                const int32_t k = fill[size_t(d->ray[e])]++;
+                rbit_o[size_t(k)] = i;
+                rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
+                rbit_n[size_t(k)] = C.inverse[size_t(i)];
+                ra[size_t(k)] = d->a[e];
             }
-            rrow[size_t(b) + 1] = run;
-        }
-#pragma omp parallel for num_threads(T) schedule(static, 1)
-        for (int t = 0; t < T; ++t) {
-            int i0, i1;
-            bits_of(t, &i0, &i1);
-            auto& fill = cnt[size_t(t)];
-            for (int i = i0; i < i1; ++i)
-                for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
-                    const int32_t k = fill[size_t(d->ray[e])]++;
-                    rbit_o[size_t(k)] = i;
-                    rbit_h[size_t(k)] = P.bit_home[size_t(C.inverse[size_t(i)])];
-                    rbit_n[size_t(k)] = C.inverse[size_t(i)];
-                    ra[size_t(k)] = d->a[e];
-                }
-        }
+    }
+}
+
+qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream_t st, int64_t* bytes) {
+    const int n = P.n, nr = P.n_rays;
+    const Colouring& C = P.col;
+    const bool lock = P.variant == QB_RESID_LOCKSTEP;
+    qb_status s;
+    // the O(nnz) tables: assembled on the device from the caller's CSR unless a
+    // ray is too long for the device sort (QB_RESID_BUILD=host forces the host)
+    const char* bv = std::getenv("QB_RESID_BUILD");
+    const bool on_device = P.max_ray_len <= kRaySortMax && !(bv && std::strcmp(bv, "host") == 0);
+    RawVec<uint32_t> ent;
+    std::vector<int32_t> rrow;
+    RawVec<int32_t> rbit_o, rbit_n;
+    RawVec<uint32_t> rbit_h;
+    RawVec<float> ra;
+    DevBuf t_row_ptr, t_ray, t_a, t_inverse, t_home, t_rcount, t_cursor, t_rkey, t_rbit_n;
+    if (on_device) {
+        if ((s = upload(t_row_ptr, d->row_ptr, (size_t(n) + 1) * 4, st))) return s;
+        if ((s = upload(t_ray, d->ray, size_t(P.nnz) * 4, st))) return s;
+        if ((s = upload(t_a, d->a, size_t(P.nnz) * 4, st))) return s;
+        if ((s = upload_vec(t_inverse, C.inverse, st))) return s;
+        if ((s = upload_vec(t_home, P.bit_home, st))) return s;
+        if ((s = upload_vec(P.d_row, P.h_row, st))) return s;
+        if ((s = upload_vec(P.d_order, C.order, st))) return s;
+        if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
+        if ((s = P.d_ent.alloc(size_t(P.nnz) * 16))) return s;
+        if ((s = P.d_rrow.alloc((size_t(nr) + 1) * 4))) return s;
+        if ((s = P.d_o_rbit.alloc(size_t(P.nnz) * 4))) return s;
+        if ((s = P.d_rbit.alloc(size_t(P.nnz) * 4))) return s;
+        if ((s = P.d_ra.alloc(size_t(P.nnz) * 4))) return s;
+        DevBuf& rbn = lock ? P.d_rbit_new : t_rbit_n;   // sweep positions: kept by the lockstep sweep only
+        if ((s = rbn.alloc(size_t(P.nnz) * 4))) return s;
+        if ((s = t_rcount.alloc(size_t(std::max(nr, 1)) * 4))) return s;
+        if ((s = t_cursor.alloc(size_t(std::max(nr, 1)) * 4))) return s;
+        if ((s = t_rkey.alloc(size_t(P.nnz) * 8))) return s;
+        ResidBuildArgs A{};
+        A.n = n;
+        A.n_rays = nr;
+        A.row_ptr = t_row_ptr.as<int32_t>();
+        A.ray = t_ray.as<int32_t>();
+        A.a = t_a.as<float>();
+        A.w = P.d_w64.as<double>();
+        A.order = P.d_order.as<int32_t>();
+        A.inverse = t_inverse.as<int32_t>();
+        A.h_row = P.d_row.as<int32_t>();
+        A.bit_home = t_home.as<uint32_t>();
+        A.ent = P.d_ent.as<uint4>();
+        A.rrow = P.d_rrow.as<int32_t>();
+        A.rbit_o = P.d_o_rbit.as<int32_t>();
+        A.rbit_n = rbn.as<int32_t>();
+        A.rbit_h = P.d_rbit.as<uint32_t>();
+        A.ra = P.d_ra.as<float>();
+        A.rcount = t_rcount.as<int32_t>();
+        A.cursor = t_cursor.as<int32_t>();
+        A.rkey = t_rkey.as<unsigned long long>();
+        if ((s = launch_resid_build(A, st))) return s;
+    } else {
+        host_build_residual(P, d, ent, rrow, rbit_o, rbit_h, rbit_n, ra);
     }
     std::vector<double> o_lin(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) o_lin[size_t(i)] = d->field ? d->field[i] : d->kappa;
-    qb_status s;
 #define QB_UP(buf, vec) if ((s = upload_vec(P.buf, vec, st))) return s
-    QB_UP(d_ent, P.h_ent); QB_UP(d_row, P.h_row); QB_UP(d_lin, P.h_lin); QB_UP(d_q, P.h_q);
-    QB_UP(d_nbr_ptr, P.h_nbr_ptr); QB_UP(d_nbr_home, P.h_nbr_home); QB_UP(d_order, C.order);
+    if (!on_device) {
+        QB_UP(d_ent, ent); QB_UP(d_row, P.h_row); QB_UP(d_order, C.order);
+        QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra); QB_UP(d_o_rbit, rbit_o);
+        if (lock) QB_UP(d_rbit_new, rbit_n);
+        if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
+    }
+    QB_UP(d_lin, P.h_lin); QB_UP(d_q, P.h_q);
+    QB_UP(d_nbr_ptr, P.h_nbr_ptr); QB_UP(d_nbr_home, P.h_nbr_home);
     QB_UP(d_class_ptr, C.class_ptr); QB_UP(d_chunks, P.chunks); QB_UP(d_chunk_ptr, P.chunk_ptr);
-    QB_UP(d_rrow, rrow); QB_UP(d_rbit, rbit_h); QB_UP(d_ra, ra);
-    QB_UP(d_o_rbit, rbit_o); QB_UP(d_o_lin, o_lin);
-    if (P.variant == QB_RESID_LOCKSTEP) {
-        QB_UP(d_meta, P.h_meta); QB_UP(d_nbr_new, P.h_nbr_new); QB_UP(d_rbit_new, rbit_n);
+    QB_UP(d_o_lin, o_lin);
+    if (lock) {
+        QB_UP(d_meta, P.h_meta); QB_UP(d_nbr_new, P.h_nbr_new);
     }
 #undef QB_UP
     if ((s = upload(P.d_d, d->d, size_t(nr) * 8, st))) return s;
-    if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
     if ((s = upload(P.d_o_nbr_ptr, d->nbr_ptr, (size_t(n) + 1) * 4, st))) return s;
     if ((s = upload(P.d_o_nbr, d->nbr, size_t(P.n_nbr) * 4, st))) return s;
-    QB_CUDA(cudaStreamSynchronize(st));   // the host vectors above are locals
+    QB_CUDA(cudaStreamSynchronize(st));   // the host vectors and device scratch above are locals
     const DevBuf* all[] = {&P.d_row, &P.d_ent, &P.d_lin, &P.d_q, &P.d_nbr_ptr, &P.d_nbr_home, &P.d_order,
                            &P.d_class_ptr, &P.d_chunks, &P.d_chunk_ptr, &P.d_d, &P.d_w64, &P.d_rrow, &P.d_rbit,
                            &P.d_ra, &P.d_o_rbit, &P.d_o_nbr_ptr, &P.d_o_nbr, &P.d_o_lin,
@@ -628,9 +698,6 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
     int64_t tot = 0;
     for (const DevBuf* b : all) tot += int64_t(b->bytes);
     *bytes = tot;
-    // the plan's host copies are not needed after the upload (unless the
-    // problem may go to the device again)
-    if (!keep_host) RawVec<uint32_t>().swap(P.h_ent);
     return QB_OK;
 }
 
@@ -692,7 +759,7 @@ qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
         const qb_residual_desc d{p->resid.n, p->resid.n_rays, h.d.data(), h.w.data(), h.row_ptr.data(), h.ray.data(),
                                  h.a.data(), h.nbr_ptr.data(), h.nbr.data(), h.lambda, h.kappa,
                                  h.has_field ? h.field.data() : nullptr};
-        s = upload_residual(p->resid, &d, st, &p->device_bytes, true);
+        s = upload_residual(p->resid, &d, st, &p->device_bytes);
     }
     if (s != QB_OK) return s;
     p->uploaded = true;   // host copies stay: the problem can go to the device again after a release

@@ -61,7 +61,7 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
     return c;
 }
 
-Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32_t* ray,
+Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* row_ptr, const int32_t* ray,
                           const int32_t* nbr_ptr, const int32_t* nbr) {
     Colouring c;
     c.colour.assign(size_t(n), -1);
@@ -91,6 +91,7 @@ Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32
     std::vector<int32_t> raylen(static_cast<size_t>(std::max(n_rays, 1)), 0);
     for (int i = 0; i < n; ++i)
         for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) raylen[size_t(ray[k])]++;
+    if (max_ray_len) *max_ray_len = n_rays > 0 ? *std::max_element(raylen.begin(), raylen.begin() + n_rays) : 0;
     std::vector<int64_t> conf(static_cast<size_t>(n), 0);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {

@@ -120,7 +120,7 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
 // Colouring of the residual conflict graph: bits conflict when they share a
 // ray or are neighbours in the prior. Rays are cliques, handled with per-ray
 // used-colour bitsets (no explicit conflict graph is built).
-Colouring colour_residual(int n, int n_rays, const int32_t* row_ptr, const int32_t* ray,
+Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* row_ptr, const int32_t* ray,
                           const int32_t* nbr_ptr, const int32_t* nbr);
 
 void finish_colouring(Colouring& c, int n);
@@ -175,7 +175,7 @@ struct ResidualPlan {
     std::vector<uint32_t> h_meta;     // lockstep: per bit 8 words {row start, rays, nbr start, nbrs, lin, q, index, 0}
     // host copies of the sweep-order arrays (h_ent is released after upload)
     std::vector<int32_t> h_row, h_nbr_ptr;
-    RawVec<uint32_t> h_ent;
+    int max_ray_len = 0;              // most bits on one ray
     std::vector<uint32_t> h_nbr_home;
     std::vector<float> h_lin, h_q;
     // device arrays in sweep order

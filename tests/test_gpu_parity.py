@@ -15,7 +15,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from qublar_b200 import Budget, IsingProblem, ResidualProblem, Schedule, branch_fractions, classify, synth
+from qublar_b200 import (OPT_RESID_CLUSTER, Budget, IsingProblem, ResidualProblem, Schedule, branch_fractions, classify,
+                         synth)
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
@@ -261,3 +262,25 @@ def test_freezing_keeps_the_void_map_within_seed_spread():
 
     assert kept.size < n
     assert jaccard(got, ref) >= jaccard(other, ref) - 0.15
+
+
+@pytest.mark.parametrize("flags", [0, OPT_RESID_CLUSTER], ids=["lockstep", "cluster"])
+def test_device_and_host_assembly_agree(monkeypatch, flags):
+    """The sweep-order entry table and the ray-major CSR assembled on the
+    device equal the host assembly: branches, fp64 energies (the verifier reads
+    the ray-major CSR) and fractions are identical bit for bit."""
+    arr = synth.tomography(synth.small_tomo_params(0.2, 24))
+    sched = Schedule(50.0, 1.0, 60, 20, 20)
+    out = []
+    for build in ("device", "host"):
+        if build == "host":
+            monkeypatch.setenv("QB_RESID_BUILD", "host")
+        P = ResidualProblem.from_arrays(arr, flags=flags)
+        r = P.solve(sched, 16, 3)
+        out.append((r.branches(), r.energies(), r.marginals()))
+        r.close()
+        P.close()
+    (x1, e1, p1), (x2, e2, p2) = out
+    assert (x1 == x2).all()
+    assert (e1 == e2).all()
+    assert (p1 == p2).all()
