@@ -8,6 +8,7 @@
 // or a prior bond (residual form): the dE each one sees is exact.
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "qb_internal.hpp"
@@ -38,7 +39,8 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
     Colouring c;
     c.colour.assign(size_t(n), -1);
     // Largest degree first (Welsh-Powell order), ties by index: fewer classes
-    // than index order on irregular graphs, identical on regular ones.
+    // than index order on irregular graphs, identical on regular ones; then
+    // the classes are balanced (below).
     std::vector<int32_t> vis(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
     std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) {
@@ -56,6 +58,35 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
         int cc = 0;
         while (size_t(cc) < mark.size() && mark[size_t(cc)] == i) ++cc;
         c.colour[size_t(i)] = cc;
+    }
+    // Balance the classes: a sweep of a class costs ceil(size / workers)
+    // passes, so lopsided greedy classes (27k bits down to 14 on the weighted
+    // lattice) waste passes. Bits of classes above ceil(n / K), in index order,
+    // move to the smallest class below that size that holds none of their
+    // neighbours (the class count does not change).
+    // (QB_GRAPH_BALANCE=0 keeps the greedy classes)
+    const char* bal = std::getenv("QB_GRAPH_BALANCE");
+    int K = 0;
+    for (int i = 0; i < n; ++i) K = std::max(K, c.colour[size_t(i)] + 1);
+    if (K > 1 && !(bal && std::strcmp(bal, "0") == 0)) {
+        const int target = (n + K - 1) / K;
+        std::vector<int32_t> size(static_cast<size_t>(K), 0), seen(static_cast<size_t>(K), -1);
+        for (int i = 0; i < n; ++i) size[size_t(c.colour[size_t(i)])]++;
+        for (int i = 0; i < n; ++i) {
+            const int ci = c.colour[size_t(i)];
+            if (size[size_t(ci)] <= target) continue;
+            for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k) seen[size_t(c.colour[size_t(col[size_t(k)])])] = i;
+            int best = -1;
+            for (int q = 0; q < K; ++q)
+                if (q != ci && size[size_t(q)] < target && seen[size_t(q)] != i &&
+                    (best < 0 || size[size_t(q)] < size[size_t(best)]))
+                    best = q;
+            if (best >= 0) {
+                c.colour[size_t(i)] = best;
+                size[size_t(ci)]--;
+                size[size_t(best)]++;
+            }
+        }
     }
     finish_colouring(c, n);
     return c;
