@@ -495,6 +495,72 @@ qb_status qb_roi_qubo(const qb_residual_desc* p, const int32_t* roi, int32_t n_r
 qb_status qb_enumerate_qubo(int32_t n, const double* h, const double* J, double T, const qb_opts* opts,
                             qb_enum_result* out, double* marginals);
 
+/* The machine export of a tomography solve; replaces the export block of
+ * src/check_ising.cu:507-525 and the masks of tools/export_machine_map.py
+ * (:47-55, :130-145). In directory `dir` it writes
+ *   ising_out_pvoid.bin          float32 nx^3, C order (z, y, x): the p_void of
+ *                                the voxel's bit, -1 outside the unknown domain;
+ *   ising_out_pvoid_noprior.bin  the same for p_void_noprior (when not NULL);
+ *   ising_out_truth.bin          uint8 nx^3, as given (when truth is not NULL);
+ *   ising_out_branches.bin       n_branches x n_vars bytes, branch-major (when not NULL);
+ *   ising_out.meta               text: nx, voxel, lo, branches, vars, lambda, kappa;
+ *   ising_out_tristate.bin       uint8 nx^3: 0 Exists (p <= 0.1), 1 NotThere
+ *                                (p >= 0.9), 2 Undecided (argos::classify,
+ *                                ising_recon.hpp:305-309, in fp32), 255 outside;
+ *   ising_out_traversable.bin    uint8 nx^3: 1 only where Exists;
+ *   ising_out_machine.meta       the loader keys of the two masks.
+ * var_voxel[i] is bit i's voxel index in nx^3; two bits on one voxel are
+ * refused. Host only. */
+typedef struct qb_export_desc {
+    int32_t nx;
+    double voxel;
+    double lo[3];
+    int32_t n_vars;
+    const int32_t* var_voxel;
+    const float* p_void;
+    const float* p_void_noprior;   /* may be NULL */
+    const uint8_t* truth;          /* nx^3, may be NULL */
+    const uint8_t* branches;       /* n_branches x n_vars, may be NULL */
+    int32_t n_branches;
+    double lambda;
+    double kappa;
+} qb_export_desc;
+qb_status qb_write_ising_out(const char* dir, const qb_export_desc* d);
+
+/* A region's QUBO as text for tensor tooling; replaces the writers of
+ * build/ising_out_roi.txt and ising_out_roi_uncertain.txt
+ * (src/check_ising.cu:568-591): line 1 n; n lines "voxel p truth h"; then the
+ * n x n matrix J row by row (qb_roi_qubo fills the upper triangle), every value
+ * followed by a space; reals with 17 significant digits. truth may be NULL
+ * (written as 0). Host only. */
+qb_status qb_write_roi_text(const char* path, int32_t n, const int32_t* voxel, const float* p, const uint8_t* truth,
+                            const double* h, const double* J);
+
+/* General QUBO text, the format the reference writes for its sequencing QUBOs
+ * (src/check_ree_qubo.cu:277-283, read by tools/ree_neal.py):
+ *   line 1: n m offset P optimum
+ *   n lines: i Qd_i c_i           (i = 0..n-1 in order; c = cost / P)
+ *   m lines: i j Qo_ij            (0 <= i < j < n, ascending (i, j))
+ * with E(x) = offset + sum_i Qd_i x_i + sum Qo_ij x_i x_j and reals as %.17g.
+ * qb_parse_qubo_text refuses a bad header, a malformed or short line, linear
+ * lines out of order, a pair with i >= j or out of range, pairs out of order or
+ * repeated, non-finite values and trailing text (reason in qb_last_error).
+ * qb_qubo_text_arrays copies the fp64 data into caller buffers (n, n, m, m, m
+ * elements; any may be NULL); qb_qubo_text_desc points a weighted-QUBO
+ * descriptor at fp32 copies (Qd -> h, Qo -> J, the offset) for
+ * qb_problem_create_qubo, valid until qb_qubo_text_destroy. qb_write_qubo_text
+ * writes the format. Host only. */
+typedef struct qb_qubo_text qb_qubo_text;
+qb_status qb_parse_qubo_text(const char* text, size_t size, qb_qubo_text** out);
+qb_status qb_qubo_text_info(const qb_qubo_text* q, int32_t* n, int64_t* m, double* offset, double* penalty,
+                            double* optimum);
+qb_status qb_qubo_text_arrays(const qb_qubo_text* q, double* qd, double* cost, int32_t* eu, int32_t* ev, double* qo);
+qb_status qb_qubo_text_desc(const qb_qubo_text* q, qb_qubo_desc* d);
+void qb_qubo_text_destroy(qb_qubo_text* q);
+qb_status qb_write_qubo_text(const char* path, int32_t n, int64_t m, double offset, double penalty, double optimum,
+                             const double* qd, const double* cost, const int32_t* eu, const int32_t* ev,
+                             const double* qo);
+
 /* Device energies of k caller states (k x n bytes, 0/1) by an independent
  * edge-list kernel: gising::device_energies (src/ising_gpu.cuh:461-475). */
 qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e);

@@ -18,19 +18,21 @@ call falls back to a CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
 
 from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
                    REQ_FAILED, REQ_PENDING, REQ_RUNNING, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts,
-                   ProblemInfo, QBError, QuboDesc, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig, ServerStats,
-                   check, lib, ptr)
+                   ExportDesc, ProblemInfo, QBError, QuboDesc, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig,
+                   ServerStats, check, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
            "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "parse_rudy",
-           "freeze_rock", "roi_qubo", "enumerate_qubo"]
+           "freeze_rock", "roi_qubo", "enumerate_qubo", "parse_qubo_text", "write_qubo_text", "write_ising_out",
+           "write_roi_text"]
 
 
 @dataclass
@@ -269,6 +271,13 @@ class QuboProblem(_Problem):
     def from_dict(cls, q: dict, **kw) -> "QuboProblem":
         return cls(q["n"], q["eu"], q["ev"], q["ew"], q.get("h"), q.get("offset", 0.0), **kw)
 
+    @classmethod
+    def from_qubo_text(cls, text, **kw) -> "QuboProblem":
+        """A QUBO read from the general QUBO text (parse_qubo_text), its fp64
+        Qd and Qo rounded once to fp32."""
+        q = parse_qubo_text(text)
+        return cls(q["n"], q["eu"], q["ev"], q["Qo"].astype(np.float32), q["Qd"].astype(np.float32), q["offset"], **kw)
+
     def energies(self, X) -> np.ndarray:
         X = np.ascontiguousarray(X, dtype=np.uint8).reshape(-1, self.n)
         e = np.empty(X.shape[0], dtype=np.float64)
@@ -291,6 +300,64 @@ def parse_rudy(text):
         return int(d.n), arr(d.eu), arr(d.ev), arr(d.ew)
     finally:
         lib().qb_graph_destroy(h)
+
+
+def parse_qubo_text(text) -> dict:
+    """The general QUBO text the reference writes for its sequencing QUBOs
+    (check_ree_qubo.cu:277-283): {"n", "offset", "P", "opt", "Qd", "cost", "eu",
+    "ev", "Qo"} in fp64; raises QBError with the refusal reason."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    h = C.c_void_p()
+    check(lib().qb_parse_qubo_text(data, len(data), C.byref(h)))
+    try:
+        n, m = C.c_int32(), C.c_int64()
+        off, pen, opt = C.c_double(), C.c_double(), C.c_double()
+        check(lib().qb_qubo_text_info(h, C.byref(n), C.byref(m), C.byref(off), C.byref(pen), C.byref(opt)))
+        qd, cost = np.empty(n.value), np.empty(n.value)
+        eu, ev, qo = np.empty(m.value, np.int32), np.empty(m.value, np.int32), np.empty(m.value)
+        check(lib().qb_qubo_text_arrays(h, ptr(qd), ptr(cost), ptr(eu), ptr(ev), ptr(qo)))
+        return {"n": int(n.value), "offset": off.value, "P": pen.value, "opt": opt.value, "Qd": qd, "cost": cost,
+                "eu": eu, "ev": ev, "Qo": qo}
+    finally:
+        lib().qb_qubo_text_destroy(h)
+
+
+def write_qubo_text(path, q: dict) -> None:
+    """Writes q (the keys of parse_qubo_text) in the general QUBO text format."""
+    qd = np.ascontiguousarray(q["Qd"], dtype=np.float64)
+    cost = np.ascontiguousarray(q["cost"], dtype=np.float64)
+    eu, ev = _c32(q["eu"]), _c32(q["ev"])
+    qo = np.ascontiguousarray(q["Qo"], dtype=np.float64)
+    check(lib().qb_write_qubo_text(os.fsencode(path), int(q["n"]), int(eu.size), float(q["offset"]), float(q["P"]),
+                                   float(q["opt"]), ptr(qd), ptr(cost), ptr(eu), ptr(ev), ptr(qo)))
+
+
+def write_ising_out(directory, nx: int, voxel: float, lo, var_voxel, p_void, branches=None, p_void_noprior=None,
+                    truth=None, lam: float = 0.0, kappa: float = 0.0) -> None:
+    """The machine export of a tomography solve (check_ising.cu:507-525 and
+    the masks of tools/export_machine_map.py): ising_out_pvoid.bin, .meta,
+    _tristate.bin, _traversable.bin, _machine.meta, and the optional
+    noprior / truth / branches files, in `directory`."""
+    vv = _c32(var_voxel)
+    pv = np.ascontiguousarray(p_void, dtype=np.float32)
+    pd = None if p_void_noprior is None else np.ascontiguousarray(p_void_noprior, dtype=np.float32)
+    tr = None if truth is None else np.ascontiguousarray(truth, dtype=np.uint8)
+    br = None if branches is None else np.ascontiguousarray(branches, dtype=np.uint8)
+    nb = 0 if br is None else int(br.shape[0])
+    d = ExportDesc(int(nx), float(voxel), (C.c_double * 3)(*[float(v) for v in lo]), int(vv.size), ptr(vv), ptr(pv),
+                   ptr(pd), ptr(tr), ptr(br), nb, float(lam), float(kappa))
+    check(lib().qb_write_ising_out(os.fsencode(directory), C.byref(d)))
+
+
+def write_roi_text(path, voxel, p, h, J, truth=None) -> None:
+    """A region's QUBO as text for tensor tooling (the ising_out_roi*.txt
+    writers of check_ising.cu:568-591)."""
+    vv = _c32(voxel)
+    pp = np.ascontiguousarray(p, dtype=np.float32)
+    hh = np.ascontiguousarray(h, dtype=np.float64)
+    JJ = np.ascontiguousarray(J, dtype=np.float64)
+    tr = None if truth is None else np.ascontiguousarray(truth, dtype=np.uint8)
+    check(lib().qb_write_roi_text(os.fsencode(path), int(vv.size), ptr(vv), ptr(pp), ptr(tr), ptr(hh), ptr(JJ)))
 
 
 def freeze_rock(arrays: dict, margin: float, device: int = -1):

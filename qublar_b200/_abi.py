@@ -44,6 +44,13 @@ class QuboDesc(C.Structure):
                 ("h", C.c_void_p), ("offset", C.c_double)]
 
 
+class ExportDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("voxel", C.c_double), ("lo", C.c_double * 3), ("n_vars", C.c_int32),
+                ("var_voxel", C.c_void_p), ("p_void", C.c_void_p), ("p_void_noprior", C.c_void_p),
+                ("truth", C.c_void_p), ("branches", C.c_void_p), ("n_branches", C.c_int32),
+                ("lambda_", C.c_double), ("kappa", C.c_double)]
+
+
 class ResidualDesc(C.Structure):
     _fields_ = [("n_vars", C.c_int32), ("n_rays", C.c_int32), ("d", C.c_void_p), ("w", C.c_void_p),
                 ("row_ptr", C.c_void_p), ("ray", C.c_void_p), ("a", C.c_void_p), ("nbr_ptr", C.c_void_p),
@@ -189,6 +196,16 @@ SIGNATURES = {
     "qb_tomo_arrays": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "qb_tomo_desc": (C.c_int, [_P, C.POINTER(ResidualDesc)]),
     "qb_tomo_destroy": (None, [_P]),
+    "qb_write_ising_out": (C.c_int, [C.c_char_p, C.POINTER(ExportDesc)]),
+    "qb_write_roi_text": (C.c_int, [C.c_char_p, C.c_int32, _P, _P, _P, _P, _P]),
+    "qb_parse_qubo_text": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(_P)]),
+    "qb_qubo_text_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "qb_qubo_text_arrays": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "qb_qubo_text_desc": (C.c_int, [_P, C.POINTER(QuboDesc)]),
+    "qb_qubo_text_destroy": (None, [_P]),
+    "qb_write_qubo_text": (C.c_int, [C.c_char_p, C.c_int32, C.c_int64, C.c_double, C.c_double, C.c_double, _P, _P,
+                                     _P, _P, _P]),
 }
 
 _lib = None

@@ -7,6 +7,8 @@ default /root/reference) and oracle/_ref/libqbref.so has been built from it
 * ree_qubo.json -- the reference's committed REE sequencing QUBOs (six
   instances), its brute-force minima, its engine_check maxima and its per-seed
   anneal_branch energies (experiments/ree_cascade/*.csv, *.txt), copied as data;
+* ree_text/qubo_<id>.txt -- the same six QUBO files byte for byte (the general
+  QUBO text format the reader and writer are checked against);
 * ref_runs.npz -- outputs of the reference's own annealers run here through
   oracle/_ref: wising::anneal on the 800-node ER Max-Cut instance and
   anneal_branch on the small pyramid, 64 seeds each (final energies, per-sweep
@@ -66,6 +68,17 @@ def ree():
         json.dump(out, f, indent=0)
 
 
+def ree_text():
+    base = os.path.join(REF, "experiments", "ree_cascade")
+    out = os.path.join(OUT, "ree_text")
+    os.makedirs(out, exist_ok=True)
+    for iid in REE_IDS:
+        with open(os.path.join(base, f"qubo_{iid}.txt"), "rb") as f:
+            data = f.read()
+        with open(os.path.join(out, f"qubo_{iid}.txt"), "wb") as f:
+            f.write(data)
+
+
 def ref_runs():
     res = {}
     # 800-node ER Max-Cut, T 3 -> 0.05 geometric over 1000 sweeps
@@ -99,5 +112,7 @@ def ref_runs():
 
 if __name__ == "__main__":
     ree()
-    ref_runs()
+    ree_text()
+    if "--no-runs" not in sys.argv:   # the reference's annealer runs take minutes
+        ref_runs()
     print("golden fixtures written to", OUT)

@@ -10,6 +10,9 @@ on N(0,1) couplings. Statistical: final energies agree with the reference's
 own annealer run on the pair-ray encoding of the same QUBO (anneal_branch,
 ising_recon.hpp:121-144), Welch z < 4.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -17,6 +20,8 @@ from oracle import oracle as O
 from qublar_b200 import QuboProblem, Schedule, synth
 
 pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 E_RTOL = 1e-12
 
@@ -97,3 +102,22 @@ def test_maxcut_through_the_qubo_sweep_equals_the_ising_sweep(gen):
     assert (rq.branches() == ri.branches()).all()
     assert (rq.energies() == ri.energies_tracked().astype(np.float64)).all()
     assert rq.info().max_energy_error == 0.0
+
+
+@pytest.mark.parametrize("iid", ["MP_P507-A", "R4_0", "R5_0"])
+def test_ree_text_qubo_reaches_the_brute_force_minimum(iid):
+    """A sequencing QUBO read from the reference's own file (the general QUBO
+    text, check_ree_qubo.cu:277-283) and annealed by the weighted sweep under
+    the reference's MAP schedule: the best of 64 replicas reaches the
+    reference's brute-force minimum (brute_force.csv; fp32 coefficients, so
+    within 1e-6), and every energy is the oracle's qubo_energy."""
+    with open(os.path.join(GOLD, "ree_qubo.json")) as f:
+        want = float(json.load(f)["brute_force"][iid]["qubo_min_energy"])
+    with open(os.path.join(GOLD, "ree_text", f"qubo_{iid}.txt"), "rb") as f:
+        P = QuboProblem.from_qubo_text(f.read())
+    r = P.solve(Schedule(5.0, 1e-3, 400, 20, 64), 64)
+    E, X = r.energies(), r.branches()
+    assert abs(float(E.min()) - want) < 1e-6
+    q = {"n": P.n, "eu": P.eu, "ev": P.ev, "ew": P.ew, "h": P.h, "offset": P.offset}
+    for b in range(0, 64, 9):
+        assert abs(E[b] - O.qubo_energy(q, X[b])) <= 1e-12 * max(1.0, abs(E[b]))
