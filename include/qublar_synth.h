@@ -51,6 +51,14 @@ void qb_tomo_params_default(qb_tomo_params* p);
 typedef struct qb_tomo qb_tomo;
 
 qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out);
+/* The same builder with the ray march on the device (one thread per sky bin;
+ * opts picks the device and stream, may be NULL): the bits, rays, entries,
+ * coefficients and counts equal qb_synth_tomography's bit for bit. The march
+ * is the reference builder's O(rays x path) step (muon_rows,
+ * src/op_muon.hpp:22-51; the exposure walk of src/muon.cuh:66-134); the
+ * Poisson draws and the ray selection stay on the host. QB_ENOTSUP when a sky
+ * bin reaches more than 512 bits (qb_synth_tomography builds those). */
+qb_status qb_synth_tomography_device(const qb_tomo_params* p, const qb_opts* opts, qb_tomo** out);
 /* Sizes: bits, rays, bit-ray entries, neighbour entries. */
 qb_status qb_tomo_sizes(const qb_tomo* t, int32_t* n_vars, int32_t* n_rays, int64_t* nnz, int64_t* n_nbr);
 /* Copy the problem into caller arrays sized by qb_tomo_sizes; truth (n_vars

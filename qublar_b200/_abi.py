@@ -191,6 +191,7 @@ SIGNATURES = {
     "qb_colour_residual": (C.c_int, [C.POINTER(ResidualDesc), _P, _P, C.POINTER(C.c_int32)]),
     "qb_tomo_params_default": (None, [C.POINTER(TomoParams)]),
     "qb_synth_tomography": (C.c_int, [C.POINTER(TomoParams), C.POINTER(_P)]),
+    "qb_synth_tomography_device": (C.c_int, [C.POINTER(TomoParams), C.POINTER(Opts), C.POINTER(_P)]),
     "qb_tomo_sizes": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int64)]),
     "qb_tomo_arrays": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "qb_internal.hpp"
+#include "qb_synth_march.hpp"
 #include "qublar_synth.h"
 
 namespace {
@@ -52,12 +53,9 @@ int64_t poisson(double lam, uint64_t& s) {
     return v < 0.0 ? 0 : int64_t(v);
 }
 
-struct Grid {
-    double lo[3];
-    double v;
-    int n[3];
-    int64_t cells() const { return int64_t(n[0]) * n[1] * n[2]; }
-};
+using qb::BinMarch;
+using qb::Grid;
+using qb::SynthMarch;
 
 // Voxel walk: visit(cell, chord) for every cell the ray crosses, in order.
 template <class Visit>
@@ -110,6 +108,58 @@ void march(const Grid& g, const double o[3], const double d[3], Visit visit) {
         if (c[ax] < 0 || c[ax] >= g.n[ax]) break;
         tmax[ax] += tdel[ax];
     }
+}
+
+// Every sky bin's row on the host: chords averaged over the S x S sub-rays
+// spread over the bin's solid angle (S = 1: the bin's centre line), bits in
+// the order the sub-rays first reach them.
+qb_status march_host(const SynthMarch& M, std::vector<BinMarch>& bins, std::vector<int32_t>& e_bit,
+                     std::vector<float>& e_a) {
+    const int S = M.S;
+    bins.assign(size_t(M.n_det) * M.n_theta * M.n_phi, BinMarch{});
+    std::vector<int64_t> stamp(size_t(M.n_bits), -1);
+    std::vector<int32_t> slot(size_t(M.n_bits), 0);
+    std::vector<double> e_len;
+    int64_t stamp_id = 0;
+    for (int k = 0; k < M.n_det; ++k) {
+        const double* o = &M.det[3 * k];
+        for (int it = 0; it < M.n_theta; ++it)
+            for (int ip = 0; ip < M.n_phi; ++ip) {
+                BinMarch& B = bins[(size_t(k) * M.n_theta + it) * M.n_phi + ip];
+                double tau0 = 0.0, tau = 0.0;
+                const int64_t first = int64_t(e_bit.size());
+                for (int su = 0; su < S; ++su)
+                    for (int sv = 0; sv < S; ++sv) {
+                        const double cs = M.cth[size_t(it) * S + su], ss = M.sth[size_t(it) * S + su];
+                        const size_t pi = (size_t(k) * M.n_phi + ip) * S + sv;
+                        const double dir[3] = {ss * M.cph[pi], ss * M.sph[pi], cs};
+                        tau0 += M.inv_s2 * M.mu_rock * (-o[2]) / cs;   // rock under the base
+                        tau += M.inv_s2 * M.mu_rock * (-o[2]) / cs;
+                        march(M.g, o, dir, [&](int64_t c, double seg) {
+                            if (!M.rock[size_t(c)]) return;
+                            tau0 += M.inv_s2 * M.mu_rock * seg;
+                            tau += M.inv_s2 * (M.is_void[size_t(c)] ? M.mu_air : M.mu_rock) * seg;
+                            const int b = M.cell_bit[size_t(c)];
+                            if (b < 0) return;
+                            if (stamp[size_t(b)] != stamp_id) {
+                                stamp[size_t(b)] = stamp_id;
+                                slot[size_t(b)] = int32_t(int64_t(e_bit.size()) - first);
+                                e_bit.push_back(b);
+                                e_len.push_back(0.0);
+                            }
+                            e_len[size_t(slot[size_t(b)])] += M.inv_s2 * seg;
+                        });
+                    }
+                ++stamp_id;
+                for (double len : e_len) e_a.push_back(float(M.mu_rock * len));
+                e_len.clear();
+                B.tau0 = tau0;
+                B.tau = tau;
+                B.first = first;
+                B.cnt = int64_t(e_bit.size()) - first;
+            }
+    }
+    return QB_OK;
 }
 
 }  // namespace
@@ -165,7 +215,9 @@ extern "C" void qb_tomo_params_default(qb_tomo_params* p) {
     p->seed = 20260929ull;
 }
 
-extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out) {
+namespace {
+
+qb_status synth_tomography(const qb_tomo_params* p, bool on_device, const qb_opts* opts, qb_tomo** out) {
     if (!p || !out) return qb::fail(QB_EINVAL, "qb_synth_tomography: null argument");
     *out = nullptr;
     if (p->voxel <= 0 || p->half_base <= 0 || p->height <= 0 || p->n_detectors < 1 || p->n_detectors > 4 ||
@@ -235,75 +287,75 @@ extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out)
         }
         t->nbr_ptr[size_t(b) + 1] = int32_t(t->nbr.size());
     }
-    // rays
-    struct RayRec { double d, w, open; int64_t first, count; };
-    std::vector<RayRec> rays;
-    std::vector<int32_t> e_bit;
-    std::vector<float> e_a;
-    uint64_t rs = p->seed;
-    const double mu_air = p->mu_rock * (1.2 / 2700.0);
-    const int S = p->sub_rays > 0 ? p->sub_rays : 1;
-    const double inv_s2 = 1.0 / double(S * S);
-    std::vector<int64_t> stamp(size_t(n), -1);
-    std::vector<int32_t> slot(size_t(n), 0);
-    std::vector<double> e_len;
-    int64_t stamp_id = 0;
+    // rays: march every sky bin (host or device), then draw the counts bin
+    // by bin from one stream
+    SynthMarch M;
+    M.g = g;
+    M.rock = std::move(rock);
+    M.is_void = std::move(is_void);
+    M.cell_bit = std::move(cell_bit);
+    M.n_det = p->n_detectors;
+    std::memcpy(M.det, p->det, sizeof M.det);
+    M.n_theta = p->n_theta;
+    M.n_phi = p->n_phi;
+    M.S = p->sub_rays > 0 ? p->sub_rays : 1;
+    M.n_bits = n;
+    M.inv_s2 = 1.0 / double(M.S * M.S);
+    M.mu_rock = p->mu_rock;
+    M.mu_air = p->mu_rock * (1.2 / 2700.0);
     const double dth = (p->theta_max - p->theta_min) / p->n_theta;
     const double dph = 2.0 * p->phi_half / p->n_phi;
+    // sub-ray angles: th_s depends on (zenith bin, su), ph_s on (detector, azimuth bin, sv)
+    M.cth.resize(size_t(p->n_theta) * M.S);
+    M.sth.resize(M.cth.size());
+    for (int it = 0; it < p->n_theta; ++it) {
+        const double th = p->theta_min + (it + 0.5) * dth;
+        for (int su = 0; su < M.S; ++su) {
+            const double th_s = th + ((su + 0.5) / M.S - 0.5) * dth;
+            M.cth[size_t(it) * M.S + su] = std::cos(th_s);
+            M.sth[size_t(it) * M.S + su] = std::sin(th_s);
+        }
+    }
+    M.cph.resize(size_t(p->n_detectors) * p->n_phi * M.S);
+    M.sph.resize(M.cph.size());
     for (int k = 0; k < p->n_detectors; ++k) {
         const double* o = &p->det[3 * k];
         const double axis_phi = std::atan2(-o[1], -o[0]);
+        for (int ip = 0; ip < p->n_phi; ++ip) {
+            const double ph = axis_phi - p->phi_half + (ip + 0.5) * dph;
+            for (int sv = 0; sv < M.S; ++sv) {
+                const double ph_s = ph + ((sv + 0.5) / M.S - 0.5) * dph;
+                M.cph[(size_t(k) * p->n_phi + ip) * M.S + sv] = std::cos(ph_s);
+                M.sph[(size_t(k) * p->n_phi + ip) * M.S + sv] = std::sin(ph_s);
+            }
+        }
+    }
+    std::vector<BinMarch> bins;
+    std::vector<int32_t> e_bit;
+    std::vector<float> e_a;
+    qb_status ms = on_device ? qb::synth_march_device(M, opts, bins, e_bit, e_a) : march_host(M, bins, e_bit, e_a);
+    if (ms != QB_OK) {
+        delete t;
+        return ms;
+    }
+    struct RayRec { double d, w, open; int64_t first, count; };
+    std::vector<RayRec> rays;
+    uint64_t rs = p->seed;
+    for (int k = 0; k < p->n_detectors; ++k)
         for (int it = 0; it < p->n_theta; ++it) {
             const double th = p->theta_min + (it + 0.5) * dth;
             const double ct = std::cos(th), st = std::sin(th);
             for (int ip = 0; ip < p->n_phi; ++ip) {
-                const double ph = axis_phi - p->phi_half + (ip + 0.5) * dph;
-                // The row of a sky bin: chords averaged over S x S sub-rays
-                // spread over the bin's solid angle (S = 1: the bin's centre line).
-                double tau0 = 0.0, tau = 0.0;
-                const int64_t first = int64_t(e_bit.size());
-                for (int su = 0; su < S; ++su)
-                    for (int sv = 0; sv < S; ++sv) {
-                        const double th_s = th + ((su + 0.5) / S - 0.5) * dth;
-                        const double ph_s = ph + ((sv + 0.5) / S - 0.5) * dph;
-                        const double cs = std::cos(th_s), ss = std::sin(th_s);
-                        const double dir[3] = {ss * std::cos(ph_s), ss * std::sin(ph_s), cs};
-                        tau0 += inv_s2 * p->mu_rock * (-o[2]) / cs;   // rock under the base
-                        tau += inv_s2 * p->mu_rock * (-o[2]) / cs;
-                        march(g, o, dir, [&](int64_t c, double seg) {
-                            if (!rock[size_t(c)]) return;
-                            tau0 += inv_s2 * p->mu_rock * seg;
-                            tau += inv_s2 * (is_void[size_t(c)] ? mu_air : p->mu_rock) * seg;
-                            const int b = cell_bit[size_t(c)];
-                            if (b < 0) return;
-                            if (stamp[size_t(b)] != stamp_id) {
-                                stamp[size_t(b)] = stamp_id;
-                                slot[size_t(b)] = int32_t(int64_t(e_bit.size()) - first);
-                                e_bit.push_back(b);
-                                e_a.push_back(0.0f);
-                                e_len.push_back(0.0);
-                            }
-                            e_len[size_t(slot[size_t(b)])] += inv_s2 * seg;
-                        });
-                    }
-                ++stamp_id;
-                for (size_t e = size_t(first); e < e_bit.size(); ++e) e_a[e] = float(p->mu_rock * e_len[e - size_t(first)]);
-                e_len.clear();
-                const int64_t cnt = int64_t(e_bit.size()) - first;
+                const BinMarch& B = bins[(size_t(k) * p->n_theta + it) * p->n_phi + ip];
                 const double lam_open = p->exposure * ct * ct * st * dth * dph;
                 const int64_t n_open = poisson(lam_open, rs);
-                const int64_t n_det = poisson(double(n_open) * std::exp(-tau), rs);
-                if (cnt == 0 || double(n_open) < p->min_open) {
-                    e_bit.resize(size_t(first));
-                    e_a.resize(size_t(first));
-                    continue;
-                }
+                const int64_t n_det = poisson(double(n_open) * std::exp(-B.tau), rs);
+                if (B.cnt == 0 || double(n_open) < p->min_open) continue;
                 const double det = std::max(double(n_det), 1.0);
                 const double tt = -std::log(det / double(n_open));
-                rays.push_back({tau0 - tt, det, double(n_open), first, cnt});
+                rays.push_back({B.tau0 - tt, det, double(n_open), B.first, B.cnt});
             }
         }
-    }
     // keep target_rays: the most-exposed rays, original order preserved
     std::vector<uint8_t> keep(rays.size(), 1);
     if (p->target_rays > 0) {
@@ -343,6 +395,16 @@ extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out)
     }
     *out = t;
     return QB_OK;
+}
+
+}  // namespace
+
+extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out) {
+    return synth_tomography(p, false, nullptr, out);
+}
+
+extern "C" qb_status qb_synth_tomography_device(const qb_tomo_params* p, const qb_opts* opts, qb_tomo** out) {
+    return synth_tomography(p, true, opts, out);
 }
 
 extern "C" qb_status qb_tomo_sizes(const qb_tomo* t, int32_t* n_vars, int32_t* n_rays, int64_t* nnz, int64_t* n_nbr) {

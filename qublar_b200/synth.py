@@ -408,12 +408,18 @@ def small_tomo_params(scale: float = 0.2, bins: int = 24, **overrides) -> TomoPa
     return tomo_params(**kw)
 
 
-def tomography(params: TomoParams | None = None, truth: bool = False):
+def tomography(params: TomoParams | None = None, truth: bool = False, device: int | None = None):
     """Build the muon-tomography QUBO; returns the residual-form arrays (and
-    the void truth per bit when asked)."""
+    the void truth per bit when asked). With `device` (a CUDA ordinal) the ray
+    march runs on that GPU; the arrays are the same bit for bit."""
     p = params if params is not None else tomo_params()
     h = C.c_void_p()
-    check(lib().qb_synth_tomography(C.byref(p), C.byref(h)))
+    if device is None:
+        check(lib().qb_synth_tomography(C.byref(p), C.byref(h)))
+    else:
+        from ._abi import Opts
+        o = Opts(None, int(device), 0)
+        check(lib().qb_synth_tomography_device(C.byref(p), C.byref(o), C.byref(h)))
     try:
         n, nr, nnz, nn = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
         check(lib().qb_tomo_sizes(h, C.byref(n), C.byref(nr), C.byref(nnz), C.byref(nn)))
