@@ -6,17 +6,18 @@
 // All replicas (up to 64 per launch) of one problem run in lockstep on a
 // cooperative grid. A warp visits one bit for every replica: lane l serves
 // replicas l and l + 32. The state lives in global memory, L2-resident:
-//   xw[i]  -- 64-bit word, bit r = x_i of replica r;
-//   fw[i]  -- 64-bit word, bit r = "replica r flipped x_i at its latest visit";
+//   xf[i].x -- 64-bit word, bit r = x_i of replica r;
+//   xf[i].y -- 64-bit word, bit r = "replica r flipped x_i at its latest visit"
+//             (one 16-byte pair, so a neighbour's value and flips arrive in one load);
 //   L[i][r] -- the local field L_i = h_i + sum_j J_ij x_j as an unevaluated
-//             sum hi + lo of two fp32 numbers.
+//             sum hi + lo of two fp32 numbers (a float2).
 // Incremental fields, deterministically: when bit i is visited, every
 // neighbour j has been visited exactly once since i's previous visit (colour
-// classes in a fixed order, no two bits of a class coupled), so fw[j] names
+// classes in a fixed order, no two bits of a class coupled), so xf[j].y names
 // exactly the changes i has not seen. The visit adds their deltas +-J_ij to
 // L_i in CSR order with the TwoSum error carried in lo (compensated
 // summation), scores dE = (1 - 2 x_i)(hi + lo), decides, and publishes its
-// own flips in fw[i]. Pushing deltas with atomics instead would make fp32
+// own flips in xf[i].y. Pushing deltas with atomics instead would make fp32
 // results depend on arrival order; pulling them keeps every bit reproducible.
 // Every `refresh` sweeps a visit also recomputes L_i from scratch in fp64,
 // records |fp32 - fp64| (the drift) and restarts hi + lo from it. The final
@@ -54,10 +55,8 @@ struct QuboArgs {
     const float* h;
     const int32_t* order;
     const double* temp;
-    float* Lhi;                    // n x 64
-    float* Llo;                    // n x 64
-    unsigned long long* xw;        // n
-    unsigned long long* fw;        // n
+    float2* L;                     // n x 64 (hi, lo)
+    ulonglong2* xf;                // n (value word, flip word)
     unsigned* bar;
     int* err;
     uint8_t* x_out;                // R x n, original order
@@ -105,14 +104,9 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
     for (int j = gw; j < A.n; j += tw) {
         const float hj = A.h[j];
         const size_t base = size_t(j) * 64;
-        A.Lhi[base + r0] = hj;
-        A.Lhi[base + r1] = hj;
-        A.Llo[base + r0] = 0.0f;
-        A.Llo[base + r1] = 0.0f;
-        if (lane == 0) {
-            A.xw[j] = 0ull;
-            A.fw[j] = 0ull;
-        }
+        A.L[base + r0] = make_float2(hj, 0.0f);
+        A.L[base + r1] = make_float2(hj, 0.0f);
+        if (lane == 0) A.xf[j] = make_ulonglong2(0ull, 0ull);
     }
     bool ok = grid_barrier(A.bar, A.err, ++round);
     for (int sweep = 0; sweep < A.sweeps && ok; ++sweep) {
@@ -123,8 +117,9 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
             const int c1 = A.class_ptr[c + 1];
             for (int j = A.class_ptr[c] + gw; j < c1; j += tw) {
                 const size_t base = size_t(j) * 64;
-                float hi0 = __ldcg(A.Lhi + base + r0), lo0 = __ldcg(A.Llo + base + r0);
-                float hi1 = __ldcg(A.Lhi + base + r1), lo1 = __ldcg(A.Llo + base + r1);
+                const float2 l0 = __ldcg(A.L + base + r0), l1 = __ldcg(A.L + base + r1);
+                const unsigned long long xj = __ldcg(A.xf + j).x;
+                float hi0 = l0.x, lo0 = l0.y, hi1 = l1.x, lo1 = l1.y;
                 double a0 = 0.0, a1 = 0.0;
                 if (refresh) a0 = a1 = double(__ldg(A.h + j));
                 const int k0 = __ldg(A.row + j), k1 = __ldg(A.row + j + 1);
@@ -136,8 +131,9 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                     if (k < k1) {
                         const int nb = __ldg(A.adj + k);
                         Jk = __ldg(A.J + k);
-                        f = __ldcg(A.fw + nb);
-                        if (f != 0ull || refresh) x = __ldcg(A.xw + nb);
+                        const ulonglong2 w = __ldcg(A.xf + nb);
+                        x = w.x;
+                        f = w.y;
                     }
                     if (!refresh) {
                         // each lane walks, in CSR order, the neighbours that one of its two
@@ -150,14 +146,28 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                         const unsigned xlo = uint32_t(x), xhi = uint32_t(x >> 32);
                         unsigned todo = F0 | F1;
                         while (__any_sync(kFullMask, todo != 0u)) {
-                            const unsigned bit = todo & (0u - todo);
-                            const int q = bit ? __ffs(bit) - 1 : 0;
-                            todo ^= bit;
-                            const float Jq = __shfl_sync(kFullMask, Jk, q);
-                            const unsigned xl = __shfl_sync(kFullMask, xlo, q);
-                            const unsigned xh = __shfl_sync(kFullMask, xhi, q);
-                            if (F0 & bit) two_sum_acc(hi0, lo0, ((xl >> lane) & 1u) ? Jq : -Jq);
-                            if (F1 & bit) two_sum_acc(hi1, lo1, ((xh >> lane) & 1u) ? Jq : -Jq);
+                            // the lane's next 2 flipped neighbours (ascending: CSR order per
+                            // replica); their shuffles issue together
+                            unsigned bit[2];
+                            float Jq[2];
+                            unsigned xl[2], xh[2];
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                bit[u] = todo & (0u - todo);
+                                todo ^= bit[u];
+                            }
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                const int q = bit[u] ? __ffs(bit[u]) - 1 : 0;
+                                Jq[u] = __shfl_sync(kFullMask, Jk, q);
+                                xl[u] = __shfl_sync(kFullMask, xlo, q);
+                                xh[u] = __shfl_sync(kFullMask, xhi, q);
+                            }
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                if (F0 & bit[u]) two_sum_acc(hi0, lo0, ((xl[u] >> lane) & 1u) ? Jq[u] : -Jq[u]);
+                                if (F1 & bit[u]) two_sum_acc(hi1, lo1, ((xh[u] >> lane) & 1u) ? Jq[u] : -Jq[u]);
+                            }
                         }
                         continue;
                     }
@@ -186,7 +196,6 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                     hi1 = float(a1);
                     lo1 = float(a1 - double(hi1));
                 }
-                const unsigned long long xj = __ldcg(A.xw + j);
                 const bool b0 = (xj >> r0) & 1ull, b1 = (xj >> r1) & 1ull;
                 const float L0 = __fadd_rn(hi0, lo0), L1 = __fadd_rn(hi1, lo1);
                 const float dE0 = b0 ? -L0 : L0, dE1 = b1 ? -L1 : L1;
@@ -199,8 +208,7 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                 const unsigned m0 = __ballot_sync(kFullMask, acc0), m1 = __ballot_sync(kFullMask, acc1);
                 const unsigned long long mask = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
                 if (lane == 0) {
-                    A.fw[j] = mask;
-                    A.xw[j] = xj ^ mask;
+                    A.xf[j] = make_ulonglong2(xj ^ mask, mask);
                 }
                 if (acc0) {
                     two_sum_acc(eh0, el0, dE0);
@@ -210,17 +218,15 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                     two_sum_acc(eh1, el1, dE1);
                     ++acc_b;
                 }
-                A.Lhi[base + r0] = hi0;
-                A.Llo[base + r0] = lo0;
-                A.Lhi[base + r1] = hi1;
-                A.Llo[base + r1] = lo1;
+                A.L[base + r0] = make_float2(hi0, lo0);
+                A.L[base + r1] = make_float2(hi1, lo1);
             }
             ok = grid_barrier(A.bar, A.err, ++round);
         }
     }
     if (ok) {
         for (int j = gw; j < A.n; j += tw) {
-            const unsigned long long xj = __ldcg(A.xw + j);
+            const unsigned long long xj = __ldcg(A.xf + j).x;
             const size_t o = size_t(__ldg(A.order + j));
             if (has0) A.x_out[size_t(r0) * size_t(A.n) + o] = uint8_t((xj >> r0) & 1ull);
             if (has1) A.x_out[size_t(r1) * size_t(A.n) + o] = uint8_t((xj >> r1) & 1ull);
@@ -299,10 +305,8 @@ qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, i
     char* sc = static_cast<char*>(b.scratch);
     A.bar = reinterpret_cast<unsigned*>(sc);
     A.err = reinterpret_cast<int*>(sc + 16);
-    A.Lhi = reinterpret_cast<float*>(sc + 64);
-    A.Llo = A.Lhi + size_t(p.n) * 64;
-    A.xw = reinterpret_cast<unsigned long long*>(A.Llo + size_t(p.n) * 64);
-    A.fw = A.xw + p.n;
+    A.L = reinterpret_cast<float2*>(sc + 64);
+    A.xf = reinterpret_cast<ulonglong2*>(A.L + size_t(p.n) * 64);
     A.x_out = b.x;
     A.drift = b.drift;
     A.e_track = b.e_track;
