@@ -537,7 +537,7 @@ def run_serve(args):
 # committed ncu capture of a 100-sweep launch on the same 200,000-bit QUBO with
 # 64 replicas (profiles/qubo_lockstep_lattice.md): the replicas' compensated
 # fields stream once per sweep, so a full launch moves this times its sweeps.
-QUBO_NCU_TRAFFIC_PER_SWEEP = (13.342204e9 + 10.197507e9) / 100
+QUBO_NCU_TRAFFIC_PER_SWEEP = (13.313979e9 + 10.124942e9) / 100
 QUBO_WORKLOAD = ("weighted QUBO on a 58^3 periodic lattice + 4,888 extra sites with random long-range edges "
                  "(N = 200,000, average degree 20), J and h ~ N(0,1) fp32, 64 replicas, 5000 sweeps T 3 -> 0.05, "
                  "compensated fp32 fields with an fp64 refresh every 64 sweeps")
