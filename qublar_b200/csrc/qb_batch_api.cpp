@@ -325,35 +325,65 @@ extern "C" qb_status qb_batch_autotune(const qb_batch_item* items, int32_t count
     const int cap = batch_max_smem();
     const int threads_c[] = {256, 512, 1024};
     const int smem_c[] = {48 * 1024, 96 * 1024, cap};
-    const int group_c[] = {8, 32};
+    const int group_c[] = {8, 16, 32};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    float best = -1.0f;
-    qb_batch_config best_c{};
+    // time one shape on `its`; < 0 when it does not fit an SM
+    auto time_shape = [&](const qb_batch_config& c, const std::vector<IsingItem>& its, float* ms) -> qb_status {
+        *ms = -1.0f;
+        BatchShape sh{c.threads, c.smem_bytes, 0};
+        int ctas = 0;
+        if (batch_ctas(sh, &ctas) != QB_OK) return QB_OK;   // shape does not fit an SM
+        cudaEventRecord(e0, b->stream);
+        qb_status r = run_items(b, c, its);
+        if (r != QB_OK) return r;
+        cudaEventRecord(e1, b->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess)
+            return cuda_fail(cudaGetLastError(), "cudaEventSynchronize", __FILE__, __LINE__);
+        cudaEventElapsedTime(ms, e0, e1);
+        return QB_OK;
+    };
+    // every shape on the short sample, then the three fastest again on a
+    // sample four times longer (short samples cannot separate close shapes)
+    std::vector<std::pair<float, qb_batch_config>> timed;
     for (int th : threads_c)
         for (int sm : smem_c)
             for (int g : group_c) {
                 qb_batch_config c{th, std::min(sm, cap), g, 0};
                 std::vector<IsingItem> its;
                 if ((s = build_items(b, c, S, d_st.as<double>(), its)) != QB_OK) break;
-                BatchShape sh{c.threads, c.smem_bytes, 0};
-                int ctas = 0;
-                if (batch_ctas(sh, &ctas) != QB_OK) continue;   // shape does not fit an SM
-                cudaEventRecord(e0, b->stream);
-                if ((s = run_items(b, c, its)) != QB_OK) break;
-                cudaEventRecord(e1, b->stream);
-                if (cudaEventSynchronize(e1) != cudaSuccess) {
-                    s = cuda_fail(cudaGetLastError(), "cudaEventSynchronize", __FILE__, __LINE__);
-                    break;
-                }
                 float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (best < 0.0f || ms < best) {
-                    best = ms;
-                    best_c = c;
-                }
+                if ((s = time_shape(c, its, &ms)) != QB_OK) break;
+                if (ms >= 0.0f) timed.emplace_back(ms, c);
             }
+    float best = -1.0f;
+    qb_batch_config best_c{};
+    if (s == QB_OK && !timed.empty()) {
+        std::stable_sort(timed.begin(), timed.end(),
+                         [](const std::pair<float, qb_batch_config>& a, const std::pair<float, qb_batch_config>& b_) {
+                             return a.first < b_.first;
+                         });
+        const int S4 = 4 * S;
+        std::vector<double> st4(b->inst.size() * size_t(S4));
+        for (size_t k = 0; k < b->inst.size(); ++k) {
+            const std::vector<double> t = temperatures(b->inst[k].sched);
+            for (int j = 0; j < S4; ++j)
+                st4[k * size_t(S4) + size_t(j)] = t[size_t(int64_t(j) * int64_t(t.size()) / S4)];
+        }
+        DevBuf d_st4;
+        s = upload_vec(d_st4, st4, b->stream);
+        for (size_t q = 0; s == QB_OK && q < std::min<size_t>(3, timed.size()); ++q) {
+            std::vector<IsingItem> its;
+            if ((s = build_items(b, timed[q].second, S4, d_st4.as<double>(), its)) != QB_OK) break;
+            float ms = 0.0f;
+            if ((s = time_shape(timed[q].second, its, &ms)) != QB_OK) break;
+            if (ms >= 0.0f && (best < 0.0f || ms < best)) {
+                best = ms;
+                best_c = timed[q].second;
+            }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     qb_batch_destroy(b);

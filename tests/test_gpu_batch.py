@@ -99,7 +99,7 @@ def test_results_do_not_depend_on_the_launch_shape(batch_case, cfg):
 def test_autotune_returns_a_working_shape(batch_case):
     gens, items, B = batch_case
     cfg = autotune_batch(items, 4)
-    assert cfg.threads in (256, 512, 1024) and cfg.max_group in (8, 32) and cfg.smem_bytes > 0
+    assert cfg.threads in (256, 512, 1024) and cfg.max_group in (8, 16, 32) and cfg.smem_bytes > 0
     again = autotune_batch(items, 4)   # cached per batch shape
     assert (again.threads, again.smem_bytes, again.max_group) == (cfg.threads, cfg.smem_bytes, cfg.max_group)
     B2 = solve_batch(items, cfg)
