@@ -784,114 +784,120 @@ void qb::problem_release_device(qb_problem* p) {
 }
 
 extern "C" qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb_opts* opts, qb_problem** out) {
-    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_ising: null argument");
-    *out = nullptr;
-    qb_problem* p = new (std::nothrow) qb_problem();
-    if (!p) return fail(QB_ENOMEM, "qb_problem_create_ising: out of host memory");
-    p->kind = QB_KIND_ISING;
-    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
-    qb_status s = plan_ising(desc, p->ising);
-    if (s == QB_OK && p->ising.w_min == 0) s = fail(QB_EREFUSED, "ising: all weights are zero");   // ising_gpu.cuh:94
-    if (s == QB_OK) s = select_device(opts, &p->device);
-    if (s == QB_OK && defer) {
-        const size_t m = size_t(desc->m);
-        p->host.eu.assign(desc->eu, desc->eu + m);
-        p->host.ev.assign(desc->ev, desc->ev + m);
-        p->host.ew.assign(desc->ew, desc->ew + m);
-        p->device_bytes = ising_device_bytes(p->ising);
-    } else if (s == QB_OK) {
-        s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
-        p->uploaded = s == QB_OK;
-    }
-    if (s != QB_OK) {
-        delete p;
-        return s;
-    }
-    *out = p;
-    return QB_OK;
+    return qb::guarded("qb_problem_create_ising", [&]() -> qb_status {
+        if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_ising: null argument");
+        *out = nullptr;
+        qb_problem* p = new (std::nothrow) qb_problem();
+        if (!p) return fail(QB_ENOMEM, "qb_problem_create_ising: out of host memory");
+        p->kind = QB_KIND_ISING;
+        const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
+        qb_status s = plan_ising(desc, p->ising);
+        if (s == QB_OK && p->ising.w_min == 0) s = fail(QB_EREFUSED, "ising: all weights are zero");   // ising_gpu.cuh:94
+        if (s == QB_OK) s = select_device(opts, &p->device);
+        if (s == QB_OK && defer) {
+            const size_t m = size_t(desc->m);
+            p->host.eu.assign(desc->eu, desc->eu + m);
+            p->host.ev.assign(desc->ev, desc->ev + m);
+            p->host.ew.assign(desc->ew, desc->ew + m);
+            p->device_bytes = ising_device_bytes(p->ising);
+        } else if (s == QB_OK) {
+            s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
+            p->uploaded = s == QB_OK;
+        }
+        if (s != QB_OK) {
+            delete p;
+            return s;
+        }
+        *out = p;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts* opts, qb_problem** out) {
-    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_residual: null argument");
-    *out = nullptr;
-    // QB_PLAN_TIMES=1 prints the host check, plan and upload times to stderr
-    const bool times = std::getenv("QB_PLAN_TIMES") != nullptr;
-    auto now = [] { return std::chrono::steady_clock::now(); };
-    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
-        return std::chrono::duration<double, std::milli>(b - a).count();
-    };
-    const auto t0 = now();
-    qb_status s = check_residual(desc);
-    if (s != QB_OK) return s;
-    qb_problem* p = new (std::nothrow) qb_problem();
-    if (!p) return fail(QB_ENOMEM, "qb_problem_create_residual: out of host memory");
-    p->kind = QB_KIND_RESIDUAL;
-    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
-    const bool cluster = opts && (opts->flags & QB_OPT_RESID_CLUSTER);
-    s = select_device(opts, &p->device);
-    const auto t1 = now();
-    if (s == QB_OK) s = plan_residual(desc, p->resid, cluster ? 0 : resid_lockstep_grid());
-    if (s == QB_OK && p->resid.variant == QB_RESID_CLUSTER) s = resid_check_fit(p->resid);
-    const auto t2 = now();
-    if (s == QB_OK && defer) {
-        HostDesc& h = p->host;
-        const int n = desc->n_vars, nr = desc->n_rays;
-        const size_t nnz = size_t(desc->row_ptr[n]), nn = size_t(desc->nbr_ptr[n]);
-        h.d.assign(desc->d, desc->d + nr);
-        h.w.assign(desc->w, desc->w + nr);
-        h.row_ptr.assign(desc->row_ptr, desc->row_ptr + n + 1);
-        h.ray.assign(desc->ray, desc->ray + nnz);
-        h.a.assign(desc->a, desc->a + nnz);
-        h.nbr_ptr.assign(desc->nbr_ptr, desc->nbr_ptr + n + 1);
-        h.nbr.assign(desc->nbr, desc->nbr + nn);
-        h.has_field = desc->field != nullptr;
-        if (h.has_field) h.field.assign(desc->field, desc->field + n);
-        h.lambda = desc->lambda;
-        h.kappa = desc->kappa;
-        p->device_bytes = residual_device_bytes(p->resid);
-    } else if (s == QB_OK) {
-        s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
-        p->uploaded = s == QB_OK;
-    }
-    if (times)
-        std::fprintf(stderr, "[qb plan] check %.1f ms, plan %.1f ms, upload %.1f ms\n", ms(t0, t1), ms(t1, t2),
-                     ms(t2, now()));
-    if (s != QB_OK) {
-        delete p;
-        return s;
-    }
-    *out = p;
-    return QB_OK;
+    return qb::guarded("qb_problem_create_residual", [&]() -> qb_status {
+        if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_residual: null argument");
+        *out = nullptr;
+        // QB_PLAN_TIMES=1 prints the host check, plan and upload times to stderr
+        const bool times = std::getenv("QB_PLAN_TIMES") != nullptr;
+        auto now = [] { return std::chrono::steady_clock::now(); };
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        const auto t0 = now();
+        qb_status s = check_residual(desc);
+        if (s != QB_OK) return s;
+        qb_problem* p = new (std::nothrow) qb_problem();
+        if (!p) return fail(QB_ENOMEM, "qb_problem_create_residual: out of host memory");
+        p->kind = QB_KIND_RESIDUAL;
+        const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
+        const bool cluster = opts && (opts->flags & QB_OPT_RESID_CLUSTER);
+        s = select_device(opts, &p->device);
+        const auto t1 = now();
+        if (s == QB_OK) s = plan_residual(desc, p->resid, cluster ? 0 : resid_lockstep_grid());
+        if (s == QB_OK && p->resid.variant == QB_RESID_CLUSTER) s = resid_check_fit(p->resid);
+        const auto t2 = now();
+        if (s == QB_OK && defer) {
+            HostDesc& h = p->host;
+            const int n = desc->n_vars, nr = desc->n_rays;
+            const size_t nnz = size_t(desc->row_ptr[n]), nn = size_t(desc->nbr_ptr[n]);
+            h.d.assign(desc->d, desc->d + nr);
+            h.w.assign(desc->w, desc->w + nr);
+            h.row_ptr.assign(desc->row_ptr, desc->row_ptr + n + 1);
+            h.ray.assign(desc->ray, desc->ray + nnz);
+            h.a.assign(desc->a, desc->a + nnz);
+            h.nbr_ptr.assign(desc->nbr_ptr, desc->nbr_ptr + n + 1);
+            h.nbr.assign(desc->nbr, desc->nbr + nn);
+            h.has_field = desc->field != nullptr;
+            if (h.has_field) h.field.assign(desc->field, desc->field + n);
+            h.lambda = desc->lambda;
+            h.kappa = desc->kappa;
+            p->device_bytes = residual_device_bytes(p->resid);
+        } else if (s == QB_OK) {
+            s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
+            p->uploaded = s == QB_OK;
+        }
+        if (times)
+            std::fprintf(stderr, "[qb plan] check %.1f ms, plan %.1f ms, upload %.1f ms\n", ms(t0, t1), ms(t1, t2),
+                         ms(t2, now()));
+        if (s != QB_OK) {
+            delete p;
+            return s;
+        }
+        *out = p;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_opts* opts, qb_problem** out) {
-    if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_qubo: null argument");
-    *out = nullptr;
-    qb_problem* p = new (std::nothrow) qb_problem();
-    if (!p) return fail(QB_ENOMEM, "qb_problem_create_qubo: out of host memory");
-    p->kind = QB_KIND_QUBO;
-    const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
-    qb_status s = plan_qubo(desc, p->qubo);
-    if (s == QB_OK) s = select_device(opts, &p->device);
-    if (s == QB_OK && defer) {
-        const size_t m = size_t(desc->m);
-        HostDesc& h = p->host;
-        h.eu.assign(desc->eu, desc->eu + m);
-        h.ev.assign(desc->ev, desc->ev + m);
-        h.wf.assign(desc->ew, desc->ew + m);
-        if (desc->h) h.hf.assign(desc->h, desc->h + desc->n);
-        h.offset = desc->offset;
-        p->device_bytes = qubo_device_bytes(p->qubo);
-    } else if (s == QB_OK) {
-        s = upload_qubo(p->qubo, desc, stream_of(opts), &p->device_bytes);
-        p->uploaded = s == QB_OK;
-    }
-    if (s != QB_OK) {
-        delete p;
-        return s;
-    }
-    *out = p;
-    return QB_OK;
+    return qb::guarded("qb_problem_create_qubo", [&]() -> qb_status {
+        if (!desc || !out) return fail(QB_EINVAL, "qb_problem_create_qubo: null argument");
+        *out = nullptr;
+        qb_problem* p = new (std::nothrow) qb_problem();
+        if (!p) return fail(QB_ENOMEM, "qb_problem_create_qubo: out of host memory");
+        p->kind = QB_KIND_QUBO;
+        const bool defer = opts && (opts->flags & QB_OPT_DEFER_UPLOAD);
+        qb_status s = plan_qubo(desc, p->qubo);
+        if (s == QB_OK) s = select_device(opts, &p->device);
+        if (s == QB_OK && defer) {
+            const size_t m = size_t(desc->m);
+            HostDesc& h = p->host;
+            h.eu.assign(desc->eu, desc->eu + m);
+            h.ev.assign(desc->ev, desc->ev + m);
+            h.wf.assign(desc->ew, desc->ew + m);
+            if (desc->h) h.hf.assign(desc->h, desc->h + desc->n);
+            h.offset = desc->offset;
+            p->device_bytes = qubo_device_bytes(p->qubo);
+        } else if (s == QB_OK) {
+            s = upload_qubo(p->qubo, desc, stream_of(opts), &p->device_bytes);
+            p->uploaded = s == QB_OK;
+        }
+        if (s != QB_OK) {
+            delete p;
+            return s;
+        }
+        *out = p;
+        return QB_OK;
+    });
 }
 
 extern "C" void qb_problem_destroy(qb_problem* p) {
@@ -945,27 +951,31 @@ extern "C" qb_status qb_problem_colouring(const qb_problem* p, int32_t* order, i
 }
 
 extern "C" qb_status qb_colour_ising(const qb_ising_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
-    if (!desc) return fail(QB_EINVAL, "qb_colour_ising: null descriptor");
-    IsingPlan P;
-    qb_status s = plan_ising(desc, P);
-    if (s != QB_OK) return s;
-    if (order) std::memcpy(order, P.col.order.data(), P.col.order.size() * sizeof(int32_t));
-    if (class_ptr) std::memcpy(class_ptr, P.col.class_ptr.data(), P.col.class_ptr.size() * sizeof(int32_t));
-    if (n_colours) *n_colours = P.col.n_colours();
-    return QB_OK;
+    return qb::guarded("qb_colour_ising", [&]() -> qb_status {
+        if (!desc) return fail(QB_EINVAL, "qb_colour_ising: null descriptor");
+        IsingPlan P;
+        qb_status s = plan_ising(desc, P);
+        if (s != QB_OK) return s;
+        if (order) std::memcpy(order, P.col.order.data(), P.col.order.size() * sizeof(int32_t));
+        if (class_ptr) std::memcpy(class_ptr, P.col.class_ptr.data(), P.col.class_ptr.size() * sizeof(int32_t));
+        if (n_colours) *n_colours = P.col.n_colours();
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_colour_residual(const qb_residual_desc* desc, int32_t* order, int32_t* class_ptr, int32_t* n_colours) {
-    if (!desc) return fail(QB_EINVAL, "qb_colour_residual: null descriptor");
-    qb_status s = check_residual(desc);
-    if (s != QB_OK) return s;
-    ResidualPlan P;
-    if ((s = plan_residual(desc, P, kHostLockSlices)) != QB_OK) return s;
-    const Colouring& c = P.col;
-    if (order) std::memcpy(order, c.order.data(), c.order.size() * sizeof(int32_t));
-    if (class_ptr) std::memcpy(class_ptr, c.class_ptr.data(), c.class_ptr.size() * sizeof(int32_t));
-    if (n_colours) *n_colours = c.n_colours();
-    return QB_OK;
+    return qb::guarded("qb_colour_residual", [&]() -> qb_status {
+        if (!desc) return fail(QB_EINVAL, "qb_colour_residual: null descriptor");
+        qb_status s = check_residual(desc);
+        if (s != QB_OK) return s;
+        ResidualPlan P;
+        if ((s = plan_residual(desc, P, kHostLockSlices)) != QB_OK) return s;
+        const Colouring& c = P.col;
+        if (order) std::memcpy(order, c.order.data(), c.order.size() * sizeof(int32_t));
+        if (class_ptr) std::memcpy(class_ptr, c.class_ptr.data(), c.class_ptr.size() * sizeof(int32_t));
+        if (n_colours) *n_colours = c.n_colours();
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_schedule_scaled(const qb_problem* p, int32_t anneal_sweeps, int32_t hold_sweeps, qb_schedule* out) {
@@ -983,135 +993,137 @@ extern "C" qb_status qb_schedule_scaled(const qb_problem* p, int32_t anneal_swee
 
 extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_branches, uint64_t seed_offset,
                               const qb_opts* opts, qb_result** out) {
-    if (!p || !out) return fail(QB_EINVAL, "qb_solve: null argument");
-    *out = nullptr;
-    qb_status s = check_schedule(sch);
-    if (s != QB_OK) return s;
-    if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_solve: n_branches must be in [1, 2^20]");
-    QB_CUDA(cudaSetDevice(p->device));
-    cudaStream_t st = stream_of(opts);
-    if ((s = problem_upload(p, st)) != QB_OK) return s;
-    qb_result* r = new (std::nothrow) qb_result();
-    if (!r) return fail(QB_ENOMEM, "qb_solve: out of host memory");
-    r->prob = p;
-    r->device = p->device;
-    r->stream = st;
-    r->R = int(n_branches);
-    r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
-    const int R = r->R;
-    const int n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
-    r->n = n;
-    const uint64_t seed0 = 1 + seed_offset;   // branch b: seed b + 1 + offset (ising_recon.hpp:157)
-    auto bail = [&](qb_status e) {
-        qb_result_destroy(r);
-        return e;
-    };
-    const bool same = p->d_temp.p && p->temp_sched.t_hot == sch->t_hot && p->temp_sched.t_cold == sch->t_cold &&
-                      p->temp_sched.anneal_sweeps == sch->anneal_sweeps && p->temp_sched.hold_sweeps == sch->hold_sweeps;
-    if (!same) {
-        const std::vector<double> temp = temperatures(*sch);
-        QB_CUDA(cudaStreamSynchronize(st));   // a solve in flight may still read the old table
-        if ((s = upload_vec(p->d_temp, temp, st))) return bail(s);
-        QB_CUDA(cudaStreamSynchronize(st));
-        p->temp_sched = *sch;
-    }
-    if ((s = alloc_async(r->d_x, size_t(R) * size_t(n), st))) return bail(s);
-    if ((s = alloc_async(r->d_e_f64, size_t(R) * sizeof(double), st))) return bail(s);
-    if ((s = alloc_async(r->d_p, size_t(n) * sizeof(float), st))) return bail(s);
-    if (cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
-        cudaEventCreate(&r->ev2) != cudaSuccess)
-        return bail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
-    SolveBuffers b;
-    b.x = r->d_x.as<uint8_t>();
-    b.e_f64 = r->d_e_f64.as<double>();
-    b.p = r->d_p.as<float>();
-    b.temp = p->d_temp.as<double>();
-    if (p->kind == QB_KIND_ISING) {
-        const IsingPlan& P = p->ising;
-        if ((s = alloc_async(r->d_f, size_t(R) * size_t(n) * 4, st))) return bail(s);
-        if ((s = alloc_async(r->d_e_i64, size_t(R) * 8, st))) return bail(s);
-        if ((s = alloc_async(r->d_e_scr, size_t(R) * 8, st))) return bail(s);
-        if (ising_smem_bytes(P) == 0 && (s = alloc_async(r->d_scratch, size_t(R) * size_t(n) * 5, st))) return bail(s);
-        b.f = r->d_f.as<int32_t>();
-        b.e_i64 = r->d_e_i64.as<long long>();
-        b.scratch = r->d_scratch.p;
-        cudaEventRecord(r->ev0, st);
-        if ((s = launch_ising_anneal(P, b, R, r->sweeps, seed0, st))) return bail(s);
-        cudaEventRecord(r->ev1, st);
-        if ((s = launch_ising_energies(P, b.x, R, r->d_e_scr.as<long long>(), st))) return bail(s);
-        if ((s = launch_i64_to_f64(r->d_e_scr.as<long long>(), R, b.e_f64, st))) return bail(s);
-        r->launches = 3;
-    } else if (p->kind == QB_KIND_QUBO) {
-        const QuboPlan& P = p->qubo;
-        if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
-        if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
-        if ((s = alloc_async(r->d_e_track, size_t(R) * 8, st))) return bail(s);
-        if ((s = alloc_async(r->d_scratch, qubo_scratch(P), st))) return bail(s);
-        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
-            cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess ||
-            cudaMemsetAsync(r->d_e_track.p, 0, size_t(R) * 8, st) != cudaSuccess ||
-            cudaMemsetAsync(r->d_scratch.p, 0, 64, st) != cudaSuccess)
-            return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
-        r->d_err = reinterpret_cast<const int*>(static_cast<const char*>(r->d_scratch.p) + 16);
-        const int RB = qubo_max_branches();
-        cudaEventRecord(r->ev0, st);
-        int anneal_launches = 0;
-        for (int b0 = 0; b0 < R && s == QB_OK; b0 += RB, ++anneal_launches) {
-            QuboBuffers qbuf;
-            qbuf.x = b.x + size_t(b0) * size_t(n);
-            qbuf.temp = b.temp;
-            qbuf.drift = r->d_drift.as<float>() + b0;
-            qbuf.e_track = r->d_e_track.as<double>() + b0;
-            qbuf.accepts = r->d_accepts.as<unsigned long long>() + b0;
-            qbuf.scratch = r->d_scratch.p;
-            s = launch_qubo_lockstep(P, qbuf, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
-                                     seed0 + uint64_t(b0), st);
+    return qb::guarded("qb_solve", [&]() -> qb_status {
+        if (!p || !out) return fail(QB_EINVAL, "qb_solve: null argument");
+        *out = nullptr;
+        qb_status s = check_schedule(sch);
+        if (s != QB_OK) return s;
+        if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_solve: n_branches must be in [1, 2^20]");
+        QB_CUDA(cudaSetDevice(p->device));
+        cudaStream_t st = stream_of(opts);
+        if ((s = problem_upload(p, st)) != QB_OK) return s;
+        qb_result* r = new (std::nothrow) qb_result();
+        if (!r) return fail(QB_ENOMEM, "qb_solve: out of host memory");
+        r->prob = p;
+        r->device = p->device;
+        r->stream = st;
+        r->R = int(n_branches);
+        r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
+        const int R = r->R;
+        const int n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
+        r->n = n;
+        const uint64_t seed0 = 1 + seed_offset;   // branch b: seed b + 1 + offset (ising_recon.hpp:157)
+        auto bail = [&](qb_status e) {
+            qb_result_destroy(r);
+            return e;
+        };
+        const bool same = p->d_temp.p && p->temp_sched.t_hot == sch->t_hot && p->temp_sched.t_cold == sch->t_cold &&
+                          p->temp_sched.anneal_sweeps == sch->anneal_sweeps && p->temp_sched.hold_sweeps == sch->hold_sweeps;
+        if (!same) {
+            const std::vector<double> temp = temperatures(*sch);
+            QB_CUDA(cudaStreamSynchronize(st));   // a solve in flight may still read the old table
+            if ((s = upload_vec(p->d_temp, temp, st))) return bail(s);
+            QB_CUDA(cudaStreamSynchronize(st));
+            p->temp_sched = *sch;
         }
-        if (s != QB_OK) return bail(s);
-        cudaEventRecord(r->ev1, st);
-        if ((s = launch_qubo_energies(P, b.x, R, b.e_f64, st))) return bail(s);
-        r->launches = anneal_launches + 1;
-    } else {
-        const ResidualPlan& P = p->resid;
-        if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
-        if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
-        if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
-            cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess)
-            return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
-        b.drift = r->d_drift.as<float>();
-        b.accepts = r->d_accepts.as<unsigned long long>();
-        const int RB = std::min(R, resid_lockstep_max_branches());   // branches per lockstep launch
-        if (P.variant == QB_RESID_LOCKSTEP) {
-            if ((s = alloc_async(r->d_scratch, resid_lockstep_scratch(P, RB), st))) return bail(s);
+        if ((s = alloc_async(r->d_x, size_t(R) * size_t(n), st))) return bail(s);
+        if ((s = alloc_async(r->d_e_f64, size_t(R) * sizeof(double), st))) return bail(s);
+        if ((s = alloc_async(r->d_p, size_t(n) * sizeof(float), st))) return bail(s);
+        if (cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+            cudaEventCreate(&r->ev2) != cudaSuccess)
+            return bail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
+        SolveBuffers b;
+        b.x = r->d_x.as<uint8_t>();
+        b.e_f64 = r->d_e_f64.as<double>();
+        b.p = r->d_p.as<float>();
+        b.temp = p->d_temp.as<double>();
+        if (p->kind == QB_KIND_ISING) {
+            const IsingPlan& P = p->ising;
+            if ((s = alloc_async(r->d_f, size_t(R) * size_t(n) * 4, st))) return bail(s);
+            if ((s = alloc_async(r->d_e_i64, size_t(R) * 8, st))) return bail(s);
+            if ((s = alloc_async(r->d_e_scr, size_t(R) * 8, st))) return bail(s);
+            if (ising_smem_bytes(P) == 0 && (s = alloc_async(r->d_scratch, size_t(R) * size_t(n) * 5, st))) return bail(s);
+            b.f = r->d_f.as<int32_t>();
+            b.e_i64 = r->d_e_i64.as<long long>();
             b.scratch = r->d_scratch.p;
-            QB_CUDA(cudaMemsetAsync(r->d_scratch.p, 0, 64, st));   // control block, timeout flag included
+            cudaEventRecord(r->ev0, st);
+            if ((s = launch_ising_anneal(P, b, R, r->sweeps, seed0, st))) return bail(s);
+            cudaEventRecord(r->ev1, st);
+            if ((s = launch_ising_energies(P, b.x, R, r->d_e_scr.as<long long>(), st))) return bail(s);
+            if ((s = launch_i64_to_f64(r->d_e_scr.as<long long>(), R, b.e_f64, st))) return bail(s);
+            r->launches = 3;
+        } else if (p->kind == QB_KIND_QUBO) {
+            const QuboPlan& P = p->qubo;
+            if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
+            if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
+            if ((s = alloc_async(r->d_e_track, size_t(R) * 8, st))) return bail(s);
+            if ((s = alloc_async(r->d_scratch, qubo_scratch(P), st))) return bail(s);
+            if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
+                cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess ||
+                cudaMemsetAsync(r->d_e_track.p, 0, size_t(R) * 8, st) != cudaSuccess ||
+                cudaMemsetAsync(r->d_scratch.p, 0, 64, st) != cudaSuccess)
+                return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
             r->d_err = reinterpret_cast<const int*>(static_cast<const char*>(r->d_scratch.p) + 16);
-        }
-        cudaEventRecord(r->ev0, st);
-        int anneal_launches = 0;
-        if (P.variant == QB_RESID_LOCKSTEP) {
-            // blocks of at most RB branches, one cooperative launch each
+            const int RB = qubo_max_branches();
+            cudaEventRecord(r->ev0, st);
+            int anneal_launches = 0;
             for (int b0 = 0; b0 < R && s == QB_OK; b0 += RB, ++anneal_launches) {
-                SolveBuffers bb = b;
-                bb.x = b.x + size_t(b0) * size_t(n);
-                bb.drift = b.drift + b0;
-                s = launch_resid_lockstep(P, bb, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
-                                          seed0 + uint64_t(b0), st);
+                QuboBuffers qbuf;
+                qbuf.x = b.x + size_t(b0) * size_t(n);
+                qbuf.temp = b.temp;
+                qbuf.drift = r->d_drift.as<float>() + b0;
+                qbuf.e_track = r->d_e_track.as<double>() + b0;
+                qbuf.accepts = r->d_accepts.as<unsigned long long>() + b0;
+                qbuf.scratch = r->d_scratch.p;
+                s = launch_qubo_lockstep(P, qbuf, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
+                                         seed0 + uint64_t(b0), st);
             }
+            if (s != QB_OK) return bail(s);
+            cudaEventRecord(r->ev1, st);
+            if ((s = launch_qubo_energies(P, b.x, R, b.e_f64, st))) return bail(s);
+            r->launches = anneal_launches + 1;
         } else {
-            s = launch_resid_anneal(P, b, R, r->sweeps, sch->refresh_sweeps, seed0, st);
-            anneal_launches = 1;
+            const ResidualPlan& P = p->resid;
+            if ((s = alloc_async(r->d_drift, size_t(R) * sizeof(float), st))) return bail(s);
+            if ((s = alloc_async(r->d_accepts, size_t(R) * 8, st))) return bail(s);
+            if (cudaMemsetAsync(r->d_drift.p, 0, size_t(R) * sizeof(float), st) != cudaSuccess ||
+                cudaMemsetAsync(r->d_accepts.p, 0, size_t(R) * 8, st) != cudaSuccess)
+                return bail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+            b.drift = r->d_drift.as<float>();
+            b.accepts = r->d_accepts.as<unsigned long long>();
+            const int RB = std::min(R, resid_lockstep_max_branches());   // branches per lockstep launch
+            if (P.variant == QB_RESID_LOCKSTEP) {
+                if ((s = alloc_async(r->d_scratch, resid_lockstep_scratch(P, RB), st))) return bail(s);
+                b.scratch = r->d_scratch.p;
+                QB_CUDA(cudaMemsetAsync(r->d_scratch.p, 0, 64, st));   // control block, timeout flag included
+                r->d_err = reinterpret_cast<const int*>(static_cast<const char*>(r->d_scratch.p) + 16);
+            }
+            cudaEventRecord(r->ev0, st);
+            int anneal_launches = 0;
+            if (P.variant == QB_RESID_LOCKSTEP) {
+                // blocks of at most RB branches, one cooperative launch each
+                for (int b0 = 0; b0 < R && s == QB_OK; b0 += RB, ++anneal_launches) {
+                    SolveBuffers bb = b;
+                    bb.x = b.x + size_t(b0) * size_t(n);
+                    bb.drift = b.drift + b0;
+                    s = launch_resid_lockstep(P, bb, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
+                                              seed0 + uint64_t(b0), st);
+                }
+            } else {
+                s = launch_resid_anneal(P, b, R, r->sweeps, sch->refresh_sweeps, seed0, st);
+                anneal_launches = 1;
+            }
+            if (s != QB_OK) return bail(s);
+            cudaEventRecord(r->ev1, st);
+            if ((s = launch_resid_energies(P, b.x, R, b.e_f64, st))) return bail(s);
+            r->launches = anneal_launches + 1;
         }
-        if (s != QB_OK) return bail(s);
-        cudaEventRecord(r->ev1, st);
-        if ((s = launch_resid_energies(P, b.x, R, b.e_f64, st))) return bail(s);
-        r->launches = anneal_launches + 1;
-    }
-    if ((s = launch_marginals(b.x, R, n, b.p, st))) return bail(s);
-    r->launches += 1;
-    cudaEventRecord(r->ev2, st);
-    *out = r;
-    return QB_OK;
+        if ((s = launch_marginals(b.x, R, n, b.p, st))) return bail(s);
+        r->launches += 1;
+        cudaEventRecord(r->ev2, st);
+        *out = r;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_result_info_get(qb_result* r, qb_result_info* info) {
@@ -1205,46 +1217,52 @@ extern "C" void qb_result_destroy(qb_result* r) {
 // ---- evaluators -------------------------------------------------------------------------------
 
 extern "C" qb_status qb_energies_ising(const qb_problem* p, const uint8_t* x, int32_t k, int64_t* e) {
-    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_ising: bad argument");
-    if (p->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_energies_ising: ising problems only");
-    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_ising: the problem is not on the device");
-    if (k == 0) return QB_OK;
-    QB_CUDA(cudaSetDevice(p->device));
-    DevBuf dx, de;
-    qb_status s;
-    if ((s = upload(dx, x, size_t(k) * size_t(p->ising.n), nullptr))) return s;
-    if ((s = de.alloc(size_t(k) * 8))) return s;
-    if ((s = launch_ising_energies(p->ising, dx.as<uint8_t>(), k, de.as<long long>(), nullptr))) return s;
-    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
-    return QB_OK;
+    return qb::guarded("qb_energies_ising", [&]() -> qb_status {
+        if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_ising: bad argument");
+        if (p->kind != QB_KIND_ISING) return fail(QB_EINVAL, "qb_energies_ising: ising problems only");
+        if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_ising: the problem is not on the device");
+        if (k == 0) return QB_OK;
+        QB_CUDA(cudaSetDevice(p->device));
+        DevBuf dx, de;
+        qb_status s;
+        if ((s = upload(dx, x, size_t(k) * size_t(p->ising.n), nullptr))) return s;
+        if ((s = de.alloc(size_t(k) * 8))) return s;
+        if ((s = launch_ising_energies(p->ising, dx.as<uint8_t>(), k, de.as<long long>(), nullptr))) return s;
+        QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_energies_qubo(const qb_problem* p, const uint8_t* x, int32_t k, double* e) {
-    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_qubo: bad argument");
-    if (p->kind != QB_KIND_QUBO) return fail(QB_EINVAL, "qb_energies_qubo: weighted qubo problems only");
-    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_qubo: the problem is not on the device");
-    if (k == 0) return QB_OK;
-    QB_CUDA(cudaSetDevice(p->device));
-    DevBuf dx, de;
-    qb_status s;
-    if ((s = upload(dx, x, size_t(k) * size_t(p->qubo.n), nullptr))) return s;
-    if ((s = de.alloc(size_t(k) * 8))) return s;
-    if ((s = launch_qubo_energies(p->qubo, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
-    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
-    return QB_OK;
+    return qb::guarded("qb_energies_qubo", [&]() -> qb_status {
+        if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_qubo: bad argument");
+        if (p->kind != QB_KIND_QUBO) return fail(QB_EINVAL, "qb_energies_qubo: weighted qubo problems only");
+        if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_qubo: the problem is not on the device");
+        if (k == 0) return QB_OK;
+        QB_CUDA(cudaSetDevice(p->device));
+        DevBuf dx, de;
+        qb_status s;
+        if ((s = upload(dx, x, size_t(k) * size_t(p->qubo.n), nullptr))) return s;
+        if ((s = de.alloc(size_t(k) * 8))) return s;
+        if ((s = launch_qubo_energies(p->qubo, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
+        QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x, int32_t k, double* e) {
-    if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_residual: bad argument");
-    if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_energies_residual: residual problems only");
-    if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_residual: the problem is not on the device");
-    if (k == 0) return QB_OK;
-    QB_CUDA(cudaSetDevice(p->device));
-    DevBuf dx, de;
-    qb_status s;
-    if ((s = upload(dx, x, size_t(k) * size_t(p->resid.n), nullptr))) return s;
-    if ((s = de.alloc(size_t(k) * 8))) return s;
-    if ((s = launch_resid_energies(p->resid, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
-    QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
-    return QB_OK;
+    return qb::guarded("qb_energies_residual", [&]() -> qb_status {
+        if (!p || (!x && k > 0) || (!e && k > 0) || k < 0) return fail(QB_EINVAL, "qb_energies_residual: bad argument");
+        if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_energies_residual: residual problems only");
+        if (!p->uploaded) return fail(QB_EINVAL, "qb_energies_residual: the problem is not on the device");
+        if (k == 0) return QB_OK;
+        QB_CUDA(cudaSetDevice(p->device));
+        DevBuf dx, de;
+        qb_status s;
+        if ((s = upload(dx, x, size_t(k) * size_t(p->resid.n), nullptr))) return s;
+        if ((s = de.alloc(size_t(k) * 8))) return s;
+        if ((s = launch_resid_energies(p->resid, dx.as<uint8_t>(), k, de.as<double>(), nullptr))) return s;
+        QB_CUDA(cudaMemcpy(e, de.p, size_t(k) * 8, cudaMemcpyDeviceToHost));
+        return QB_OK;
+    });
 }

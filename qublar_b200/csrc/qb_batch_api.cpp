@@ -288,158 +288,162 @@ std::map<std::tuple<int, int64_t, int64_t, int64_t, int>, qb_batch_config> g_tun
 
 extern "C" qb_status qb_batch_autotune(const qb_batch_item* items, int32_t count, int32_t sample_sweeps,
                                        const qb_opts* opts, qb_batch_config* out) {
-    if (!out) return fail(QB_EINVAL, "qb_batch_autotune: null output");
-    if (sample_sweeps < 0) return fail(QB_EINVAL, "qb_batch_autotune: sample_sweeps must be non-negative");
-    qb_status s0 = check_items(items, count);
-    if (s0 != QB_OK) return s0;
-    QB_CUDA(cudaSetDevice(items[0].problem->device));
-    const int S = sample_sweeps ? sample_sweeps : 8;
-    qb_batch* b = new (std::nothrow) qb_batch();
-    if (!b) return fail(QB_ENOMEM, "qb_batch_autotune: out of host memory");
-    qb_status s = prepare(items, count, opts, b);
-    if (s != QB_OK) {
-        qb_batch_destroy(b);
-        return s;
-    }
-    const auto key = std::make_tuple(count, b->total_bits, b->total_nnz, b->total_r, b->device);
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto hit = g_tuned.find(key);
-        if (hit != g_tuned.end()) {
-            *out = hit->second;
+    return qb::guarded("qb_batch_autotune", [&]() -> qb_status {
+        if (!out) return fail(QB_EINVAL, "qb_batch_autotune: null output");
+        if (sample_sweeps < 0) return fail(QB_EINVAL, "qb_batch_autotune: sample_sweeps must be non-negative");
+        qb_status s0 = check_items(items, count);
+        if (s0 != QB_OK) return s0;
+        QB_CUDA(cudaSetDevice(items[0].problem->device));
+        const int S = sample_sweeps ? sample_sweeps : 8;
+        qb_batch* b = new (std::nothrow) qb_batch();
+        if (!b) return fail(QB_ENOMEM, "qb_batch_autotune: out of host memory");
+        qb_status s = prepare(items, count, opts, b);
+        if (s != QB_OK) {
             qb_batch_destroy(b);
-            return QB_OK;
+            return s;
         }
-    }
-    // each instance's schedule sampled at S evenly spaced sweeps
-    std::vector<double> st(b->inst.size() * size_t(S));
-    for (size_t k = 0; k < b->inst.size(); ++k) {
-        const std::vector<double> t = temperatures(b->inst[k].sched);
-        for (int j = 0; j < S; ++j) st[k * size_t(S) + size_t(j)] = t[size_t(int64_t(j) * int64_t(t.size()) / S)];
-    }
-    DevBuf d_st;
-    if ((s = upload_vec(d_st, st, b->stream))) {
-        qb_batch_destroy(b);
-        return s;
-    }
-    const int cap = batch_max_smem();
-    const int threads_c[] = {256, 512, 1024};
-    const int smem_c[] = {48 * 1024, 96 * 1024, cap};
-    const int group_c[] = {8, 16, 32};
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    // time one shape on `its`; < 0 when it does not fit an SM
-    auto time_shape = [&](const qb_batch_config& c, const std::vector<IsingItem>& its, float* ms) -> qb_status {
-        *ms = -1.0f;
-        BatchShape sh{c.threads, c.smem_bytes, 0};
-        int ctas = 0;
-        if (batch_ctas(sh, &ctas) != QB_OK) return QB_OK;   // shape does not fit an SM
-        cudaEventRecord(e0, b->stream);
-        qb_status r = run_items(b, c, its);
-        if (r != QB_OK) return r;
-        cudaEventRecord(e1, b->stream);
-        if (cudaEventSynchronize(e1) != cudaSuccess)
-            return cuda_fail(cudaGetLastError(), "cudaEventSynchronize", __FILE__, __LINE__);
-        cudaEventElapsedTime(ms, e0, e1);
-        return QB_OK;
-    };
-    // every shape on the short sample, then the three fastest again on a
-    // sample four times longer (short samples cannot separate close shapes)
-    std::vector<std::pair<float, qb_batch_config>> timed;
-    for (int th : threads_c)
-        for (int sm : smem_c)
-            for (int g : group_c) {
-                qb_batch_config c{th, std::min(sm, cap), g, 0};
-                std::vector<IsingItem> its;
-                if ((s = build_items(b, c, S, d_st.as<double>(), its)) != QB_OK) break;
-                float ms = 0.0f;
-                if ((s = time_shape(c, its, &ms)) != QB_OK) break;
-                if (ms >= 0.0f) timed.emplace_back(ms, c);
+        const auto key = std::make_tuple(count, b->total_bits, b->total_nnz, b->total_r, b->device);
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto hit = g_tuned.find(key);
+            if (hit != g_tuned.end()) {
+                *out = hit->second;
+                qb_batch_destroy(b);
+                return QB_OK;
             }
-    float best = -1.0f;
-    qb_batch_config best_c{};
-    if (s == QB_OK && !timed.empty()) {
-        std::stable_sort(timed.begin(), timed.end(),
-                         [](const std::pair<float, qb_batch_config>& a, const std::pair<float, qb_batch_config>& b_) {
-                             return a.first < b_.first;
-                         });
-        const int S4 = 4 * S;
-        std::vector<double> st4(b->inst.size() * size_t(S4));
+        }
+        // each instance's schedule sampled at S evenly spaced sweeps
+        std::vector<double> st(b->inst.size() * size_t(S));
         for (size_t k = 0; k < b->inst.size(); ++k) {
             const std::vector<double> t = temperatures(b->inst[k].sched);
-            for (int j = 0; j < S4; ++j)
-                st4[k * size_t(S4) + size_t(j)] = t[size_t(int64_t(j) * int64_t(t.size()) / S4)];
+            for (int j = 0; j < S; ++j) st[k * size_t(S) + size_t(j)] = t[size_t(int64_t(j) * int64_t(t.size()) / S)];
         }
-        DevBuf d_st4;
-        s = upload_vec(d_st4, st4, b->stream);
-        for (size_t q = 0; s == QB_OK && q < std::min<size_t>(3, timed.size()); ++q) {
-            std::vector<IsingItem> its;
-            if ((s = build_items(b, timed[q].second, S4, d_st4.as<double>(), its)) != QB_OK) break;
-            float ms = 0.0f;
-            if ((s = time_shape(timed[q].second, its, &ms)) != QB_OK) break;
-            if (ms >= 0.0f && (best < 0.0f || ms < best)) {
-                best = ms;
-                best_c = timed[q].second;
+        DevBuf d_st;
+        if ((s = upload_vec(d_st, st, b->stream))) {
+            qb_batch_destroy(b);
+            return s;
+        }
+        const int cap = batch_max_smem();
+        const int threads_c[] = {256, 512, 1024};
+        const int smem_c[] = {48 * 1024, 96 * 1024, cap};
+        const int group_c[] = {8, 16, 32};
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        // time one shape on `its`; < 0 when it does not fit an SM
+        auto time_shape = [&](const qb_batch_config& c, const std::vector<IsingItem>& its, float* ms) -> qb_status {
+            *ms = -1.0f;
+            BatchShape sh{c.threads, c.smem_bytes, 0};
+            int ctas = 0;
+            if (batch_ctas(sh, &ctas) != QB_OK) return QB_OK;   // shape does not fit an SM
+            cudaEventRecord(e0, b->stream);
+            qb_status r = run_items(b, c, its);
+            if (r != QB_OK) return r;
+            cudaEventRecord(e1, b->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess)
+                return cuda_fail(cudaGetLastError(), "cudaEventSynchronize", __FILE__, __LINE__);
+            cudaEventElapsedTime(ms, e0, e1);
+            return QB_OK;
+        };
+        // every shape on the short sample, then the three fastest again on a
+        // sample four times longer (short samples cannot separate close shapes)
+        std::vector<std::pair<float, qb_batch_config>> timed;
+        for (int th : threads_c)
+            for (int sm : smem_c)
+                for (int g : group_c) {
+                    qb_batch_config c{th, std::min(sm, cap), g, 0};
+                    std::vector<IsingItem> its;
+                    if ((s = build_items(b, c, S, d_st.as<double>(), its)) != QB_OK) break;
+                    float ms = 0.0f;
+                    if ((s = time_shape(c, its, &ms)) != QB_OK) break;
+                    if (ms >= 0.0f) timed.emplace_back(ms, c);
+                }
+        float best = -1.0f;
+        qb_batch_config best_c{};
+        if (s == QB_OK && !timed.empty()) {
+            std::stable_sort(timed.begin(), timed.end(),
+                             [](const std::pair<float, qb_batch_config>& a, const std::pair<float, qb_batch_config>& b_) {
+                                 return a.first < b_.first;
+                             });
+            const int S4 = 4 * S;
+            std::vector<double> st4(b->inst.size() * size_t(S4));
+            for (size_t k = 0; k < b->inst.size(); ++k) {
+                const std::vector<double> t = temperatures(b->inst[k].sched);
+                for (int j = 0; j < S4; ++j)
+                    st4[k * size_t(S4) + size_t(j)] = t[size_t(int64_t(j) * int64_t(t.size()) / S4)];
+            }
+            DevBuf d_st4;
+            s = upload_vec(d_st4, st4, b->stream);
+            for (size_t q = 0; s == QB_OK && q < std::min<size_t>(3, timed.size()); ++q) {
+                std::vector<IsingItem> its;
+                if ((s = build_items(b, timed[q].second, S4, d_st4.as<double>(), its)) != QB_OK) break;
+                float ms = 0.0f;
+                if ((s = time_shape(timed[q].second, its, &ms)) != QB_OK) break;
+                if (ms >= 0.0f && (best < 0.0f || ms < best)) {
+                    best = ms;
+                    best_c = timed[q].second;
+                }
             }
         }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    qb_batch_destroy(b);
-    if (s != QB_OK) return s;
-    if (best < 0.0f) return fail(QB_EREFUSED, "qb_batch_autotune: no candidate shape fits the device");
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[key] = best_c;
-    }
-    *out = best_c;
-    return QB_OK;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        qb_batch_destroy(b);
+        if (s != QB_OK) return s;
+        if (best < 0.0f) return fail(QB_EREFUSED, "qb_batch_autotune: no candidate shape fits the device");
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tuned[key] = best_c;
+        }
+        *out = best_c;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_solve_batch(const qb_batch_item* items, int32_t count, const qb_batch_config* cfg,
                                     const qb_opts* opts, qb_batch** out) {
-    if (!out) return fail(QB_EINVAL, "qb_solve_batch: null output");
-    *out = nullptr;
-    qb_status s = check_items(items, count);
-    if (s != QB_OK) return s;
-    qb_batch_config c{};
-    if ((s = resolve_config(cfg, &c)) != QB_OK) return s;
-    QB_CUDA(cudaSetDevice(items[0].problem->device));
-    const int cap = batch_max_smem();
-    if (cap <= 0) return fail(QB_ECUDA, "batch: cannot read the device's shared-memory limit");
-    c.smem_bytes = std::min(c.smem_bytes, cap);
-    qb_batch* b = new (std::nothrow) qb_batch();
-    if (!b) return fail(QB_ENOMEM, "qb_solve_batch: out of host memory");
-    auto bail = [&](qb_status e) {
-        qb_batch_destroy(b);
-        return e;
-    };
-    if ((s = prepare(items, count, opts, b)) != QB_OK) return bail(s);
-    b->cfg = c;
-    if ((s = build_items(b, c, 0, nullptr, b->h_items)) != QB_OK) return bail(s);
-    b->work_items = int(b->h_items.size());
-    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
-        cudaEventCreate(&b->ev2) != cudaSuccess)
-        return bail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
-    // the descriptors go up before the timed region
-    if ((s = b->d_items.alloc(b->h_items.size() * sizeof(IsingItem)))) return bail(s);
-    QB_CUDA(cudaMemcpyAsync(b->d_items.p, b->h_items.data(), b->h_items.size() * sizeof(IsingItem),
-                            cudaMemcpyHostToDevice, b->stream));
-    BatchShape sh{c.threads, c.smem_bytes, c.ctas};
-    if (sh.ctas <= 0 && (s = batch_ctas(sh, &sh.ctas))) return bail(s);
-    b->ctas = std::min<int>(sh.ctas, b->work_items);
-    cudaEventRecord(b->ev0, b->stream);
-    if ((s = launch_ising_batch(b->d_items.as<IsingItem>(), b->work_items, b->d_counter.as<int>(), sh, b->stream)))
-        return bail(s);
-    cudaEventRecord(b->ev1, b->stream);
-    if ((s = launch_batch_marginals(b->d_x.as<uint8_t>(), b->d_inst.as<BatchInstDev>(), int(b->inst.size()),
-                                    b->total_bits, b->d_p.as<float>(), b->stream)))
-        return bail(s);
-    cudaEventRecord(b->ev2, b->stream);
-    b->launches = 2;
-    *out = b;
-    return QB_OK;
+    return qb::guarded("qb_solve_batch", [&]() -> qb_status {
+        if (!out) return fail(QB_EINVAL, "qb_solve_batch: null output");
+        *out = nullptr;
+        qb_status s = check_items(items, count);
+        if (s != QB_OK) return s;
+        qb_batch_config c{};
+        if ((s = resolve_config(cfg, &c)) != QB_OK) return s;
+        QB_CUDA(cudaSetDevice(items[0].problem->device));
+        const int cap = batch_max_smem();
+        if (cap <= 0) return fail(QB_ECUDA, "batch: cannot read the device's shared-memory limit");
+        c.smem_bytes = std::min(c.smem_bytes, cap);
+        qb_batch* b = new (std::nothrow) qb_batch();
+        if (!b) return fail(QB_ENOMEM, "qb_solve_batch: out of host memory");
+        auto bail = [&](qb_status e) {
+            qb_batch_destroy(b);
+            return e;
+        };
+        if ((s = prepare(items, count, opts, b)) != QB_OK) return bail(s);
+        b->cfg = c;
+        if ((s = build_items(b, c, 0, nullptr, b->h_items)) != QB_OK) return bail(s);
+        b->work_items = int(b->h_items.size());
+        if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+            cudaEventCreate(&b->ev2) != cudaSuccess)
+            return bail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
+        // the descriptors go up before the timed region
+        if ((s = b->d_items.alloc(b->h_items.size() * sizeof(IsingItem)))) return bail(s);
+        QB_CUDA(cudaMemcpyAsync(b->d_items.p, b->h_items.data(), b->h_items.size() * sizeof(IsingItem),
+                                cudaMemcpyHostToDevice, b->stream));
+        BatchShape sh{c.threads, c.smem_bytes, c.ctas};
+        if (sh.ctas <= 0 && (s = batch_ctas(sh, &sh.ctas))) return bail(s);
+        b->ctas = std::min<int>(sh.ctas, b->work_items);
+        cudaEventRecord(b->ev0, b->stream);
+        if ((s = launch_ising_batch(b->d_items.as<IsingItem>(), b->work_items, b->d_counter.as<int>(), sh, b->stream)))
+            return bail(s);
+        cudaEventRecord(b->ev1, b->stream);
+        if ((s = launch_batch_marginals(b->d_x.as<uint8_t>(), b->d_inst.as<BatchInstDev>(), int(b->inst.size()),
+                                        b->total_bits, b->d_p.as<float>(), b->stream)))
+            return bail(s);
+        cudaEventRecord(b->ev2, b->stream);
+        b->launches = 2;
+        *out = b;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_batch_info_get(qb_batch* b, qb_batch_info* info) {

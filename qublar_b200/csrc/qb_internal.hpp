@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
 #include <memory>
 #include <new>
 #include <string>
@@ -20,6 +21,22 @@ namespace qb {
 
 void set_error(const std::string& msg);
 qb_status fail(qb_status s, const std::string& msg);
+
+// Runs the body of a C ABI entry point: an exception (a failed host
+// allocation above all, for sizes the caller chose) becomes a status instead
+// of crossing the C ABI and ending the caller's process.
+template <typename F>
+qb_status guarded(const char* name, F&& body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(QB_ENOMEM, std::string(name) + ": out of host memory");
+    } catch (const std::exception& e) {
+        return fail(QB_EINVAL, std::string(name) + ": " + e.what());
+    } catch (...) {
+        return fail(QB_EINVAL, std::string(name) + ": unexpected failure");
+    }
+}
 qb_status cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 
 #define QB_CUDA(call)                                                              \

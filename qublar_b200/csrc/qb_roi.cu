@@ -108,127 +108,131 @@ __global__ void __launch_bounds__(kEnumThreads) enumerate_kernel(int n, const do
 
 extern "C" qb_status qb_roi_qubo(const qb_residual_desc* p, const int32_t* roi, int32_t n_roi, const uint8_t* x_bar,
                                  double* h, double* J) {
-    using qb::fail;
-    if (!p || !roi || !x_bar || !h || !J || n_roi < 0) return fail(QB_EINVAL, "qb_roi_qubo: null argument");
-    const int nv = p->n_vars, nr = p->n_rays, n = n_roi;
-    std::vector<int32_t> pos(static_cast<size_t>(nv), -1);
-    for (int i = 0; i < n; ++i) {
-        if (roi[i] < 0 || roi[i] >= nv) return fail(QB_EINVAL, "qb_roi_qubo: region index out of range");
-        if (pos[size_t(roi[i])] >= 0) return fail(QB_EINVAL, "qb_roi_qubo: a bit appears twice in the region");
-        pos[size_t(roi[i])] = i;
-    }
-    std::fill(h, h + n, 0.0);
-    std::fill(J, J + size_t(n) * size_t(n), 0.0);
-    // residuals with the region switched off
-    std::vector<double> r(static_cast<size_t>(nr));
-    for (int b = 0; b < nr; ++b) r[size_t(b)] = -p->d[b];
-    for (int v = 0; v < nv; ++v)
-        if (x_bar[v] && pos[size_t(v)] < 0)
-            for (int k = p->row_ptr[v]; k < p->row_ptr[v + 1]; ++k) r[size_t(p->ray[k])] += p->a[k];
-    // data terms through the rays the region touches (in ray order for the couplings)
-    std::vector<std::vector<std::pair<int, double>>> on_ray;
-    std::vector<int32_t> slot(static_cast<size_t>(nr), -1);
-    std::vector<int32_t> touched;
-    for (int i = 0; i < n; ++i)
-        for (int k = p->row_ptr[roi[i]]; k < p->row_ptr[roi[i] + 1]; ++k) {
-            const int b = p->ray[k];
-            const double a = p->a[k];
-            h[i] += p->w[b] * (r[size_t(b)] * a + 0.5 * a * a);
-            if (slot[size_t(b)] < 0) {
-                slot[size_t(b)] = int32_t(on_ray.size());
-                on_ray.emplace_back();
-                touched.push_back(b);
-            }
-            on_ray[size_t(slot[size_t(b)])].push_back({i, a});
+    return qb::guarded("qb_roi_qubo", [&]() -> qb_status {
+        using qb::fail;
+        if (!p || !roi || !x_bar || !h || !J || n_roi < 0) return fail(QB_EINVAL, "qb_roi_qubo: null argument");
+        const int nv = p->n_vars, nr = p->n_rays, n = n_roi;
+        std::vector<int32_t> pos(static_cast<size_t>(nv), -1);
+        for (int i = 0; i < n; ++i) {
+            if (roi[i] < 0 || roi[i] >= nv) return fail(QB_EINVAL, "qb_roi_qubo: region index out of range");
+            if (pos[size_t(roi[i])] >= 0) return fail(QB_EINVAL, "qb_roi_qubo: a bit appears twice in the region");
+            pos[size_t(roi[i])] = i;
         }
-    std::sort(touched.begin(), touched.end());
-    for (int b : touched) {
-        const auto& L = on_ray[size_t(slot[size_t(b)])];
-        for (size_t u = 0; u < L.size(); ++u)
-            for (size_t v = u + 1; v < L.size(); ++v) {
-                int i = L[u].first, j = L[v].first;
-                if (i > j) std::swap(i, j);
-                J[size_t(i) * size_t(n) + size_t(j)] += p->w[b] * L[u].second * L[v].second;
-            }
-    }
-    // the prior: the linear field, bonds inside the region, bonds to fixed neighbours
-    for (int i = 0; i < n; ++i) {
-        const int vi = roi[i];
-        h[i] += p->field ? p->field[vi] : p->kappa;
-        for (int k = p->nbr_ptr[vi]; k < p->nbr_ptr[vi + 1]; ++k) {
-            const int vj = p->nbr[k];
-            const int pj = pos[size_t(vj)];
-            if (pj >= 0) {
-                if (pj > i) {
-                    h[i] += p->lambda;
-                    h[pj] += p->lambda;
-                    J[size_t(i) * size_t(n) + size_t(pj)] -= 2.0 * p->lambda;
+        std::fill(h, h + n, 0.0);
+        std::fill(J, J + size_t(n) * size_t(n), 0.0);
+        // residuals with the region switched off
+        std::vector<double> r(static_cast<size_t>(nr));
+        for (int b = 0; b < nr; ++b) r[size_t(b)] = -p->d[b];
+        for (int v = 0; v < nv; ++v)
+            if (x_bar[v] && pos[size_t(v)] < 0)
+                for (int k = p->row_ptr[v]; k < p->row_ptr[v + 1]; ++k) r[size_t(p->ray[k])] += p->a[k];
+        // data terms through the rays the region touches (in ray order for the couplings)
+        std::vector<std::vector<std::pair<int, double>>> on_ray;
+        std::vector<int32_t> slot(static_cast<size_t>(nr), -1);
+        std::vector<int32_t> touched;
+        for (int i = 0; i < n; ++i)
+            for (int k = p->row_ptr[roi[i]]; k < p->row_ptr[roi[i] + 1]; ++k) {
+                const int b = p->ray[k];
+                const double a = p->a[k];
+                h[i] += p->w[b] * (r[size_t(b)] * a + 0.5 * a * a);
+                if (slot[size_t(b)] < 0) {
+                    slot[size_t(b)] = int32_t(on_ray.size());
+                    on_ray.emplace_back();
+                    touched.push_back(b);
                 }
-            } else {
-                h[i] += p->lambda * (x_bar[vj] ? -1.0 : 1.0);
+                on_ray[size_t(slot[size_t(b)])].push_back({i, a});
+            }
+        std::sort(touched.begin(), touched.end());
+        for (int b : touched) {
+            const auto& L = on_ray[size_t(slot[size_t(b)])];
+            for (size_t u = 0; u < L.size(); ++u)
+                for (size_t v = u + 1; v < L.size(); ++v) {
+                    int i = L[u].first, j = L[v].first;
+                    if (i > j) std::swap(i, j);
+                    J[size_t(i) * size_t(n) + size_t(j)] += p->w[b] * L[u].second * L[v].second;
+                }
+        }
+        // the prior: the linear field, bonds inside the region, bonds to fixed neighbours
+        for (int i = 0; i < n; ++i) {
+            const int vi = roi[i];
+            h[i] += p->field ? p->field[vi] : p->kappa;
+            for (int k = p->nbr_ptr[vi]; k < p->nbr_ptr[vi + 1]; ++k) {
+                const int vj = p->nbr[k];
+                const int pj = pos[size_t(vj)];
+                if (pj >= 0) {
+                    if (pj > i) {
+                        h[i] += p->lambda;
+                        h[pj] += p->lambda;
+                        J[size_t(i) * size_t(n) + size_t(pj)] -= 2.0 * p->lambda;
+                    }
+                } else {
+                    h[i] += p->lambda * (x_bar[vj] ? -1.0 : 1.0);
+                }
             }
         }
-    }
-    return QB_OK;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_enumerate_qubo(int32_t n, const double* h, const double* J, double T, const qb_opts* opts,
                                        qb_enum_result* out, double* marginals) {
-    using namespace qb;
-    if (!h || !J || !out || !marginals) return fail(QB_EINVAL, "qb_enumerate_qubo: null argument");
-    if (n < 1 || n > kEnumMaxN) return fail(QB_EINVAL, "qb_enumerate_qubo: n must be in [1, 34]");
-    if (!(T > 0.0) || !std::isfinite(T)) return fail(QB_EINVAL, "qb_enumerate_qubo: T must be positive");
-    for (int i = 0; i < n; ++i) {
-        if (!std::isfinite(h[i])) return fail(QB_EINVAL, "qb_enumerate_qubo: non-finite h");
-        for (int j = i + 1; j < n; ++j)
-            if (!std::isfinite(J[size_t(i) * size_t(n) + size_t(j)])) return fail(QB_EINVAL, "qb_enumerate_qubo: non-finite J");
-    }
-    cudaStream_t st = opts ? static_cast<cudaStream_t>(opts->stream) : nullptr;
-    if (opts && opts->device >= 0) QB_CUDA(cudaSetDevice(opts->device));
-    // the upper triangle as a symmetric matrix with a zero diagonal
-    std::vector<double> Js(size_t(n) * size_t(n), 0.0);
-    for (int i = 0; i < n; ++i)
-        for (int j = i + 1; j < n; ++j) Js[size_t(i) * n + j] = Js[size_t(j) * n + i] = J[size_t(i) * n + j];
-    const uint64_t total = uint64_t(1) << n;
-    const uint64_t max_threads = uint64_t(148) * 4 * kEnumThreads;
-    uint64_t per = 1;
-    while (total / per > max_threads) per <<= 1;
-    const uint64_t threads = (total + per - 1) / per;
-    const unsigned blocks = unsigned((threads + kEnumThreads - 1) / kEnumThreads);
-    DevBuf d_h, d_J, d_part;
-    qb_status s;
-    if ((s = upload(d_h, h, size_t(n) * 8, st))) return s;
-    if ((s = upload(d_J, Js.data(), Js.size() * 8, st))) return s;
-    const size_t stride = size_t(kPartHead + n);
-    if ((s = d_part.alloc(size_t(threads) * stride * 8))) return s;
-    enumerate_kernel<<<blocks, kEnumThreads, 0, st>>>(n, d_h.as<double>(), d_J.as<double>(), 1.0 / T, per, total,
-                                                      d_part.as<double>());
-    QB_CUDA(cudaGetLastError());
-    std::vector<double> part(size_t(threads) * stride);
-    QB_CUDA(cudaMemcpyAsync(part.data(), d_part.p, part.size() * 8, cudaMemcpyDeviceToHost, st));
-    QB_CUDA(cudaStreamSynchronize(st));
-    // combine in thread order
-    double m = INFINITY, e_min = INFINITY;
-    for (uint64_t t = 0; t < threads; ++t) m = std::min(m, part[size_t(t) * stride]);
-    double z = 0.0, ze = 0.0;
-    uint64_t x_min = 0;
-    std::vector<double> zi(static_cast<size_t>(n), 0.0);
-    for (uint64_t t = 0; t < threads; ++t) {
-        const double* o = &part[size_t(t) * stride];
-        const double c = std::exp(-(o[0] - m) / T);
-        z += o[1] * c;
-        ze += o[2] * c;
-        for (int i = 0; i < n; ++i) zi[size_t(i)] += o[kPartHead + i] * c;
-        if (o[3] < e_min) {
-            e_min = o[3];
-            std::memcpy(&x_min, &o[4], 8);
+    return qb::guarded("qb_enumerate_qubo", [&]() -> qb_status {
+        using namespace qb;
+        if (!h || !J || !out || !marginals) return fail(QB_EINVAL, "qb_enumerate_qubo: null argument");
+        if (n < 1 || n > kEnumMaxN) return fail(QB_EINVAL, "qb_enumerate_qubo: n must be in [1, 34]");
+        if (!(T > 0.0) || !std::isfinite(T)) return fail(QB_EINVAL, "qb_enumerate_qubo: T must be positive");
+        for (int i = 0; i < n; ++i) {
+            if (!std::isfinite(h[i])) return fail(QB_EINVAL, "qb_enumerate_qubo: non-finite h");
+            for (int j = i + 1; j < n; ++j)
+                if (!std::isfinite(J[size_t(i) * size_t(n) + size_t(j)])) return fail(QB_EINVAL, "qb_enumerate_qubo: non-finite J");
         }
-    }
-    out->log_z = std::log(z) - m / T;
-    out->e_min = e_min;
-    out->x_min = x_min;
-    out->mean_energy = ze / z;
-    out->states = total;
-    for (int i = 0; i < n; ++i) marginals[i] = zi[size_t(i)] / z;
-    return QB_OK;
+        cudaStream_t st = opts ? static_cast<cudaStream_t>(opts->stream) : nullptr;
+        if (opts && opts->device >= 0) QB_CUDA(cudaSetDevice(opts->device));
+        // the upper triangle as a symmetric matrix with a zero diagonal
+        std::vector<double> Js(size_t(n) * size_t(n), 0.0);
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j) Js[size_t(i) * n + j] = Js[size_t(j) * n + i] = J[size_t(i) * n + j];
+        const uint64_t total = uint64_t(1) << n;
+        const uint64_t max_threads = uint64_t(148) * 4 * kEnumThreads;
+        uint64_t per = 1;
+        while (total / per > max_threads) per <<= 1;
+        const uint64_t threads = (total + per - 1) / per;
+        const unsigned blocks = unsigned((threads + kEnumThreads - 1) / kEnumThreads);
+        DevBuf d_h, d_J, d_part;
+        qb_status s;
+        if ((s = upload(d_h, h, size_t(n) * 8, st))) return s;
+        if ((s = upload(d_J, Js.data(), Js.size() * 8, st))) return s;
+        const size_t stride = size_t(kPartHead + n);
+        if ((s = d_part.alloc(size_t(threads) * stride * 8))) return s;
+        enumerate_kernel<<<blocks, kEnumThreads, 0, st>>>(n, d_h.as<double>(), d_J.as<double>(), 1.0 / T, per, total,
+                                                          d_part.as<double>());
+        QB_CUDA(cudaGetLastError());
+        std::vector<double> part(size_t(threads) * stride);
+        QB_CUDA(cudaMemcpyAsync(part.data(), d_part.p, part.size() * 8, cudaMemcpyDeviceToHost, st));
+        QB_CUDA(cudaStreamSynchronize(st));
+        // combine in thread order
+        double m = INFINITY, e_min = INFINITY;
+        for (uint64_t t = 0; t < threads; ++t) m = std::min(m, part[size_t(t) * stride]);
+        double z = 0.0, ze = 0.0;
+        uint64_t x_min = 0;
+        std::vector<double> zi(static_cast<size_t>(n), 0.0);
+        for (uint64_t t = 0; t < threads; ++t) {
+            const double* o = &part[size_t(t) * stride];
+            const double c = std::exp(-(o[0] - m) / T);
+            z += o[1] * c;
+            ze += o[2] * c;
+            for (int i = 0; i < n; ++i) zi[size_t(i)] += o[kPartHead + i] * c;
+            if (o[3] < e_min) {
+                e_min = o[3];
+                std::memcpy(&x_min, &o[4], 8);
+            }
+        }
+        out->log_z = std::log(z) - m / T;
+        out->e_min = e_min;
+        out->x_min = x_min;
+        out->mean_energy = ze / z;
+        out->states = total;
+        for (int i = 0; i < n; ++i) marginals[i] = zi[size_t(i)] / z;
+        return QB_OK;
+    });
 }

@@ -681,101 +681,105 @@ Request* find_locked(qb_server* S, uint64_t id) {
 // ---- C ABI -------------------------------------------------------------------------------------
 
 extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** out) {
-    if (!out) return fail(QB_EINVAL, "qb_server_create: null output");
-    *out = nullptr;
-    qb_server_config c{};
-    if (cfg) c = *cfg;
-    if (c.max_active == 0) c.max_active = kDefaultActive;
-    if (c.residual_streams == 0) c.residual_streams = kDefaultResidStreams;
-    if (c.tick_target_us == 0) c.tick_target_us = kDefaultTickUs;
-    if (c.hbm_budget_bytes < 0 || c.max_active < 0 || c.residual_streams < 0 || c.residual_streams > 64 ||
-        c.tick_target_us < 0 || c.max_pending < 0)
-        return fail(QB_EINVAL, "qb_server_create: negative or out-of-range setting");
-    if (c.batch.threads == 0) c.batch.threads = 512;
-    if (c.batch.smem_bytes == 0) c.batch.smem_bytes = 96 * 1024;
-    if (c.batch.max_group == 0) c.batch.max_group = 32;
-    if (c.batch.threads < 32 || c.batch.threads > 1024 || c.batch.threads % 32 || c.batch.max_group < 1 ||
-        c.batch.max_group > 32 || (c.batch.max_group & (c.batch.max_group - 1)))
-        return fail(QB_EINVAL, "qb_server_create: bad packed-kernel shape");
-    int dev = c.device;
-    if (dev < 0) QB_CUDA(cudaGetDevice(&dev));
-    QB_CUDA(cudaSetDevice(dev));
-    std::unique_ptr<qb_server> S(new (std::nothrow) qb_server());
-    if (!S) return fail(QB_ENOMEM, "qb_server_create: out of host memory");
-    S->device = dev;
-    size_t free_b = 0, total_b = 0;
-    QB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    int64_t budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : kDefaultBudget;
-    if (c.hbm_budget_bytes == 0) budget = std::min<int64_t>(budget, int64_t(double(free_b) * 0.9));
-    S->budget = budget;
-    const int cap = batch_max_smem();
-    if (cap <= 0) return fail(QB_ECUDA, "qb_server_create: cannot read the shared-memory limit");
-    c.batch.smem_bytes = std::min(c.batch.smem_bytes, cap);
-    S->cfg = c;
-    S->shape.threads = c.batch.threads;
-    S->shape.smem_bytes = c.batch.smem_bytes;
-    qb_status s = batch_ctas(S->shape, &S->shape.ctas);
-    if (s != QB_OK) return s;
-    if (c.batch.ctas > 0) S->shape.ctas = std::min(S->shape.ctas, c.batch.ctas);
-    QB_CUDA(cudaStreamCreateWithFlags(&S->upload_stream, cudaStreamNonBlocking));
-    QB_CUDA(cudaStreamCreateWithFlags(&S->tick_stream, cudaStreamNonBlocking));
-    for (int k = 0; k < c.residual_streams; ++k) {
-        cudaStream_t st;
-        QB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        S->resid_streams.push_back(st);
-    }
-    QB_CUDA(cudaEventCreateWithFlags(&S->upload_ev, cudaEventDisableTiming));
-    QB_CUDA(cudaEventCreateWithFlags(&S->tick_ev, cudaEventDisableTiming));
-    if (const char* fa = std::getenv("QB_SERVER_FAIL_ADMIT")) S->fail_admission = std::atoll(fa);
-    qb_server* raw = S.release();
-    raw->worker = std::thread(worker_main, raw);
-    *out = raw;
-    return QB_OK;
+    return qb::guarded("qb_server_create", [&]() -> qb_status {
+        if (!out) return fail(QB_EINVAL, "qb_server_create: null output");
+        *out = nullptr;
+        qb_server_config c{};
+        if (cfg) c = *cfg;
+        if (c.max_active == 0) c.max_active = kDefaultActive;
+        if (c.residual_streams == 0) c.residual_streams = kDefaultResidStreams;
+        if (c.tick_target_us == 0) c.tick_target_us = kDefaultTickUs;
+        if (c.hbm_budget_bytes < 0 || c.max_active < 0 || c.residual_streams < 0 || c.residual_streams > 64 ||
+            c.tick_target_us < 0 || c.max_pending < 0)
+            return fail(QB_EINVAL, "qb_server_create: negative or out-of-range setting");
+        if (c.batch.threads == 0) c.batch.threads = 512;
+        if (c.batch.smem_bytes == 0) c.batch.smem_bytes = 96 * 1024;
+        if (c.batch.max_group == 0) c.batch.max_group = 32;
+        if (c.batch.threads < 32 || c.batch.threads > 1024 || c.batch.threads % 32 || c.batch.max_group < 1 ||
+            c.batch.max_group > 32 || (c.batch.max_group & (c.batch.max_group - 1)))
+            return fail(QB_EINVAL, "qb_server_create: bad packed-kernel shape");
+        int dev = c.device;
+        if (dev < 0) QB_CUDA(cudaGetDevice(&dev));
+        QB_CUDA(cudaSetDevice(dev));
+        std::unique_ptr<qb_server> S(new (std::nothrow) qb_server());
+        if (!S) return fail(QB_ENOMEM, "qb_server_create: out of host memory");
+        S->device = dev;
+        size_t free_b = 0, total_b = 0;
+        QB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        int64_t budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : kDefaultBudget;
+        if (c.hbm_budget_bytes == 0) budget = std::min<int64_t>(budget, int64_t(double(free_b) * 0.9));
+        S->budget = budget;
+        const int cap = batch_max_smem();
+        if (cap <= 0) return fail(QB_ECUDA, "qb_server_create: cannot read the shared-memory limit");
+        c.batch.smem_bytes = std::min(c.batch.smem_bytes, cap);
+        S->cfg = c;
+        S->shape.threads = c.batch.threads;
+        S->shape.smem_bytes = c.batch.smem_bytes;
+        qb_status s = batch_ctas(S->shape, &S->shape.ctas);
+        if (s != QB_OK) return s;
+        if (c.batch.ctas > 0) S->shape.ctas = std::min(S->shape.ctas, c.batch.ctas);
+        QB_CUDA(cudaStreamCreateWithFlags(&S->upload_stream, cudaStreamNonBlocking));
+        QB_CUDA(cudaStreamCreateWithFlags(&S->tick_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < c.residual_streams; ++k) {
+            cudaStream_t st;
+            QB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            S->resid_streams.push_back(st);
+        }
+        QB_CUDA(cudaEventCreateWithFlags(&S->upload_ev, cudaEventDisableTiming));
+        QB_CUDA(cudaEventCreateWithFlags(&S->tick_ev, cudaEventDisableTiming));
+        if (const char* fa = std::getenv("QB_SERVER_FAIL_ADMIT")) S->fail_admission = std::atoll(fa);
+        qb_server* raw = S.release();
+        raw->worker = std::thread(worker_main, raw);
+        *out = raw;
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_schedule* sch, uint32_t n_branches,
                                       uint64_t seed_offset, uint64_t* id) {
-    if (!S || !p || !sch || !id) return fail(QB_EINVAL, "qb_server_submit: null argument");
-    if (p->device != S->device) return fail(QB_EINVAL, "qb_server_submit: the problem is on another device");
-    if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_server_submit: n_branches must be in [1, 2^20]");
-    if (sch->anneal_sweeps < 0 || sch->hold_sweeps < 0 || sch->anneal_sweeps + sch->hold_sweeps < 1 ||
-        !(sch->t_hot > 0.0) || !(sch->t_cold > 0.0) || !std::isfinite(sch->t_hot) || !std::isfinite(sch->t_cold) ||
-        sch->refresh_sweeps < 0)
-        return fail(QB_EINVAL, "qb_server_submit: bad schedule");
+    return qb::guarded("qb_server_submit", [&]() -> qb_status {
+        if (!S || !p || !sch || !id) return fail(QB_EINVAL, "qb_server_submit: null argument");
+        if (p->device != S->device) return fail(QB_EINVAL, "qb_server_submit: the problem is on another device");
+        if (n_branches < 1 || n_branches > (1u << 20)) return fail(QB_EINVAL, "qb_server_submit: n_branches must be in [1, 2^20]");
+        if (sch->anneal_sweeps < 0 || sch->hold_sweeps < 0 || sch->anneal_sweeps + sch->hold_sweeps < 1 ||
+            !(sch->t_hot > 0.0) || !(sch->t_cold > 0.0) || !std::isfinite(sch->t_hot) || !std::isfinite(sch->t_cold) ||
+            sch->refresh_sweeps < 0)
+            return fail(QB_EINVAL, "qb_server_submit: bad schedule");
 
-    std::unique_ptr<Request> r(new (std::nothrow) Request());
-    if (!r) return fail(QB_ENOMEM, "qb_server_submit: out of host memory");
-    r->prob = p;
-    r->sched = *sch;
-    r->kind = p->kind;
-    r->R = int(n_branches);
-    r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
-    r->exclusive = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
-    r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
-    r->seed0 = 1 + seed_offset;
-    if (p->kind == QB_KIND_ISING) {
-        r->charge_work = ising_work_bytes(p, r->R, r->sweeps);
-        r->charge_results = ising_result_bytes(r->n, r->R);
-    } else {
-        r->charge_work = resid_work_bytes(p, r->R, r->sweeps);
-        r->charge_results = resid_result_bytes(r->n, r->R);
-    }
-    r->t_submit = now_s();
-    std::lock_guard<std::mutex> lk(S->mu);
-    if (S->stop) return fail(QB_EINVAL, "qb_server_submit: the server is stopping");
-    if (S->cfg.max_pending > 0 && int64_t(S->pending.size()) >= S->cfg.max_pending)
-        return fail(QB_EBUSY, "qb_server_submit: the queue is full");
-    for (auto& kv : S->reqs)
-        if (kv.second->prob == p && (kv.second->state == QB_REQ_PENDING || kv.second->state == QB_REQ_RUNNING))
-            return fail(QB_EBUSY, "qb_server_submit: the problem already has a request in flight");
-    r->id = S->next_id++;
-    *id = r->id;
-    S->pending.push_back(r->id);
-    S->reqs[r->id] = std::move(r);
-    ++S->submitted;
-    S->kick = true;
-    S->cv_work.notify_one();
-    return QB_OK;
+        std::unique_ptr<Request> r(new (std::nothrow) Request());
+        if (!r) return fail(QB_ENOMEM, "qb_server_submit: out of host memory");
+        r->prob = p;
+        r->sched = *sch;
+        r->kind = p->kind;
+        r->R = int(n_branches);
+        r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
+        r->exclusive = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
+        r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
+        r->seed0 = 1 + seed_offset;
+        if (p->kind == QB_KIND_ISING) {
+            r->charge_work = ising_work_bytes(p, r->R, r->sweeps);
+            r->charge_results = ising_result_bytes(r->n, r->R);
+        } else {
+            r->charge_work = resid_work_bytes(p, r->R, r->sweeps);
+            r->charge_results = resid_result_bytes(r->n, r->R);
+        }
+        r->t_submit = now_s();
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stop) return fail(QB_EINVAL, "qb_server_submit: the server is stopping");
+        if (S->cfg.max_pending > 0 && int64_t(S->pending.size()) >= S->cfg.max_pending)
+            return fail(QB_EBUSY, "qb_server_submit: the queue is full");
+        for (auto& kv : S->reqs)
+            if (kv.second->prob == p && (kv.second->state == QB_REQ_PENDING || kv.second->state == QB_REQ_RUNNING))
+                return fail(QB_EBUSY, "qb_server_submit: the problem already has a request in flight");
+        r->id = S->next_id++;
+        *id = r->id;
+        S->pending.push_back(r->id);
+        S->reqs[r->id] = std::move(r);
+        ++S->submitted;
+        S->kick = true;
+        S->cv_work.notify_one();
+        return QB_OK;
+    });
 }
 
 extern "C" qb_status qb_server_poll(qb_server* S, uint64_t id, int32_t* state) {

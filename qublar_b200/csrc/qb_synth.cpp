@@ -400,11 +400,15 @@ qb_status synth_tomography(const qb_tomo_params* p, bool on_device, const qb_opt
 }  // namespace
 
 extern "C" qb_status qb_synth_tomography(const qb_tomo_params* p, qb_tomo** out) {
-    return synth_tomography(p, false, nullptr, out);
+    return qb::guarded("qb_synth_tomography", [&]() -> qb_status {
+        return synth_tomography(p, false, nullptr, out);
+    });
 }
 
 extern "C" qb_status qb_synth_tomography_device(const qb_tomo_params* p, const qb_opts* opts, qb_tomo** out) {
-    return synth_tomography(p, true, opts, out);
+    return qb::guarded("qb_synth_tomography_device", [&]() -> qb_status {
+        return synth_tomography(p, true, opts, out);
+    });
 }
 
 extern "C" qb_status qb_tomo_sizes(const qb_tomo* t, int32_t* n_vars, int32_t* n_rays, int64_t* nnz, int64_t* n_nbr) {

@@ -54,6 +54,8 @@ GOOD = "3 2 0.5 2 1\n0 1 0.1\n1 -2 0\n2 0.25 0\n0 1 -1\n1 2 3e-05\n"
     ("3 2 0.5 2\n", "bad header"),
     ("3 2 0.5 2 1 7\n", "bad header"),
     ("0 0 0 1 0\n", "header counts"),
+    ("5 0 0 1 0\n0 0 0\n", "more lines than the text holds"),
+    ("2000000000 0 0 1 0\n", "more lines than the text holds"),
     ("3 4 0 1 0\n0 0 0\n1 0 0\n2 0 0\n", "header counts"),
     ("3 0 nan 1 0\n0 0 0\n1 0 0\n2 0 0\n", "non-finite header"),
     ("3 0 0 1 0\n0 0 0\n2 0 0\n1 0 0\n", "out of order"),
