@@ -510,8 +510,8 @@ qb_status qb_enumerate_qubo(int32_t n, const double* h, const double* J, double 
  *                                ising_recon.hpp:305-309, in fp32), 255 outside;
  *   ising_out_traversable.bin    uint8 nx^3: 1 only where Exists;
  *   ising_out_machine.meta       the loader keys of the two masks.
- * var_voxel[i] is bit i's voxel index in nx^3; two bits on one voxel are
- * refused. Host only. */
+ * var_voxel[i] is bit i's voxel index in nx^3 (nx <= 1024); two bits on one
+ * voxel are refused. Host only. */
 typedef struct qb_export_desc {
     int32_t nx;
     double voxel;

@@ -54,7 +54,7 @@ std::string join(const char* dir, const char* name) {
 extern "C" qb_status qb_write_ising_out(const char* dir, const qb_export_desc* d) {
     return qb::guarded("qb_write_ising_out", [&]() -> qb_status {
         if (!dir || !d || !d->var_voxel || !d->p_void) return fail(QB_EINVAL, "qb_write_ising_out: null argument");
-        if (d->nx <= 0 || d->nx > 2048) return fail(QB_EINVAL, "qb_write_ising_out: nx must be in [1, 2048]");
+        if (d->nx <= 0 || d->nx > 1024) return fail(QB_EINVAL, "qb_write_ising_out: nx must be in [1, 1024]");
         if (d->n_vars < 0) return fail(QB_EINVAL, "qb_write_ising_out: n_vars must be non-negative");
         if (d->branches && d->n_branches <= 0) return fail(QB_EINVAL, "qb_write_ising_out: branches given without a count");
         const size_t cells = size_t(d->nx) * size_t(d->nx) * size_t(d->nx);
