@@ -651,16 +651,26 @@ void reap_cancelled_ising(qb_server* S) {
 void worker_main(qb_server* S) {
     cudaSetDevice(S->device);
     for (;;) {
-        poll_resid(S);
-        poll_tick(S);
-        poll_exclusive(S);
-        if (!S->tick_inflight) reap_cancelled_ising(S);
-        admit_pending(S);
-        if (!S->tick_inflight && !S->running_ising.empty() && S->fatal.empty()) {
-            if (launch_tick(S) != QB_OK) {
-                S->fatal = qb_last_error();
-                fail_all_running(S, QB_ECUDA, S->fatal);
+        try {
+            poll_resid(S);
+            poll_tick(S);
+            poll_exclusive(S);
+            if (!S->tick_inflight) reap_cancelled_ising(S);
+            admit_pending(S);
+            if (!S->tick_inflight && !S->running_ising.empty() && S->fatal.empty()) {
+                if (launch_tick(S) != QB_OK) {
+                    S->fatal = qb_last_error();
+                    fail_all_running(S, QB_ECUDA, S->fatal);
+                }
             }
+        } catch (const std::exception& e) {
+            // a failed host allocation (or any exception) must not end the
+            // caller's process: let the device's work end (every kernel's waits
+            // are bounded), then fail the running requests with the reason
+            cudaDeviceSynchronize();
+            S->fatal = dynamic_cast<const std::bad_alloc*>(&e) ? std::string("server worker: out of host memory")
+                                                               : std::string("server worker: ") + e.what();
+            fail_all_running(S, QB_ENOMEM, S->fatal);
         }
         std::unique_lock<std::mutex> lk(S->mu);
         const bool busy = S->tick_inflight || !S->running_resid.empty() || S->exclusive_run != nullptr;
