@@ -144,29 +144,33 @@ __global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A)
                         const unsigned F0 = warp_transpose32(uint32_t(f), lane);
                         const unsigned F1 = warp_transpose32(uint32_t(f >> 32), lane);
                         const unsigned xlo = uint32_t(x), xhi = uint32_t(x >> 32);
-                        unsigned todo = F0 | F1;
-                        while (__any_sync(kFullMask, todo != 0u)) {
-                            // the lane's next 2 flipped neighbours (ascending: CSR order per
-                            // replica); their shuffles issue together
-                            unsigned bit[2];
-                            float Jq[2];
+                        // each replica walks its own flipped neighbours (ascending: CSR
+                        // order), two steps of both lists per iteration, so the warp runs
+                        // max(flips of r0, flips of r1) of its busiest lane, not their union
+                        unsigned t0 = F0, t1 = F1;
+                        while (__any_sync(kFullMask, (t0 | t1) != 0u)) {
+                            unsigned b0[2], b1[2];
+                            float J0[2], J1[2];
                             unsigned xl[2], xh[2];
 #pragma unroll
                             for (int u = 0; u < 2; ++u) {
-                                bit[u] = todo & (0u - todo);
-                                todo ^= bit[u];
+                                b0[u] = t0 & (0u - t0);
+                                t0 ^= b0[u];
+                                b1[u] = t1 & (0u - t1);
+                                t1 ^= b1[u];
                             }
 #pragma unroll
                             for (int u = 0; u < 2; ++u) {
-                                const int q = bit[u] ? __ffs(bit[u]) - 1 : 0;
-                                Jq[u] = __shfl_sync(kFullMask, Jk, q);
-                                xl[u] = __shfl_sync(kFullMask, xlo, q);
-                                xh[u] = __shfl_sync(kFullMask, xhi, q);
+                                const int q0 = b0[u] ? __ffs(b0[u]) - 1 : 0, q1 = b1[u] ? __ffs(b1[u]) - 1 : 0;
+                                J0[u] = __shfl_sync(kFullMask, Jk, q0);
+                                J1[u] = __shfl_sync(kFullMask, Jk, q1);
+                                xl[u] = __shfl_sync(kFullMask, xlo, q0);
+                                xh[u] = __shfl_sync(kFullMask, xhi, q1);
                             }
 #pragma unroll
                             for (int u = 0; u < 2; ++u) {
-                                if (F0 & bit[u]) two_sum_acc(hi0, lo0, ((xl[u] >> lane) & 1u) ? Jq[u] : -Jq[u]);
-                                if (F1 & bit[u]) two_sum_acc(hi1, lo1, ((xh[u] >> lane) & 1u) ? Jq[u] : -Jq[u]);
+                                if (b0[u]) two_sum_acc(hi0, lo0, ((xl[u] >> lane) & 1u) ? J0[u] : -J0[u]);
+                                if (b1[u]) two_sum_acc(hi1, lo1, ((xh[u] >> lane) & 1u) ? J1[u] : -J1[u]);
                             }
                         }
                         continue;
