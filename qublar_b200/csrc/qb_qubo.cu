@@ -39,7 +39,7 @@ namespace qb {
 namespace {
 
 constexpr unsigned kFullMask = 0xffffffffu;
-constexpr int kQThreads = 512;
+constexpr int kQThreads = 1024;
 
 struct QuboArgs {
     int n;
@@ -88,7 +88,7 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float v) {
     lo = __fadd_rn(lo, e);
 }
 
-__global__ void __launch_bounds__(kQThreads, 2) qubo_lockstep_kernel(QuboArgs A) {
+__global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A) {
     const int lane = int(threadIdx.x & 31u);
     const int wpc = int(blockDim.x >> 5);
     const int gw = int(blockIdx.x) * wpc + int(threadIdx.x >> 5);
