@@ -83,6 +83,100 @@ int env_int(const char* name, int dflt) {
     return v && *v ? std::atoi(v) : dflt;
 }
 
+// Stage times of a planner, printed to stderr at the end when QB_PLAN_TIMES is set.
+class PlanMarks {
+public:
+    PlanMarks() : on_(std::getenv("QB_PLAN_TIMES") != nullptr) { (*this)("start"); }
+    void operator()(const char* what) {
+        if (on_) marks_.emplace_back(what, std::chrono::steady_clock::now());
+    }
+    void print() const {
+        for (size_t k = 1; k < marks_.size(); ++k)
+            std::fprintf(stderr, "[qb plan]   %s %.1f ms\n", marks_[k].first,
+                         std::chrono::duration<double, std::milli>(marks_[k].second - marks_[k - 1].second).count());
+    }
+
+private:
+    bool on_;
+    std::vector<std::pair<const char*, std::chrono::steady_clock::time_point>> marks_;
+};
+
+// Symmetric CSR of an edge list in edge order: edge (a, b) appends b to row a
+// and a to row b, as parse_rudy builds its adjacency (ising_weighted.hpp:135-147).
+// Each thread owns a contiguous range of rows and scans the whole edge list,
+// so the order inside a row is the sequential one. Indices must be in range.
+template <class W>
+void sym_csr(int n, int64_t m, const int32_t* eu, const int32_t* ev, const W* ew, std::vector<int64_t>& row,
+             std::vector<int32_t>& col, std::vector<W>& w) {
+    const int T = m >= (int64_t(1) << 16) ? std::max(1, omp_get_max_threads()) : 1;
+    row.assign(size_t(n) + 1, 0);
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const uint32_t lo = uint32_t(int64_t(n) * t / nt), span = uint32_t(int64_t(n) * (t + 1) / nt) - lo;
+        int64_t* r = row.data() + 1;
+        for (int64_t e = 0; e < m; ++e) {
+            const uint32_t a = uint32_t(eu[e]), b = uint32_t(ev[e]);
+            if (a - lo < span) r[a]++;
+            if (b - lo < span) r[b]++;
+        }
+    }
+    for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
+    col.resize(size_t(2 * m));
+    w.resize(size_t(2 * m));
+    std::vector<int64_t> fill(row.begin(), row.end() - 1);
+#pragma omp parallel num_threads(T)
+    {
+        // rows split by entry count
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        auto first_row = [&](int q) {
+            return uint32_t(std::lower_bound(row.begin(), row.end() - 1, 2 * m * q / nt) - row.begin());
+        };
+        const uint32_t lo = t == 0 ? 0u : first_row(t), hi = t + 1 == nt ? uint32_t(n) : first_row(t + 1);
+        const uint32_t span = hi - lo;
+        for (int64_t e = 0; e < m; ++e) {
+            const uint32_t a = uint32_t(eu[e]), b = uint32_t(ev[e]);
+            if (a - lo < span) {
+                const int64_t k = fill[a]++;
+                col[size_t(k)] = int32_t(b);
+                w[size_t(k)] = ew[e];
+            }
+            if (b - lo < span) {
+                const int64_t k = fill[b]++;
+                col[size_t(k)] = int32_t(a);
+                w[size_t(k)] = ew[e];
+            }
+        }
+    }
+}
+
+// True when some row of a symmetric CSR lists a neighbour twice: an edge given
+// twice, in either orientation.
+bool has_duplicate_edge(int n, const std::vector<int64_t>& row, const std::vector<int32_t>& col) {
+    bool dup = false;
+#pragma omp parallel reduction(|| : dup) if (row[size_t(n)] >= (int64_t(1) << 16))
+    {
+        std::vector<int32_t> buf;
+#pragma omp for schedule(dynamic, 2048)
+        for (int i = 0; i < n; ++i) {
+            buf.assign(col.begin() + row[size_t(i)], col.begin() + row[size_t(i) + 1]);
+            std::sort(buf.begin(), buf.end());
+            if (std::adjacent_find(buf.begin(), buf.end()) != buf.end()) dup = true;
+        }
+    }
+    return dup;
+}
+
+// Row offsets of the sweep-order CSR: row k holds the neighbours of bit order[k].
+void sweep_rows(const Colouring& C, const std::vector<int64_t>& row, std::vector<int32_t>& out) {
+    const size_t n = C.order.size();
+    out.assign(n + 1, 0);
+    for (size_t k = 0; k < n; ++k) {
+        const size_t i = size_t(C.order[k]);
+        out[k + 1] = out[k] + int32_t(row[i + 1] - row[i]);
+    }
+}
+
 // ---- ising planning -------------------------------------------------------------------
 
 qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
@@ -93,30 +187,22 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
     if (m > 0 && (!g->eu || !g->ev || !g->ew)) return fail(QB_EINVAL, "ising: null edge arrays");
     if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "ising: more than 2^30 edges");
     // loader refusals of parse_rudy (ising_weighted.hpp:113-133)
-    std::vector<uint64_t> key(static_cast<size_t>(m));
+    PlanMarks mark;
     for (int64_t e = 0; e < m; ++e) {
         const int32_t u = g->eu[e], v = g->ev[e];
         if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "ising: vertex index out of range");
         if (u == v) return fail(QB_EINVAL, "ising: self-loop");
-        key[size_t(e)] = (uint64_t(std::min(u, v)) << 32) | uint64_t(std::max(u, v));
     }
-    std::sort(key.begin(), key.end());
-    for (size_t k = 1; k < key.size(); ++k)
-        if (key[k] == key[k - 1]) return fail(QB_EINVAL, "ising: duplicate edge");
+    // symmetric CSR in edge order, as parse_rudy builds it (ising_weighted.hpp:135-147)
+    std::vector<int64_t> row;
+    std::vector<int32_t> col, w;
+    sym_csr(n, m, g->eu, g->ev, g->ew, row, col, w);
+    mark("csr");
+    if (has_duplicate_edge(n, row, col)) return fail(QB_EINVAL, "ising: duplicate edge");
+    mark("duplicates");
     P.n = n;
     P.m = m;
     P.nnz = 2 * m;
-    // symmetric CSR in edge order, as parse_rudy builds it (ising_weighted.hpp:135-147)
-    std::vector<int64_t> row(size_t(n) + 1, 0);
-    for (int64_t e = 0; e < m; ++e) { row[size_t(g->eu[e]) + 1]++; row[size_t(g->ev[e]) + 1]++; }
-    for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
-    std::vector<int32_t> col(size_t(2 * m)), w(size_t(2 * m));
-    std::vector<int64_t> fill(row.begin(), row.end() - 1);
-    for (int64_t e = 0; e < m; ++e) {
-        const int32_t a = g->eu[e], b = g->ev[e], wt = g->ew[e];
-        col[size_t(fill[size_t(a)])] = b; w[size_t(fill[size_t(a)]++)] = wt;
-        col[size_t(fill[size_t(b)])] = a; w[size_t(fill[size_t(b)]++)] = wt;
-    }
     // plan figures of gising::make_plan (ising_gpu.cuh:74-101)
     double sum_w2 = 0.0;
     P.w_min = 0;
@@ -136,13 +222,16 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
     if (P.B > 2147483647LL) return fail(QB_EREFUSED, "ising: field bound exceeds int32");
     P.sigma = std::sqrt(2.0 * sum_w2 / double(n));
     P.weight_bytes = P.max_w <= 127 ? 1 : 4;
+    mark("figures");
     P.col = colour_graph(n, row, col);
+    mark("colour");
     // sweep-order CSR
     const Colouring& C = P.col;
-    P.row.assign(size_t(n) + 1, 0);
+    sweep_rows(C, row, P.row);
     P.adj.resize(size_t(2 * m));
     P.wgt.resize(size_t(2 * m));
     P.f0.assign(size_t(n), 0);
+#pragma omp parallel for schedule(dynamic, 4096) if (m >= (int64_t(1) << 16))
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
         int32_t pos = P.row[size_t(k)];
@@ -153,9 +242,10 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
             acc -= w[size_t(e)];
             ++pos;
         }
-        P.row[size_t(k) + 1] = pos;
         P.f0[size_t(k)] = int32_t(acc);   // x = 0: s = -1 everywhere (wising::State, ising_weighted.hpp:199-208)
     }
+    mark("arrays");
+    mark.print();
     return QB_OK;
 }
 
@@ -199,42 +289,36 @@ qb_status plan_qubo(const qb_qubo_desc* g, QuboPlan& P) {
     if (m > 0 && (!g->eu || !g->ev || !g->ew)) return fail(QB_EINVAL, "qubo: null edge arrays");
     if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "qubo: more than 2^30 edges");
     if (!std::isfinite(g->offset)) return fail(QB_EINVAL, "qubo: offset must be finite");
-    std::vector<uint64_t> key(static_cast<size_t>(m));
+    PlanMarks mark;
     for (int64_t e = 0; e < m; ++e) {
         const int32_t u = g->eu[e], v = g->ev[e];
         if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "qubo: vertex index out of range");
         if (u == v) return fail(QB_EINVAL, "qubo: self-loop (put diagonal terms in h)");
         if (!std::isfinite(g->ew[e])) return fail(QB_EINVAL, "qubo: coupling is not finite");
-        key[size_t(e)] = (uint64_t(std::min(u, v)) << 32) | uint64_t(std::max(u, v));
     }
-    std::sort(key.begin(), key.end());
-    for (size_t k = 1; k < key.size(); ++k)
-        if (key[k] == key[k - 1]) return fail(QB_EINVAL, "qubo: duplicate edge");
+    // symmetric CSR, edge order per vertex
+    std::vector<int64_t> row;
+    std::vector<int32_t> col;
+    std::vector<float> w;
+    sym_csr(n, m, g->eu, g->ev, g->ew, row, col, w);
+    mark("csr");
+    if (has_duplicate_edge(n, row, col)) return fail(QB_EINVAL, "qubo: duplicate edge");
     if (g->h)
         for (int i = 0; i < n; ++i)
             if (!std::isfinite(g->h[i])) return fail(QB_EINVAL, "qubo: linear term is not finite");
+    mark("duplicates");
     P.n = n;
     P.m = m;
     P.nnz = 2 * m;
     P.offset = g->offset;
-    // symmetric CSR, edge order per vertex
-    std::vector<int64_t> row(size_t(n) + 1, 0);
-    for (int64_t e = 0; e < m; ++e) { row[size_t(g->eu[e]) + 1]++; row[size_t(g->ev[e]) + 1]++; }
-    for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
-    std::vector<int32_t> col(size_t(2 * m));
-    std::vector<float> w(size_t(2 * m));
-    std::vector<int64_t> fill(row.begin(), row.end() - 1);
-    for (int64_t e = 0; e < m; ++e) {
-        const int32_t a = g->eu[e], b = g->ev[e];
-        col[size_t(fill[size_t(a)])] = b; w[size_t(fill[size_t(a)]++)] = g->ew[e];
-        col[size_t(fill[size_t(b)])] = a; w[size_t(fill[size_t(b)]++)] = g->ew[e];
-    }
     P.col = colour_graph(n, row, col);
+    mark("colour");
     const Colouring& C = P.col;
-    P.row.assign(size_t(n) + 1, 0);
+    sweep_rows(C, row, P.row);
     P.adj.resize(size_t(2 * m));
     P.J.resize(size_t(2 * m));
     P.h.assign(size_t(n), 0.0f);
+#pragma omp parallel for schedule(dynamic, 4096) if (m >= (int64_t(1) << 16))
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
         int32_t pos = P.row[size_t(k)];
@@ -243,9 +327,10 @@ qb_status plan_qubo(const qb_qubo_desc* g, QuboPlan& P) {
             P.J[size_t(pos)] = w[size_t(e)];
             ++pos;
         }
-        P.row[size_t(k) + 1] = pos;
         P.h[size_t(k)] = g->h ? g->h[i] : 0.0f;
     }
+    mark("arrays");
+    mark.print();
     return QB_OK;
 }
 
@@ -352,12 +437,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     P.nnz = d->row_ptr[n];
     P.n_nbr = d->nbr_ptr[n];
     P.lambda = d->lambda;
-    const bool times = std::getenv("QB_PLAN_TIMES") != nullptr;
-    std::vector<std::pair<const char*, std::chrono::steady_clock::time_point>> marks;
-    auto mark = [&](const char* what) {
-        if (times) marks.emplace_back(what, std::chrono::steady_clock::now());
-    };
-    mark("start");
+    PlanMarks mark;
     P.col = colour_residual(n, nr, &P.max_ray_len, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
     mark("colour");
     Colouring& C = P.col;
@@ -522,9 +602,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
         P.chunk_ptr[size_t(t) + 1] = int32_t(P.chunks.size() / 8);
     }
     mark("chunks");
-    for (size_t k = 1; k < marks.size(); ++k)
-        std::fprintf(stderr, "[qb plan]   %s %.1f ms\n", marks[k].first,
-                     std::chrono::duration<double, std::milli>(marks[k].second - marks[k - 1].second).count());
+    mark.print();
     return QB_OK;
 }
 

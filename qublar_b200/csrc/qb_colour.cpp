@@ -40,23 +40,27 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
     c.colour.assign(size_t(n), -1);
     // Largest degree first (Welsh-Powell order), ties by index: fewer classes
     // than index order on irregular graphs, identical on regular ones; then
-    // the classes are balanced (below).
+    // the classes are balanced (below). A stable counting sort by decreasing
+    // degree.
+    auto deg = [&](int i) { return int(row[size_t(i) + 1] - row[size_t(i)]); };
+    int maxdeg = 0;
+    for (int i = 0; i < n; ++i) maxdeg = std::max(maxdeg, deg(i));
     std::vector<int32_t> vis(static_cast<size_t>(n));
-    for (int i = 0; i < n; ++i) vis[size_t(i)] = i;
-    std::stable_sort(vis.begin(), vis.end(), [&](int a, int b) {
-        return row[size_t(a) + 1] - row[size_t(a)] > row[size_t(b) + 1] - row[size_t(b)];
-    });
-    std::vector<int32_t> mark;   // mark[colour] == i: colour used by a neighbour of i
+    {
+        std::vector<int32_t> start(size_t(maxdeg) + 2, 0);
+        for (int i = 0; i < n; ++i) start[size_t(maxdeg - deg(i)) + 1]++;
+        for (int d = 0; d <= maxdeg; ++d) start[size_t(d) + 1] += start[size_t(d)];
+        for (int i = 0; i < n; ++i) vis[size_t(start[size_t(maxdeg - deg(i))]++)] = i;
+    }
+    // Each bit takes the smallest colour none of its neighbours holds, so no
+    // colour exceeds the largest degree. mark[colour + 1] == i: a neighbour of
+    // i holds that colour; slot 0 collects the uncoloured neighbours.
+    std::vector<int32_t> mark(size_t(maxdeg) + 2, -1);
     for (int i : vis) {
-        for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k) {
-            const int cj = c.colour[size_t(col[size_t(k)])];
-            if (cj >= 0) {
-                if (size_t(cj) >= mark.size()) mark.resize(size_t(cj) + 1, -1);
-                mark[size_t(cj)] = i;
-            }
-        }
+        for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k)
+            mark[size_t(c.colour[size_t(col[size_t(k)])] + 1)] = i;
         int cc = 0;
-        while (size_t(cc) < mark.size() && mark[size_t(cc)] == i) ++cc;
+        while (mark[size_t(cc) + 1] == i) ++cc;
         c.colour[size_t(i)] = cc;
     }
     // Balance the classes: a sweep of a class costs ceil(size / workers)

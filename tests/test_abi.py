@@ -130,6 +130,80 @@ def test_graph_colouring_is_valid(gen):
     assert (colour[eu] != colour[ev]).all()
 
 
+def _greedy_balanced(n, eu, ev):
+    """The planner's graph colouring restated: bits by decreasing degree (ties
+    by index) take the smallest colour no neighbour holds; then, in index
+    order, a bit of a class above ceil(n / K) moves to the smallest class
+    below that size that none of its neighbours holds."""
+    adj = [[] for _ in range(n)]
+    for a, b in zip(eu.tolist(), ev.tolist()):
+        adj[a].append(b)
+        adj[b].append(a)
+    col = [-1] * n
+    for i in sorted(range(n), key=lambda i: -len(adj[i])):
+        used = {col[j] for j in adj[i]}
+        c = 0
+        while c in used:
+            c += 1
+        col[i] = c
+    K = max(col) + 1
+    target = -(-n // K)
+    size = [col.count(c) for c in range(K)]
+    for i in range(n):
+        ci = col[i]
+        if size[ci] <= target:
+            continue
+        seen = {col[j] for j in adj[i]}
+        best = -1
+        for q in range(K):
+            if q != ci and size[q] < target and q not in seen and (best < 0 or size[q] < size[best]):
+                best = q
+        if best >= 0:
+            col[i] = best
+            size[ci] -= 1
+            size[best] += 1
+    order = sorted(range(n), key=lambda i: col[i])
+    return np.array(order, np.int32), np.concatenate([[0], np.cumsum(size)]).astype(np.int32)
+
+
+def _random_edges(n, m, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, n, 3 * m)
+    b = rng.integers(0, n, 3 * m)
+    keep = a != b
+    key = np.minimum(a, b)[keep] * n + np.maximum(a, b)[keep]
+    _, first = np.unique(key, return_index=True)
+    idx = np.sort(first)[:m]
+    eu, ev = a[keep][idx].astype(np.int32), b[keep][idx].astype(np.int32)
+    assert eu.size == m
+    return eu, ev
+
+
+def test_graph_colouring_matches_the_greedy_rule_on_a_threaded_plan():
+    # 80,000 edges: the planner builds its adjacency with several threads
+    n = 20000
+    eu, ev = _random_edges(n, 80000, 7)
+    ew = np.ones(eu.size, np.int32)
+    d = IsingDesc(n, eu.size, ptr(eu), ptr(ev), ptr(ew))
+    order, cptr = _colour("ising", d, n)
+    want_order, want_cptr = _greedy_balanced(n, eu, ev)
+    assert (cptr == want_cptr).all()
+    assert (order == want_order).all()
+
+
+def test_duplicate_edge_refused_on_a_large_edge_list():
+    n = 20000
+    eu, ev = _random_edges(n, 80000, 11)
+    for flip in (False, True):
+        k = 56789
+        du = np.insert(eu, 70000, ev[k] if flip else eu[k])
+        dv = np.insert(ev, 70000, eu[k] if flip else ev[k])
+        st, msg = _ising_status(n, du, dv, np.ones(du.size, np.int32))
+        assert st == 1 and "duplicate edge" in msg
+        st, msg = _qubo_status(n, du, dv, np.ones(du.size, np.float32))
+        assert st == 1 and "duplicate edge" in msg
+
+
 def test_residual_colouring_is_valid():
     a = synth.tomography(synth.small_tomo_params())
     n = a["row_ptr"].size - 1
