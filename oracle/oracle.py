@@ -2,7 +2,10 @@
 
 * ``orc``  -- libqb_oracle.so, this project's C restatement (qb_oracle.c);
 * ``ref``  -- oracle/_ref/libqbref.so, the reference's own annealers compiled
-  from its sources (absent when the reference was never built here).
+  from its sources (absent when the reference was never built here);
+* ``ref_gpu`` -- oracle/_ref/libqbref_gpu.so, the reference's GPU annealer
+  (ising_gpu.cuh) compiled from its sources for sm_100a: the existing-kernel
+  comparator, for GPU tests only.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module, and only to check or time the CPU side; the solver never does.
@@ -17,6 +20,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(_HERE, "libqb_oracle.so")
 REF_PATH = os.path.join(_HERE, "_ref", "libqbref.so")
+REF_GPU_PATH = os.path.join(_HERE, "_ref", "libqbref_gpu.so")
 
 
 class ResidDesc(C.Structure):
@@ -38,6 +42,7 @@ def resid_desc(arr: dict) -> ResidDesc:
 
 _orc = None
 _ref = None
+_ref_gpu = None
 
 
 def orc() -> C.CDLL:
@@ -106,6 +111,32 @@ def ref() -> C.CDLL:
             f.restype, f.argtypes = res, args
         _ref = L
     return _ref
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_PATH)
+
+
+REF_GPU_SYMBOLS = {
+    "refgpu_graph_new": (C.c_void_p, [C.c_char_p, C.c_size_t, C.c_int, C.c_char_p, C.c_int]),
+    "refgpu_graph_free": (None, [C.c_void_p]),
+    "refgpu_plan": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "refgpu_run_batch": (C.c_double, [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+}
+
+
+def ref_gpu() -> C.CDLL:
+    """The reference's GPU annealer. Loading calls no CUDA function; every
+    refgpu_* call but refgpu_plan needs a GPU."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        L = C.CDLL(REF_GPU_PATH)
+        for name, (res, args) in REF_GPU_SYMBOLS.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _ref_gpu = L
+    return _ref_gpu
 
 
 # ---- integer helpers -----------------------------------------------------------------------------
@@ -275,6 +306,39 @@ def classify(p, lo=0.1, hi=0.9) -> np.ndarray:
 
 
 # ---- the compiled reference -------------------------------------------------------------------------
+
+class RefGpuGraph:
+    """The reference's GPU path: parse_rudy, make_plan and DeviceGraph
+    (ising_gpu.cuh:74-101, 278-343), then run_batch (:396-458)."""
+
+    def __init__(self, text: bytes, force_global: bool = False):
+        err = C.create_string_buffer(256)
+        self.h = ref_gpu().refgpu_graph_new(text, len(text), int(force_global), err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        f, w, d, s = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ref_gpu().refgpu_plan(self.h, C.byref(f), C.byref(w), C.byref(d), C.byref(s))
+        self.plan = {"field_bytes": f.value, "weight_bytes": w.value, "dense": bool(d.value),
+                     "shared_state": bool(s.value)}
+        self.n = int(text.split(maxsplit=1)[0])
+
+    def close(self):
+        if getattr(self, "h", None):
+            ref_gpu().refgpu_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def run_batch(self, t_hot, t_cold, anneal, hold, seed_base, R):
+        """Seeds seed_base .. seed_base + R - 1: (X, E, kernel_ms, launches, wall_s)."""
+        X = np.empty((R, self.n), np.uint8)
+        E = np.empty(R, np.int64)
+        kms, launches = C.c_double(), C.c_int()
+        wall = ref_gpu().refgpu_run_batch(self.h, t_hot, t_cold, anneal, hold, seed_base, R, _p(X), _p(E),
+                                          C.byref(kms), C.byref(launches))
+        return X, E, kms.value, launches.value, wall
+
 
 class RefGraph:
     """argos::wising::WeightedGraph parsed by the reference's own loader."""

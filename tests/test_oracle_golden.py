@@ -159,6 +159,13 @@ def test_restatement_matches_compiled_reference_integer():
         assert g.energy_scratch(x) == rg.energy_scratch(x) == e
 
 
+@pytest.mark.skipif(not O.ref_gpu_available(), reason="oracle/_ref not built (the reference tree is absent)")
+def test_reference_gpu_comparator_loads_and_exports_its_entry_points():
+    L = O.ref_gpu()   # no CUDA call: the kernels run only in the GPU tests
+    for name in O.REF_GPU_SYMBOLS:
+        assert getattr(L, name) is not None
+
+
 @needs_ref
 def test_restatement_matches_compiled_reference_residual():
     a = synth.tomography(synth.small_tomo_params(0.12, 12))
