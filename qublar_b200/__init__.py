@@ -26,7 +26,7 @@ import numpy as np
 from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
                    REQ_FAILED, REQ_PENDING, REQ_RUNNING, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts,
                    ExportDesc, ProblemInfo, QBError, QuboDesc, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig,
-                   ServerStats, check, lib, ptr)
+                   ServerStats, check, check_edge_lengths, check_residual_lengths, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
@@ -187,6 +187,7 @@ class IsingProblem(_Problem):
         super().__init__()
         self.n = int(n)
         self.eu, self.ev, self.ew = _c32(eu), _c32(ev), _c32(ew)
+        check_edge_lengths("ising", self.n, self.eu, self.ev, self.ew)
         self.m = int(self.eu.size)
         d = self.desc()
         h = C.c_void_p()
@@ -223,6 +224,7 @@ class ResidualProblem(_Problem):
         self.nbr_ptr, self.nbr = _c32(nbr_ptr), _c32(nbr)
         self.lam, self.kappa = float(lam), float(kappa)
         self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float64)
+        check_residual_lengths(self.d, self.w, self.row_ptr, self.ray, self.a, self.nbr_ptr, self.nbr, self.field)
         self.n = int(self.row_ptr.size - 1)
         self.n_rays = int(self.d.size)
         d_ = self.desc()
@@ -260,6 +262,7 @@ class QuboProblem(_Problem):
         self.ew = np.ascontiguousarray(ew, dtype=np.float32)
         self.h = None if h is None else np.ascontiguousarray(h, dtype=np.float32)
         self.offset = float(offset)
+        check_edge_lengths("qubo", self.n, self.eu, self.ev, self.ew, self.h)
         self.m = int(self.eu.size)
         d = QuboDesc(self.n, self.m, ptr(self.eu), ptr(self.ev), ptr(self.ew), ptr(self.h), self.offset)
         h_ = C.c_void_p()

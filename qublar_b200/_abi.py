@@ -35,6 +35,34 @@ class QBError(RuntimeError):
         self.message = message
 
 
+# The C ABI takes plain pointers: it reads as many entries as the sizes and
+# offsets in a descriptor say, and cannot see how long the caller's arrays
+# are. The Python mirror knows, and refuses (QB_EINVAL) arrays shorter than
+# their descriptor before any call.
+
+def check_edge_lengths(kind: str, n: int, eu, ev, ew, h=None) -> None:
+    if not (eu.size == ev.size == ew.size):
+        raise QBError(1, f"{kind}: eu, ev and ew differ in length")
+    if h is not None and h.size < n:
+        raise QBError(1, f"{kind}: h is shorter than n")
+
+
+def check_residual_lengths(d, w, row_ptr, ray, a, nbr_ptr, nbr, field=None) -> None:
+    if row_ptr.size < 1:
+        raise QBError(1, "residual: row_ptr is empty")
+    n = row_ptr.size - 1
+    if d.size != w.size:
+        raise QBError(1, "residual: d and w differ in length")
+    if nbr_ptr.size != n + 1:
+        raise QBError(1, "residual: nbr_ptr and row_ptr differ in length")
+    if not 0 <= int(row_ptr[-1]) <= min(ray.size, a.size):
+        raise QBError(1, "residual: row_ptr[n] exceeds the length of ray or a")
+    if not 0 <= int(nbr_ptr[-1]) <= nbr.size:
+        raise QBError(1, "residual: nbr_ptr[n] exceeds the length of nbr")
+    if field is not None and field.size < n:
+        raise QBError(1, "residual: field is shorter than n")
+
+
 class IsingDesc(C.Structure):
     _fields_ = [("n", C.c_int32), ("m", C.c_int64), ("eu", C.c_void_p), ("ev", C.c_void_p), ("ew", C.c_void_p)]
 

@@ -12,7 +12,7 @@ import math
 
 import numpy as np
 
-from ._abi import ResidualDesc, TomoParams, check, lib, ptr
+from ._abi import ResidualDesc, TomoParams, check, check_residual_lengths, lib, ptr
 
 GAMMA = np.uint64(0x9E3779B97F4A7C15)
 _M1 = np.uint64(0xBF58476D1CE4E5B9)
@@ -441,7 +441,10 @@ def tomography(params: TomoParams | None = None, truth: bool = False, device: in
 
 
 def residual_desc(arr: dict) -> ResidualDesc:
-    """A qb_residual_desc over numpy arrays (the caller keeps them alive)."""
+    """A qb_residual_desc over numpy arrays (the caller keeps them alive);
+    arrays shorter than their offsets are refused."""
+    check_residual_lengths(arr["d"], arr["w"], arr["row_ptr"], arr["ray"], arr["a"], arr["nbr_ptr"], arr["nbr"],
+                           arr.get("field"))
     return ResidualDesc(int(arr["row_ptr"].size - 1), int(arr["d"].size), ptr(arr["d"]), ptr(arr["w"]),
                         ptr(arr["row_ptr"]), ptr(arr["ray"]), ptr(arr["a"]), ptr(arr["nbr_ptr"]), ptr(arr["nbr"]),
                         float(arr["lambda"]), float(arr["kappa"]),

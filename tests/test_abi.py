@@ -100,6 +100,31 @@ def test_residual_refusals():
     assert st == 1 and "out of range" in msg
 
 
+def test_python_mirror_refuses_arrays_shorter_than_their_offsets():
+    # the C ABI reads as many entries as the offsets say; the mirror checks the
+    # lengths first, so no call reads past an array
+    a = synth.tiny6()
+    cases = [("nbr_ptr", lambda b: b["nbr_ptr"].__setitem__(-1, 2**31 - 1), "exceeds the length of nbr"),
+             ("row_ptr", lambda b: b["row_ptr"].__setitem__(-1, b["ray"].size + 1), "exceeds the length of ray or a"),
+             ("a", lambda b: b.__setitem__("a", b["a"][:-1]), "exceeds the length of ray or a"),
+             ("w", lambda b: b.__setitem__("w", b["w"][:-1]), "d and w differ in length"),
+             ("nbr_ptr", lambda b: b.__setitem__("nbr_ptr", b["nbr_ptr"][:-1]), "differ in length"),
+             ("field", lambda b: b.__setitem__("field", np.zeros(2)), "field is shorter than n")]
+    for key, mutate, why in cases:
+        b = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in a.items()}
+        mutate(b)
+        for make in (lambda: synth.residual_desc(b), lambda: qb.ResidualProblem.from_arrays(b)):
+            with pytest.raises(qb.QBError) as e:
+                make()
+            assert e.value.status == 1 and why in e.value.message, (key, e.value.message)
+    with pytest.raises(qb.QBError, match="differ in length"):
+        qb.IsingProblem(3, [0, 1], [1], [1, 1])
+    with pytest.raises(qb.QBError, match="differ in length"):
+        qb.QuboProblem(3, [0, 1], [1, 2], [1.0])
+    with pytest.raises(qb.QBError, match="h is shorter than n"):
+        qb.QuboProblem(3, [0], [1], [1.0], h=[0.0, 1.0])
+
+
 def test_solve_rejects_null_and_bad_schedule():
     L = lib()
     out = C.c_void_p()
