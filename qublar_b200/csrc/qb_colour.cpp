@@ -11,6 +11,8 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <omp.h>
+
 #include "qb_internal.hpp"
 
 namespace qb {
@@ -124,8 +126,26 @@ Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* ro
     // count near the longest ray (340 classes on the 306,328-bit pyramid whose
     // longest ray crosses 288 bits; ordering by ray count gives 349).
     std::vector<int32_t> raylen(static_cast<size_t>(std::max(n_rays, 1)), 0);
-    for (int i = 0; i < n; ++i)
-        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) raylen[size_t(ray[k])]++;
+    const int nnz = row_ptr[n];
+    const int T = omp_get_max_threads();
+    if (T > 1 && nnz >= (1 << 20) && int64_t(T) * n_rays <= (int64_t(1) << 24)) {
+        // per-thread counts over slices of the entries, then summed per ray
+        std::vector<int32_t> part(size_t(T) * size_t(n_rays), 0);
+#pragma omp parallel num_threads(T)
+        {
+            int32_t* cnt = part.data() + size_t(omp_get_thread_num()) * size_t(n_rays);
+#pragma omp for schedule(static)
+            for (int k = 0; k < nnz; ++k) cnt[ray[k]]++;
+#pragma omp for schedule(static)
+            for (int r = 0; r < n_rays; ++r) {
+                int32_t s = 0;
+                for (int t = 0; t < T; ++t) s += part[size_t(t) * size_t(n_rays) + size_t(r)];
+                raylen[size_t(r)] = s;
+            }
+        }
+    } else {
+        for (int k = 0; k < nnz; ++k) raylen[size_t(ray[k])]++;
+    }
     if (max_ray_len) *max_ray_len = n_rays > 0 ? *std::max_element(raylen.begin(), raylen.begin() + n_rays) : 0;
     std::vector<int64_t> conf(static_cast<size_t>(n), 0);
 #pragma omp parallel for schedule(static)
