@@ -858,7 +858,7 @@ def main():
         "config": {"workload": WORKLOAD, "bits": n, "rays": int(a["d"].size), "entries": int(a["ray"].size),
                    "branches": BRANCHES, "sweeps": sched.sweeps, "colours": int(pinfo.n_colours),
                    "l2": "flushed (256 MB write) before every timed step; problem footprint "
-                         f"{pinfo.device_bytes / 2**20:.0f} MiB", "parallelism": f"{world} independent replicas"},
+                         f"{pinfo.device_bytes / 2**20:.0f} MiB", "parallelism": f"{world} independent replica{'' if world == 1 else 's'} (one per GPU)"},
         "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                 "s_per_step": e2e_mean, "warmup_steps": e2e_warm},
         "gpu_launches": launches,
