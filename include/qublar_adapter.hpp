@@ -20,6 +20,7 @@
 // (the GPU replaces the thread pool).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -55,8 +56,22 @@ struct Result {
 // residuals every this many sweeps).
 constexpr int32_t kRefreshSweeps = 50;
 
+// The C ABI reads as many entries as the offsets say; the vectors know their
+// lengths, so an inconsistent problem is refused here before any call.
+inline void require(bool ok, const char* why) {
+    if (!ok) throw std::runtime_error(std::string("qublar adapter: ") + why);
+}
+
 template <class BinaryProblemT>
 qb_residual_desc residual_desc(const BinaryProblemT& p) {
+    const size_t n = p.var_voxel.size();
+    require(p.row_ptr.size() == n + 1 && p.nbr_ptr.size() == n + 1, "row_ptr and nbr_ptr need n_vars + 1 entries");
+    require(p.w.size() == p.d.size(), "d and w differ in length");
+    require(p.row_ptr.back() >= 0 && size_t(p.row_ptr.back()) <= std::min(p.ray.size(), p.a.size()),
+            "row_ptr[n_vars] exceeds the length of ray or a");
+    require(p.nbr_ptr.back() >= 0 && size_t(p.nbr_ptr.back()) <= p.nbr.size(),
+            "nbr_ptr[n_vars] exceeds the length of nbr");
+    require(p.field.empty() || p.field.size() >= n, "field is shorter than n_vars");
     qb_residual_desc d{};
     d.n_vars = int32_t(p.var_voxel.size());
     d.n_rays = int32_t(p.d.size());
@@ -118,6 +133,8 @@ std::vector<uint8_t> anneal_branch(const BinaryProblemT& p, const ScheduleT& s, 
 
 template <class WeightedGraphT>
 qb_ising_desc ising_desc(const WeightedGraphT& g) {
+    require(g.m >= 0 && g.eu.size() == size_t(g.m) && g.ev.size() == size_t(g.m) && g.ew.size() == size_t(g.m),
+            "eu, ev and ew need m entries each");
     qb_ising_desc d{};
     d.n = int32_t(g.n);
     d.m = int64_t(g.m);

@@ -5,10 +5,14 @@
 //   adapter_check <dir> cpu   -> a call without a device must throw cleanly
 //   adapter_check <dir> gpu   -> branch_fractions / anneal / run_batch results
 //                                are written to <dir> for the test to compare
+//   adapter_check <dir> lengths -> problems whose vectors are shorter than
+//                                their offsets say are refused by the adapter,
+//                                before any call into the library
 // <dir> holds the problem as raw little-endian arrays written by the test.
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -85,6 +89,41 @@ int main(int argc, char** argv) {
     Budget b;
     b.anneal_sweeps = 100;
     b.hold_sweeps = 10;
+    if (mode == "lengths") {
+        int refused = 0, cases = 0;
+        auto expect_refusal = [&](auto call) {
+            ++cases;
+            try {
+                call();
+            } catch (const std::runtime_error& e) {
+                if (std::string(e.what()).rfind("qublar adapter: ", 0) == 0) ++refused;
+            }
+        };
+        auto fractions = [&](const BinaryProblem& q) { return [&q, &s] { qublar::compat::branch_fractions(q, s, 1, 1u); }; };
+        BinaryProblem q = p;
+        q.nbr_ptr.back() = int(q.nbr.size()) + 1;
+        expect_refusal(fractions(q));
+        q = p;
+        q.a.pop_back();
+        expect_refusal(fractions(q));
+        q = p;
+        q.row_ptr.pop_back();
+        expect_refusal(fractions(q));
+        q = p;
+        q.w.pop_back();
+        expect_refusal(fractions(q));
+        q = p;
+        q.field.assign(2, 0.0);
+        expect_refusal(fractions(q));
+        WeightedGraph h = g;
+        h.ew.pop_back();
+        expect_refusal([&] { qublar::compat::anneal<RunOut>(h, b, 1); });
+        h = g;
+        h.m += 1;
+        expect_refusal([&] { qublar::compat::run_batch(h, b, 1, 2); });
+        std::printf("refused %d of %d\n", refused, cases);
+        return refused == cases ? 0 : 1;
+    }
     try {
         std::vector<std::vector<uint8_t>> keep;
         const std::vector<float> frac = qublar::compat::branch_fractions(p, s, 4, 16u, &keep, 5);

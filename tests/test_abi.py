@@ -6,7 +6,8 @@
 * the planner's colour classes are valid (no two interacting bits in a class)
   and cover every bit once;
 * the C++ adapter compiles against stand-in types with the reference's member
-  names and fails cleanly without a device;
+  names, fails cleanly without a device and refuses vectors shorter than their
+  offsets (as the Python mirror refuses arrays);
 * branches spread over two ranks (gloo) give the single-process fractions.
 """
 import ctypes as C
@@ -267,6 +268,18 @@ def test_adapter_compiles_and_fails_cleanly_without_a_device(tmp_path):
     r = subprocess.run([str(exe), str(tmp_path), "cpu"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "exception" in r.stdout
+
+
+def test_adapter_refuses_vectors_shorter_than_their_offsets(tmp_path):
+    exe = tmp_path / "adapter_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-I" + INCLUDE, os.path.join(ROOT, "tests", "adapter_check.cpp"),
+           "-L" + os.path.join(ROOT, "qublar_b200"), "-lqublar_b200", "-Wl,-rpath," + os.path.join(ROOT, "qublar_b200"),
+           "-o", str(exe)]
+    subprocess.run(cmd, check=True)
+    write_adapter_inputs(tmp_path)
+    r = subprocess.run([str(exe), str(tmp_path), "lengths"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "refused 7 of 7" in r.stdout
 
 
 def write_adapter_inputs(d):
