@@ -346,6 +346,13 @@ def write_ising_out(directory, nx: int, voxel: float, lo, var_voxel, p_void, bra
     pd = None if p_void_noprior is None else np.ascontiguousarray(p_void_noprior, dtype=np.float32)
     tr = None if truth is None else np.ascontiguousarray(truth, dtype=np.uint8)
     br = None if branches is None else np.ascontiguousarray(branches, dtype=np.uint8)
+    n = int(vv.size)
+    if pv.size < n or (pd is not None and pd.size < n):
+        raise QBError(1, "write_ising_out: p_void needs one value per bit of var_voxel")
+    if tr is not None and tr.size < int(nx) ** 3:
+        raise QBError(1, "write_ising_out: truth needs nx^3 cells")
+    if br is not None and (br.ndim != 2 or br.shape[1] != n):
+        raise QBError(1, "write_ising_out: branches must be n_branches x n_vars")
     nb = 0 if br is None else int(br.shape[0])
     d = ExportDesc(int(nx), float(voxel), (C.c_double * 3)(*[float(v) for v in lo]), int(vv.size), ptr(vv), ptr(pv),
                    ptr(pd), ptr(tr), ptr(br), nb, float(lam), float(kappa))
@@ -360,6 +367,11 @@ def write_roi_text(path, voxel, p, h, J, truth=None) -> None:
     hh = np.ascontiguousarray(h, dtype=np.float64)
     JJ = np.ascontiguousarray(J, dtype=np.float64)
     tr = None if truth is None else np.ascontiguousarray(truth, dtype=np.uint8)
+    n = int(vv.size)
+    if pp.size < n or hh.size < n or (tr is not None and tr.size < n):
+        raise QBError(1, "write_roi_text: p, h and truth need one value per bit")
+    if JJ.size < n * n:
+        raise QBError(1, "write_roi_text: J must be n x n")
     check(lib().qb_write_roi_text(os.fsencode(path), int(vv.size), ptr(vv), ptr(pp), ptr(tr), ptr(hh), ptr(JJ)))
 
 

@@ -129,6 +129,19 @@ def test_ising_out_refusals(tmp_path):
         write_ising_out(tmp_path / "missing" / "dir", 2, 1.0, (0, 0, 0), [3], [0.5])
 
 
+def test_exports_refuse_arrays_shorter_than_their_bits(tmp_path):
+    with pytest.raises(QBError, match="one value per bit of var_voxel"):
+        write_ising_out(tmp_path, 2, 1.0, (0, 0, 0), [1, 2], [0.5])
+    with pytest.raises(QBError, match="truth needs nx"):
+        write_ising_out(tmp_path, 2, 1.0, (0, 0, 0), [1, 2], [0.5, 0.5], truth=[1, 0])
+    with pytest.raises(QBError, match="n_branches x n_vars"):
+        write_ising_out(tmp_path, 2, 1.0, (0, 0, 0), [1, 2], [0.5, 0.5], branches=[1, 0])
+    with pytest.raises(QBError, match="one value per bit"):
+        write_roi_text(tmp_path / "r.txt", [1, 2], [0.5], [1.0, 2.0], np.zeros((2, 2)))
+    with pytest.raises(QBError, match="n x n"):
+        write_roi_text(tmp_path / "r.txt", [1, 2], [0.5, 0.5], [1.0, 2.0], np.zeros(3))
+
+
 def test_roi_text(tmp_path):
     n = 3
     voxel = np.array([7, 11, 30], np.int32)
