@@ -416,6 +416,8 @@ def roi_qubo(arrays: dict, roi, x_bar):
     d = residual_desc(arrays)
     roi = np.ascontiguousarray(roi, np.int32)
     x_bar = np.ascontiguousarray(x_bar, np.uint8)
+    if x_bar.size < d.n_vars:
+        raise QBError(1, "roi_qubo: x_bar needs one value per bit")
     h = np.empty(roi.size, np.float64)
     J = np.empty((roi.size, roi.size), np.float64)
     check(lib().qb_roi_qubo(C.byref(d), ptr(roi), int(roi.size), ptr(x_bar), ptr(h), ptr(J)))
@@ -429,6 +431,8 @@ def enumerate_qubo(h, J, T: float = 1.0, device: int = -1):
     h = np.ascontiguousarray(h, np.float64)
     J = np.ascontiguousarray(J, np.float64)
     n = int(h.size)
+    if J.size < n * n:
+        raise QBError(1, "enumerate_qubo: J must be n x n")
     p = np.empty(n, np.float64)
     res = EnumResult()
     o = _opts(device, None)

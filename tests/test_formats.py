@@ -142,6 +142,14 @@ def test_exports_refuse_arrays_shorter_than_their_bits(tmp_path):
         write_roi_text(tmp_path / "r.txt", [1, 2], [0.5, 0.5], [1.0, 2.0], np.zeros(3))
 
 
+def test_region_calls_refuse_short_arrays():
+    from qublar_b200 import enumerate_qubo, roi_qubo, synth
+    with pytest.raises(QBError, match="x_bar needs one value per bit"):
+        roi_qubo(synth.tiny6(), [0, 1], [0, 1])
+    with pytest.raises(QBError, match="J must be n x n"):
+        enumerate_qubo([0.0, 1.0, 2.0], np.zeros((2, 2)))
+
+
 def test_roi_text(tmp_path):
     n = 3
     voxel = np.array([7, 11, 30], np.int32)
