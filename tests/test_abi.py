@@ -250,6 +250,41 @@ def test_residual_colouring_is_valid():
     assert cptr.size - 1 >= np.bincount(a["ray"]).max()
 
 
+@pytest.mark.parametrize("make", [lambda: synth.tomography(synth.small_tomo_params()),
+                                  lambda: synth.tomography_of_size(60000, seed=5)])   # 1.3 M entries: threaded counts
+def test_residual_colouring_matches_the_first_fit_rule(make):
+    """The planner's residual colouring restated: bits by decreasing conflict
+    degree counted with multiplicity (the sum of their rays' lengths; ties by
+    index) take the lowest colour on none of their rays and on none of their
+    coloured prior neighbours. Checked per bit (the planner reorders bits
+    inside a class, which changes no result)."""
+    a = make()
+    rp, ray, npt, nbr = a["row_ptr"], a["ray"], a["nbr_ptr"], a["nbr"]
+    n = rp.size - 1
+    raylen = np.bincount(ray, minlength=a["d"].size)
+    conf = np.bincount(np.repeat(np.arange(n), np.diff(rp)), weights=raylen[ray], minlength=n).astype(np.int64)
+    used = [0] * a["d"].size          # bit c set: colour c is on the ray
+    want = [-1] * n
+    rays_of = [ray[rp[i]:rp[i + 1]].tolist() for i in range(n)]
+    nbrs_of = [nbr[npt[i]:npt[i + 1]].tolist() for i in range(n)]
+    for i in np.argsort(-conf, kind="stable").tolist():
+        forbid = 0
+        for r in rays_of[i]:
+            forbid |= used[r]
+        for j in nbrs_of[i]:
+            if want[j] >= 0:
+                forbid |= 1 << want[j]
+        c = (~forbid & (forbid + 1)).bit_length() - 1   # the lowest clear bit
+        want[i] = c
+        for r in rays_of[i]:
+            used[r] |= 1 << c
+    order, cptr = _colour("residual", synth.residual_desc(a), n)
+    got = np.empty(n, np.int64)
+    for c in range(cptr.size - 1):
+        got[order[cptr[c]:cptr[c + 1]]] = c
+    assert (got == np.array(want)).all()
+
+
 def test_benchmark_pyramid_sizes():
     a = synth.tomography()
     assert a["row_ptr"].size - 1 == 306328 and a["d"].size == 75594
