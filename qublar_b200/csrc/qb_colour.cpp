@@ -172,10 +172,25 @@ Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* ro
     std::vector<uint64_t> forbid;
     for (size_t v = 0; v < vis.size(); ++v) {
         const int i = vis[v];
-        if (v + 2 < vis.size()) {   // the rows of the bit after next into cache (they are random rays)
+        // a pipeline of prefetches, each stage on data the one before brought
+        // in: the offsets of the bit 12 visits ahead, the ray and neighbour
+        // lists of the bit 6 ahead, and the rows of the bit 2 ahead (random
+        // rays)
+        if (v + 12 < vis.size()) {
+            const int i12 = vis[v + 12];
+            __builtin_prefetch(row_ptr + i12);
+            __builtin_prefetch(nbr_ptr + i12);
+        }
+        if (v + 6 < vis.size()) {
+            const int i6 = vis[v + 6];
+            for (int k = row_ptr[i6]; k < row_ptr[i6 + 1]; k += 16) __builtin_prefetch(ray + k);
+            if (nbr_ptr[i6] < nbr_ptr[i6 + 1]) __builtin_prefetch(nbr + nbr_ptr[i6]);
+        }
+        if (v + 2 < vis.size()) {
             const int i2 = vis[v + 2];
             for (int k = row_ptr[i2]; k < row_ptr[i2 + 1]; ++k)
                 __builtin_prefetch(used + size_t(ray[k]) * size_t(words), 1);
+            for (int k = nbr_ptr[i2]; k < nbr_ptr[i2 + 1]; ++k) __builtin_prefetch(c.colour.data() + nbr[k]);
         }
         int cc = -1;
         if (words == kColourWords) {
