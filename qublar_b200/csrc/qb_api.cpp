@@ -526,18 +526,23 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     // sweep-order per-bit arrays (the entry table itself is assembled at upload)
     P.h_row.assign(size_t(n) + 1, 0);
     P.h_nbr_ptr.assign(size_t(n) + 1, 0);
-    for (int k = 0; k < n; ++k) {
+#pragma omp parallel for schedule(static, 4096)
+    for (int k = 0; k < n; ++k) {   // the degrees gathered in sweep order, then summed
         const int i = C.order[size_t(k)];
-        P.h_row[size_t(k) + 1] = P.h_row[size_t(k)] + (d->row_ptr[i + 1] - d->row_ptr[i]);
-        P.h_nbr_ptr[size_t(k) + 1] = P.h_nbr_ptr[size_t(k)] + (d->nbr_ptr[i + 1] - d->nbr_ptr[i]);
+        P.h_row[size_t(k) + 1] = d->row_ptr[i + 1] - d->row_ptr[i];
+        P.h_nbr_ptr[size_t(k) + 1] = d->nbr_ptr[i + 1] - d->nbr_ptr[i];
+    }
+    for (int k = 0; k < n; ++k) {
+        P.h_row[size_t(k) + 1] += P.h_row[size_t(k)];
+        P.h_nbr_ptr[size_t(k) + 1] += P.h_nbr_ptr[size_t(k)];
     }
     P.h_lin.resize(size_t(n));
     P.h_q.resize(size_t(n));
     P.h_nbr_home.resize(size_t(P.n_nbr));
     P.h_nbr_new.resize(size_t(P.n_nbr));
 #pragma omp parallel for schedule(static, 1024)
-    for (int k = 0; k < n; ++k) {
-        const int i = C.order[size_t(k)];
+    for (int i = 0; i < n; ++i) {   // in the caller's bit order: the entries stream
+        const int k = C.inverse[size_t(i)];
         double qd = 0.0;
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
             const float a = d->a[e];
