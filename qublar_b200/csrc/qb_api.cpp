@@ -232,8 +232,8 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
     P.wgt.resize(size_t(2 * m));
     P.f0.assign(size_t(n), 0);
 #pragma omp parallel for schedule(dynamic, 4096) if (m >= (int64_t(1) << 16))
-    for (int k = 0; k < n; ++k) {
-        const int i = C.order[size_t(k)];
+    for (int i = 0; i < n; ++i) {   // in the caller's bit order: the adjacency streams
+        const int k = C.inverse[size_t(i)];
         int32_t pos = P.row[size_t(k)];
         int64_t acc = 0;
         for (int64_t e = row[size_t(i)]; e < row[size_t(i) + 1]; ++e) {
@@ -319,8 +319,8 @@ qb_status plan_qubo(const qb_qubo_desc* g, QuboPlan& P) {
     P.J.resize(size_t(2 * m));
     P.h.assign(size_t(n), 0.0f);
 #pragma omp parallel for schedule(dynamic, 4096) if (m >= (int64_t(1) << 16))
-    for (int k = 0; k < n; ++k) {
-        const int i = C.order[size_t(k)];
+    for (int i = 0; i < n; ++i) {   // in the caller's bit order: the adjacency streams
+        const int k = C.inverse[size_t(i)];
         int32_t pos = P.row[size_t(k)];
         for (int64_t e = row[size_t(i)]; e < row[size_t(i) + 1]; ++e) {
             P.adj[size_t(pos)] = C.inverse[size_t(col[size_t(e)])];

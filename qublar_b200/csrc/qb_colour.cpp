@@ -58,7 +58,21 @@ Colouring colour_graph(int n, const std::vector<int64_t>& row, const std::vector
     // colour exceeds the largest degree. mark[colour + 1] == i: a neighbour of
     // i holds that colour; slot 0 collects the uncoloured neighbours.
     std::vector<int32_t> mark(size_t(maxdeg) + 2, -1);
-    for (int i : vis) {
+    for (size_t v = 0; v < vis.size(); ++v) {
+        const int i = vis[v];
+        // prefetches in stages, as in the residual first fit: the offsets of
+        // the bit 12 visits ahead, its neighbour list 6 ahead, the neighbours'
+        // colours 2 ahead
+        if (v + 12 < vis.size()) __builtin_prefetch(row.data() + vis[v + 12]);
+        if (v + 6 < vis.size()) {
+            const int i6 = vis[v + 6];
+            for (int64_t k = row[size_t(i6)]; k < row[size_t(i6) + 1]; k += 16) __builtin_prefetch(col.data() + k);
+        }
+        if (v + 2 < vis.size()) {
+            const int i2 = vis[v + 2];
+            for (int64_t k = row[size_t(i2)]; k < row[size_t(i2) + 1]; ++k)
+                __builtin_prefetch(c.colour.data() + col[size_t(k)]);
+        }
         for (int64_t k = row[size_t(i)]; k < row[size_t(i) + 1]; ++k)
             mark[size_t(c.colour[size_t(col[size_t(k)])] + 1)] = i;
         int cc = 0;
