@@ -103,13 +103,71 @@ private:
 
 // Symmetric CSR of an edge list in edge order: edge (a, b) appends b to row a
 // and a to row b, as parse_rudy builds its adjacency (ising_weighted.hpp:135-147).
-// Each thread owns a contiguous range of rows and scans the whole edge list,
-// so the order inside a row is the sequential one. Indices must be in range.
+// With threads, each takes a contiguous slice of the edges: it counts its
+// slice's endpoints per vertex, the counts are turned into write positions
+// (a row holds slice 0's entries, then slice 1's, ...), and it writes its
+// slice in edge order, so every row is in edge order. When threads x vertices
+// counters would not fit in 2^26 words, each thread instead owns a range of
+// rows and scans the whole edge list. Indices must be in range; 2m < 2^31.
 template <class W>
 void sym_csr(int n, int64_t m, const int32_t* eu, const int32_t* ev, const W* ew, std::vector<int64_t>& row,
              std::vector<int32_t>& col, std::vector<W>& w) {
     const int T = m >= (int64_t(1) << 16) ? std::max(1, omp_get_max_threads()) : 1;
     row.assign(size_t(n) + 1, 0);
+    col.resize(size_t(2 * m));
+    w.resize(size_t(2 * m));
+    if (T > 1 && int64_t(T) * n <= (int64_t(1) << 26)) {
+        RawVec<int32_t> at(size_t(T) * size_t(n));   // [slice][vertex]: counts, then write positions
+#pragma omp parallel num_threads(T)
+        {
+            const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+            int32_t* cnt = at.data() + size_t(t) * size_t(n);
+            std::fill(cnt, cnt + n, 0);
+            const int64_t e0 = m * t / nt, e1 = m * (t + 1) / nt;
+            for (int64_t e = e0; e < e1; ++e) {
+                cnt[eu[e]]++;
+                cnt[ev[e]]++;
+            }
+#pragma omp barrier
+            // degrees, then write positions, in blocks of vertices so each
+            // slice's counters are read in order
+            constexpr int kBlock = 2048;
+#pragma omp for schedule(static)
+            for (int vb = 0; vb < n; vb += kBlock) {
+                const int ve = std::min(n, vb + kBlock);
+                for (int q = 0; q < nt; ++q) {
+                    const int32_t* cq = at.data() + size_t(q) * size_t(n);
+                    for (int v = vb; v < ve; ++v) row[size_t(v) + 1] += cq[v];
+                }
+            }
+#pragma omp single
+            for (int v = 0; v < n; ++v) row[size_t(v) + 1] += row[size_t(v)];
+#pragma omp for schedule(static)
+            for (int vb = 0; vb < n; vb += kBlock) {
+                const int ve = std::min(n, vb + kBlock);
+                int32_t pos[kBlock];
+                for (int v = vb; v < ve; ++v) pos[v - vb] = int32_t(row[size_t(v)]);
+                for (int q = 0; q < nt; ++q) {
+                    int32_t* cq = at.data() + size_t(q) * size_t(n);
+                    for (int v = vb; v < ve; ++v) {
+                        const int32_t k = cq[v];
+                        cq[v] = pos[v - vb];
+                        pos[v - vb] += k;
+                    }
+                }
+            }
+            for (int64_t e = e0; e < e1; ++e) {
+                const int32_t a = eu[e], b = ev[e];
+                int32_t k = cnt[a]++;
+                col[size_t(k)] = b;
+                w[size_t(k)] = ew[e];
+                k = cnt[b]++;
+                col[size_t(k)] = a;
+                w[size_t(k)] = ew[e];
+            }
+        }
+        return;
+    }
 #pragma omp parallel num_threads(T)
     {
         const int t = omp_get_thread_num(), nt = omp_get_num_threads();
@@ -122,8 +180,6 @@ void sym_csr(int n, int64_t m, const int32_t* eu, const int32_t* ev, const W* ew
         }
     }
     for (int i = 0; i < n; ++i) row[size_t(i) + 1] += row[size_t(i)];
-    col.resize(size_t(2 * m));
-    w.resize(size_t(2 * m));
     std::vector<int64_t> fill(row.begin(), row.end() - 1);
 #pragma omp parallel num_threads(T)
     {
@@ -148,6 +204,17 @@ void sym_csr(int n, int64_t m, const int32_t* eu, const int32_t* ev, const W* ew
             }
         }
     }
+}
+
+// The first edge for which bad(e) holds, or m (a parallel scan for the lowest
+// index, so the reason reported is the one a sequential scan finds).
+template <class F>
+int64_t first_bad_edge(int64_t m, F bad) {
+    int64_t first = m;
+#pragma omp parallel for schedule(static) reduction(min : first) if (m >= (int64_t(1) << 16))
+    for (int64_t e = 0; e < m; ++e)
+        if (bad(e)) first = std::min(first, e);
+    return first;
 }
 
 // True when some row of a symmetric CSR lists a neighbour twice: an edge given
@@ -188,11 +255,12 @@ qb_status plan_ising(const qb_ising_desc* g, IsingPlan& P) {
     if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "ising: more than 2^30 edges");
     // loader refusals of parse_rudy (ising_weighted.hpp:113-133)
     PlanMarks mark;
-    for (int64_t e = 0; e < m; ++e) {
+    auto out_of_range = [&](int64_t e) {
         const int32_t u = g->eu[e], v = g->ev[e];
-        if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "ising: vertex index out of range");
-        if (u == v) return fail(QB_EINVAL, "ising: self-loop");
-    }
+        return u < 0 || u >= n || v < 0 || v >= n;
+    };
+    const int64_t bad = first_bad_edge(m, [&](int64_t e) { return out_of_range(e) || g->eu[e] == g->ev[e]; });
+    if (bad < m) return fail(QB_EINVAL, out_of_range(bad) ? "ising: vertex index out of range" : "ising: self-loop");
     // symmetric CSR in edge order, as parse_rudy builds it (ising_weighted.hpp:135-147)
     std::vector<int64_t> row;
     std::vector<int32_t> col, w;
@@ -290,11 +358,16 @@ qb_status plan_qubo(const qb_qubo_desc* g, QuboPlan& P) {
     if (2 * m >= (int64_t(1) << 31)) return fail(QB_EREFUSED, "qubo: more than 2^30 edges");
     if (!std::isfinite(g->offset)) return fail(QB_EINVAL, "qubo: offset must be finite");
     PlanMarks mark;
-    for (int64_t e = 0; e < m; ++e) {
+    auto out_of_range = [&](int64_t e) {
         const int32_t u = g->eu[e], v = g->ev[e];
-        if (u < 0 || u >= n || v < 0 || v >= n) return fail(QB_EINVAL, "qubo: vertex index out of range");
-        if (u == v) return fail(QB_EINVAL, "qubo: self-loop (put diagonal terms in h)");
-        if (!std::isfinite(g->ew[e])) return fail(QB_EINVAL, "qubo: coupling is not finite");
+        return u < 0 || u >= n || v < 0 || v >= n;
+    };
+    const int64_t bad = first_bad_edge(
+        m, [&](int64_t e) { return out_of_range(e) || g->eu[e] == g->ev[e] || !std::isfinite(g->ew[e]); });
+    if (bad < m) {
+        if (out_of_range(bad)) return fail(QB_EINVAL, "qubo: vertex index out of range");
+        if (g->eu[bad] == g->ev[bad]) return fail(QB_EINVAL, "qubo: self-loop (put diagonal terms in h)");
+        return fail(QB_EINVAL, "qubo: coupling is not finite");
     }
     // symmetric CSR, edge order per vertex
     std::vector<int64_t> row;

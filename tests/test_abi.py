@@ -217,6 +217,26 @@ def test_graph_colouring_matches_the_greedy_rule_on_a_threaded_plan():
     assert (order == want_order).all()
 
 
+def test_large_edge_list_reports_the_first_failing_edge():
+    # the edges are checked in parallel; the reason is the lowest failing edge's
+    n = 20000
+    eu, ev = _random_edges(n, 80000, 13)
+    for first, second, why in [(60000, 70000, "out of range"), (70000, 60000, "self-loop")]:
+        bu, bv = eu.copy(), ev.copy()
+        bu[first] = n            # an index out of range
+        bv[second] = bu[second]  # a self-loop
+        st, msg = _ising_status(n, bu, bv, np.ones(bu.size, np.int32))
+        assert st == 1 and why in msg, msg
+        st, msg = _qubo_status(n, bu, bv, np.ones(bu.size, np.float32))
+        assert st == 1 and why in msg, msg
+    bw = np.ones(eu.size, np.float32)
+    bw[65000] = np.nan
+    bu = eu.copy()
+    bu[75000] = -1
+    st, msg = _qubo_status(n, bu, ev, bw)
+    assert st == 1 and "not finite" in msg, msg
+
+
 def test_duplicate_edge_refused_on_a_large_edge_list():
     n = 20000
     eu, ev = _random_edges(n, 80000, 11)
