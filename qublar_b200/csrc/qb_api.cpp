@@ -655,8 +655,13 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     auto segs = [&](int k) { return (row[size_t(k) + 1] - row[size_t(k)] + kSeg - 1) / kSeg; };
     P.chunks.clear();
     P.chunk_ptr.assign(size_t(S) + 1, 0);
+    // each slice's chunks on its own thread, joined in slice order
+    std::vector<std::vector<int32_t>> per(static_cast<size_t>(S));
+    int too_big = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : too_big)
     for (int t = 0; t < S; ++t) {
-        for (int c = 0; c < nc; ++c) {
+        std::vector<int32_t>& out = per[size_t(t)];
+        for (int c = 0; c < nc && !too_big; ++c) {
             const int b0 = slice_ptr[size_t(c) * (S + 1) + size_t(t)], b1 = slice_ptr[size_t(c) * (S + 1) + size_t(t) + 1];
             const int slot0 = P.slot_base[size_t(c) * S + size_t(t)];
             int s0 = b0;
@@ -668,15 +673,22 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
                     nseg += lock ? segs(e) : 0;
                     ++e;
                 }
-                if (e == s0 && s0 < b1) return fail(QB_ENOTSUP, "residual: a bit has more rays or neighbours than a chunk holds");
+                if (e == s0 && s0 < b1) {
+                    too_big = 1;
+                    break;
+                }
                 int nh = 0;
                 while (s0 + nh < e && row[size_t(s0 + nh) + 1] - row[size_t(s0 + nh)] > heavy) ++nh;
                 const int32_t rec[8] = {s0, e, lock ? nseg : slot0 + (s0 - b0), (e == b1 ? 1 : 0) | (nh << 1),
                                         row[size_t(s0)], row[size_t(e)], nbp[size_t(s0)], nbp[size_t(e)]};
-                P.chunks.insert(P.chunks.end(), rec, rec + 8);
+                out.insert(out.end(), rec, rec + 8);
                 s0 = e;
             } while (s0 < b1);
         }
+    }
+    if (too_big) return fail(QB_ENOTSUP, "residual: a bit has more rays or neighbours than a chunk holds");
+    for (int t = 0; t < S; ++t) {
+        P.chunks.insert(P.chunks.end(), per[size_t(t)].begin(), per[size_t(t)].end());
         P.chunk_ptr[size_t(t) + 1] = int32_t(P.chunks.size() / 8);
     }
     mark("chunks");
