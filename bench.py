@@ -154,32 +154,58 @@ def cpu_baseline(a, sched, threads, branches):
     return attempts / wall, wall, kind
 
 
+class _Sched:
+    """A schedule's four numbers (the reference arm imports nothing of the solver)."""
+
+    def __init__(self, t_hot, t_cold, anneal_sweeps, hold_sweeps, refresh_sweeps=50):
+        self.t_hot, self.t_cold = t_hot, t_cold
+        self.anneal_sweeps, self.hold_sweeps, self.refresh_sweeps = anneal_sweeps, hold_sweeps, refresh_sweeps
+
+    @property
+    def sweeps(self):
+        return self.anneal_sweeps + self.hold_sweeps
+
+
+POSTERIOR = _Sched(50.0, 1.0, 200, 50, 50)   # ising_recon.hpp:81-86
+
+
+def workload_config(a, sweeps, gpus):
+    """The workload's identity, the same in both arms' lines."""
+    return {"workload": WORKLOAD, "bits": int(a["row_ptr"].size - 1), "rays": int(a["d"].size),
+            "entries": int(a["ray"].size), "branches": BRANCHES, "sweeps": sweeps,
+            "schedule": "T 50 -> 1 geometric over 200 sweeps, then 50 sweeps at T = 1",
+            "parallelism": f"{gpus} independent replica{'' if gpus == 1 else 's'} (one per GPU)",
+            "l2": "GPU arm: flushed (256 MB write) before every timed step"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from qublar_b200 import Schedule, synth
-    a = synth.tomography()
+    from oracle import oracle as O
+    a = O.tomography()   # the pyramid from oracle/libqb_inputs.so: the solver library is not loaded
     threads = os.cpu_count() or 1
-    # each step: the full 306,328-bit problem, min(16, cores) branches of a
-    # 25-sweep sample of the schedule (T 50 -> 1 over 20 sweeps, 5 held)
+    # each step: the reference's branch_fractions on the full 306,328-bit
+    # problem with the full posterior schedule; min(16, cores) branches
     branches = min(BRANCHES, threads)
-    sample = Schedule(50.0, 1.0, 20, 5, 0)
-    rates = []
+    rates, walls = [], []
+    kind = None
     for k in range(args.warmup + args.steps):
-        rate, wall, kind = cpu_baseline(a, sample, threads, branches)
+        rate, wall, kind = cpu_baseline(a, POSTERIOR, threads, branches)
         if k >= args.warmup:
             rates.append(rate)
+            walls.append(wall)
     value = statistics.mean(rates)
     n = int(a["row_ptr"].size - 1)
-    ms = branches * sample.sweeps * n / value * 1e3
+    ms = BRANCHES * POSTERIOR.sweeps * n / value * 1e3
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bits": n, "rays": int(a["d"].size), "entries": int(a["ray"].size)},
+            "config": workload_config(a, POSTERIOR.sweeps, args.gpus),
             "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": threads, "kind": kind,
-                             "sample": f"{branches} branches x 25-sweep sample of the schedule per step, "
-                                       f"full 306,328-bit problem, {threads} threads"},
+                             "sample": f"{branches} of the 16 branches per step (branch_fractions), the full "
+                                       f"250-sweep schedule on the full problem, {threads} threads, "
+                                       f"{statistics.mean(walls):.1f} s per step"},
             "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -771,7 +797,7 @@ def main():
     stream = torch.cuda.current_stream()
     a = synth.tomography()
     n = int(a["row_ptr"].size - 1)
-    sched = Schedule()   # 50 -> 1, 200 + 50, refresh 50
+    sched = Schedule()   # 50 -> 1, 200 + 50, refresh 50 (POSTERIOR)
     if args.sweeps != 250:
         hold = args.sweeps // 5
         sched = Schedule(50.0, 1.0, args.sweeps - hold, hold, 50)
@@ -780,9 +806,10 @@ def main():
     attempts_step = BRANCHES * sched.sweeps * n
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    for _ in range(args.warmup):
-        r = P.solve(sched, BRANCHES, stream=stream)
-        r.info()
+    energy_err = None   # the last warm-up solve is traced: E(0) + accepted fp32 dE against the fp64 energy
+    for k in range(args.warmup):
+        r = P.solve(sched, BRANCHES, stream=stream, trace=k == args.warmup - 1)
+        energy_err = r.info().max_energy_error
         r.close()
 
     sampler = ClockSampler(local) if rank == 0 else None
@@ -854,11 +881,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "attempts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "bits": n, "rays": int(a["d"].size), "entries": int(a["ray"].size),
-                   "branches": BRANCHES, "sweeps": sched.sweeps, "colours": int(pinfo.n_colours),
-                   "l2": "flushed (256 MB write) before every timed step; problem footprint "
-                         f"{pinfo.device_bytes / 2**20:.0f} MiB", "parallelism": f"{world} independent replica{'' if world == 1 else 's'} (one per GPU)"},
+        "vs_baseline": None, "dtype": "f32 dE; residuals compensated f32 (hi + lo), f64 refresh every 50 sweeps",
+        "data": "synthetic",
+        "config": workload_config(a, sched.sweeps, world),
+        "plan": {"colours": int(pinfo.n_colours), "footprint_mib": round(pinfo.device_bytes / 2**20)},
         "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                 "s_per_step": e2e_mean, "warmup_steps": e2e_warm},
         "gpu_launches": launches,
@@ -866,6 +892,7 @@ def main():
                      "peak_kind": peak_kind, "traffic": traffic, "kernel": "resid_lockstep_kernel",
                      "kernel_ms": anneal_ms, "algorithmic_bytes": alg, "accepted_flips": accepted},
         "max_residual_drift": drift,
+        "max_energy_error": energy_err,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -168,6 +168,9 @@ typedef struct qb_opts {
  *                        sweep. */
 #define QB_OPT_DEFER_UPLOAD 1u
 #define QB_OPT_RESID_CLUSTER 2u
+/* qb_opts.flags of qb_solve: QB_OPT_TRACE records every branch's energy after
+ * every sweep (qb_result_energy_trace). */
+#define QB_OPT_TRACE 4u
 
 /* Upload an integer graph and plan it (colouring, field width).
  * Replaces gising::make_plan + DeviceGraph (src/ising_gpu.cuh:74-101, :278-336). */
@@ -260,6 +263,15 @@ qb_status qb_result_fields_i64(qb_result* r, int64_t* f);
 qb_status qb_result_energies_f64(qb_result* r, double* e);
 /* Per-bit fraction of branches with x = 1 (branch_fractions, ising_recon.hpp:160-163). */
 qb_status qb_result_marginals(qb_result* r, float* p);
+/* The energy of every branch after every sweep, n_branches x sweeps, for a
+ * solve made with QB_OPT_TRACE: the per-sweep energy the reference's
+ * instrumented annealers record (check_ree_qubo.cu:195-216 anneal_trace; the
+ * tracked State::energy of ising_weighted.hpp:209-217). Ising: the exact
+ * tracked integer energy. Residual: the fp64 energy of x = 0 plus the
+ * accepted fp32 dE summed in fp64 (the sum's order across CTAs is not fixed,
+ * so the last bits may vary from run to run). QUBO: offset plus the accepted
+ * dE summed in fp64 in a fixed order. */
+qb_status qb_result_energy_trace(qb_result* r, double* trace);
 /* Tri-state per bit: 1 = NotThere (p >= hi), 0 = Exists (p <= lo), 2 = Undecided
  * (argos::classify, ising_recon.hpp:302-309; defaults lo = 0.1, hi = 0.9). */
 qb_status qb_result_tristate(qb_result* r, float lo, float hi, uint8_t* bits);
@@ -267,9 +279,9 @@ void qb_result_destroy(qb_result* r);
 
 /* Size of the static device scratch of qb_solve_residual_noalloc: held by
  * every GPU that loads the library, from its first use until the process
- * exits (8 MiB: the 306,328-bit, 75,594-ray pyramid at 16 branches needs
- * about 6.1 MB). */
-#define QB_NOALLOC_SCRATCH_BYTES (8u << 20)
+ * exits (16 MiB: the 306,328-bit, 75,594-ray pyramid at 16 branches needs
+ * about 11 MB). */
+#define QB_NOALLOC_SCRATCH_BYTES (16u << 20)
 
 /* A residual solve that allocates nothing, for callers that must not call
  * cudaMalloc/cudaFree while they run: a host that owns all device memory
@@ -279,16 +291,19 @@ void qb_result_destroy(qb_result* r);
  * sweep of qb_solve for one block of at most 64 branches and writes the
  * branches (n_branches x n bytes, 0/1, input bit order) into x_out, a device
  * buffer the caller owns; the branches equal qb_solve's for the same
- * arguments. Its per-solve scratch lives in one static device array of
- * QB_NOALLOC_SCRATCH_BYTES; problems that need more return QB_ENOMEM with the
- * size. The first call on a device looks up that array's device address;
- * make it before any stream capture. Calls share the array: calls whose work
- * overlaps on the GPU race, so serialise them. The problem must come from
- * qb_problem_create_residual with the lockstep plan (qb_problem_info.variant
- * == QB_RESID_LOCKSTEP). Returns once the work is queued on `stream`
- * (cudaStream_t, NULL = legacy default stream). */
+ * arguments. status is a device int32 the caller owns: the call sets it to
+ * QB_OK on `stream`, and the sweep sets it to QB_ETIMEDOUT when one of its
+ * bounded grid barriers gives up, in which case x_out is not written; read it
+ * after the stream's work is done. Its per-solve scratch lives in one static
+ * device array of QB_NOALLOC_SCRATCH_BYTES; problems that need more return
+ * QB_ENOMEM with the size. The first call on a device looks up that array's
+ * device address; make it before any stream capture. Calls share the array:
+ * calls whose work overlaps on the GPU race, so serialise them. The problem
+ * must come from qb_problem_create_residual with the lockstep plan
+ * (qb_problem_info.variant == QB_RESID_LOCKSTEP). Returns once the work is
+ * queued on `stream` (cudaStream_t, NULL = legacy default stream). */
 qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
-                                    uint64_t seed_offset, uint8_t* x_out, void* stream);
+                                    uint64_t seed_offset, uint8_t* x_out, int32_t* status, void* stream);
 
 /* ---- batches: many ising instances in one persistent launch ----------------
  *

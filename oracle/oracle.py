@@ -5,7 +5,11 @@
   from its sources (absent when the reference was never built here);
 * ``ref_gpu`` -- oracle/_ref/libqbref_gpu.so, the reference's GPU annealer
   (ising_gpu.cuh) compiled from its sources for sm_100a: the existing-kernel
-  comparator, for GPU tests only.
+  comparator, for GPU tests only;
+* ``tomography`` -- oracle/libqb_inputs.so, the synthetic pyramid builder
+  compiled on its own (host code only), so the CPU legs build their inputs
+  without loading the solver library; its arrays equal
+  ``qublar_b200.synth.tomography``'s byte for byte (tests/test_oracle_golden.py).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module, and only to check or time the CPU side; the solver never does.
@@ -21,6 +25,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(_HERE, "libqb_oracle.so")
 REF_PATH = os.path.join(_HERE, "_ref", "libqbref.so")
 REF_GPU_PATH = os.path.join(_HERE, "_ref", "libqbref_gpu.so")
+INPUTS_PATH = os.path.join(_HERE, "libqb_inputs.so")
 
 
 class ResidDesc(C.Structure):
@@ -65,7 +70,7 @@ def orc() -> C.CDLL:
             "orc_binary_energy_batch": (None, [C.POINTER(ResidDesc), P, I64, P]),
             "orc_local_field_dE": (D, [C.POINTER(ResidDesc), P, P, C.c_int]),
             "orc_anneal_branch": (None, [C.POINTER(ResidDesc), D, D, C.c_int, C.c_int, U64, P, P]),
-            "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, C.c_int, P, P, P]),
+            "orc_resid_anneal_coloured": (None, [C.POINTER(ResidDesc), P, P, C.c_int, C.c_int, U64, C.c_int, P, P, P, P]),
             "orc_classify": (None, [P, I64, C.c_float, C.c_float, P]),
             "orc_fractions": (None, [P, C.c_int, I64, P]),
             "orc_qubo_energy": (D, [C.c_int, I64, P, P, P, P, D, P]),
@@ -247,8 +252,10 @@ def anneal_branch(arr: dict, t_hot, t_cold, anneal, hold, seed, trace=False):
     return (x, tr) if trace else x
 
 
-def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False, mode=1):
-    """mode: the summation order of the kernel variant (1 lockstep, 2 cluster)."""
+def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False, mode=1, track=False):
+    """mode: the summation order of the kernel variant (1 lockstep, 2 cluster).
+    Returns (x, drift) plus the per-sweep binary_energy trace when `trace` and
+    the per-sweep tracked energy (E(0) + accepted dE) when `track`."""
     d = resid_desc(arr)
     n = int(arr["row_ptr"].size - 1)
     order = np.ascontiguousarray(order, np.int32)
@@ -256,9 +263,15 @@ def resid_anneal_coloured(arr: dict, order, temps, refresh, seed, trace=False, m
     x = np.empty(n, np.uint8)
     drift = C.c_float(0.0)
     tr = np.empty(temps.size, np.float64) if trace else None
+    tk = np.empty(temps.size, np.float64) if track else None
     orc().orc_resid_anneal_coloured(C.byref(d), _p(order), _p(temps), int(temps.size), int(refresh), seed, int(mode),
-                                    _p(x), C.byref(drift), _p(tr))
-    return (x, float(drift.value), tr) if trace else (x, float(drift.value))
+                                    _p(x), C.byref(drift), _p(tr), _p(tk))
+    out = (x, float(drift.value))
+    if trace:
+        out = out + (tr,)
+    if track:
+        out = out + (tk,)
+    return out
 
 
 def qubo_energy(q: dict, x) -> float:
@@ -433,3 +446,63 @@ class RefProblem:
         J = np.empty(roi.size * roi.size, np.float64)
         ref().ref_roi_qubo(self.h, _p(roi), int(roi.size), _p(x_bar), _p(h), _p(J))
         return h, J.reshape(roi.size, roi.size)
+
+
+# ---- synthetic inputs without the solver library ------------------------------------------------
+
+class TomoParams(C.Structure):
+    """The layout of qb_tomo_params (include/qublar_synth.h)."""
+    _fields_ = [("target_bits", C.c_int32), ("target_rays", C.c_int32), ("voxel", C.c_double),
+                ("half_base", C.c_double), ("height", C.c_double), ("n_detectors", C.c_int32),
+                ("det", C.c_double * 12), ("n_theta", C.c_int32), ("n_phi", C.c_int32),
+                ("theta_min", C.c_double), ("theta_max", C.c_double), ("phi_half", C.c_double),
+                ("sub_rays", C.c_int32), ("room_radius", C.c_double), ("mu_rock", C.c_double),
+                ("void_center", C.c_double * 3), ("void_side", C.c_double), ("exposure", C.c_double),
+                ("min_open", C.c_double), ("lambda_", C.c_double), ("kappa", C.c_double), ("seed", C.c_uint64)]
+
+
+_inputs = None
+
+
+def inputs() -> C.CDLL:
+    global _inputs
+    if _inputs is None:
+        L = C.CDLL(INPUTS_PATH)
+        P = C.c_void_p
+        sig = {"qb_tomo_params_default": (None, [P]), "qb_synth_tomography": (C.c_int, [P, P]),
+               "qb_tomo_sizes": (C.c_int, [P, P, P, P, P]), "qb_tomo_arrays": (C.c_int, [P] + [P] * 8),
+               "qb_tomo_destroy": (None, [P]), "qb_last_error": (C.c_char_p, [])}
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _inputs = L
+    return _inputs
+
+
+def tomography(params=None) -> dict:
+    """The pyramid QUBO's residual-form arrays from oracle/libqb_inputs.so:
+    the default benchmark pyramid, or `params` (a qb_tomo_params structure of
+    either binding's class)."""
+    L = inputs()
+    p = params
+    if p is None:
+        p = TomoParams()
+        L.qb_tomo_params_default(C.addressof(p))
+    h = C.c_void_p()
+    if L.qb_synth_tomography(C.addressof(p), C.byref(h)) != 0:
+        raise RuntimeError(L.qb_last_error().decode())
+    try:
+        n, nr, nnz, nn = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+        L.qb_tomo_sizes(h, C.byref(n), C.byref(nr), C.byref(nnz), C.byref(nn))
+        out = {"d": np.empty(nr.value, np.float64), "w": np.empty(nr.value, np.float64),
+               "row_ptr": np.empty(n.value + 1, np.int32), "ray": np.empty(nnz.value, np.int32),
+               "a": np.empty(nnz.value, np.float32), "nbr_ptr": np.empty(n.value + 1, np.int32),
+               "nbr": np.empty(nn.value, np.int32)}
+        L.qb_tomo_arrays(h, _p(out["d"]), _p(out["w"]), _p(out["row_ptr"]), _p(out["ray"]), _p(out["a"]),
+                         _p(out["nbr_ptr"]), _p(out["nbr"]), None)
+        out["lambda"] = float(p.lambda_)
+        out["kappa"] = float(p.kappa)
+        out["field"] = None
+        return out
+    finally:
+        L.qb_tomo_destroy(h)

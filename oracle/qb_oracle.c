@@ -312,40 +312,70 @@ void orc_anneal_branch(const orc_resid* p, double t_hot, double t_cold, int anne
     free(r);
 }
 
+/* hi + lo += v with the fp32 rounding error carried in lo (TwoSum), the
+ * compensated update of the GPU sweeps (qb_device.cuh two_sum_add). */
+static void orc_two_sum(float* hi, float* lo, float v) {
+    const float s = *hi + v;
+    const float bp = s - *hi;
+    const float e = (*hi - (s - bp)) + (v - bp);
+    *hi = s;
+    *lo = *lo + e;
+}
+
+/* The fp32 pair nearest an fp64 value: hi = fp32(v), lo = fp32(v - hi). */
+static void orc_split(double v, float* hi, float* lo) {
+    *hi = (float)v;
+    *lo = (float)(v - (double)*hi);
+}
+
 /* The coloured-Philox residual annealer, in the fp32 operation order of the
- * sm_100a cluster kernel:
- *   rw_b = float(w_b * (sum a x - d_b)) (weighted residual), q_i = float(sum
- *   0.5 w a a), lin_i = float(lin); h = sum of a * rw over the bit's rays in
- *   the kernel's order: mode 1 (lockstep) 16-entry segments added in order,
- *   each the fmaf chain over its even entries plus the chain over its odd
- *   ones; mode 2 (cluster) G = ORC_GROUP or 32 strided fmaf chains joined by
- *   an xor butterfly; dE = ((delta * (lin + h)) + q) + lambda * (deg - 2
- *   unlike); accept as wising::anneal; scatter rw += (float(w) * a) * delta;
- *   fp64 refresh of rw every `refresh` sweeps (a sequential double sum over
- *   the ray's set bits in ascending index). drift_out: max |fp32 - fp64|. */
+ * sm_100a kernels. State per ray: the scaled residual rho_b = s_b (sum a x -
+ * d_b), s_b = sqrt|w_b|, as an fp32 pair hi + lo; entry coefficient a' =
+ * fp32(s_b a) (fp64 product rounded once) and sign(w_b); q_i = fp32(sum
+ * sign(w) a'^2 / 2) summed in fp64 in entry order, lin_i = fp32(lin). h = sum
+ * of sign(w) a' * fp32(hi + lo) over the bit's rays in the kernel's order:
+ * mode 1 (lockstep) 16-entry segments added in order, each the fmaf chain over
+ * its even entries plus the chain over its odd ones; mode 2 (cluster) G =
+ * ORC_GROUP or 32 strided fmaf chains joined by an xor butterfly. dE =
+ * ((delta * (lin + h)) + q) + lambda * (deg - 2 unlike); accept as
+ * wising::anneal; a flip adds delta a' into each of its rays' pairs (TwoSum).
+ * Every `refresh` sweeps rho is recomputed in fp64 (the ray's set bits in
+ * ascending index, sum of fp64(a') minus s d) and split into the pair;
+ * drift_out: max |fp64(hi) + fp64(lo) - rho|. trace (nullable): binary_energy
+ * after each sweep; track (nullable): the energy of x = 0 plus the accepted dE
+ * (fp64, visiting order) after each sweep. */
 void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const double* temps, int sweeps, int refresh,
-                               uint64_t seed, int mode, uint8_t* x, float* drift_out, double* trace) {
+                               uint64_t seed, int mode, uint8_t* x, float* drift_out, double* trace, double* track) {
     const int n = p->n_vars, nr = p->n_rays;
     const int64_t nnz = p->row_ptr[n];
-    float* rw = (float*)malloc(sizeof(float) * (size_t)(nr > 0 ? nr : 1));
-    float* wf = (float*)malloc(sizeof(float) * (size_t)(nr > 0 ? nr : 1));
+    float* hi = (float*)malloc(sizeof(float) * (size_t)(nr > 0 ? nr : 1));
+    float* lo = (float*)malloc(sizeof(float) * (size_t)(nr > 0 ? nr : 1));
+    double* sw = (double*)malloc(sizeof(double) * (size_t)(nr > 0 ? nr : 1));
+    float* ap = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));   /* a' per bit-major entry */
+    float* cf = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));   /* sign(w) a' */
     float* linf = (float*)malloc(sizeof(float) * (size_t)n);
     float* qf = (float*)malloc(sizeof(float) * (size_t)n);
+    double e0 = 0.0;
     for (int b = 0; b < nr; ++b) {
-        rw[b] = (float)(p->w[b] * (-p->d[b]));
-        wf[b] = (float)p->w[b];
+        sw[b] = sqrt(fabs(p->w[b]));
+        orc_split(-(sw[b] * p->d[b]), &hi[b], &lo[b]);
+        e0 += 0.5 * p->w[b] * p->d[b] * p->d[b];
     }
     for (int i = 0; i < n; ++i) {
         double qd = 0.0;
-        for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k)
-            qd += 0.5 * p->w[p->ray[k]] * (double)p->a[k] * (double)p->a[k];
+        for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k) {
+            const double w = p->w[p->ray[k]];
+            ap[k] = (float)(sw[p->ray[k]] * (double)p->a[k]);
+            cf[k] = w < 0.0 ? -ap[k] : ap[k];
+            qd += (w < 0.0 ? -0.5 : 0.5) * (double)ap[k] * (double)ap[k];
+        }
         qf[i] = (float)qd;
         linf[i] = (float)lin_of(p, i);
     }
     /* ray-major CSR, bits ascending */
     int32_t* rrow = (int32_t*)calloc((size_t)nr + 1, sizeof(int32_t));
     int32_t* rbit = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1));
-    float* ra = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
+    float* rap = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
     for (int64_t k = 0; k < nnz; ++k) rrow[p->ray[k] + 1]++;
     for (int b = 0; b < nr; ++b) rrow[b + 1] += rrow[b];
     int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nr > 0 ? nr : 1));
@@ -354,29 +384,28 @@ void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const d
         for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k) {
             const int32_t q = fill[p->ray[k]]++;
             rbit[q] = i;
-            ra[q] = p->a[k];
+            rap[q] = ap[k];
         }
     free(fill);
     memset(x, 0, (size_t)n);
     const float lam = (float)p->lambda;
     float drift = 0.0f;
+    double E = e0;
     for (int sweep = 0; sweep < sweeps; ++sweep) {
         if (refresh > 0 && sweep > 0 && sweep % refresh == 0) {
             for (int b = 0; b < nr; ++b) {
                 double acc = 0.0;
                 for (int k = rrow[b]; k < rrow[b + 1]; ++k)
-                    if (x[rbit[k]]) acc += (double)ra[k];
-                const float nv = (float)(p->w[b] * (acc - p->d[b]));
-                const float dv = fabsf(nv - rw[b]);
+                    if (x[rbit[k]]) acc += (double)rap[k];
+                const double v = acc - sw[b] * p->d[b];
+                const float dv = (float)fabs(((double)hi[b] + (double)lo[b]) - v);
                 if (dv > drift) drift = dv;
-                rw[b] = nv;
+                orc_split(v, &hi[b], &lo[b]);
             }
         }
         const double T = temps[sweep];
         for (int kk = 0; kk < n; ++kk) {
             const int i = order[kk];
-            /* ORC_GROUP lanes: lane l sums entries l, l + G, ... as an fmaf
-             * chain; an xor butterfly (G/2, ..., 1) joins them; lane 0 wins */
             float hl = 0.0f;
             if (mode == 1) {
                 /* lockstep kernel: 16-entry segments in order; a segment's
@@ -385,17 +414,19 @@ void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const d
                 for (int s0 = r0; s0 < r1; s0 += ORC_SEG) {
                     const int s1 = s0 + ORC_SEG < r1 ? s0 + ORC_SEG : r1;
                     float ev = 0.0f, od = 0.0f;
-                    for (int k = s0; k < s1; k += 2) ev = fmaf(p->a[k], rw[p->ray[k]], ev);
-                    for (int k = s0 + 1; k < s1; k += 2) od = fmaf(p->a[k], rw[p->ray[k]], od);
+                    for (int k = s0; k < s1; k += 2) ev = fmaf(cf[k], hi[p->ray[k]] + lo[p->ray[k]], ev);
+                    for (int k = s0 + 1; k < s1; k += 2) od = fmaf(cf[k], hi[p->ray[k]] + lo[p->ray[k]], od);
                     hl = hl + (ev + od);
                 }
             }
+            /* cluster kernel: G lanes, lane l sums entries l, l + G, ... as an
+             * fmaf chain; an xor butterfly (G/2, ..., 1) joins them; lane 0 wins */
             const int G = mode == 1 ? 1 : (p->row_ptr[i + 1] - p->row_ptr[i] > ORC_HEAVY ? 32 : ORC_GROUP);
             float lane[32];
             for (int l = 0; l < G; ++l) lane[l] = 0.0f;
             for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k) {
                 const int l = (k - p->row_ptr[i]) % G;
-                lane[l] = fmaf(p->a[k], rw[p->ray[k]], lane[l]);
+                lane[l] = fmaf(cf[k], hi[p->ray[k]] + lo[p->ray[k]], lane[l]);
             }
             for (int off = G / 2; off > 0; off >>= 1) {
                 float nx[32];
@@ -414,17 +445,17 @@ void orc_resid_anneal_coloured(const orc_resid* p, const int32_t* order, const d
             const double dEd = (double)dE;
             if (dEd <= 0.0 ||
                 (double)orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u) * 0x1.0p-53 < exp(-dEd / T)) {
-                for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k) {
-                    const float upd = wf[p->ray[k]] * p->a[k];
-                    rw[p->ray[k]] = xi ? rw[p->ray[k]] - upd : rw[p->ray[k]] + upd;
-                }
+                for (int k = p->row_ptr[i]; k < p->row_ptr[i + 1]; ++k)
+                    orc_two_sum(&hi[p->ray[k]], &lo[p->ray[k]], delta * ap[k]);
                 x[i] = (uint8_t)(xi ^ 1u);
+                E += dEd;
             }
         }
         if (trace) trace[sweep] = orc_binary_energy(p, x);
+        if (track) track[sweep] = E;
     }
     if (drift_out) *drift_out = drift;
-    free(rw); free(wf); free(linf); free(qf); free(rrow); free(rbit); free(ra);
+    free(hi); free(lo); free(sw); free(ap); free(cf); free(linf); free(qf); free(rrow); free(rbit); free(rap);
 }
 
 /* classify: ising_recon.hpp:305-309 (NotThere = 1, Exists = 0, Undecided = 2). */
@@ -456,15 +487,6 @@ double orc_qubo_energy(int n, int64_t m, const int32_t* eu, const int32_t* ev, c
     return e;
 }
 
-/* hi + lo += v with the fp32 rounding error carried in lo (TwoSum), the
- * compensated update of the GPU sweep. */
-static void orc_two_sum(float* hi, float* lo, float v) {
-    const float s = *hi + v;
-    const float bp = s - *hi;
-    const float e = (*hi - (s - bp)) + (v - bp);
-    *hi = s;
-    *lo = *lo + e;
-}
 
 /* Mirror of the weighted-QUBO sweep of qublar_b200/csrc/qb_qubo.cu for one
  * replica: bits in colour-class order (order[k] = original bit at sweep

@@ -23,14 +23,14 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, REQ_CANCELLED, REQ_DONE,
+from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_RESID_CLUSTER, OPT_TRACE, REQ_CANCELLED, REQ_DONE,
                    REQ_FAILED, REQ_PENDING, REQ_RUNNING, BatchConfig, BatchInfo, BatchItem, IsingDesc, Opts,
                    ExportDesc, ProblemInfo, QBError, QuboDesc, RequestInfo, ResidualDesc, ResultInfo, ScheduleC, ServerConfig,
                    ServerStats, check, check_edge_lengths, check_residual_lengths, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
            "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
-           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "parse_rudy",
+           "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "OPT_TRACE", "parse_rudy",
            "freeze_rock", "roi_qubo", "enumerate_qubo", "parse_qubo_text", "write_qubo_text", "write_ising_out",
            "write_roi_text"]
 
@@ -135,6 +135,14 @@ class Result:
         check(lib().qb_result_marginals(self._h, ptr(p)))
         return p
 
+    def energy_trace(self) -> np.ndarray:
+        """Every branch's energy after every sweep (n_branches x sweeps) of a
+        solve made with ``trace=True``."""
+        i = self.info()
+        t = np.empty((i.n_branches, i.sweeps), dtype=np.float64)
+        check(lib().qb_result_energy_trace(self._h, ptr(t)))
+        return t
+
     def tristate(self, lo: float = 0.1, hi: float = 0.9) -> np.ndarray:
         t = np.empty(self.n, dtype=np.uint8)
         check(lib().qb_result_tristate(self._h, C.c_float(lo), C.c_float(hi), ptr(t)))
@@ -171,9 +179,12 @@ class _Problem:
         check(lib().qb_problem_colouring(self._h, ptr(order), ptr(cptr), C.byref(nc)))
         return order, cptr[: nc.value + 1].copy()
 
-    def solve(self, schedule: Schedule, n_branches: int, seed_offset: int = 0, stream=None) -> Result:
+    def solve(self, schedule: Schedule, n_branches: int, seed_offset: int = 0, stream=None,
+              trace: bool = False) -> Result:
+        """qb_solve; trace=True also records every branch's energy after every
+        sweep (Result.energy_trace)."""
         out = C.c_void_p()
-        o = _opts(-1, stream)
+        o = _opts(-1, stream, OPT_TRACE if trace else 0)
         s = schedule.to_c()
         check(lib().qb_solve(self._h, C.byref(s), int(n_branches), int(seed_offset), C.byref(o), C.byref(out)))
         return Result(out.value, self)

@@ -18,9 +18,10 @@ STATUS_NAMES = {0: "QB_OK", 1: "QB_EINVAL", 2: "QB_ENOMEM", 3: "QB_EREFUSED", 4:
 KIND_ISING = 1
 KIND_RESIDUAL = 2
 KIND_QUBO = 3
-NOALLOC_SCRATCH_BYTES = 8 << 20
+NOALLOC_SCRATCH_BYTES = 16 << 20
 OPT_DEFER_UPLOAD = 1
 OPT_RESID_CLUSTER = 2
+OPT_TRACE = 4
 REQ_PENDING, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 RESID_LOCKSTEP = 1
 RESID_CLUSTER = 2
@@ -177,11 +178,12 @@ SIGNATURES = {
     "qb_result_energies_f64": (C.c_int, [_P, _P]),
     "qb_result_marginals": (C.c_int, [_P, _P]),
     "qb_result_tristate": (C.c_int, [_P, C.c_float, C.c_float, _P]),
+    "qb_result_energy_trace": (C.c_int, [_P, _P]),
     "qb_result_destroy": (None, [_P]),
     "qb_energies_ising": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_energies_residual": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_energies_qubo": (C.c_int, [_P, _P, C.c_int32, _P]),
-    "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P]),
+    "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P, _P]),
     "qb_batch_autotune": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.c_int32, C.POINTER(Opts),
                                     C.POINTER(BatchConfig)]),
     "qb_solve_batch": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.POINTER(BatchConfig), C.POINTER(Opts),

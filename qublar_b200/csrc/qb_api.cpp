@@ -510,6 +510,8 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     P.nnz = d->row_ptr[n];
     P.n_nbr = d->nbr_ptr[n];
     P.lambda = d->lambda;
+    P.e0 = 0.0;
+    for (int b = 0; b < nr; ++b) P.e0 += 0.5 * d->w[b] * d->d[b] * d->d[b];
     PlanMarks mark;
     P.col = colour_residual(n, nr, &P.max_ray_len, d->row_ptr, d->ray, d->nbr_ptr, d->nbr);
     mark("colour");
@@ -527,7 +529,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     const int candidates[5] = {1, 2, 4, 8, 16};
     for (int t = 0; t < 5 && CL == 0; ++t) {
         const int c = candidates[t];
-        const size_t bytes = size_t((nr + c - 1) / c) * 4 + size_t(n / c + nc + 64) / 8 + resid_stage_bytes();
+        const size_t bytes = size_t((nr + c - 1) / c) * 8 + size_t(n / c + nc + 64) / 8 + resid_stage_bytes();
         if (bytes <= size_t(112) * 1024) CL = c;
     }
     if (P.variant == QB_RESID_CLUSTER) {
@@ -616,10 +618,13 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
 #pragma omp parallel for schedule(static, 1024)
     for (int i = 0; i < n; ++i) {   // in the caller's bit order: the entries stream
         const int k = C.inverse[size_t(i)];
+        // q = 1/2 sum sign(w) a'^2 over the bit's entries, a' = fp32(sqrt|w| a):
+        // the flip's own term of the data energy in the sweep's coefficients
         double qd = 0.0;
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e) {
-            const float a = d->a[e];
-            qd += 0.5 * d->w[d->ray[e]] * double(a) * double(a);
+            const double w = d->w[d->ray[e]];
+            const double ap = double(ray_coef(w, d->a[e]));
+            qd += (w < 0.0 ? -0.5 : 0.5) * ap * ap;
         }
         P.h_q[size_t(k)] = float(qd);
         P.h_lin[size_t(k)] = float(d->field ? d->field[i] : d->kappa);
@@ -699,7 +704,7 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
 // Device bytes upload_residual will take.
 int64_t residual_device_bytes(const ResidualPlan& P) {
     const int64_t n = P.n, nr = P.n_rays, nnz = P.nnz;
-    int64_t b = int64_t(P.nnz * 4 + int64_t(P.h_row.size()) + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
+    int64_t b = int64_t(P.nnz * 2 + int64_t(P.h_row.size()) + P.h_lin.size() + P.h_q.size() + P.h_nbr_ptr.size() +
                         P.h_nbr_home.size() + P.col.order.size() + P.col.class_ptr.size() + P.chunks.size() +
                         P.chunk_ptr.size()) * 4;
     b += (nr + 1) * 4 + nnz * 12 + n * 8 + nr * 16 + (n + 1) * 4 + P.n_nbr * 4;   // ray-major CSR (two bit orders)
@@ -714,19 +719,17 @@ static void host_build_residual(const ResidualPlan& P, const qb_residual_desc* d
                                 RawVec<int32_t>& rbit_n, RawVec<float>& ra) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
-    ent.resize(size_t(P.nnz) * 4);
+    ent.resize(size_t(P.nnz) * 2);
 #pragma omp parallel for schedule(static, 1024)
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
         int32_t pos = P.h_row[size_t(k)];
         for (int e = d->row_ptr[i]; e < d->row_ptr[i + 1]; ++e, ++pos) {
-            const float a = d->a[e];
-            const float wa = float(d->w[d->ray[e]]) * a;   // the fp32 scatter increment
-            uint32_t* en = &ent[size_t(pos) * 4];
-            en[0] = uint32_t(d->ray[e]);
-            std::memcpy(&en[1], &a, 4);
-            std::memcpy(&en[2], &wa, 4);
-            en[3] = 0u;
+            const double w = d->w[d->ray[e]];
+            const float ap = ray_coef(w, d->a[e]);   // the residual's exact step
+            uint32_t* en = &ent[size_t(pos) * 2];
+            en[0] = uint32_t(d->ray[e]) | (w < 0.0 ? 0x80000000u : 0u);
+            std::memcpy(&en[1], &ap, 4);
         }
     }
     // ray-major CSR, bits ascending in input order inside a ray: a counting
@@ -804,7 +807,7 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
         if ((s = upload_vec(P.d_row, P.h_row, st))) return s;
         if ((s = upload_vec(P.d_order, C.order, st))) return s;
         if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
-        if ((s = P.d_ent.alloc(size_t(P.nnz) * 16))) return s;
+        if ((s = P.d_ent.alloc(size_t(P.nnz) * 8))) return s;
         if ((s = P.d_rrow.alloc((size_t(nr) + 1) * 4))) return s;
         if ((s = P.d_o_rbit.alloc(size_t(P.nnz) * 4))) return s;
         if ((s = P.d_rbit.alloc(size_t(P.nnz) * 4))) return s;
@@ -825,7 +828,7 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
         A.inverse = t_inverse.as<int32_t>();
         A.h_row = P.d_row.as<int32_t>();
         A.bit_home = t_home.as<uint32_t>();
-        A.ent = P.d_ent.as<uint4>();
+        A.ent = P.d_ent.as<uint2>();
         A.rrow = P.d_rrow.as<int32_t>();
         A.rbit_o = P.d_o_rbit.as<int32_t>();
         A.rbit_n = rbn.as<int32_t>();
@@ -1205,6 +1208,13 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
         b.e_f64 = r->d_e_f64.as<double>();
         b.p = r->d_p.as<float>();
         b.temp = p->d_temp.as<double>();
+        if (opts && (opts->flags & QB_OPT_TRACE)) {
+            const size_t tb = size_t(R) * size_t(r->sweeps) * 8;
+            if ((s = alloc_async(r->d_trace, tb, st))) return bail(s);
+            QB_CUDA(cudaMemsetAsync(r->d_trace.p, 0, tb, st));
+            b.trace = r->d_trace.as<double>();
+            r->trace_base = p->kind == QB_KIND_RESIDUAL ? p->resid.e0 : p->kind == QB_KIND_QUBO ? p->qubo.offset : 0.0;
+        }
         if (p->kind == QB_KIND_ISING) {
             const IsingPlan& P = p->ising;
             if ((s = alloc_async(r->d_f, size_t(R) * size_t(n) * 4, st))) return bail(s);
@@ -1242,6 +1252,7 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
                 qbuf.drift = r->d_drift.as<float>() + b0;
                 qbuf.e_track = r->d_e_track.as<double>() + b0;
                 qbuf.accepts = r->d_accepts.as<unsigned long long>() + b0;
+                qbuf.trace = b.trace ? b.trace + size_t(b0) * size_t(r->sweeps) : nullptr;
                 qbuf.scratch = r->d_scratch.p;
                 s = launch_qubo_lockstep(P, qbuf, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
                                          seed0 + uint64_t(b0), st);
@@ -1274,6 +1285,7 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
                     SolveBuffers bb = b;
                     bb.x = b.x + size_t(b0) * size_t(n);
                     bb.drift = b.drift + b0;
+                    if (b.trace) bb.trace = b.trace + size_t(b0) * size_t(r->sweeps);
                     s = launch_resid_lockstep(P, bb, std::min(RB, R - b0), r->sweeps, sch->refresh_sweeps,
                                               seed0 + uint64_t(b0), st);
                 }
@@ -1314,6 +1326,17 @@ extern "C" qb_status qb_result_info_get(qb_result* r, qb_result_info* info) {
         for (size_t k = 0; k < et.size(); ++k)
             info->max_energy_error = std::max(info->max_energy_error, std::fabs(r->prob->qubo.offset + et[k] - ef[k]));
     }
+    if (r->prob->kind == QB_KIND_RESIDUAL && r->d_trace.p) {
+        // a traced residual solve: E(x = 0) plus the accepted dE against the fp64 energy
+        std::vector<double> tr(size_t(r->R) * size_t(r->sweeps)), ef(static_cast<size_t>(r->R));
+        QB_CUDA(cudaMemcpy(tr.data(), r->d_trace.p, tr.size() * 8, cudaMemcpyDeviceToHost));
+        QB_CUDA(cudaMemcpy(ef.data(), r->d_e_f64.p, ef.size() * 8, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < r->R; ++k) {
+            double e = r->trace_base;
+            for (int t = 0; t < r->sweeps; ++t) e += tr[size_t(k) * size_t(r->sweeps) + size_t(t)];
+            info->max_energy_error = std::max(info->max_energy_error, std::fabs(e - ef[size_t(k)]));
+        }
+    }
     if (r->prob->kind == QB_KIND_RESIDUAL || r->prob->kind == QB_KIND_QUBO) {
         std::vector<float> dr(static_cast<size_t>(r->R));
         QB_CUDA(cudaMemcpy(dr.data(), r->d_drift.p, dr.size() * sizeof(float), cudaMemcpyDeviceToHost));
@@ -1351,6 +1374,34 @@ extern "C" qb_status qb_result_energies_f64(qb_result* r, double* e) {
     return download(r, e, r->d_e_f64, size_t(r->R) * 8);
 }
 
+extern "C" qb_status qb_result_energy_trace(qb_result* r, double* trace) {
+    return qb::guarded("qb_result_energy_trace", [&]() -> qb_status {
+        if (!r || !trace) return fail(QB_EINVAL, "qb_result_energy_trace: null argument");
+        if (!r->d_trace.p) return fail(QB_EINVAL, "qb_result_energy_trace: the solve was not made with QB_OPT_TRACE");
+        const size_t R = size_t(r->R), S = size_t(r->sweeps);
+        if (r->prob->kind == QB_KIND_ISING) {
+            std::vector<long long> t(R * S);
+            qb_status s = download(r, t.data(), r->d_trace, t.size() * 8);
+            if (s != QB_OK) return s;
+            for (size_t k = 0; k < t.size(); ++k) trace[k] = double(t[k]);
+            return QB_OK;
+        }
+        // per-sweep sums of accepted dE, accumulated from the energy of x = 0
+        // (residual) or the offset (qubo) in sweep order
+        std::vector<double> t(R * S);
+        qb_status s = download(r, t.data(), r->d_trace, t.size() * 8);
+        if (s != QB_OK) return s;
+        for (size_t k = 0; k < R; ++k) {
+            double e = r->trace_base;
+            for (size_t q = 0; q < S; ++q) {
+                e += t[k * S + q];
+                trace[k * S + q] = e;
+            }
+        }
+        return QB_OK;
+    });
+}
+
 extern "C" qb_status qb_result_marginals(qb_result* r, float* p) {
     if (!r) return fail(QB_EINVAL, "qb_result_marginals: null result");
     return download(r, p, r->d_p, size_t(r->n) * 4);
@@ -1374,7 +1425,7 @@ extern "C" void qb_result_destroy(qb_result* r) {
     cudaSetDevice(r->device);
     cudaStream_t st = r->stream;
     DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift,
-                     &r->d_accepts, &r->d_e_track, &r->d_scratch};
+                     &r->d_accepts, &r->d_e_track, &r->d_scratch, &r->d_trace};
     for (DevBuf* b : all) free_async(*b, st);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);

@@ -3,12 +3,12 @@
 // ray-major CSR with its three bit columns. The host plans the colouring,
 // the slices and the per-bit tables; only the O(nnz) tables are built here,
 // so the upload moves the 8 bytes per entry the caller already holds instead
-// of 32 bytes per entry built on the host.
+// of 24 bytes per entry built on the host.
 //
 // The arrays are the host build's to the bit:
-//   ent[h_row[k] + q] = {ray, a, fp32(w[ray]) * a, 0} for the q-th entry of
-//     the bit at sweep position k (one fp32 rounding of the product, as the
-//     host computes it);
+//   ent[h_row[k] + q] = {ray | (w[ray] < 0) << 31, fp32(sqrt|w[ray]| * a)} for
+//     the q-th entry of the bit at sweep position k (the fp64 product rounded
+//     once, as the host computes it);
 //   the ray-major CSR lists every ray's bits in ascending input order (the
 //     fp64 energy verifier and the residual refresh sum in that order): the
 //     entries are scattered to their rays with atomics, then each ray's
@@ -37,9 +37,9 @@ __global__ void __launch_bounds__(kBuildWarps * 32) build_entries_kernel(ResidBu
         const int dst = A.h_row[k];
         for (int q = lane; q < len; q += 32) {
             const int r = A.ray[e0 + q];
-            const float av = A.a[e0 + q];
-            const float wa = __fmul_rn(float(A.w[r]), av);
-            A.ent[dst + q] = make_uint4(uint32_t(r), __float_as_uint(av), __float_as_uint(wa), 0u);
+            const double w = A.w[r];
+            const float ap = __double2float_rn(__dmul_rn(sqrt(fabs(w)), double(A.a[e0 + q])));
+            A.ent[dst + q] = make_uint2(uint32_t(r) | (w < 0.0 ? 0x80000000u : 0u), __float_as_uint(ap));
             atomicAdd(&A.rcount[r], 1);
         }
     }

@@ -24,7 +24,7 @@ struct ResidBuildArgs {
     const int32_t* inverse;    // input bit -> sweep position
     const int32_t* h_row;      // n + 1 sweep-order entry offsets
     const uint32_t* bit_home;  // sweep position -> home word (cluster sweep)
-    uint4* ent;                // nnz sweep-order entries {ray, a, fp32(w) * a, 0}
+    uint2* ent;                // nnz sweep-order entries {ray | (w < 0) << 31, fp32(sqrt|w| a)}
     int32_t* rrow;             // n_rays + 1 ray-major offsets
     int32_t* rbit_o;           // nnz: input bit
     int32_t* rbit_n;           // nnz: sweep position

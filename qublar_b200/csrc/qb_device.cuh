@@ -22,16 +22,19 @@ __device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
 // Grid barrier of a cooperative launch: arrive, then poll the counter until
 // every CTA of barrier round `round` has arrived. A poll limit turns a lost
 // CTA into an error flag instead of a hang; every CTA then leaves its loops.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned round) {
+// per_round: arrivals that complete a round (0 = gridDim.x); limit: polls
+// before giving up.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned round, unsigned per_round = 0,
+                                             unsigned limit = kSpinLimit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned target = round * gridDim.x;
+        const unsigned target = round * (per_round ? per_round : gridDim.x);
         red_release_gpu(bar, 1u);
         unsigned spins = 0;
         int ok = 1;
         while (ld_acquire_gpu(bar) < target) {
-            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+            if (++spins > limit || *reinterpret_cast<volatile int*>(err)) {
                 atomicExch(err, 1);
                 ok = 0;
                 break;
@@ -51,14 +54,15 @@ __device__ __forceinline__ void grid_arrive(unsigned* bar) {
     if (threadIdx.x == 0) red_release_gpu(bar, 1u);
 }
 
-__device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned round) {
+__device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned round, unsigned per_round = 0,
+                                          unsigned limit = kSpinLimit) {
     __shared__ int s_ok2;
     if (threadIdx.x == 0) {
-        const unsigned target = round * gridDim.x;
+        const unsigned target = round * (per_round ? per_round : gridDim.x);
         unsigned spins = 0;
         int ok = 1;
         while (ld_acquire_gpu(bar) < target) {
-            if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+            if (++spins > limit || *reinterpret_cast<volatile int*>(err)) {
                 atomicExch(err, 1);
                 ok = 0;
                 break;
@@ -86,6 +90,33 @@ __device__ __forceinline__ bool uphill_accept(uint64_t u53, double dE, double T,
     if (u + 0x1p-32f < 0.999f * p) return true;
     if (u > 1.001f * p) return false;
     return double(u53) * 0x1.0p-53 < exp(-dE / T);
+}
+
+// ---- compensated residuals of the residual-form sweeps ----------------------------
+//
+// A branch's state per ray b is the scaled residual rho_b = s_b (sum_v a_bv x_v
+// - d_b) with s_b = sqrt|w_b|, carried as an fp32 pair hi + lo. A bit-ray
+// entry holds the fp32 coefficient a' = fp32(s_b a) (one rounding of the fp64
+// product), so a flip changes rho_b by exactly +-a' and the TwoSum below keeps
+// hi + lo equal to the running sum up to the rounding of lo. A bit's data term
+// is sum_k sign(w_k) a'_k rho_k = sum_k w_k a_k r_k of local_field_dE
+// (src/ising_recon.hpp:105-118) with r = rho / s.
+
+// a' = fp32(sqrt|w| * a), the fp64 product rounded once.
+__device__ __forceinline__ float scaled_coef(double sw, float a) { return __double2float_rn(__dmul_rn(sw, double(a))); }
+
+// The fp32 pair (hi, lo) nearest an fp64 value: hi = fp32(v), lo = fp32(v - hi).
+__device__ __forceinline__ float2 split_pair(double v) {
+    const float hi = __double2float_rn(v);
+    return make_float2(hi, __double2float_rn(__dsub_rn(v, double(hi))));
+}
+
+// hi + lo += v: TwoSum of hi and v, its rounding error added into lo.
+__device__ __forceinline__ float2 two_sum_add(float2 p, float v) {
+    const float s = __fadd_rn(p.x, v);
+    const float bp = __fsub_rn(s, p.x);
+    const float e = __fadd_rn(__fsub_rn(p.x, __fsub_rn(s, bp)), __fsub_rn(v, bp));
+    return make_float2(s, __fadd_rn(p.y, e));
 }
 
 // Raises a kernel's dynamic shared-memory limit to the device maximum (the

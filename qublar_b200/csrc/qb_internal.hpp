@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <exception>
 #include <memory>
@@ -115,6 +116,10 @@ struct NoInitAlloc : std::allocator<T> {
 template <typename T>
 using RawVec = std::vector<T, NoInitAlloc<T>>;
 
+// The residual sweeps' fp32 coefficient of a bit-ray entry: a' = fp32(sqrt|w| a),
+// the fp64 product rounded once (the device's scaled_coef, qb_device.cuh).
+inline float ray_coef(double w, float a) { return float(std::sqrt(std::fabs(w)) * double(a)); }
+
 // The temperature of every sweep of a schedule (host, double).
 std::vector<double> temperatures(const qb_schedule& s);
 
@@ -175,6 +180,7 @@ struct ResidualPlan {
     int64_t nnz = 0;
     int64_t n_nbr = 0;
     double lambda = 0.0;
+    double e0 = 0.0;                  // energy of x = 0: 1/2 sum_b w_b d_b^2 (fp64, ray order)
     Colouring col;
     // cluster decomposition of one branch: CL CTAs; ray b lives on CTA b % CL,
     // slot b / CL; bit k of class c belongs to CTA t = (k - class start) / chunk(c)
@@ -279,6 +285,8 @@ struct qb_result {
     qb::DevBuf d_accepts;    // R accepted-flip counts (residual, qubo)
     qb::DevBuf d_e_track;    // R tracked energies minus offset (qubo)
     qb::DevBuf d_scratch;    // per-branch state that does not fit on chip
+    qb::DevBuf d_trace;      // R x sweeps: ising int64 tracked energies; residual, qubo fp64 per-sweep dE sums
+    double trace_base = 0.0; // residual: energy of x = 0; qubo: the offset
     const int* d_err = nullptr;   // timeout flag of a cooperative sweep (inside d_scratch), or null
     bool synced = false;
 };

@@ -51,7 +51,7 @@ constexpr int kResidThreads = 512;
 constexpr int kGroup = 8;       // lanes per bit in the residual sweep
 constexpr int kHeavy = 64;      // bits with more rays take a full warp
 constexpr int kChunkB = 1024;   // stage bits per chunk
-constexpr int kChunkE = 8192;   // stage entries per chunk
+constexpr int kChunkE = 4096;   // stage entries per chunk
 constexpr int kChunkN = 6144;   // stage neighbour entries per chunk
 constexpr uint32_t kSlotBits = 27;
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
@@ -82,6 +82,7 @@ struct IsingArgs {
     uint8_t* x_out;       // R x n
     int32_t* f_out;       // R x n
     long long* e_out;     // R
+    long long* trace;     // nullable: R x sweeps tracked energies after each sweep (zeroed)
 };
 
 // Accepted bits of a class listed for the warp-wide neighbour update, used
@@ -158,6 +159,14 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
             __syncthreads();
             if (threadIdx.x == 0) acc_count[parity] = 0;   // reused two classes later, after two barriers
         }
+        if (A.trace) {   // the tracked energy after this sweep: each warp adds its threads' running sums
+            long long Ew = E;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) Ew += __shfl_xor_sync(kFull, Ew, off);
+            if (lane == 0 && Ew != 0)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&A.trace[size_t(rep) * A.sweeps + sweep]),
+                          (unsigned long long)Ew);
+        }
     }
     for (int i = int(threadIdx.x); i < n; i += blockDim.x) {
         const size_t o = size_t(rep) * size_t(n) + size_t(A.order[i]);
@@ -205,7 +214,7 @@ struct ResidArgs {
     const int4* chunks;         // per CTA rank: 2 x int4 per chunk (see ResidualPlan)
     const int32_t* chunk_ptr;   // CL + 1
     const int32_t* row;
-    const uint4* ent;           // per bit-ray entry: {ray, a bits, float(w_ray) * a bits, 0}
+    const uint2* ent;           // per bit-ray entry: {ray | (w < 0) << 31, a' = fp32(sqrt|w| a)}
     const float* lin;
     const float* q;
     const int32_t* nbr_ptr;
@@ -220,6 +229,7 @@ struct ResidArgs {
     uint8_t* x_out;
     float* drift;
     unsigned long long* accepts;
+    double* trace;              // nullable: R x sweeps, the sum of accepted dE of each sweep
     unsigned long long* phase;  // PHASES builds: per CTA {gather, score, barrier, chunks} clock64 sums
 };
 
@@ -231,13 +241,13 @@ __device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
     return r;
 }
-__device__ __forceinline__ float ld_cluster_f32(uint32_t addr) {
-    float v;
-    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+__device__ __forceinline__ float2 ld_cluster_f32x2(uint32_t addr) {
+    float2 v;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
     return v;
 }
-__device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
-    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v));
+__device__ __forceinline__ void st_cluster_f32x2(uint32_t addr, float2 v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y));
 }
 __device__ __forceinline__ uint32_t ld_cluster_u32(uint32_t addr) {
     uint32_t v;
@@ -257,7 +267,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 // Shared memory of the residual sweep's stage buffers.
 struct ResidStage {
     unsigned long long* u;   // kChunkB Philox draws (53-bit)
-    float* rv;               // kChunkE gathered residuals
+    float2* rv;              // kChunkE gathered residual pairs (hi, lo)
     int32_t* row;            // kChunkB + 1 entry offsets (chunk-relative)
     int32_t* nbp;            // kChunkB + 1 neighbour offsets (chunk-relative)
     float* lin;              // kChunkB
@@ -266,16 +276,21 @@ struct ResidStage {
 };
 
 // Score, decide and (on accept) scatter bit k of the chunk with a group of G
-// lanes: lane l sums a * rw over entries l, l + G, ... as an fmaf chain, an
-// xor butterfly joins the lanes (the oracle mirrors this order).
+// lanes: lane l sums sign(w) a' * fp32(hi + lo) over entries l, l + G, ... as
+// an fmaf chain, an xor butterfly joins the lanes (the oracle mirrors this
+// order).
 template <int CL, int G>
 __device__ __forceinline__ bool score_bit(int k, int gl, unsigned gmask, int leader, const ResidStage& S,
-                                          const uint4* ent, uint32_t rw_base, uint32_t* xs, int slot0, float lambda,
-                                          double T, float inv_T) {
+                                          const uint2* ent, uint32_t rw_base, uint32_t* xs, int slot0, float lambda,
+                                          double T, float inv_T, double* s_trace) {
     constexpr int kShift = CL == 1 ? 0 : CL == 2 ? 1 : CL == 4 ? 2 : CL == 8 ? 3 : 4;
     const int rs = S.row[k], re = S.row[k + 1], ns = S.nbp[k], ne = S.nbp[k + 1];
     float acc = 0.0f;
-    for (int e = rs + gl; e < re; e += G) acc = fmaf(__uint_as_float(__ldg(&ent[e]).y), S.rv[e], acc);
+    for (int e = rs + gl; e < re; e += G) {
+        const uint2 en = __ldg(&ent[e]);
+        const float c = (en.x >> 31) ? -__uint_as_float(en.y) : __uint_as_float(en.y);
+        acc = fmaf(c, __fadd_rn(S.rv[e].x, S.rv[e].y), acc);
+    }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(gmask, acc, off));
     const int slot = slot0 + k;
@@ -291,14 +306,16 @@ __device__ __forceinline__ bool score_bit(int k, int gl, unsigned gmask, int lea
         const float prior = __fmul_rn(lambda, float((ne - ns) - 2 * unlike));
         const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), S.q[k]), prior);
         accept = (dE <= 0.0f || uphill_accept(S.u[k], double(dE), T, inv_T)) ? 1 : 0;
+        if (accept && s_trace) atomicAdd(s_trace, double(dE));
     }
     accept = __shfl_sync(gmask, accept, leader);
     if (accept) {
+        const float dl = xi ? -1.0f : 1.0f;
         for (int e = rs + gl; e < re; e += G) {
-            const uint4 en = __ldg(&ent[e]);
-            const uint32_t ad = map_rank(rw_base + (en.x >> kShift) * 4u, en.x & (CL - 1));
-            const float wa = __uint_as_float(en.z);
-            st_cluster_f32(ad, xi ? __fsub_rn(S.rv[e], wa) : __fadd_rn(S.rv[e], wa));
+            const uint2 en = __ldg(&ent[e]);
+            const uint32_t ray = en.x & 0x7FFFFFFFu;
+            const uint32_t ad = map_rank(rw_base + (ray >> kShift) * 8u, ray & (CL - 1));
+            st_cluster_f32x2(ad, two_sum_add(S.rv[e], __fmul_rn(dl, __uint_as_float(en.y))));
         }
         if (gl == 0) atomicXor(&xs[slot >> 5], 1u << (slot & 31));
     }
@@ -328,7 +345,7 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
     constexpr int kWarps = kResidThreads / 32;
     ResidStage S;
     S.u = reinterpret_cast<unsigned long long*>(smem);
-    float* rw = reinterpret_cast<float*>(S.u + kChunkB);                     // w r per owned ray
+    float2* rw = reinterpret_cast<float2*>(S.u + kChunkB);                   // (hi, lo) of rho per owned ray
     S.rv = rw + A.ray_slots;
     S.row = reinterpret_cast<int32_t*>(S.rv + kChunkE);
     S.nbp = S.row + (kChunkB + 1);
@@ -337,6 +354,7 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
     S.xn = reinterpret_cast<uint8_t*>(S.q + kChunkB);
     uint32_t* xs = reinterpret_cast<uint32_t*>(S.xn + kChunkN);             // owned bits, packed
     __shared__ unsigned long long s_acc_count;
+    __shared__ double s_trace;   // accepted dE of this CTA's bits in the current sweep
     cg::cluster_group cluster = cg::this_cluster();
     const uint32_t rank = cluster.block_rank();
     const int branch = int(blockIdx.x) / CL;
@@ -354,29 +372,33 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
 
     for (int sl = tid; sl < A.ray_slots; sl += kResidThreads) {
         const int b = (sl << kShift) + int(rank);
-        rw[sl] = b < A.n_rays ? float(A.w64[b] * (-A.d[b])) : 0.0f;
+        rw[sl] = b < A.n_rays ? split_pair(-__dmul_rn(sqrt(fabs(A.w64[b])), A.d[b])) : make_float2(0.0f, 0.0f);
     }
     for (int sl = tid; sl < A.bit_words; sl += kResidThreads) xs[sl] = 0u;
-    if (tid == 0) s_acc_count = 0;
+    if (tid == 0) {
+        s_acc_count = 0;
+        s_trace = 0.0;
+    }
     cluster.sync();
 
     unsigned long long my_accepts = 0;
     long long ph_gather = 0, ph_score = 0, ph_bar = 0, ph_chunks = 0, t_ph = 0;
     for (int sweep = 0; sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
-            // fp64 refresh of the owned residuals: r_b = (sum over the ray's
-            // set bits of a, in ray order) - d_b
+            // fp64 refresh of the owned residuals: rho_b = (sum over the
+            // ray's set bits of a', in ray order) - sqrt|w_b| d_b
             float dmax = 0.0f;
             for (int sl = tid; sl < A.ray_slots; sl += kResidThreads) {
                 const int b = (sl << kShift) + int(rank);
                 if (b >= A.n_rays) continue;
+                const double sw = sqrt(fabs(A.w64[b]));
                 double acc = 0.0;
                 const int k1 = A.rrow[b + 1];
                 for (int k = A.rrow[b]; k < k1; ++k)
-                    if (ld_home_bit(xs_base, A.rbit_home[k])) acc += double(A.ra[k]);
-                const float nv = float(A.w64[b] * (acc - A.d[b]));
-                dmax = fmaxf(dmax, fabsf(nv - rw[sl]));
-                rw[sl] = nv;
+                    if (ld_home_bit(xs_base, A.rbit_home[k])) acc = __dadd_rn(acc, double(scaled_coef(sw, A.ra[k])));
+                const double v = __dsub_rn(acc, __dmul_rn(sw, A.d[b]));
+                dmax = fmaxf(dmax, __double2float_rn(fabs(__dsub_rn(__dadd_rn(double(rw[sl].x), double(rw[sl].y)), v))));
+                rw[sl] = split_pair(v);
             }
             if (dmax > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[branch]), __float_as_int(dmax));
             cluster.sync();
@@ -391,7 +413,7 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
             if (tid == 0) {   // the next chunk's entries into L2
                 const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
                 const int4 c1n = chunks[2 * nx + 1];
-                if (c1n.y > c1n.x) prefetch_l2(&A.ent[c1n.x], uint32_t(c1n.y - c1n.x) * 16u);
+                if (c1n.y > c1n.x) prefetch_l2(&A.ent[c1n.x], uint32_t(c1n.y - c1n.x) * 8u);
             }
             // 1. gather
             for (int k = tid; k <= nb; k += kResidThreads) {
@@ -405,18 +427,18 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
                 }
             }
             for (int e0 = c1.x + tid; e0 < c1.y; e0 += 4 * kResidThreads) {
-                uint4 en[4];
+                uint32_t ray[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int e = e0 + u * kResidThreads;
-                    en[u] = e < c1.y ? __ldg(&A.ent[e]) : make_uint4(0u, 0u, 0u, 0u);
+                    ray[u] = e < c1.y ? (__ldg(&A.ent[e]).x & 0x7FFFFFFFu) : 0u;
                 }
-                float rv[4];
+                float2 rv[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     rv[u] = e0 + u * kResidThreads < c1.y
-                                ? ld_cluster_f32(map_rank(rw_base + (en[u].x >> kShift) * 4u, en[u].x & (CL - 1)))
-                                : 0.0f;
+                                ? ld_cluster_f32x2(map_rank(rw_base + (ray[u] >> kShift) * 8u, ray[u] & (CL - 1)))
+                                : make_float2(0.0f, 0.0f);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int e = e0 + u * kResidThreads;
@@ -432,13 +454,14 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
                 t_ph = t1;
             }
             // 2. score, decide, scatter
-            const uint4* ent = A.ent + c1.x;
+            const uint2* ent = A.ent + c1.x;
             const int nh = c0.w >> 1;
             for (int k = warp; k < nh; k += kWarps)
-                my_accepts += (score_bit<CL, 32>(k, lane, kFull, 0, S, ent, rw_base, xs, c0.z, A.lambda, T, inv_T) && lane == 0);
+                my_accepts += (score_bit<CL, 32>(k, lane, kFull, 0, S, ent, rw_base, xs, c0.z, A.lambda, T, inv_T,
+                                                 A.trace ? &s_trace : nullptr) && lane == 0);
             for (int k = nh + grp; k < nb; k += kGroups)
                 my_accepts += (score_bit<CL, kGroup>(k, gl, gmask, lane & ~(kGroup - 1), S, ent, rw_base, xs, c0.z,
-                                                     A.lambda, T, inv_T) && gl == 0);
+                                                     A.lambda, T, inv_T, A.trace ? &s_trace : nullptr) && gl == 0);
             if (PHASES) {
                 __syncthreads();
                 const long long t1 = clock64();
@@ -450,6 +473,13 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
             if (PHASES) {
                 ph_bar += clock64() - t_ph;
                 ++ph_chunks;
+            }
+        }
+        if (A.trace) {   // this CTA's part of the sweep's tracked energy change
+            __syncthreads();
+            if (tid == 0) {
+                if (s_trace != 0.0) atomicAdd(&A.trace[size_t(branch) * A.sweeps + sweep], s_trace);
+                s_trace = 0.0;
             }
         }
     }
@@ -476,13 +506,15 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
 // ---- residual form, all branches in lockstep ------------------------------------------
 //
 // Every CTA of a co-resident (cooperative) grid takes a balanced slice of
-// each colour class; a warp scores one bit for 16 branches at once: lane l
-// serves branch l % 16 and entries of parity l / 16, so one coalesced 64-byte
-// load of rw[ray][16 branches] feeds 16 branches. Residuals and bits live in
-// global memory (L2-resident: 4.8 MB of residuals and 1.2 MB of bit words for
-// the benchmark pyramid at 16 branches); a bounded grid barrier closes each
-// class. Branch b of a bit sums h = fmaf chain over its even entries + fmaf
-// chain over its odd entries (the oracle's "lockstep" order).
+// each colour class; a warp sums one 16-entry segment of a bit for 16 branches
+// at once: lane l serves branch l % 16 and entries of parity l / 16, so one
+// coalesced 128-byte load of rho[ray][16 branches] (hi, lo pairs) feeds 16
+// branches. Residuals and bits live in global memory (L2-resident: 9.7 MB of
+// residual pairs and 1.2 MB of bit words for the benchmark pyramid at 16
+// branches); a bounded grid barrier closes each class. Branch b of a bit sums
+// h = sum over its 16-entry segments in order of (the fmaf chain over the
+// segment's even entries + the chain over its odd entries), each term
+// c * fp32(hi + lo) with c = sign(w) a' (the oracle's "lockstep" order).
 
 constexpr int kLockThreads = 1024;
 constexpr int kLockE = 2048;   // staged entries per chunk
@@ -491,6 +523,7 @@ constexpr int kLockN = 1536;   // staged neighbour entries per chunk
 constexpr int kSeg = 16;       // entries per segment: one warp, one batch of loads
 constexpr int kLockSegs = kLockE / kSeg + kLockB;   // segments a chunk can hold
 constexpr int kLockMaxNG = 4;  // branch groups of 16 one launch serves (64 branches)
+constexpr uint32_t kRayMask = 0x7FFFFFFFu;   // entry word 0: ray | (w < 0) << 31
 
 struct ResidLockArgs {
     int n;
@@ -501,10 +534,10 @@ struct ResidLockArgs {
     int NG;             // groups of 16 branches
     float lambda;
     uint64_t seed0;
-    const int4* chunks;         // per CTA: 2 x int4 per chunk {b0, b1, -, last} {e0, e1, n0, n1}
+    const int4* chunks;         // per CTA: 2 x int4 per chunk {b0, b1, segments, last} {e0, e1, n0, n1}
     const int32_t* chunk_ptr;   // gridDim + 1
-    const uint4* ent;           // {ray, a, w a, 0} per bit-ray entry, sweep order
-    const uint4* meta;          // per bit, 2 x uint4: {row start, rays, nbr start, nbrs} {lin, q, input index, 0}
+    const uint2* ent;           // {ray | (w < 0) << 31, a'} per bit-ray entry, sweep order
+    const uint4* meta;          // per bit, 2 x uint4: {row start, rays, nbr start, nbrs} {lin, q, input index, first segment}
     const int32_t* nbr;         // sweep-order index of each neighbour
     const int32_t* order;
     const double* d;
@@ -513,18 +546,25 @@ struct ResidLockArgs {
     const int32_t* rbit;        // sweep-order bit of each ray-major entry
     const float* ra;
     const double* temp;
-    float* rw;                  // n_rays x (16 NG): weighted residuals of every branch
+    float2* rp;                 // n_rays x (16 NG): (hi, lo) of every branch's scaled residual
     uint32_t* xb;               // n x NG: bit words, branch 16 g + l at bit l of word g
     unsigned* bar;              // grid barrier counter (zero at launch)
     int* err;                   // 1: a barrier timed out
+    int* status;                // nullable: set to QB_ETIMEDOUT when a barrier times out
+    unsigned bar_extra;         // arrivals a barrier round waits for beyond the grid (0; test hook)
+    unsigned spin_limit;        // polls of a barrier before it gives up
     uint8_t* x_out;
     float* drift;
     unsigned long long* accepts;
+    double* trace;              // nullable: R x sweeps, the sum of accepted dE of each sweep
     unsigned long long* phase;  // PHASES builds: per CTA {stage wait, items, barrier, chunks} clock64 sums
 };
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
@@ -532,14 +572,22 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
 struct LockStage {
-    uint4* ent;      // kLockE
+    uint2* ent;      // kLockE
     uint4* meta;     // 2 kLockB
     int32_t* nbr;    // kLockN
 };
 
-// Stage a chunk's entries, bit records and neighbour lists (async copies).
+// Stage a chunk's entries, bit records and neighbour lists (async copies;
+// 16-byte copies for the entries where both ends allow, 8-byte ones at a
+// chunk's odd edge).
 __device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0, const int4 c1, const LockStage& S) {
-    for (int e = c1.x + int(threadIdx.x); e < c1.y; e += kLockThreads) cp_async16(&S.ent[e - c1.x], &A.ent[e]);
+    const int e0 = c1.x, e1 = c1.y;
+    if ((e0 & 1) == 0) {
+        for (int e = e0 + 2 * int(threadIdx.x); e + 1 < e1; e += 2 * kLockThreads) cp_async16(&S.ent[e - e0], &A.ent[e]);
+        if (((e1 - e0) & 1) && threadIdx.x == 0) cp_async8(&S.ent[e1 - 1 - e0], &A.ent[e1 - 1]);
+    } else {
+        for (int e = e0 + int(threadIdx.x); e < e1; e += kLockThreads) cp_async8(&S.ent[e - e0], &A.ent[e]);
+    }
     for (int k = 2 * c0.x + int(threadIdx.x); k < 2 * c0.y; k += kLockThreads) cp_async16(&S.meta[k - 2 * c0.x], &A.meta[k]);
     for (int j = c1.z + int(threadIdx.x); j < c1.w; j += kLockThreads) cp_async4(&S.nbr[j - c1.z], &A.nbr[j]);
 }
@@ -547,14 +595,14 @@ __device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0
 // Every CTA of a cooperative grid works its chunk list (a balanced slice of
 // each colour class); the next chunk's structure is staged in shared memory
 // while the current one runs. Per chunk:
-//   A. a warp sums one 16-entry segment of one bit for 16 branches: lane l
-//      serves branch l % 16 and the segment's entries of parity l / 16, so one
-//      coalesced 64-byte load of rw[ray][16 branches] feeds 16 branches and
-//      each lane issues its eight loads at once; segment sum = the even-entry
-//      fmaf chain + the odd-entry chain;
-//   B. a warp per bit adds its segments in order, counts unlike neighbours,
-//      decides, and scatters w a delta with fire-and-forget reductions (a
-//      class touches a residual at most once: the result is deterministic).
+//   A. a warp sums one 16-entry segment of one bit for 16 branches and keeps
+//      the (hi, lo) pairs it loaded (its first segment's); other warps count
+//      each (bit, group)'s unlike neighbours;
+//   B. a warp per (bit, group) adds the bit's segment sums in order, decides,
+//      and records which branches flip;
+//   C. the warps of phase A add delta a' into the flipped branches' pairs by
+//      TwoSum and store them (a class touches a residual at most once, so
+//      plain stores suffice and the result is deterministic).
 // A bounded grid barrier closes each class.
 template <bool PHASES>
 __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLockArgs A) {
@@ -567,15 +615,18 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     const int half = lane >> 4;         // entry parity
     const int P = int(gridDim.x);
     const int p = int(blockIdx.x);
-    const int RP = 16 * A.NG;           // residual row pitch (floats)
-    constexpr size_t kStageBytes = size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
+    const int RP = 16 * A.NG;           // residual row pitch (pairs)
+    constexpr size_t kStageBytes = size_t(kLockE) * 8 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
     // one group of 16 branches: the Philox draws of the next chunk are made
     // while the grid barrier is pending and wait in two 16-branch tables
     unsigned long long* s_draw = reinterpret_cast<unsigned long long*>(smem + 2 * kStageBytes);
     const bool pre_draw = A.NG == 1;
     float* hseg = reinterpret_cast<float*>(s_draw + (pre_draw ? 2 * size_t(kLockB) * 16 : 0));   // kLockSegs x NG x 16 segment sums
-    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * A.NG * 16);   // kLockB x NG bit words
-    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_xw + size_t(kLockB) * A.NG);           // kLockB x NG x 16 unlike counts
+    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * A.NG * 16);   // kLockB x NG bit words (before)
+    uint32_t* s_amask = s_xw + size_t(kLockB) * A.NG;                                   // kLockB x NG flipped branches
+    int32_t* s_segbit = reinterpret_cast<int32_t*>(s_amask + size_t(kLockB) * A.NG);    // kLockSegs: bit of each segment
+    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_segbit + kLockSegs);                  // kLockB x NG x 16 unlike counts
+    __shared__ double s_trace[16 * kLockMaxNG];
     // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`, into table `t`
     auto make_draws = [&](int t, int b0, int nb, int sw) {
         unsigned long long* d = s_draw + size_t(t) * kLockB * 16;
@@ -587,27 +638,29 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     auto stage = [&](int b) {
         LockStage L;
         unsigned char* q = smem + size_t(b) * kStageBytes;
-        L.ent = reinterpret_cast<uint4*>(q);
-        L.meta = reinterpret_cast<uint4*>(q + size_t(kLockE) * 16);
-        L.nbr = reinterpret_cast<int32_t*>(q + size_t(kLockE) * 16 + size_t(kLockB) * 32);
+        L.ent = reinterpret_cast<uint2*>(q);
+        L.meta = reinterpret_cast<uint4*>(q + size_t(kLockE) * 8);
+        L.nbr = reinterpret_cast<int32_t*>(q + size_t(kLockE) * 8 + size_t(kLockB) * 32);
         return L;
     };
+    const unsigned per_round = unsigned(P) + A.bar_extra;
     const int4* chunks = A.chunks + 2 * A.chunk_ptr[p];
     const int n_chunks = A.chunk_ptr[p + 1] - A.chunk_ptr[p];
     unsigned round = 0;
     unsigned long long my_accepts = 0;
     __shared__ unsigned long long s_acc_count;
     if (tid == 0) s_acc_count = 0;
-    // x = 0: rw_b = w_b (-d_b) for every branch
+    if (tid < 16 * kLockMaxNG) s_trace[tid] = 0.0;
+    // x = 0: rho_b = -sqrt|w_b| d_b for every branch
     for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n_rays) * RP; k += size_t(P) * kLockThreads) {
         const int b = int(k / RP);
-        A.rw[k] = float(A.w64[b] * (-A.d[b]));
+        A.rp[k] = split_pair(-__dmul_rn(sqrt(fabs(A.w64[b])), A.d[b]));
     }
     for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
     if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0));
     cp_async_commit();
     if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
-    bool ok = grid_barrier(A.bar, A.err, ++round);
+    bool ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
     int4 cur0 = make_int4(0, 0, 0, 0), cur1 = make_int4(0, 0, 0, 0);   // descriptor of the chunk in hand
     if (n_chunks > 0) {
@@ -617,20 +670,23 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0, ph_a = 0, ph_b = 0, t_a = 0;
     for (int sweep = 0; ok && sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
-            // fp64 refresh: thread per (ray, branch), bits of the ray in order
+            // fp64 refresh: thread per (ray, branch), the ray's set bits in
+            // order: rho = sum a' - sqrt|w| d, the drift |hi + lo - rho| recorded
             for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n_rays) * RP; k += size_t(P) * kLockThreads) {
                 const int b = int(k / RP), j = int(k % RP);
                 if (j >= A.R) continue;
                 const int g = j >> 4, l = j & 15;
+                const double sw = sqrt(fabs(A.w64[b]));
                 double acc = 0.0;
                 for (int e = A.rrow[b]; e < A.rrow[b + 1]; ++e)
-                    if ((__ldcg(&A.xb[size_t(A.rbit[e]) * A.NG + g]) >> l) & 1u) acc += double(A.ra[e]);
-                const float nv = float(A.w64[b] * (acc - A.d[b]));
-                const float dv = fabsf(nv - __ldcg(&A.rw[k]));
+                    if ((__ldcg(&A.xb[size_t(A.rbit[e]) * A.NG + g]) >> l) & 1u) acc = __dadd_rn(acc, double(scaled_coef(sw, A.ra[e])));
+                const double v = __dsub_rn(acc, __dmul_rn(sw, A.d[b]));
+                const float2 cur = __ldcg(&A.rp[k]);
+                const float dv = __double2float_rn(fabs(__dsub_rn(__dadd_rn(double(cur.x), double(cur.y)), v)));
                 if (dv > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[j]), __float_as_int(dv));
-                __stcg(&A.rw[k], nv);
+                __stcg(&A.rp[k], split_pair(v));
             }
-            ok = grid_barrier(A.bar, A.err, ++round);
+            ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
             if (!ok) break;
         }
         const double T = A.temp[sweep];
@@ -657,6 +713,10 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             // A. segment sums, and per (bit, group) the bit word and the
             // unlike-neighbour counts, in one round of loads
             const int nseg_items = nseg * A.NG;
+            float2 held[kSeg / 2];   // the pairs of this warp's first segment item, for phase C
+            int held_it = -1;
+#pragma unroll
+            for (int u = 0; u < kSeg / 2; ++u) held[u] = make_float2(0.0f, 0.0f);
             for (int it = warp; it < nseg_items + nb * A.NG; it += kWarps) {
                 if (it >= nseg_items) {
                     const int k = (it - nseg_items) / A.NG, g = (it - nseg_items) % A.NG;
@@ -683,29 +743,36 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     const int mid = (lo + hi + 1) >> 1;
                     if (int(St.meta[2 * mid + 1].w) <= sg) lo = mid; else hi = mid - 1;
                 }
+                if (g == 0 && lane == 0) s_segbit[sg] = lo;
                 const uint4 m0 = St.meta[2 * lo];
                 const int seg_in_bit = sg - int(St.meta[2 * lo + 1].w);
                 const int rs = int(m0.x) - c1.x + seg_in_bit * kSeg;
                 const int re = min(int(m0.x) - c1.x + int(m0.y), rs + kSeg);
-                float av[kSeg / 2], rv[kSeg / 2];
+                float cv[kSeg / 2];
+                float2 rv[kSeg / 2];
 #pragma unroll
                 for (int u = 0; u < kSeg / 2; ++u) {
                     const int e = rs + half + 2 * u;
                     if (e < re) {
-                        const uint4 en = St.ent[e];
-                        av[u] = __uint_as_float(en.y);
-                        rv[u] = __ldcg(&A.rw[size_t(en.x) * RP + 16 * g + br]);
+                        const uint2 en = St.ent[e];
+                        cv[u] = (en.x >> 31) ? -__uint_as_float(en.y) : __uint_as_float(en.y);
+                        rv[u] = __ldcg(&A.rp[size_t(en.x & kRayMask) * RP + 16 * g + br]);
                     } else {
-                        av[u] = 0.0f;
-                        rv[u] = 0.0f;
+                        cv[u] = 0.0f;
+                        rv[u] = make_float2(0.0f, 0.0f);
                     }
                 }
                 float acc = 0.0f;
 #pragma unroll
                 for (int u = 0; u < kSeg / 2; ++u)
-                    if (rs + half + 2 * u < re) acc = fmaf(av[u], rv[u], acc);
+                    if (rs + half + 2 * u < re) acc = fmaf(cv[u], __fadd_rn(rv[u].x, rv[u].y), acc);
                 const float other = __shfl_xor_sync(kFull, acc, 16);
                 if (half == 0) hseg[(sg * A.NG + g) * 16 + br] = __fadd_rn(acc, other);
+                if (held_it < 0) {
+                    held_it = it;
+#pragma unroll
+                    for (int u = 0; u < kSeg / 2; ++u) held[u] = rv[u];
+                }
             }
             __syncthreads();
             if (PHASES) {
@@ -713,14 +780,14 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 ph_a += t1 - t_a;
                 t_a = t1;
             }
-            // B. decide and scatter, a warp per (bit, group)
+            // B. decide, a warp per (bit, group)
             for (int it = warp; it < nb * A.NG; it += kWarps) {
                 const int k = it / A.NG, g = it % A.NG;
                 const int branch = 16 * g + br;
                 const bool live = branch < A.R && half == 0;
                 const uint4 m0 = St.meta[2 * k], m1 = St.meta[2 * k + 1];
                 const int i = c0.x + k;
-                const int ns = 0, ne = int(m0.w);
+                const int ne = int(m0.w);
                 const uint32_t xw = s_xw[k * A.NG + g];
                 const uint32_t xi = (xw >> br) & 1u;
                 const int unlike = s_unl[(k * A.NG + g) * 16 + br];
@@ -728,6 +795,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                                      : pre_draw ? s_draw[size_t(gci & 1) * kLockB * 16 + size_t(k) * 16 + br]
                                                 : draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u);
                 int flip = 0;
+                float dE = 0.0f;
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
                     const int s0 = int(m1.w);
@@ -735,23 +803,59 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * A.NG + g) * 16 + br]);
                     const float delta = xi ? -1.0f : 1.0f;
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
-                    const float prior = __fmul_rn(A.lambda, float((ne - ns) - 2 * unlike));
-                    const float dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), __uint_as_float(m1.y)), prior);
+                    const float prior = __fmul_rn(A.lambda, float(ne - 2 * unlike));
+                    dE = __fadd_rn(__fadd_rn(__fmul_rn(delta, t), __uint_as_float(m1.y)), prior);
                     flip = (dE <= 0.0f || uphill_accept(u53, double(dE), T, inv_T)) ? 1 : 0;
                 }
                 const unsigned amask = __ballot_sync(kFull, flip) & 0xFFFFu;
-                if (amask) {
-                    if ((amask >> br) & 1u) {
-                        const int rs = int(m0.x) - c1.x, re = rs + int(m0.y);
-                        for (int e = rs + half; e < re; e += 2) {
-                            const uint4 en = St.ent[e];
-                            const float wa = __uint_as_float(en.z);
-                            atomicAdd(&A.rw[size_t(en.x) * RP + 16 * g + br], xi ? -wa : wa);
-                        }
-                    }
-                    if (lane == 0) {
+                if (lane == 0) {
+                    s_amask[k * A.NG + g] = amask;
+                    if (amask) {
                         __stcg(&A.xb[size_t(i) * A.NG + g], xw ^ amask);
                         my_accepts += unsigned(__popc(amask));
+                    }
+                }
+                if (A.trace && flip) atomicAdd(&s_trace[branch], double(dE));
+            }
+            __syncthreads();
+            // the sweep's tracked energy change, once per CTA per sweep
+            if (A.trace && ci == n_chunks - 1 && tid < A.R) {
+                atomicAdd(&A.trace[size_t(tid) * A.sweeps + sweep], s_trace[tid]);
+                s_trace[tid] = 0.0;
+            }
+            // C. the flipped branches' residuals: rho += delta a' (TwoSum)
+            for (int it = warp; it < nseg_items; it += kWarps) {
+                const int sg = it / A.NG, g = it % A.NG;
+                const int k = s_segbit[sg];
+                const uint32_t amask = s_amask[k * A.NG + g];
+                if (!amask) continue;   // warp-uniform
+                const bool mine = (amask >> br) & 1u;
+                const float dl = ((s_xw[k * A.NG + g] >> br) & 1u) ? -1.0f : 1.0f;
+                const uint4 m0 = St.meta[2 * k];
+                const int seg_in_bit = sg - int(St.meta[2 * k + 1].w);
+                const int rs = int(m0.x) - c1.x + seg_in_bit * kSeg;
+                const int re = min(int(m0.x) - c1.x + int(m0.y), rs + kSeg);
+                float2 cur[kSeg / 2];
+                if (it == held_it) {
+#pragma unroll
+                    for (int u = 0; u < kSeg / 2; ++u) cur[u] = held[u];
+                } else {
+#pragma unroll
+                    for (int u = 0; u < kSeg / 2; ++u) {
+                        const int e = rs + half + 2 * u;
+                        cur[u] = mine && e < re ? __ldcg(&A.rp[size_t(St.ent[e].x & kRayMask) * RP + 16 * g + br])
+                                                : make_float2(0.0f, 0.0f);
+                    }
+                }
+                if (mine) {
+#pragma unroll
+                    for (int u = 0; u < kSeg / 2; ++u) {
+                        const int e = rs + half + 2 * u;
+                        if (e < re) {
+                            const uint2 en = St.ent[e];
+                            __stcg(&A.rp[size_t(en.x & kRayMask) * RP + 16 * g + br],
+                                   two_sum_add(cur[u], __fmul_rn(dl, __uint_as_float(en.y))));
+                        }
                     }
                 }
             }
@@ -769,7 +873,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 // arrive, make the next chunk's draws while the others arrive, then wait
                 grid_arrive(A.bar);
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
-                ok = grid_wait(A.bar, A.err, ++round);
+                ok = grid_wait(A.bar, A.err, ++round, per_round, A.spin_limit);
             } else {
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
@@ -794,6 +898,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             const int i = int(k % A.n), b = int(k / A.n);
             A.x_out[size_t(b) * A.n + A.order[i]] = uint8_t((__ldcg(&A.xb[size_t(i) * A.NG + (b >> 4)]) >> (b & 15)) & 1u);
         }
+    } else if (tid == 0 && A.status) {
+        *reinterpret_cast<volatile int*>(A.status) = int(QB_ETIMEDOUT);
     }
     if (lane == 0 && my_accepts) atomicAdd(&s_acc_count, my_accepts);
     __syncthreads();
@@ -909,6 +1015,7 @@ qb_status launch_ising_anneal(const IsingPlan& p, const SolveBuffers& b, int R, 
     A.x_out = b.x;
     A.f_out = b.f;
     A.e_out = b.e_i64;
+    A.trace = reinterpret_cast<long long*>(b.trace);
     int max_deg = 0;
     for (int i = 0; i < p.n; ++i) max_deg = std::max(max_deg, p.row[size_t(i) + 1] - p.row[size_t(i)]);
     A.wide = max_deg >= kWideRow ? 1 : 0;
@@ -948,12 +1055,12 @@ qb_status launch_ising_energies(const IsingPlan& p, const uint8_t* x, int K, lon
 }
 
 size_t resid_stage_bytes() {
-    return size_t(kChunkB) * 8 + size_t(kChunkE) * 4 + size_t(kChunkB + 1) * 8 + size_t(kChunkB) * 8 + size_t(kChunkN);
+    return size_t(kChunkB) * 8 + size_t(kChunkE) * 8 + size_t(kChunkB + 1) * 8 + size_t(kChunkB) * 8 + size_t(kChunkN);
 }
 
 size_t resid_smem_bytes(const ResidualPlan& p) {
     const size_t words = (size_t(p.bit_slots) + 31) / 32;
-    return resid_stage_bytes() + size_t(p.ray_slots) * 4 + words * 4;
+    return resid_stage_bytes() + size_t(p.ray_slots) * 8 + words * 4;
 }
 
 int resid_chunk_bits() { return kChunkB; }
@@ -1007,7 +1114,7 @@ qb_status launch_resid_anneal(const ResidualPlan& p, const SolveBuffers& b, int 
     A.chunks = p.d_chunks.as<int4>();
     A.chunk_ptr = p.d_chunk_ptr.as<int32_t>();
     A.row = p.d_row.as<int32_t>();
-    A.ent = p.d_ent.as<uint4>();
+    A.ent = p.d_ent.as<uint2>();
     A.lin = p.d_lin.as<float>();
     A.q = p.d_q.as<float>();
     A.nbr_ptr = p.d_nbr_ptr.as<int32_t>();
@@ -1022,6 +1129,7 @@ qb_status launch_resid_anneal(const ResidualPlan& p, const SolveBuffers& b, int 
     A.x_out = b.x;
     A.drift = b.drift;
     A.accepts = b.accepts;
+    A.trace = b.trace;
     const size_t smem = resid_smem_bytes(p);
     // QB_PHASE_TIMES: per-CTA clock64 sums of the gather, score and barrier
     // phases, printed to stderr after the launch (diagnostics; same work)
@@ -1070,8 +1178,8 @@ qb_status resid_check_fit(const ResidualPlan& p) {
 }
 
 size_t resid_lockstep_smem(int NG) {
-    return 2 * (size_t(kLockE) * 16 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + (NG == 1 ? 2 * size_t(kLockB) * 16 * 8 : 0) +
-           size_t(kLockSegs) * NG * 16 * 4 + size_t(kLockB) * NG * (4 + 16);
+    return 2 * (size_t(kLockE) * 8 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + (NG == 1 ? 2 * size_t(kLockB) * 16 * 8 : 0) +
+           size_t(kLockSegs) * NG * 16 * 4 + size_t(kLockB) * NG * (4 + 4 + 16) + size_t(kLockSegs) * 4;
 }
 // The largest of those over the branch-group counts one launch serves.
 size_t resid_lockstep_smem_max() {
@@ -1104,7 +1212,20 @@ int resid_lockstep_grid() {
 
 size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
     const int NG = (R + 15) / 16;
-    return size_t(p.n_rays) * 16 * NG * 4 + size_t(p.n) * NG * 4 + 64;
+    return size_t(p.n_rays) * 16 * NG * 8 + size_t(p.n) * NG * 4 + 64;
+}
+
+// QB_TEST_BARRIER_STALL=k (tests only): every grid barrier of the lockstep
+// sweep also waits for one arrival that never comes and gives up after k
+// polls, so the timeout path runs to its status without a fault or a hang.
+void lock_barrier_settings(ResidLockArgs& A) {
+    A.bar_extra = 0;
+    A.spin_limit = kSpinLimit;
+    const char* v = std::getenv("QB_TEST_BARRIER_STALL");
+    if (v && std::atoi(v) > 0) {
+        A.bar_extra = 1;
+        A.spin_limit = unsigned(std::atoi(v));
+    }
 }
 
 
@@ -1121,7 +1242,7 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     A.seed0 = seed0;
     A.chunks = p.d_chunks.as<int4>();
     A.chunk_ptr = p.d_chunk_ptr.as<int32_t>();
-    A.ent = p.d_ent.as<uint4>();
+    A.ent = p.d_ent.as<uint2>();
     A.meta = p.d_meta.as<uint4>();
     A.nbr = p.d_nbr_new.as<int32_t>();
     A.order = p.d_order.as<int32_t>();
@@ -1131,15 +1252,17 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     A.rbit = p.d_rbit_new.as<int32_t>();
     A.ra = p.d_ra.as<float>();
     A.temp = b.temp;
-    // scratch: control block (barrier counter, timeout flag at +16), residuals, bit words
+    // scratch: control block (barrier counter, timeout flag at +16), residual pairs, bit words
     char* sc = static_cast<char*>(b.scratch);
     A.bar = reinterpret_cast<unsigned*>(sc);
     A.err = reinterpret_cast<int*>(sc + 16);
-    A.rw = reinterpret_cast<float*>(sc + 64);
-    A.xb = reinterpret_cast<uint32_t*>(sc + 64 + size_t(p.n_rays) * 16 * A.NG * 4);
+    A.rp = reinterpret_cast<float2*>(sc + 64);
+    A.xb = reinterpret_cast<uint32_t*>(sc + 64 + size_t(p.n_rays) * 16 * A.NG * 8);
     A.x_out = b.x;
     A.drift = b.drift;
     A.accepts = b.accepts;
+    A.trace = b.trace;
+    lock_barrier_settings(A);
     // the barrier counter restarts per launch; the timeout flag (+16) is
     // zeroed once per solve by the caller, so a timeout of any launch shows
     QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));
@@ -1263,84 +1386,92 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace qb
 
 extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
-                                               uint64_t seed_offset, uint8_t* x_out, void* stream) {
+                                               uint64_t seed_offset, uint8_t* x_out, int32_t* status, void* stream) {
     using namespace qb;
-    if (!p || !s || !x_out) return fail(QB_EINVAL, "qb_solve_residual_noalloc: null argument");
-    if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_solve_residual_noalloc: residual problems only");
-    const ResidualPlan& P = p->resid;
-    if (P.variant != QB_RESID_LOCKSTEP || P.lock_grid < 1)
-        return fail(QB_ENOTSUP, "qb_solve_residual_noalloc: the problem is not planned for the lockstep sweep");
-    if (!p->uploaded) return fail(QB_EINVAL, "qb_solve_residual_noalloc: the problem is not on the device (deferred upload)");
-    const int R = int(n_branches);
-    if (n_branches < 1 || R > 16 * kLockMaxNG)
-        return fail(QB_EINVAL, "qb_solve_residual_noalloc: n_branches must be in [1, 64]");
-    if (s->anneal_sweeps < 0 || s->hold_sweeps < 0 || s->anneal_sweeps + s->hold_sweeps < 1 || !(s->t_hot > 0.0) ||
-        !(s->t_cold > 0.0) || s->refresh_sweeps < 0)
-        return fail(QB_EINVAL, "qb_solve_residual_noalloc: bad schedule");
-    const int sweeps = s->anneal_sweeps + s->hold_sweeps;
-    const int NG = (R + 15) / 16;
-    // scratch layout: residuals | bit words | barrier counter + error flag |
-    // temperatures | drift | accepts
-    const size_t off_xb = align256(size_t(P.n_rays) * 16 * NG * 4);
-    const size_t off_bar = off_xb + align256(size_t(P.n) * NG * 4);
-    const size_t off_temp = off_bar + 256;
-    const size_t off_drift = off_temp + align256(size_t(sweeps) * 8);
-    const size_t off_acc = off_drift + align256(size_t(R) * 4);
-    const size_t need = off_acc + 256;
-    if (need > QB_NOALLOC_SCRATCH_BYTES) {
-        char msg[256];
-        std::snprintf(msg, sizeof msg,
-                      "qb_solve_residual_noalloc: %zu bytes of scratch needed, the static scratch holds %zu "
-                      "(fewer rays, bits, branches or sweeps; or use qb_solve)",
-                      need, size_t(QB_NOALLOC_SCRATCH_BYTES));
-        return fail(QB_ENOMEM, msg);
-    }
-    QB_CUDA(cudaSetDevice(p->device));
-    unsigned char* base = nullptr;
-    qb_status st = noalloc_scratch(p->device, &base);
-    if (st != QB_OK) return st;
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    const std::vector<double> temp = temperatures(*s);
-    QB_CUDA(cudaMemcpyAsync(base + off_temp, temp.data(), temp.size() * 8, cudaMemcpyHostToDevice, cs));
-    QB_CUDA(cudaMemsetAsync(base + off_bar, 0, 256, cs));
-    QB_CUDA(cudaMemsetAsync(base + off_drift, 0, size_t(R) * 4, cs));
-    QB_CUDA(cudaMemsetAsync(base + off_acc, 0, 8, cs));
-    ResidLockArgs A{};
-    A.n = P.n;
-    A.n_rays = P.n_rays;
-    A.sweeps = sweeps;
-    A.refresh = s->refresh_sweeps;
-    A.R = R;
-    A.NG = NG;
-    A.lambda = float(P.lambda);
-    A.seed0 = 1 + seed_offset;
-    A.chunks = P.d_chunks.as<int4>();
-    A.chunk_ptr = P.d_chunk_ptr.as<int32_t>();
-    A.ent = P.d_ent.as<uint4>();
-    A.meta = P.d_meta.as<uint4>();
-    A.nbr = P.d_nbr_new.as<int32_t>();
-    A.order = P.d_order.as<int32_t>();
-    A.d = P.d_d.as<double>();
-    A.w64 = P.d_w64.as<double>();
-    A.rrow = P.d_rrow.as<int32_t>();
-    A.rbit = P.d_rbit_new.as<int32_t>();
-    A.ra = P.d_ra.as<float>();
-    A.temp = reinterpret_cast<const double*>(base + off_temp);
-    A.rw = reinterpret_cast<float*>(base);
-    A.xb = reinterpret_cast<uint32_t*>(base + off_xb);
-    A.bar = reinterpret_cast<unsigned*>(base + off_bar);
-    A.err = reinterpret_cast<int*>(base + off_bar + 16);
-    A.x_out = x_out;
-    A.drift = reinterpret_cast<float*>(base + off_drift);
-    A.accepts = reinterpret_cast<unsigned long long*>(base + off_acc);
-    A.phase = nullptr;
-    QB_CUDA(cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(resid_lockstep_smem_max())));
-    void* args[] = {&A};
-    QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resid_lockstep_kernel<false>), dim3(unsigned(P.lock_grid)),
-                                        dim3(kLockThreads), args, resid_lockstep_smem(A.NG), cs));
-    return QB_OK;
+    return guarded("qb_solve_residual_noalloc", [&]() -> qb_status {
+        if (!p || !s || !x_out || !status) return fail(QB_EINVAL, "qb_solve_residual_noalloc: null argument");
+        if (p->kind != QB_KIND_RESIDUAL) return fail(QB_EINVAL, "qb_solve_residual_noalloc: residual problems only");
+        const ResidualPlan& P = p->resid;
+        if (P.variant != QB_RESID_LOCKSTEP || P.lock_grid < 1)
+            return fail(QB_ENOTSUP, "qb_solve_residual_noalloc: the problem is not planned for the lockstep sweep");
+        if (!p->uploaded)
+            return fail(QB_EINVAL, "qb_solve_residual_noalloc: the problem is not on the device (deferred upload)");
+        const int R = int(n_branches);
+        if (n_branches < 1 || R > 16 * kLockMaxNG)
+            return fail(QB_EINVAL, "qb_solve_residual_noalloc: n_branches must be in [1, 64]");
+        if (s->anneal_sweeps < 0 || s->hold_sweeps < 0 || s->anneal_sweeps + s->hold_sweeps < 1 || !(s->t_hot > 0.0) ||
+            !(s->t_cold > 0.0) || s->refresh_sweeps < 0)
+            return fail(QB_EINVAL, "qb_solve_residual_noalloc: bad schedule");
+        const int sweeps = s->anneal_sweeps + s->hold_sweeps;
+        const int NG = (R + 15) / 16;
+        // scratch layout: residual pairs | bit words | barrier counter + error
+        // flag | temperatures | drift | accepts
+        const size_t off_xb = align256(size_t(P.n_rays) * 16 * NG * 8);
+        const size_t off_bar = off_xb + align256(size_t(P.n) * NG * 4);
+        const size_t off_temp = off_bar + 256;
+        const size_t off_drift = off_temp + align256(size_t(sweeps) * 8);
+        const size_t off_acc = off_drift + align256(size_t(R) * 4);
+        const size_t need = off_acc + 256;
+        if (need > QB_NOALLOC_SCRATCH_BYTES) {
+            char msg[256];
+            std::snprintf(msg, sizeof msg,
+                          "qb_solve_residual_noalloc: %zu bytes of scratch needed, the static scratch holds %zu "
+                          "(fewer rays, bits, branches or sweeps; or use qb_solve)",
+                          need, size_t(QB_NOALLOC_SCRATCH_BYTES));
+            return fail(QB_ENOMEM, msg);
+        }
+        QB_CUDA(cudaSetDevice(p->device));
+        unsigned char* base = nullptr;
+        qb_status st = noalloc_scratch(p->device, &base);
+        if (st != QB_OK) return st;
+        cudaStream_t cs = static_cast<cudaStream_t>(stream);
+        // the table is copied from pageable memory: the copy has taken the
+        // bytes by the time the call returns, so the vector may go
+        const std::vector<double> temp = temperatures(*s);
+        QB_CUDA(cudaMemcpyAsync(base + off_temp, temp.data(), temp.size() * 8, cudaMemcpyHostToDevice, cs));
+        QB_CUDA(cudaMemsetAsync(base + off_bar, 0, 256, cs));
+        QB_CUDA(cudaMemsetAsync(base + off_drift, 0, size_t(R) * 4, cs));
+        QB_CUDA(cudaMemsetAsync(base + off_acc, 0, 8, cs));
+        QB_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t), cs));   // QB_OK unless a barrier times out
+        ResidLockArgs A{};
+        A.n = P.n;
+        A.n_rays = P.n_rays;
+        A.sweeps = sweeps;
+        A.refresh = s->refresh_sweeps;
+        A.R = R;
+        A.NG = NG;
+        A.lambda = float(P.lambda);
+        A.seed0 = 1 + seed_offset;
+        A.chunks = P.d_chunks.as<int4>();
+        A.chunk_ptr = P.d_chunk_ptr.as<int32_t>();
+        A.ent = P.d_ent.as<uint2>();
+        A.meta = P.d_meta.as<uint4>();
+        A.nbr = P.d_nbr_new.as<int32_t>();
+        A.order = P.d_order.as<int32_t>();
+        A.d = P.d_d.as<double>();
+        A.w64 = P.d_w64.as<double>();
+        A.rrow = P.d_rrow.as<int32_t>();
+        A.rbit = P.d_rbit_new.as<int32_t>();
+        A.ra = P.d_ra.as<float>();
+        A.temp = reinterpret_cast<const double*>(base + off_temp);
+        A.rp = reinterpret_cast<float2*>(base);
+        A.xb = reinterpret_cast<uint32_t*>(base + off_xb);
+        A.bar = reinterpret_cast<unsigned*>(base + off_bar);
+        A.err = reinterpret_cast<int*>(base + off_bar + 16);
+        A.status = status;
+        A.x_out = x_out;
+        A.drift = reinterpret_cast<float*>(base + off_drift);
+        A.accepts = reinterpret_cast<unsigned long long*>(base + off_acc);
+        A.trace = nullptr;
+        A.phase = nullptr;
+        lock_barrier_settings(A);
+        QB_CUDA(cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(resid_lockstep_smem_max())));
+        void* args[] = {&A};
+        QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resid_lockstep_kernel<false>),
+                                            dim3(unsigned(P.lock_grid)), dim3(kLockThreads), args,
+                                            resid_lockstep_smem(A.NG), cs));
+        return QB_OK;
+    });
 }
 
-namespace qb {
-}  // namespace qb

@@ -22,6 +22,7 @@ struct SolveBuffers {
     const double* temp = nullptr;
     float* drift = nullptr;      // R
     unsigned long long* accepts = nullptr;   // R accepted flips (residual)
+    double* trace = nullptr;     // R x sweeps per-sweep sums of accepted dE (zeroed), or null: no trace
     void* scratch = nullptr;     // ising: R x n x 5 bytes when the state does not fit on chip
 };
 

@@ -63,6 +63,7 @@ struct QuboArgs {
     float* drift;                  // R
     double* e_track;               // R: sum of accepted dE (E - offset)
     unsigned long long* accepts;   // R
+    double* trace;                 // nullable: R x sweeps, the sum of accepted dE of each sweep
 };
 
 // 32 x 32 bit transpose across the warp: lane p returns the word whose bit q
@@ -99,6 +100,9 @@ __global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A)
     float eh0 = 0.0f, el0 = 0.0f, eh1 = 0.0f, el1 = 0.0f;
     unsigned long long acc_a = 0, acc_b = 0;
     float dr0 = 0.0f, dr1 = 0.0f;
+    double tr0 = 0.0, tr1 = 0.0;   // this sweep's accepted dE (traced solves)
+    __shared__ double s_tr[64];
+    if (threadIdx.x < 64) s_tr[threadIdx.x] = 0.0;
     unsigned round = 0;
 
     for (int j = gw; j < A.n; j += tw) {
@@ -216,16 +220,28 @@ __global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A)
                 }
                 if (acc0) {
                     two_sum_acc(eh0, el0, dE0);
+                    tr0 += double(dE0);
                     ++acc_a;
                 }
                 if (acc1) {
                     two_sum_acc(eh1, el1, dE1);
+                    tr1 += double(dE1);
                     ++acc_b;
                 }
                 A.L[base + r0] = make_float2(hi0, lo0);
                 A.L[base + r1] = make_float2(hi1, lo1);
             }
             ok = grid_barrier(A.bar, A.err, ++round);
+        }
+        if (A.trace) {   // the sweep's accepted dE: lanes -> shared memory -> one add per CTA and replica
+            if (has0 && tr0 != 0.0) atomicAdd(&s_tr[r0], tr0);
+            if (has1 && tr1 != 0.0) atomicAdd(&s_tr[r1], tr1);
+            tr0 = tr1 = 0.0;
+            __syncthreads();
+            if (int(threadIdx.x) < A.R) {
+                if (s_tr[threadIdx.x] != 0.0) atomicAdd(&A.trace[size_t(threadIdx.x) * A.sweeps + sweep], s_tr[threadIdx.x]);
+                s_tr[threadIdx.x] = 0.0;
+            }
         }
     }
     if (ok) {
@@ -314,6 +330,7 @@ qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, i
     A.x_out = b.x;
     A.drift = b.drift;
     A.e_track = b.e_track;
+    A.trace = b.trace;
     A.accepts = b.accepts;
     QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));   // the timeout flag is zeroed once per solve by the caller
     void* args[] = {&A};

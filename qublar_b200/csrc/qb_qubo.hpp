@@ -15,6 +15,7 @@ struct QuboBuffers {
     float* drift = nullptr;                  // R
     double* e_track = nullptr;               // R (zeroed by the caller)
     unsigned long long* accepts = nullptr;   // R (zeroed by the caller)
+    double* trace = nullptr;                 // R x sweeps per-sweep sums of accepted dE (zeroed), or null
     void* scratch = nullptr;                 // qubo_scratch bytes
 };
 

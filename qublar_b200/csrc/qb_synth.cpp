@@ -333,7 +333,12 @@ qb_status synth_tomography(const qb_tomo_params* p, bool on_device, const qb_opt
     std::vector<BinMarch> bins;
     std::vector<int32_t> e_bit;
     std::vector<float> e_a;
+#ifdef QB_SYNTH_HOST_ONLY   // the host-only build of the builder (no device march linked in)
+    qb_status ms = on_device ? qb::fail(QB_ENOTSUP, "qb_synth_tomography_device: host-only build")
+                             : march_host(M, bins, e_bit, e_a);
+#else
     qb_status ms = on_device ? qb::synth_march_device(M, opts, bins, e_bit, e_a) : march_host(M, bins, e_bit, e_a);
+#endif
     if (ms != QB_OK) {
         delete t;
         return ms;

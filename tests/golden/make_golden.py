@@ -1,8 +1,9 @@
 """Writes the golden fixtures of tests/golden from the reference.
 
-Run in a checkout where the reference tree is present (QUBLAR_REFERENCE,
-default /root/reference) and oracle/_ref/libqbref.so has been built from it
-(``make -C oracle``). Two kinds of fixtures:
+Run in a checkout where the reference tree is present, with
+QUBLAR_REFERENCE naming its root, after oracle/_ref/libqbref.so has been
+built from it (``make -C oracle REF=$QUBLAR_REFERENCE``). Two kinds of
+fixtures:
 
 * ree_qubo.json -- the reference's committed REE sequencing QUBOs (six
   instances), its brute-force minima, its engine_check maxima and its per-seed
@@ -12,12 +13,17 @@ default /root/reference) and oracle/_ref/libqbref.so has been built from it
 * ref_runs.npz -- outputs of the reference's own annealers run here through
   oracle/_ref: wising::anneal on the 800-node ER Max-Cut instance and
   anneal_branch on the small pyramid, 64 seeds each (final energies, per-sweep
-  energy traces, per-bit void fractions).
+  energy traces, per-bit void fractions);
+* ref_pyramid.npz -- anneal_branch of the reference on the benchmark pyramid
+  (306,328 bits, 75,594 rays), seeds 1..64 with the posterior schedule (T 50
+  -> 1 over 200 sweeps, 50 held): per-bit counts of branches with x = 1, final
+  energies, and the mean and variance of the per-sweep energy traces.
 """
 import csv
 import json
 import os
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -26,7 +32,7 @@ sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 from qublar_b200 import synth  # noqa: E402
 
-REF = os.environ.get("QUBLAR_REFERENCE", "/root/reference")
+REF = os.environ.get("QUBLAR_REFERENCE")
 OUT = os.path.dirname(os.path.abspath(__file__))
 REE_IDS = ["MP_P507-A", "MP_P507-B", "R4_0", "R5_0", "R8_3", "R12_0"]
 SEEDS = 64
@@ -110,9 +116,32 @@ def ref_runs():
     np.savez_compressed(os.path.join(OUT, "ref_runs.npz"), **res)
 
 
+def ref_pyramid():
+    a = synth.tomography()
+    rp = O.RefProblem(a)
+
+    def one(seed):   # the ctypes call releases the GIL: the seeds run side by side
+        return rp.trace(50.0, 1.0, 200, 50, seed)
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 8) as ex:
+        runs = list(ex.map(one, range(1, SEEDS + 1)))
+    X = np.array([x for x, _ in runs], np.uint8)
+    T = np.array([t for _, t in runs])
+    np.savez_compressed(os.path.join(OUT, "ref_pyramid.npz"), counts=X.sum(0).astype(np.uint8),
+                        energy=T[:, -1].copy(), trace_mean=T.mean(0), trace_var=T.var(0, ddof=1),
+                        n=np.int64(X.shape[1]), branches=np.int64(SEEDS))
+
+
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        sys.exit("make_golden.py: set QUBLAR_REFERENCE to the root of the reference tree")
+    if "--pyramid-only" in sys.argv:
+        ref_pyramid()
+        print("golden fixtures written to", OUT)
+        sys.exit(0)
     ree()
     ree_text()
     if "--no-runs" not in sys.argv:   # the reference's annealer runs take minutes
         ref_runs()
+        ref_pyramid()
     print("golden fixtures written to", OUT)

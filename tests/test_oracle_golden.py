@@ -317,3 +317,17 @@ def test_roi_qubo_equals_the_reference_and_the_full_energy():
         xf[roi] = xr
         eq = float(h @ xr + xr @ np.triu(J, 1) @ xr)
         assert abs((O.binary_energy(a, xf) - e0) - eq) < 1e-6 * max(1.0, abs(e0))
+
+
+def test_oracle_side_builder_equals_the_package_builder():
+    """oracle/libqb_inputs.so (the pyramid builder compiled on its own, host
+    code only, for the legs that must not load the solver library) gives the
+    arrays of qublar_b200.synth.tomography byte for byte: the benchmark
+    pyramid and a small one."""
+    from qublar_b200 import synth
+    for params in (None, synth.small_tomo_params()):
+        a = synth.tomography(params)
+        b = O.tomography(params)
+        for k in ("d", "w", "row_ptr", "ray", "a", "nbr_ptr", "nbr"):
+            assert a[k].dtype == b[k].dtype and a[k].tobytes() == b[k].tobytes(), k
+        assert a["lambda"] == b["lambda"] and a["kappa"] == b["kappa"]
