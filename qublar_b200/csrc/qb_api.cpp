@@ -701,6 +701,10 @@ qb_status plan_residual(const qb_residual_desc* d, ResidualPlan& P, int lock_sli
     return QB_OK;
 }
 
+// Bytes after the last bit-ray entry: the cluster sweep's bulk L2 prefetch
+// moves whole 16-byte entry pairs and may reach one entry past the end.
+constexpr size_t kEntPad = 16;
+
 // Device bytes upload_residual will take.
 int64_t residual_device_bytes(const ResidualPlan& P) {
     const int64_t n = P.n, nr = P.n_rays, nnz = P.nnz;
@@ -719,7 +723,8 @@ static void host_build_residual(const ResidualPlan& P, const qb_residual_desc* d
                                 RawVec<int32_t>& rbit_n, RawVec<float>& ra) {
     const int n = P.n, nr = P.n_rays;
     const Colouring& C = P.col;
-    ent.resize(size_t(P.nnz) * 2);
+    ent.resize(size_t(P.nnz) * 2 + kEntPad / 4);
+    for (size_t k = size_t(P.nnz) * 2; k < ent.size(); ++k) ent[k] = 0u;
 #pragma omp parallel for schedule(static, 1024)
     for (int k = 0; k < n; ++k) {
         const int i = C.order[size_t(k)];
@@ -807,7 +812,7 @@ qb_status upload_residual(ResidualPlan& P, const qb_residual_desc* d, cudaStream
         if ((s = upload_vec(P.d_row, P.h_row, st))) return s;
         if ((s = upload_vec(P.d_order, C.order, st))) return s;
         if ((s = upload(P.d_w64, d->w, size_t(nr) * 8, st))) return s;
-        if ((s = P.d_ent.alloc(size_t(P.nnz) * 8))) return s;
+        if ((s = P.d_ent.alloc(size_t(P.nnz) * 8 + kEntPad))) return s;
         if ((s = P.d_rrow.alloc((size_t(nr) + 1) * 4))) return s;
         if ((s = P.d_o_rbit.alloc(size_t(P.nnz) * 4))) return s;
         if ((s = P.d_rbit.alloc(size_t(P.nnz) * 4))) return s;

@@ -411,9 +411,13 @@ __global__ void __launch_bounds__(kResidThreads, 2) resid_anneal_kernel(ResidArg
             const int nb = c0.y - c0.x;
             if (PHASES) t_ph = clock64();
             if (tid == 0) {   // the next chunk's entries into L2
+                // a bulk prefetch starts on a 16-byte boundary and moves a
+                // multiple of 16 bytes: whole entry pairs (the table carries
+                // one spare pair at its end)
                 const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
                 const int4 c1n = chunks[2 * nx + 1];
-                if (c1n.y > c1n.x) prefetch_l2(&A.ent[c1n.x], uint32_t(c1n.y - c1n.x) * 8u);
+                const int p0 = c1n.x & ~1, p1 = (c1n.y + 1) & ~1;
+                if (c1n.y > c1n.x) prefetch_l2(&A.ent[p0], uint32_t(p1 - p0) * 8u);
             }
             // 1. gather
             for (int k = tid; k <= nb; k += kResidThreads) {
@@ -553,6 +557,7 @@ struct ResidLockArgs {
     int* status;                // nullable: set to QB_ETIMEDOUT when a barrier times out
     unsigned bar_extra;         // arrivals a barrier round waits for beyond the grid (0; test hook)
     unsigned spin_limit;        // polls of a barrier before it gives up
+    int bar_ways;               // barrier counters the arrivals are spread over (grid_arrive_ways)
     uint8_t* x_out;
     float* drift;
     unsigned long long* accepts;
@@ -660,7 +665,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0));
     cp_async_commit();
     if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
-    bool ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
+    grid_arrive_ways(A.bar, A.bar_ways);
+    bool ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
     int4 cur0 = make_int4(0, 0, 0, 0), cur1 = make_int4(0, 0, 0, 0);   // descriptor of the chunk in hand
     if (n_chunks > 0) {
@@ -686,7 +692,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (dv > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[j]), __float_as_int(dv));
                 __stcg(&A.rp[k], split_pair(v));
             }
-            ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
+            grid_arrive_ways(A.bar, A.bar_ways);
+            ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
             if (!ok) break;
         }
         const double T = A.temp[sweep];
@@ -707,6 +714,10 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 t_ph = t1;
             }
             const LockStage St = stage(gci & 1);
+            // the other buffer was last read by the previous chunk, which every
+            // thread has finished: stage the next chunk into it now
+            lock_stage(A, cn0, cn1, stage((gci + 1) & 1));
+            cp_async_commit();
             const int nb = c0.y - c0.x;
             const int nseg = c0.z;                       // segments of the chunk
             if (PHASES) t_a = clock64();
@@ -799,8 +810,17 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
                     const int s0 = int(m1.w);
+                    // the segment sums in order; eight loads at a time so the adds
+                    // wait on one shared-memory round trip per eight segments
                     float h = 0.0f;
-                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * A.NG + g) * 16 + br]);
+                    for (int q0 = 0; q0 < nsg; q0 += 8) {
+                        float v[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) v[u] = q0 + u < nsg ? hseg[((s0 + q0 + u) * A.NG + g) * 16 + br] : 0.0f;
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            if (q0 + u < nsg) h = __fadd_rn(h, v[u]);
+                    }
                     const float delta = xi ? -1.0f : 1.0f;
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
                     const float prior = __fmul_rn(A.lambda, float(ne - 2 * unlike));
@@ -859,10 +879,13 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     }
                 }
             }
-            __syncthreads();   // the other buffer is free: stage the next chunk under the barrier
-            if (PHASES) ph_b += clock64() - t_a;
-            lock_stage(A, cn0, cn1, stage((gci + 1) & 1));
-            cp_async_commit();
+            // no barrier here: the next chunk's first barrier (or the grid
+            // barrier's) orders this chunk's shared-memory reads before the
+            // next chunk's writes
+            if (PHASES) {
+                __syncthreads();
+                ph_b += clock64() - t_a;
+            }
             if (PHASES) {
                 const long long t1 = clock64();
                 ph_items += t1 - t_ph;
@@ -871,9 +894,9 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             const int sweep_n = nx == 0 ? sweep + 1 : sweep;
             if (c0.w & 1) {
                 // arrive, make the next chunk's draws while the others arrive, then wait
-                grid_arrive(A.bar);
+                grid_arrive_ways(A.bar, A.bar_ways);
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
-                ok = grid_wait(A.bar, A.err, ++round, per_round, A.spin_limit);
+                ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
             } else {
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
@@ -1210,9 +1233,14 @@ int resid_lockstep_grid() {
     return per_sm >= 1 ? sms : 0;
 }
 
+// The scratch of a lockstep solve starts with a control block: the barrier
+// counters (kMaxWays of them, kWayStride bytes apart) and, at +16, the
+// timeout flag.
+constexpr size_t kLockCtl = size_t(kMaxWays) * kWayStride;
+
 size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
     const int NG = (R + 15) / 16;
-    return size_t(p.n_rays) * 16 * NG * 8 + size_t(p.n) * NG * 4 + 64;
+    return size_t(p.n_rays) * 16 * NG * 8 + size_t(p.n) * NG * 4 + kLockCtl;
 }
 
 // QB_TEST_BARRIER_STALL=k (tests only): every grid barrier of the lockstep
@@ -1221,6 +1249,9 @@ size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
 void lock_barrier_settings(ResidLockArgs& A) {
     A.bar_extra = 0;
     A.spin_limit = kSpinLimit;
+    // QB_BARRIER_WAYS=k: spread the barrier's arrivals over k counters
+    A.bar_ways = 1;
+    if (const char* w = std::getenv("QB_BARRIER_WAYS")) A.bar_ways = std::min(kMaxWays, std::max(1, std::atoi(w)));
     const char* v = std::getenv("QB_TEST_BARRIER_STALL");
     if (v && std::atoi(v) > 0) {
         A.bar_extra = 1;
@@ -1256,16 +1287,17 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     char* sc = static_cast<char*>(b.scratch);
     A.bar = reinterpret_cast<unsigned*>(sc);
     A.err = reinterpret_cast<int*>(sc + 16);
-    A.rp = reinterpret_cast<float2*>(sc + 64);
-    A.xb = reinterpret_cast<uint32_t*>(sc + 64 + size_t(p.n_rays) * 16 * A.NG * 8);
+    A.rp = reinterpret_cast<float2*>(sc + kLockCtl);
+    A.xb = reinterpret_cast<uint32_t*>(sc + kLockCtl + size_t(p.n_rays) * 16 * A.NG * 8);
     A.x_out = b.x;
     A.drift = b.drift;
     A.accepts = b.accepts;
     A.trace = b.trace;
     lock_barrier_settings(A);
-    // the barrier counter restarts per launch; the timeout flag (+16) is
+    // the barrier counters restart per launch; the timeout flag (+16) is
     // zeroed once per solve by the caller, so a timeout of any launch shows
     QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));
+    QB_CUDA(cudaMemsetAsync(sc + kWayStride, 0, kLockCtl - kWayStride, st));
     const int grid = p.lock_grid;
     if (grid < 1) return fail(QB_ENOTSUP, "residual lockstep sweep: no co-resident grid");
     DevBuf phase;
@@ -1408,7 +1440,7 @@ extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_sch
         // flag | temperatures | drift | accepts
         const size_t off_xb = align256(size_t(P.n_rays) * 16 * NG * 8);
         const size_t off_bar = off_xb + align256(size_t(P.n) * NG * 4);
-        const size_t off_temp = off_bar + 256;
+        const size_t off_temp = off_bar + kLockCtl;
         const size_t off_drift = off_temp + align256(size_t(sweeps) * 8);
         const size_t off_acc = off_drift + align256(size_t(R) * 4);
         const size_t need = off_acc + 256;
@@ -1429,7 +1461,7 @@ extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_sch
         // bytes by the time the call returns, so the vector may go
         const std::vector<double> temp = temperatures(*s);
         QB_CUDA(cudaMemcpyAsync(base + off_temp, temp.data(), temp.size() * 8, cudaMemcpyHostToDevice, cs));
-        QB_CUDA(cudaMemsetAsync(base + off_bar, 0, 256, cs));
+        QB_CUDA(cudaMemsetAsync(base + off_bar, 0, kLockCtl, cs));
         QB_CUDA(cudaMemsetAsync(base + off_drift, 0, size_t(R) * 4, cs));
         QB_CUDA(cudaMemsetAsync(base + off_acc, 0, 8, cs));
         QB_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t), cs));   // QB_OK unless a barrier times out

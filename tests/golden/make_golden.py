@@ -17,7 +17,10 @@ fixtures:
 * ref_pyramid.npz -- anneal_branch of the reference on the benchmark pyramid
   (306,328 bits, 75,594 rays), seeds 1..64 with the posterior schedule (T 50
   -> 1 over 200 sweeps, 50 held): per-bit counts of branches with x = 1, final
-  energies, and the mean and variance of the per-sweep energy traces.
+  energies, and the mean and variance of the per-sweep energy traces; once
+  with the bits in their own order and once relabelled so that the reference
+  visits them in the colour-class order of the GPU sweeps (with the plan's
+  colour of every bit, so a test can tell when the colouring has changed).
 """
 import csv
 import json
@@ -116,8 +119,41 @@ def ref_runs():
     np.savez_compressed(os.path.join(OUT, "ref_runs.npz"), **res)
 
 
-def ref_pyramid():
-    a = synth.tomography()
+def relabel(a: dict, order: np.ndarray) -> dict:
+    """The residual problem with bit k of the result = bit order[k] of `a`:
+    the reference's index-order sweep then visits the bits in `order`."""
+    n = int(a["row_ptr"].size - 1)
+    inv = np.empty(n, np.int64)
+    inv[order] = np.arange(n)
+    deg = np.diff(a["row_ptr"])[order]
+    row = np.concatenate([[0], np.cumsum(deg)]).astype(np.int32)
+    idx = np.concatenate([np.arange(a["row_ptr"][i], a["row_ptr"][i + 1]) for i in order])
+    ndeg = np.diff(a["nbr_ptr"])[order]
+    nrow = np.concatenate([[0], np.cumsum(ndeg)]).astype(np.int32)
+    nidx = np.concatenate([np.arange(a["nbr_ptr"][i], a["nbr_ptr"][i + 1]) for i in order])
+    return {"d": a["d"], "w": a["w"], "row_ptr": row, "ray": a["ray"][idx].copy(), "a": a["a"][idx].copy(),
+            "nbr_ptr": nrow, "nbr": inv[a["nbr"][nidx]].astype(np.int32), "lambda": a["lambda"],
+            "kappa": a["kappa"], "field": None}
+
+
+def colour_of_bits(a: dict):
+    """The plan's colour class of every bit (qb_colour_residual) and its sweep order."""
+    import ctypes as C
+
+    from qublar_b200._abi import lib, ptr
+    n = int(a["row_ptr"].size - 1)
+    d = synth.residual_desc(a)
+    order = np.empty(n, np.int32)
+    cptr = np.empty(n + 1, np.int32)
+    nc = C.c_int32(0)
+    assert lib().qb_colour_residual(C.byref(d), ptr(order), ptr(cptr), C.byref(nc)) == 0
+    colour = np.empty(n, np.int32)
+    for c in range(nc.value):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    return colour, order
+
+
+def _runs(a):
     rp = O.RefProblem(a)
 
     def one(seed):   # the ctypes call releases the GIL: the seeds run side by side
@@ -125,11 +161,24 @@ def ref_pyramid():
 
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 8) as ex:
         runs = list(ex.map(one, range(1, SEEDS + 1)))
-    X = np.array([x for x, _ in runs], np.uint8)
-    T = np.array([t for _, t in runs])
+    return np.array([x for x, _ in runs], np.uint8), np.array([t for _, t in runs])
+
+
+def ref_pyramid():
+    a = synth.tomography()
+    X, T = _runs(a)
+    # the same anneal with the bits relabelled so that the reference visits
+    # them in the colour-class order of the GPU sweeps (classes in order); its
+    # counts are mapped back to the input bit labels
+    colour, order = colour_of_bits(a)
+    Xc, Tc = _runs(relabel(a, order))
+    counts_colour = np.empty(Xc.shape[1], np.uint8)
+    counts_colour[order] = Xc.sum(0).astype(np.uint8)
     np.savez_compressed(os.path.join(OUT, "ref_pyramid.npz"), counts=X.sum(0).astype(np.uint8),
                         energy=T[:, -1].copy(), trace_mean=T.mean(0), trace_var=T.var(0, ddof=1),
-                        n=np.int64(X.shape[1]), branches=np.int64(SEEDS))
+                        counts_colour=counts_colour, energy_colour=Tc[:, -1].copy(),
+                        trace_mean_colour=Tc.mean(0), trace_var_colour=Tc.var(0, ddof=1),
+                        colour=colour, n=np.int64(X.shape[1]), branches=np.int64(SEEDS))
 
 
 if __name__ == "__main__":

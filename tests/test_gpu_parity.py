@@ -287,21 +287,39 @@ def test_device_and_host_assembly_agree(monkeypatch, flags):
     assert (p1 == p2).all()
 
 
+def _colour_of_bits(order, cptr, n):
+    colour = np.empty(n, np.int32)
+    for c in range(cptr.size - 1):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    return colour
+
+
 def test_residual_pyramid_statistical_vs_reference():
     """The benchmark pyramid (306,328 bits, 75,594 rays): 64 branches with the
-    posterior schedule against the reference's anneal_branch over seeds
-    1..64 (tests/golden/ref_pyramid.npz, made by the reference compiled
-    here): per-bit void fractions within binomial error (two-sample z < 5.5
-    at every bit: a Bonferroni bound over the bits), the tri-state map equal
-    except at threshold-straddling bits, the mean final energy within Welch
-    z < 4 and the per-sweep mean energy within Welch z < 4.5 at every sweep."""
+    posterior schedule against the reference's anneal_branch over seeds 1..64
+    (tests/golden/ref_pyramid.npz, made by the reference compiled here).
+
+    The reference sweeps bits in index order, the GPU in colour-class order.
+    On this pyramid 50 sweeps at T = 1 do not mix between the posterior's
+    modes, so the void fractions of some bits depend on the visiting order --
+    the reference's own fractions move by up to z = 9 when only its visiting
+    order changes. The per-bit comparison is therefore made against the
+    reference run on the same problem with its bits relabelled so that it
+    visits them in the plan's colour-class order (the same Markov chain up to
+    the random stream and the arithmetic): fractions within binomial error
+    (two-sample z < 5.5 at every bit, a Bonferroni bound over the bits), the
+    tri-state map equal except at threshold-straddling bits. Mean final
+    energies and per-sweep mean energies agree with both reference runs
+    (Welch z < 4 and < 4.5 at every sweep)."""
     a = synth.tomography()
     P = ResidualProblem.from_arrays(a)
-    r = P.solve(Schedule(), 64, trace=True)
     G = np.load(os.path.join(GOLD, "ref_pyramid.npz"))
     assert int(G["n"]) == P.n and int(G["branches"]) == 64
+    order, cptr = P.colouring()
+    assert (_colour_of_bits(order, cptr, P.n) == G["colour"]).all(), "the colouring changed: regenerate the fixture"
+    r = P.solve(Schedule(), 64, trace=True)
     pg = r.marginals().astype(np.float64)
-    pr = G["counts"].astype(np.float64) / 64
+    pr = G["counts_colour"].astype(np.float64) / 64
     pp = (pg + pr) / 2
     se = np.sqrt(np.maximum(pp * (1 - pp) * 2 / 64, 1e-12))
     z = np.abs(pg - pr) / se
@@ -311,10 +329,12 @@ def test_residual_pyramid_statistical_vs_reference():
     differ = ts_g != ts_r
     straddle = (np.minimum(pg, pr) <= 0.9) & (np.maximum(pg, pr) >= 0.1)
     assert not (differ & ~straddle).any()
-    E, Er = r.energies(), G["energy"]
-    zE = (E.mean() - Er.mean()) / np.sqrt(E.var(ddof=1) / 64 + Er.var(ddof=1) / 64)
-    assert abs(zE) < 4.0, zE
+    E = r.energies()
     T = r.energy_trace()
-    se_t = np.sqrt(T.var(0, ddof=1) / 64 + G["trace_var"] / 64)
-    zt = (T.mean(0) - G["trace_mean"]) / np.maximum(se_t, 1e-300)
-    assert np.abs(zt).max() < 4.5, (np.abs(zt).argmax(), np.abs(zt).max())
+    for suffix in ("", "_colour"):
+        Er = G["energy" + suffix]
+        zE = (E.mean() - Er.mean()) / np.sqrt(E.var(ddof=1) / 64 + Er.var(ddof=1) / 64)
+        assert abs(zE) < 4.0, (suffix, zE)
+        se_t = np.sqrt(T.var(0, ddof=1) / 64 + G["trace_var" + suffix] / 64)
+        zt = (T.mean(0) - G["trace_mean" + suffix]) / np.maximum(se_t, 1e-300)
+        assert np.abs(zt).max() < 4.5, (suffix, np.abs(zt).argmax(), np.abs(zt).max())
