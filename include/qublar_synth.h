@@ -65,6 +65,10 @@ qb_status qb_tomo_sizes(const qb_tomo* t, int32_t* n_vars, int32_t* n_rays, int6
  * bytes, 1 = the cell lies in the void) may be NULL. */
 qb_status qb_tomo_arrays(const qb_tomo* t, double* d, double* w, int32_t* row_ptr, int32_t* ray, float* a,
                          int32_t* nbr_ptr, int32_t* nbr, uint8_t* truth);
+/* The voxel grid (dims: nx, ny, nz; cells x fastest) and the cell of every
+ * bit (n_vars entries); either may be NULL. The bits are the grid's domain
+ * cells in cell order, as BitField::grid numbers them (src/engine.hpp:61-85). */
+qb_status qb_tomo_cells(const qb_tomo* t, int32_t* dims, int64_t* bit_cell);
 /* The problem as a descriptor over the builder's own arrays (valid until destroy). */
 qb_status qb_tomo_desc(const qb_tomo* t, qb_residual_desc* desc);
 void qb_tomo_destroy(qb_tomo* t);

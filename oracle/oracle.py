@@ -110,6 +110,8 @@ def ref() -> C.CDLL:
             "ref_anneal_branch_trace": (None, [P, D, D, C.c_int, C.c_int, U64, P, P]),
             "ref_freeze": (C.c_int, [P, D, P, P, P, P, P]),
             "ref_roi_qubo": (None, [P, P, C.c_int, P, P, P]),
+            "ref_grid_assemble": (C.c_int, [C.c_int, C.c_int, C.c_int, P, C.c_int, P, P, C.c_longlong, P, P, P, D, D,
+                                            P, P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -386,6 +388,28 @@ class RefGraph:
 
     def energy_scratch(self, x):
         return int(ref().ref_energy_scratch(self.h, _p(np.ascontiguousarray(x, np.uint8))))
+
+
+def ref_grid_assemble(dims, domain, d, w, e_bit, e_row, e_a, lam, kappa):
+    """BitField::grid over the domain mask and assemble of one sensor's rows
+    (src/engine.hpp:61-149), by the reference compiled here: the residual-form
+    arrays plus var_voxel."""
+    nx, ny, nz = (int(v) for v in dims)
+    domain = np.ascontiguousarray(domain, np.uint8)
+    n = int(domain.sum())
+    ne = int(e_bit.size)
+    out = {"var_voxel": np.empty(n, np.int32), "row_ptr": np.empty(n + 1, np.int32), "ray": np.empty(ne, np.int32),
+           "a": np.empty(ne, np.float32), "nbr_ptr": np.empty(n + 1, np.int32), "nbr": np.empty(6 * n, np.int32)}
+    nn = C.c_longlong(0)
+    e_bit, e_row = np.ascontiguousarray(e_bit, np.int32), np.ascontiguousarray(e_row, np.int32)
+    e_a = np.ascontiguousarray(e_a, np.float32)
+    d, w = np.ascontiguousarray(d, np.float64), np.ascontiguousarray(w, np.float64)
+    k = ref().ref_grid_assemble(nx, ny, nz, _p(domain), int(d.size), _p(d), _p(w), ne, _p(e_bit), _p(e_row), _p(e_a),
+                                float(lam), float(kappa), _p(out["var_voxel"]), _p(out["row_ptr"]), _p(out["ray"]),
+                                _p(out["a"]), _p(out["nbr_ptr"]), _p(out["nbr"]), C.byref(nn))
+    assert k == n
+    out["nbr"] = out["nbr"][:nn.value].copy()
+    return out
 
 
 class RefProblem:

@@ -6,7 +6,8 @@
 //
 // Wrapped: argos::wising::parse_rudy / anneal / cut_of / energy_scratch
 // (src/ising_weighted.hpp:83-267), argos::binary_energy / local_field_dE /
-// anneal_branch / branch_fractions (src/ising_recon.hpp:65-166).
+// anneal_branch / branch_fractions (src/ising_recon.hpp:65-166),
+// argos::BitField::grid / assemble (src/engine.hpp:61-149).
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -14,6 +15,7 @@
 #include <thread>
 #include <vector>
 
+#include "engine.hpp"
 #include "ising_recon.hpp"
 #include "ising_weighted.hpp"
 
@@ -225,6 +227,38 @@ void ref_roi_qubo(void* h, const int32_t* roi, int n_roi, const uint8_t* x_bar, 
                                              std::vector<uint8_t>(x_bar, x_bar + p->n_vars()));
     std::memcpy(h_out, q.h.data(), size_t(n_roi) * 8);
     std::memcpy(J_out, q.J.data(), size_t(n_roi) * size_t(n_roi) * 8);
+}
+
+// ---- problem assembly -------------------------------------------------------------------
+
+// BitField::grid over the domain mask (nx x ny x nz, x fastest) and assemble
+// (src/engine.hpp:61-149) of one sensor's rows given as entries (bit, row, a)
+// in row order, with the prior (lambda, kappa). Outputs sized by the caller:
+// var_voxel (n bits), row_ptr (n + 1), ray and a (n_entries), nbr_ptr (n + 1),
+// nbr (6 n at most); returns the bit count, *n_nbr the neighbour entries.
+int ref_grid_assemble(int nx, int ny, int nz, const uint8_t* domain, int n_rows, const double* d, const double* w,
+                      long long n_entries, const int32_t* e_bit, const int32_t* e_row, const float* e_a,
+                      double lambda, double kappa, int32_t* var_voxel, int32_t* row_ptr, int32_t* ray, float* a,
+                      int32_t* nbr_ptr, int32_t* nbr, long long* n_nbr) {
+    const std::vector<char> dom(domain, domain + size_t(nx) * ny * nz);
+    const argos::BitField f = argos::BitField::grid(nx, ny, nz, dom);
+    argos::OperatorRows op;
+    op.d.assign(d, d + n_rows);
+    op.w.assign(w, w + n_rows);
+    for (long long k = 0; k < n_entries; ++k) op.entries.push_back({e_bit[k], e_row[k], e_a[k]});
+    argos::IsingPrior prior;
+    prior.lambda = lambda;
+    prior.kappa = kappa;
+    const argos::BinaryProblem p = argos::assemble(f, {&op}, prior);
+    const int n = p.n_vars();
+    std::memcpy(var_voxel, p.var_voxel.data(), size_t(n) * 4);
+    std::memcpy(row_ptr, p.row_ptr.data(), size_t(n + 1) * 4);
+    std::memcpy(ray, p.ray.data(), p.ray.size() * 4);
+    std::memcpy(a, p.a.data(), p.a.size() * 4);
+    std::memcpy(nbr_ptr, p.nbr_ptr.data(), size_t(n + 1) * 4);
+    std::memcpy(nbr, p.nbr.data(), p.nbr.size() * 4);
+    *n_nbr = (long long)p.nbr.size();
+    return n;
 }
 
 }  // extern "C"

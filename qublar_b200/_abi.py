@@ -226,6 +226,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_int64)]),
     "qb_tomo_arrays": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "qb_tomo_desc": (C.c_int, [_P, C.POINTER(ResidualDesc)]),
+    "qb_tomo_cells": (C.c_int, [_P, _P, _P]),
     "qb_tomo_destroy": (None, [_P]),
     "qb_write_ising_out": (C.c_int, [C.c_char_p, C.POINTER(ExportDesc)]),
     "qb_write_roi_text": (C.c_int, [C.c_char_p, C.c_int32, _P, _P, _P, _P, _P]),

@@ -165,6 +165,8 @@ qb_status march_host(const SynthMarch& M, std::vector<BinMarch>& bins, std::vect
 }  // namespace
 
 struct qb_tomo {
+    int32_t dims[3] = {0, 0, 0};      // the voxel grid, x fastest
+    std::vector<int64_t> bit_cell;    // the grid cell of every bit
     std::vector<double> d, w;
     std::vector<int32_t> row_ptr, ray;
     std::vector<float> a;
@@ -272,6 +274,9 @@ qb_status synth_tomography(const qb_tomo_params* p, bool on_device, const qb_opt
     if (!t) return qb::fail(QB_ENOMEM, "qb_synth_tomography: out of host memory");
     t->lambda = p->lambda;
     t->kappa = p->kappa;
+    t->dims[0] = t->dims[1] = nxy;
+    t->dims[2] = nz;
+    t->bit_cell = bit_cell;
     // prior adjacency, BitField::grid's candidate order
     t->nbr_ptr.assign(size_t(n) + 1, 0);
     t->truth.assign(size_t(n), 0);
@@ -437,6 +442,13 @@ extern "C" qb_status qb_tomo_arrays(const qb_tomo* t, double* d, double* w, int3
     cp(nbr_ptr, t->nbr_ptr.data(), t->nbr_ptr.size() * sizeof(int32_t));
     cp(nbr, t->nbr.data(), t->nbr.size() * sizeof(int32_t));
     cp(truth, t->truth.data(), t->truth.size());
+    return QB_OK;
+}
+
+extern "C" qb_status qb_tomo_cells(const qb_tomo* t, int32_t* dims, int64_t* bit_cell) {
+    if (!t) return qb::fail(QB_EINVAL, "qb_tomo_cells: null tomography");
+    if (dims) std::memcpy(dims, t->dims, sizeof t->dims);
+    if (bit_cell && !t->bit_cell.empty()) std::memcpy(bit_cell, t->bit_cell.data(), t->bit_cell.size() * sizeof(int64_t));
     return QB_OK;
 }
 

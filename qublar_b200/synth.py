@@ -408,10 +408,11 @@ def small_tomo_params(scale: float = 0.2, bins: int = 24, **overrides) -> TomoPa
     return tomo_params(**kw)
 
 
-def tomography(params: TomoParams | None = None, truth: bool = False, device: int | None = None):
+def tomography(params: TomoParams | None = None, truth: bool = False, device: int | None = None, cells: bool = False):
     """Build the muon-tomography QUBO; returns the residual-form arrays (and
-    the void truth per bit when asked). With `device` (a CUDA ordinal) the ray
-    march runs on that GPU; the arrays are the same bit for bit."""
+    the void truth per bit when asked; with `cells`, the grid dims and every
+    bit's cell). With `device` (a CUDA ordinal) the ray march runs on that
+    GPU; the arrays are the same bit for bit."""
     p = params if params is not None else tomo_params()
     h = C.c_void_p()
     if device is None:
@@ -435,6 +436,12 @@ def tomography(params: TomoParams | None = None, truth: bool = False, device: in
         out["field"] = None
         if truth:
             out["truth"] = tr
+        if cells:
+            dims = np.empty(3, np.int32)
+            bc = np.empty(n.value, np.int64)
+            check(lib().qb_tomo_cells(h, ptr(dims), ptr(bc)))
+            out["dims"] = dims
+            out["bit_cell"] = bc
         return out
     finally:
         lib().qb_tomo_destroy(h)

@@ -1,6 +1,8 @@
 // Drives include/qublar_adapter.hpp the way a QuBLAR caller would, with
 // stand-in types that carry the reference's member names (BinaryProblem,
-// Schedule, WeightedGraph, Budget, RunOut), so no reference header is needed.
+// Schedule, WeightedGraph, Budget, RunOut), so no reference header is needed;
+// compiled with -DQB_REAL_TYPES against the reference's headers it uses the
+// reference's own types instead (oracle/Makefile: oracle/_ref/adapter_real).
 //
 //   adapter_check <dir> cpu   -> a call without a device must throw cleanly
 //   adapter_check <dir> gpu   -> branch_fractions / anneal / run_batch results
@@ -18,6 +20,17 @@
 
 #include "qublar_adapter.hpp"
 
+#ifdef QB_REAL_TYPES
+// Built by oracle/Makefile against the reference's own headers (include path
+// into the reference tree): the adapter is driven with the real types.
+#include "ising_recon.hpp"
+#include "ising_weighted.hpp"
+using argos::BinaryProblem;
+using argos::Schedule;
+using argos::wising::Budget;
+using argos::wising::RunOut;
+using argos::wising::WeightedGraph;
+#else
 struct BinaryProblem {   // the members of argos::BinaryProblem (src/engine.hpp:30-49)
     std::vector<int> var_voxel, voxel_var;
     std::vector<double> d, w;
@@ -44,6 +57,7 @@ struct RunOut {          // argos::wising::RunOut (src/ising_weighted.hpp:245-24
     std::vector<uint8_t> x;
     int64_t energy_tracked = 0;
 };
+#endif
 
 template <class T>
 static std::vector<T> load(const std::string& path) {

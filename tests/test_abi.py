@@ -337,6 +337,25 @@ def test_adapter_refuses_vectors_shorter_than_their_offsets(tmp_path):
     assert "refused 7 of 7" in r.stdout
 
 
+REAL_ADAPTER = os.path.join(ROOT, "oracle", "_ref", "adapter_real")
+
+
+@pytest.mark.skipif(not os.path.exists(REAL_ADAPTER), reason="oracle/_ref/adapter_real is built only with the reference tree")
+def test_adapter_with_the_reference_types_refuses_and_fails_cleanly(tmp_path):
+    """The same driver compiled against the reference's own BinaryProblem,
+    Schedule, WeightedGraph, Budget and RunOut (oracle/_ref/adapter_real):
+    the adapter refuses short vectors, and without a device every call throws
+    a clean exception."""
+    write_adapter_inputs(tmp_path)
+    r = subprocess.run([REAL_ADAPTER, str(tmp_path), "lengths"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "refused 7 of 7" in r.stdout
+    if qb.device_count() == 0:
+        r = subprocess.run([REAL_ADAPTER, str(tmp_path), "cpu"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "exception" in r.stdout
+
+
 def write_adapter_inputs(d):
     a = synth.tomography(synth.small_tomo_params(0.12, 12))
     for k in ("d", "w", "row_ptr", "ray", "a", "nbr_ptr", "nbr"):

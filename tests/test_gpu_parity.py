@@ -210,11 +210,29 @@ def test_cpp_adapter_matches_the_python_path(tmp_path):
     the same calls through the Python binding (one library underneath)."""
     import subprocess
 
-    from tests.test_abi import INCLUDE, ROOT, write_adapter_inputs
+    from tests.test_abi import INCLUDE, ROOT
     exe = tmp_path / "adapter_check"
     subprocess.run(["g++", "-std=c++17", "-O1", "-I" + INCLUDE, os.path.join(ROOT, "tests", "adapter_check.cpp"),
                     "-L" + os.path.join(ROOT, "qublar_b200"), "-lqublar_b200",
                     "-Wl,-rpath," + os.path.join(ROOT, "qublar_b200"), "-o", str(exe)], check=True)
+    _adapter_matches_the_python_path(str(exe), tmp_path)
+
+
+def test_cpp_adapter_with_the_reference_types_matches_the_python_path(tmp_path):
+    """The same calls with the reference's own types (oracle/_ref/adapter_real,
+    built against the reference's headers): argos::BinaryProblem and
+    argos::Schedule into branch_fractions, argos::wising::WeightedGraph and
+    Budget into anneal (returning argos::wising::RunOut) and run_batch."""
+    from tests.test_abi import REAL_ADAPTER
+    if not os.path.exists(REAL_ADAPTER):
+        pytest.skip("oracle/_ref/adapter_real is built only with the reference tree")
+    _adapter_matches_the_python_path(REAL_ADAPTER, tmp_path)
+
+
+def _adapter_matches_the_python_path(exe, tmp_path):
+    import subprocess
+
+    from tests.test_abi import write_adapter_inputs
     a, (n, eu, ev, ew) = write_adapter_inputs(tmp_path)
     r = subprocess.run([str(exe), str(tmp_path), "gpu"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -309,8 +327,8 @@ def test_residual_pyramid_statistical_vs_reference():
     the random stream and the arithmetic): fractions within binomial error
     (two-sample z < 5.5 at every bit, a Bonferroni bound over the bits), the
     tri-state map equal except at threshold-straddling bits. Mean final
-    energies and per-sweep mean energies agree with both reference runs
-    (Welch z < 4 and < 4.5 at every sweep)."""
+    energies agree with both reference runs (Welch z < 4); the per-sweep mean
+    energy agrees with the colour-order run (Welch z < 4.5 at every sweep)."""
     a = synth.tomography()
     P = ResidualProblem.from_arrays(a)
     G = np.load(os.path.join(GOLD, "ref_pyramid.npz"))
@@ -330,11 +348,15 @@ def test_residual_pyramid_statistical_vs_reference():
     straddle = (np.minimum(pg, pr) <= 0.9) & (np.maximum(pg, pr) >= 0.1)
     assert not (differ & ~straddle).any()
     E = r.energies()
-    T = r.energy_trace()
     for suffix in ("", "_colour"):
         Er = G["energy" + suffix]
         zE = (E.mean() - Er.mean()) / np.sqrt(E.var(ddof=1) / 64 + Er.var(ddof=1) / 64)
         assert abs(zE) < 4.0, (suffix, zE)
-        se_t = np.sqrt(T.var(0, ddof=1) / 64 + G["trace_var" + suffix] / 64)
-        zt = (T.mean(0) - G["trace_mean" + suffix]) / np.maximum(se_t, 1e-300)
-        assert np.abs(zt).max() < 4.5, (suffix, np.abs(zt).argmax(), np.abs(zt).max())
+    # the energy after every sweep: the early hot sweeps of a coloured order
+    # and of the index order differ by construction (a class moves all its
+    # bits from the same state), so the trace is held against the reference
+    # run in the same visiting order
+    T = r.energy_trace()
+    se_t = np.sqrt(T.var(0, ddof=1) / 64 + G["trace_var_colour"] / 64)
+    zt = (T.mean(0) - G["trace_mean_colour"]) / np.maximum(se_t, 1e-300)
+    assert np.abs(zt).max() < 4.5, (np.abs(zt).argmax(), np.abs(zt).max())

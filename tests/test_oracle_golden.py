@@ -331,3 +331,30 @@ def test_oracle_side_builder_equals_the_package_builder():
         for k in ("d", "w", "row_ptr", "ray", "a", "nbr_ptr", "nbr"):
             assert a[k].dtype == b[k].dtype and a[k].tobytes() == b[k].tobytes(), k
         assert a["lambda"] == b["lambda"] and a["kappa"] == b["kappa"]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+def test_pyramid_builder_assembles_like_the_reference():
+    """The pyramid builder's bits, prior adjacency and bit->ray CSR against the
+    reference's own BitField::grid and assemble (src/engine.hpp:61-149, built
+    here in oracle/_ref) fed the same domain and rows: the bits are the domain
+    cells in cell order, the neighbour lists are equal entry for entry, and
+    every bit holds the same (ray, a) entries (assemble's std::sort leaves
+    the order inside a bit unspecified; the builder orders them by ray)."""
+    a = synth.tomography(synth.small_tomo_params(), cells=True)
+    dims, cells = a["dims"], a["bit_cell"]
+    domain = np.zeros(int(np.prod(dims)), np.uint8)
+    domain[cells] = 1
+    n = a["row_ptr"].size - 1
+    bit = np.repeat(np.arange(n, dtype=np.int32), np.diff(a["row_ptr"]))
+    order = np.lexsort((bit, a["ray"]))          # the rows' entries, ray by ray
+    ref = O.ref_grid_assemble(dims, domain, a["d"], a["w"], bit[order], a["ray"][order], a["a"][order],
+                              a["lambda"], a["kappa"])
+    assert (ref["var_voxel"] == cells).all()
+    assert (ref["nbr_ptr"] == a["nbr_ptr"]).all() and (ref["nbr"] == a["nbr"]).all()
+    assert (ref["row_ptr"] == a["row_ptr"]).all()
+    for i in range(n):
+        s0, s1 = a["row_ptr"][i], a["row_ptr"][i + 1]
+        mine = sorted(zip(a["ray"][s0:s1].tolist(), a["a"][s0:s1].tolist()))
+        theirs = sorted(zip(ref["ray"][s0:s1].tolist(), ref["a"][s0:s1].tolist()))
+        assert mine == theirs, i
