@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "qb_build.hpp"
+#include "qb_batch.hpp"
 #include "qb_internal.hpp"
 #include "qb_kernels.hpp"
 #include "qb_qubo.hpp"
@@ -49,8 +50,13 @@ qb_status alloc_async(DevBuf& b, size_t bytes, cudaStream_t st) {
     return QB_OK;
 }
 
+// Stream-ordered release of a stream-ordered allocation; a buffer taken from
+// a plain allocation (the packed-replica arenas) is freed plainly.
 void free_async(DevBuf& b, cudaStream_t st) {
-    if (b.p) cudaFreeAsync(b.p, st);
+    if (b.p) {
+        if (b.pooled) cudaFreeAsync(b.p, st);
+        else cudaFree(b.p);
+    }
     b.p = nullptr;
     b.bytes = 0;
     b.pooled = false;
@@ -1220,6 +1226,25 @@ extern "C" qb_status qb_solve(qb_problem* p, const qb_schedule* sch, uint32_t n_
             b.trace = r->d_trace.as<double>();
             r->trace_base = p->kind == QB_KIND_RESIDUAL ? p->resid.e0 : p->kind == QB_KIND_QUBO ? p->qubo.offset : 0.0;
         }
+        if (p->kind == QB_KIND_ISING && !b.trace && packed_replicas_fit(p->ising, R)) {
+            // many replicas: groups of them as work items of the packed kernel
+            // (the same branches, fields and energies as one CTA per replica)
+            const IsingPlan& P = p->ising;
+            r->d_x.release();
+            r->d_p.release();
+            cudaEventRecord(r->ev0, st);
+            if ((s = packed_replicas(p, *sch, R, seed_offset, opts, &r->packed, r->d_x, r->d_f, r->d_e_i64, r->d_p)))
+                return bail(s);
+            cudaEventRecord(r->ev1, st);
+            b.x = r->d_x.as<uint8_t>();
+            if ((s = alloc_async(r->d_e_scr, size_t(R) * 8, st))) return bail(s);
+            if ((s = launch_ising_energies(P, b.x, R, r->d_e_scr.as<long long>(), st))) return bail(s);
+            if ((s = launch_i64_to_f64(r->d_e_scr.as<long long>(), R, b.e_f64, st))) return bail(s);
+            r->launches = 2 + 2;   // packed anneal + its marginals, energies, conversion
+            cudaEventRecord(r->ev2, st);
+            *out = r;
+            return QB_OK;
+        }
         if (p->kind == QB_KIND_ISING) {
             const IsingPlan& P = p->ising;
             if ((s = alloc_async(r->d_f, size_t(R) * size_t(n) * 4, st))) return bail(s);
@@ -1431,6 +1456,7 @@ extern "C" void qb_result_destroy(qb_result* r) {
     cudaStream_t st = r->stream;
     DevBuf* all[] = {&r->d_x, &r->d_f, &r->d_e_i64, &r->d_e_scr, &r->d_e_f64, &r->d_p, &r->d_temp, &r->d_drift,
                      &r->d_accepts, &r->d_e_track, &r->d_scratch, &r->d_trace};
+    if (r->packed) qb_batch_destroy(r->packed);   // waits for the stream: its tables are in use until then
     for (DevBuf* b : all) free_async(*b, st);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);

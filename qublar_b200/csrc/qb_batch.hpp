@@ -80,4 +80,17 @@ struct BatchInstDev {
 qb_status launch_batch_marginals(const uint8_t* x, const BatchInstDev* inst, int n_inst, int64_t total, float* p,
                                  cudaStream_t st);
 
+// qb_solve of many replicas of one ising problem through the packed kernel:
+// groups of G replicas (G the smallest power of two that keeps the groups
+// within the CTAs the device runs at once), each group a work item. The
+// branches, fields, tracked energies and marginals are those of the
+// CTA-per-replica sweep (the packed kernel's draws and arithmetic are the
+// same); the arenas are handed over in x, f, e, pm and the batch, which holds
+// the launch's tables, in *keep (destroy it after the stream's work).
+qb_status packed_replicas(qb_problem* p, const qb_schedule& s, int R, uint64_t seed_offset, const qb_opts* opts,
+                          qb_batch** keep, DevBuf& x, DevBuf& f, DevBuf& e, DevBuf& pm);
+// Whether packed_replicas serves R replicas of this plan (R >= 128 and a
+// group's state fits a CTA's shared memory).
+bool packed_replicas_fit(const IsingPlan& P, int R);
+
 }  // namespace qb

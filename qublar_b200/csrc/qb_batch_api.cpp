@@ -509,3 +509,51 @@ extern "C" void qb_batch_destroy(qb_batch* b) {
     if (b->ev2) cudaEventDestroy(b->ev2);
     delete b;
 }
+
+namespace qb {
+
+namespace {
+constexpr int kPackedMinReplicas = 128;
+constexpr int kPackedThreads = 256;
+
+void take(DevBuf& dst, DevBuf& src) {
+    dst.release();
+    dst.p = src.p;
+    dst.bytes = src.bytes;
+    dst.pooled = src.pooled;
+    dst.pool_stream = src.pool_stream;
+    src.p = nullptr;
+    src.bytes = 0;
+    src.pooled = false;
+}
+}  // namespace
+
+bool packed_replicas_fit(const IsingPlan& P, int R) {
+    if (R < kPackedMinReplicas || std::getenv("QB_PACKED_REPLICAS_OFF")) return false;
+    const int cap = batch_max_smem();
+    return cap > 0 && batch_item_smem(P.n, 1) <= size_t(std::min(cap, kDefaultSmem));
+}
+
+qb_status packed_replicas(qb_problem* p, const qb_schedule& s, int R, uint64_t seed_offset, const qb_opts* opts,
+                          qb_batch** keep, DevBuf& x, DevBuf& f, DevBuf& e, DevBuf& pm) {
+    *keep = nullptr;
+    BatchShape sh{kPackedThreads, std::min(batch_max_smem(), kDefaultSmem), 0};
+    qb_status st = batch_ctas(sh, &sh.ctas);
+    if (st != QB_OK) return st;
+    // the smallest group that keeps every item on a CTA of the first wave
+    int G = 1;
+    while (G < kBatchMaxGroup && (R + G - 1) / G > sh.ctas) G *= 2;
+    while (G > 1 && batch_item_smem(p->ising.n, G) > size_t(sh.smem_bytes)) G /= 2;
+    const qb_batch_item item{p, s, uint32_t(R), seed_offset};
+    qb_batch_config cfg{kPackedThreads, sh.smem_bytes, G, 0};
+    qb_batch* b = nullptr;
+    if ((st = qb_solve_batch(&item, 1, &cfg, opts, &b)) != QB_OK) return st;
+    take(x, b->d_x);
+    take(f, b->d_f);
+    take(e, b->d_e);
+    take(pm, b->d_p);
+    *keep = b;
+    return QB_OK;
+}
+
+}  // namespace qb

@@ -288,5 +288,6 @@ struct qb_result {
     qb::DevBuf d_trace;      // R x sweeps: ising int64 tracked energies; residual, qubo fp64 per-sweep dE sums
     double trace_base = 0.0; // residual: energy of x = 0; qubo: the offset
     const int* d_err = nullptr;   // timeout flag of a cooperative sweep (inside d_scratch), or null
+    qb_batch* packed = nullptr;   // many replicas solved by the packed kernel: its launch tables
     bool synced = false;
 };

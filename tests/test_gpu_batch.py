@@ -119,3 +119,24 @@ def test_batch_reaches_the_single_solve_energies_on_a_large_torus():
     r = P.solve(sched, 4)
     assert (B.branches(0) == r.branches()).all()
     assert (B.energies_tracked(0) == r.energies_tracked()).all()
+
+
+def test_many_replicas_route_equals_the_cta_per_replica_sweep(monkeypatch):
+    """qb_solve with 128 or more replicas of a graph whose groups fit a CTA's
+    shared memory runs them as work items of the packed kernel; branches,
+    tracked energies, fields and marginals equal those of one CTA per replica
+    (QB_PACKED_REPLICAS_OFF forces that form)."""
+    from qublar_b200 import Budget
+    n, eu, ev, ew = synth.erdos_renyi(800, 0.06, 1)
+    P = IsingProblem(n, eu, ev, ew)
+    b = Budget(3.0, 0.05, 100, 0)
+    r = P.solve(b, 256, 7)
+    assert r.info().launches == 4   # the packed route: anneal, marginals, energies, conversion
+    X, E, F, p = r.branches(), r.energies_tracked(), r.fields(), r.marginals()
+    monkeypatch.setenv("QB_PACKED_REPLICAS_OFF", "1")
+    q = P.solve(b, 256, 7)
+    assert q.info().launches == 3
+    assert (q.branches() == X).all()
+    assert (q.energies_tracked() == E).all() and (q.fields() == F).all()
+    assert (q.marginals() == p).all()
+    assert (r.energies() == E.astype(np.float64)).all()
