@@ -380,7 +380,7 @@ def batch_cpu_baseline(graphs, items, R, S):
 
 # ---- serve: a Poisson request stream through the serving loop -----------------------------------
 
-SERVE_LOCKSTEP_BITS = 40000
+SERVE_LOCKSTEP_BITS = int(os.environ.get("QB_SERVE_LOCKSTEP_BITS", "40000"))
 SERVE_QUBO_MAXCUT_BITS = 50000
 SERVE_WORKLOAD = ("Poisson request stream: N log-uniform 1,000..300,000, half tomography-style pyramids, half "
                   "sparse +-1 Max-Cut (d-regular, d 3..12), sweeps 500..5000, branches 8..32")
@@ -404,8 +404,8 @@ def _serve_schedule(spec, P, data):
 
 def _serve_path(P, spec):
     if spec["kind"] != "tomography":
-        return "maxcut exclusive qubo" if spec["n"] >= SERVE_QUBO_MAXCUT_BITS else "maxcut ticks"
-    return "pyramid exclusive lockstep" if P.info().variant == 1 else "pyramid cluster"
+        return "maxcut partitioned qubo" if spec["n"] >= SERVE_QUBO_MAXCUT_BITS else "maxcut ticks"
+    return "pyramid partitioned lockstep" if P.info().variant == 1 else "pyramid cluster"
 
 
 def _serve_run(probs, specs, scheds, rate, seed):
@@ -457,10 +457,11 @@ def run_serve(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
 
     def make(k, served=True):
-        # pyramids of 40,000 bits and more take the whole-device lockstep sweep
-        # (run exclusively); smaller ones one cluster per branch beside the rest.
-        # Max-Cut graphs of 50,000 bits and more run as the equal weighted QUBO
-        # on the whole-device sweep (identical branches); smaller ones in ticks.
+        # pyramids of SERVE_LOCKSTEP_BITS and more take the lockstep sweep on
+        # one partition of the device (several side by side); smaller ones one
+        # cluster per branch beside the rest. Max-Cut graphs of 50,000 bits and
+        # more run as the equal weighted QUBO on a partition (identical
+        # branches); smaller ones in ticks.
         # The plain form (served=False) is the same problem solved alone; its
         # pyramids always take the lockstep sweep, qb_solve's default plan.
         sp = specs[k]
@@ -531,10 +532,10 @@ def run_serve(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed (int32 / f32)",
         "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "requests": len(probs), "total_attempts": total,
-                   "policy": f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: whole-device lockstep sweep, run alone; "
-                             "smaller pyramids: one cluster per branch; Max-Cut >= "
-                             f"{SERVE_QUBO_MAXCUT_BITS} bits: the equal weighted QUBO on the whole-device sweep, run "
-                             "alone; smaller Max-Cut: ticks of the packed kernel",
+                   "policy": f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: lockstep sweep on one of 4 SM partitions, "
+                             "side by side; smaller pyramids: one cluster per branch; Max-Cut >= "
+                             f"{SERVE_QUBO_MAXCUT_BITS} bits: the equal weighted QUBO on a partition; smaller Max-Cut: "
+                             "ticks of the packed kernel",
                    "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
         "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
                                   "p99_s": float(np.percentile(lat_sat, 99))}, **rates},

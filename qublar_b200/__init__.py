@@ -540,13 +540,18 @@ class Server:
     """qb_server: a persistent request loop on one device (continuous batching).
 
     Problems should be created with ``flags=OPT_DEFER_UPLOAD`` (device memory
-    taken at admission) and residual ones also with ``OPT_RESID_CLUSTER``."""
+    taken at admission). Residual problems planned for the lockstep sweep and
+    weighted QUBOs run side by side on ``coop_parts`` partitions of the
+    device (a deferred lockstep problem is planned again for its partition's
+    grid at submission); residual problems made with ``OPT_RESID_CLUSTER`` run
+    as cluster launches."""
 
     def __init__(self, budget_bytes: int = 0, max_active: int = 0, residual_streams: int = 0,
                  tick_target_us: int = 0, use_graph: bool = True, batch: BatchConfig | None = None,
-                 device: int = -1, max_pending: int = 0):
+                 device: int = -1, max_pending: int = 0, coop_parts: int = 0):
         cfg = ServerConfig(int(device), int(budget_bytes), int(max_active), int(residual_streams),
-                           int(tick_target_us), 1 if use_graph else 0, batch or BatchConfig(), int(max_pending))
+                           int(tick_target_us), 1 if use_graph else 0, batch or BatchConfig(), int(max_pending),
+                           int(coop_parts))
         h = C.c_void_p()
         check(lib().qb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

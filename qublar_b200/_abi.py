@@ -136,7 +136,7 @@ class BatchInfo(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int32),
                 ("residual_streams", C.c_int32), ("tick_target_us", C.c_int32), ("use_graph", C.c_int32),
-                ("batch", BatchConfig), ("max_pending", C.c_int32)]
+                ("batch", BatchConfig), ("max_pending", C.c_int32), ("coop_parts", C.c_int32)]
 
 
 class RequestInfo(C.Structure):

@@ -948,6 +948,24 @@ qb_status qb::problem_upload(qb_problem* p, cudaStream_t st) {
     return QB_OK;
 }
 
+qb_status qb::replan_residual(qb_problem* p, int slices) {
+    if (p->kind != QB_KIND_RESIDUAL || p->resid.variant != QB_RESID_LOCKSTEP) return QB_OK;
+    if (p->resid.lock_grid == slices) return QB_OK;
+    HostDesc& h = p->host;
+    if (h.row_ptr.empty()) return fail(QB_EINVAL, "replan: the problem keeps no host copy (create it with QB_OPT_DEFER_UPLOAD)");
+    if (p->uploaded) problem_release_device(p);
+    const qb_residual_desc d{p->resid.n, p->resid.n_rays, h.d.data(), h.w.data(), h.row_ptr.data(), h.ray.data(),
+                             h.a.data(), h.nbr_ptr.data(), h.nbr.data(), h.lambda, h.kappa,
+                             h.has_field ? h.field.data() : nullptr};
+    ResidualPlan fresh;
+    qb_status s = plan_residual(&d, fresh, slices);
+    if (s != QB_OK) return s;
+    if (fresh.variant != QB_RESID_LOCKSTEP) return fail(QB_ENOTSUP, "replan: the lockstep plan was not kept");
+    p->resid = std::move(fresh);
+    p->device_bytes = residual_device_bytes(p->resid);
+    return QB_OK;
+}
+
 void qb::problem_release_device(qb_problem* p) {
     IsingPlan& I = p->ising;
     DevBuf* ib[] = {&I.d_row, &I.d_adj, &I.d_w, &I.d_f0, &I.d_order, &I.d_class_ptr, &I.d_eu, &I.d_ev, &I.d_ew};

@@ -69,6 +69,24 @@ struct DevBuf {
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), pooled(o.pooled), pool_stream(o.pool_stream) {
+        o.p = nullptr;
+        o.bytes = 0;
+        o.pooled = false;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            pooled = o.pooled;
+            pool_stream = o.pool_stream;
+            o.p = nullptr;
+            o.bytes = 0;
+            o.pooled = false;
+        }
+        return *this;
+    }
     ~DevBuf() { release(); }
     void release() {
         if (p) {
@@ -263,6 +281,11 @@ namespace qb {
 // the device), and the release of its device memory.
 qb_status problem_upload(qb_problem* p, cudaStream_t st);
 void problem_release_device(qb_problem* p);
+// Plans a lockstep residual problem again for a cooperative grid of `slices`
+// CTAs, from the host copies a deferred problem keeps (its device copy, if
+// any, is released; the next upload follows the new plan). The colouring is
+// the same, so the branches are too.
+qb_status replan_residual(qb_problem* p, int slices);
 }  // namespace qb
 
 struct qb_result {

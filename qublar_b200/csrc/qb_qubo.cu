@@ -27,6 +27,7 @@
 // most draws in fp32 with the same outcome.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "qb_device.cuh"
@@ -303,10 +304,11 @@ int qubo_max_branches() { return 64; }
 size_t qubo_scratch(const QuboPlan& p) { return 64 + size_t(p.n) * 64 * 4 * 2 + size_t(p.n) * 16; }
 
 qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, int sweeps, int refresh, uint64_t seed0,
-                               cudaStream_t st) {
+                               cudaStream_t st, int ctas) {
     if (R < 1 || R > 64) return fail(QB_EINVAL, "qubo sweep: 1 to 64 replicas per launch");
-    const int grid = qubo_lockstep_grid();
-    if (grid < 1) return fail(QB_ENOTSUP, "qubo sweep: no co-resident grid on this device");
+    const int full = qubo_lockstep_grid();
+    if (full < 1) return fail(QB_ENOTSUP, "qubo sweep: no co-resident grid on this device");
+    const int grid = ctas > 0 ? std::min(ctas, full) : full;
     QuboArgs A{};
     A.n = p.n;
     A.n_colours = p.col.n_colours();

@@ -26,8 +26,10 @@ int qubo_max_branches();
 // Scratch of one launch: a 64-byte control block (barrier counter, timeout
 // flag at +16, which the caller zeroes once per solve), fields, bit words.
 size_t qubo_scratch(const QuboPlan& p);
+// ctas: the cooperative grid (0 = the whole device; fewer CTAs leave the rest
+// of the device to other work; the branches do not depend on it).
 qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, int sweeps, int refresh, uint64_t seed0,
-                               cudaStream_t st);
+                               cudaStream_t st, int ctas = 0);
 qb_status launch_qubo_energies(const QuboPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st);
 
 }  // namespace qb

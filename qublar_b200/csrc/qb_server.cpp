@@ -1,7 +1,9 @@
 // The serving loop of the C ABI (qb_server_*): admission by a device-memory
 // budget, ising requests advanced together in ticks of the packed kernel
 // (one CUDA-graph replay per tick, state resident between ticks), residual
-// requests as cluster launches on a stream pool beside the ticks.
+// requests as cluster launches on a stream pool beside the ticks, and the
+// cooperative sweeps (lockstep residual, weighted QUBO) side by side on equal
+// partitions of the device's SMs, one cooperative grid per request.
 //
 // One worker thread owns every device call of the loop. It never holds the
 // server mutex across a CUDA call that waits, and it polls completion events
@@ -39,6 +41,7 @@ constexpr int kDefaultActive = 4096;
 constexpr int kDefaultResidStreams = 8;
 constexpr int kDefaultTickUs = 20000;
 constexpr size_t kTickHeader = 64;   // ctl words before the items
+constexpr int kDefaultParts = 4;     // SM partitions for cooperative sweeps
 
 int floor_pow2(int v) {
     int g = 1;
@@ -75,7 +78,9 @@ struct Request {
     int64_t charge_work = 0;      // problem + working memory: returned when the request finishes
     int64_t charge_results = 0;   // results: returned when the client releases them
     bool cancel = false;
-    bool exclusive = false;       // a cooperative whole-device sweep: runs with nothing beside it
+    bool coop = false;            // a cooperative sweep (lockstep residual or weighted QUBO)
+    bool exclusive = false;       // ... on the whole device, with nothing beside it (no partition plan)
+    int part = -1;                // the partition a partitioned cooperative sweep runs on
     // device memory (stream-ordered allocations)
     DevBuf d_x, d_f, d_e, d_p, d_temp, d_state, d_drift, d_accepts, d_ef64, d_etrack;
     // ising progress
@@ -119,6 +124,13 @@ struct qb_server {
     std::vector<Request*> running_ising;
     std::vector<Request*> running_resid;
     Request* exclusive_run = nullptr;
+    // cooperative sweeps side by side: `parts` partitions of the SMs, each
+    // running one request's grid of part_resid (residual) or part_qubo CTAs
+    int parts = 1;
+    int part_resid = 0, part_qubo = 0;
+    std::vector<cudaStream_t> part_streams;
+    std::vector<Request*> part_run;
+    std::vector<qb_problem*> submitting;   // problems being planned for a partition by a submitting thread
     bool tick_inflight = false;
     std::vector<std::pair<Request*, int>> tick_members;   // request, sweep end of its slice
     std::string fatal;
@@ -270,9 +282,10 @@ qb_status launch_resid(qb_server* S, Request* r) {
     return QB_OK;
 }
 
-// A whole-device cooperative sweep (lockstep residual or weighted QUBO), run
-// when nothing else runs on the device; its scratch lives in d_state.
-qb_status launch_exclusive(qb_server* S, Request* r) {
+// A cooperative sweep (lockstep residual or weighted QUBO) on stream `st`:
+// the whole device (exclusive requests) or one partition's grid; its scratch
+// lives in d_state.
+qb_status launch_coop(qb_server* S, Request* r, cudaStream_t st, int qubo_ctas) {
     qb_status s;
     const bool qubo = r->kind == QB_KIND_QUBO;
     {
@@ -295,7 +308,6 @@ qb_status launch_exclusive(qb_server* S, Request* r) {
         QB_CUDA(cudaMemsetAsync(r->d_state.p, 0, 64, S->upload_stream));   // barrier counter and timeout flag
         QB_CUDA(cudaStreamSynchronize(S->upload_stream));   // `temp` is a local
     }
-    cudaStream_t st = S->tick_stream;
     uint8_t* x = r->d_x.as<uint8_t>();
     if (qubo) {
         const int RB = qubo_max_branches();
@@ -308,7 +320,7 @@ qb_status launch_exclusive(qb_server* S, Request* r) {
             qb.accepts = r->d_accepts.as<unsigned long long>() + b0;
             qb.scratch = r->d_state.p;
             if ((s = launch_qubo_lockstep(r->prob->qubo, qb, std::min(RB, r->R - b0), r->sweeps,
-                                          r->sched.refresh_sweeps, r->seed0 + uint64_t(b0), st)))
+                                          r->sched.refresh_sweeps, r->seed0 + uint64_t(b0), st, qubo_ctas)))
                 return s;
         }
         if ((s = launch_qubo_energies(r->prob->qubo, x, r->R, r->d_ef64.as<double>(), st))) return s;
@@ -363,7 +375,17 @@ void admit_pending(qb_server* S) {
             }
             if (S->bytes_in_use + need > S->budget || S->active >= S->cfg.max_active) return;
             if (S->exclusive_run) return;
-            if (q->exclusive && (S->tick_inflight || !S->running_ising.empty() || !S->running_resid.empty())) return;
+            bool parts_busy = false;
+            for (Request* pr : S->part_run) parts_busy |= pr != nullptr;
+            if (q->exclusive && (S->tick_inflight || !S->running_ising.empty() || !S->running_resid.empty() || parts_busy))
+                return;
+            if (q->coop && !q->exclusive) {   // a free partition, or wait at the head
+                int slot = -1;
+                for (int k = 0; k < int(S->part_run.size()) && slot < 0; ++k)
+                    if (!S->part_run[size_t(k)]) slot = k;
+                if (slot < 0) return;
+                q->part = slot;
+            }
             S->pending.pop_front();
             S->bytes_in_use += need;
             S->peak_bytes = std::max(S->peak_bytes, S->bytes_in_use);
@@ -375,7 +397,8 @@ void admit_pending(qb_server* S) {
         ++S->admissions;
         const qb_status s = S->admissions == S->fail_admission
                                 ? fail(QB_ENOMEM, "injected admission failure (QB_SERVER_FAIL_ADMIT)")
-                            : r->exclusive ? launch_exclusive(S, r)
+                            : r->exclusive ? launch_coop(S, r, S->tick_stream, 0)
+                            : r->coop      ? launch_coop(S, r, S->part_streams[size_t(r->part)], S->part_qubo)
                             : r->kind == QB_KIND_ISING ? admit_ising(S, r)
                                                        : launch_resid(S, r);
         if (s != QB_OK) {
@@ -389,6 +412,7 @@ void admit_pending(qb_server* S) {
             continue;
         }
         if (r->exclusive) S->exclusive_run = r;
+        else if (r->coop) S->part_run[size_t(r->part)] = r;
         else if (r->kind == QB_KIND_ISING) S->running_ising.push_back(r);
         else S->running_resid.push_back(r);
     }
@@ -596,11 +620,11 @@ void poll_resid(qb_server* S) {
     S->running_resid.swap(keep);
 }
 
-void poll_exclusive(qb_server* S) {
-    Request* r = S->exclusive_run;
-    if (!r) return;
+// A finished cooperative sweep: its timeout flag, then its results. Returns
+// false while it runs.
+bool poll_coop(qb_server* S, Request* r) {
     cudaError_t e = cudaEventQuery(r->done_ev);
-    if (e == cudaErrorNotReady) return;
+    if (e == cudaErrorNotReady) return false;
     int timed_out = 0;
     if (e == cudaSuccess) {
         const cudaError_t c = cudaMemcpy(&timed_out, static_cast<const char*>(r->d_state.p) + 16, sizeof(int),
@@ -609,11 +633,10 @@ void poll_exclusive(qb_server* S) {
     }
     std::string msg;
     if (e != cudaSuccess) {
-        cuda_fail(e, "exclusive request", __FILE__, __LINE__);
+        cuda_fail(e, "cooperative request", __FILE__, __LINE__);
         msg = qb_last_error();
         S->fatal = msg;
     }
-    S->exclusive_run = nullptr;
     const bool cancelled = r->cancel;
     drop_work(S, r);
     std::lock_guard<std::mutex> lk(S->mu);
@@ -628,6 +651,13 @@ void poll_exclusive(qb_server* S) {
     } else {
         finish_locked(S, r, QB_REQ_DONE, QB_OK, "");
     }
+    return true;
+}
+
+void poll_exclusive(qb_server* S) {
+    if (S->exclusive_run && poll_coop(S, S->exclusive_run)) S->exclusive_run = nullptr;
+    for (Request*& r : S->part_run)
+        if (r && poll_coop(S, r)) r = nullptr;
 }
 
 // Cancelled ising requests leave between ticks.
@@ -673,7 +703,9 @@ void worker_main(qb_server* S) {
             fail_all_running(S, QB_ENOMEM, S->fatal);
         }
         std::unique_lock<std::mutex> lk(S->mu);
-        const bool busy = S->tick_inflight || !S->running_resid.empty() || S->exclusive_run != nullptr;
+        bool parts_busy = false;
+        for (Request* pr : S->part_run) parts_busy |= pr != nullptr;
+        const bool busy = S->tick_inflight || !S->running_resid.empty() || S->exclusive_run != nullptr || parts_busy;
         if (S->stop && !busy && S->running_ising.empty()) break;
         if (busy) S->cv_work.wait_for(lk, std::chrono::microseconds(50), [&] { return S->kick; });
         else S->cv_work.wait(lk, [&] { return S->kick || S->stop; });
@@ -700,7 +732,7 @@ extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** o
         if (c.residual_streams == 0) c.residual_streams = kDefaultResidStreams;
         if (c.tick_target_us == 0) c.tick_target_us = kDefaultTickUs;
         if (c.hbm_budget_bytes < 0 || c.max_active < 0 || c.residual_streams < 0 || c.residual_streams > 64 ||
-            c.tick_target_us < 0 || c.max_pending < 0)
+            c.tick_target_us < 0 || c.max_pending < 0 || c.coop_parts < 0 || c.coop_parts > 64)
             return fail(QB_EINVAL, "qb_server_create: negative or out-of-range setting");
         if (c.batch.threads == 0) c.batch.threads = 512;
         if (c.batch.smem_bytes == 0) c.batch.smem_bytes = 96 * 1024;
@@ -737,6 +769,22 @@ extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** o
         }
         QB_CUDA(cudaEventCreateWithFlags(&S->upload_ev, cudaEventDisableTiming));
         QB_CUDA(cudaEventCreateWithFlags(&S->tick_ev, cudaEventDisableTiming));
+        // partitions of the SMs for cooperative sweeps (QB_SERVER_PARTS overrides)
+        int parts = c.coop_parts > 0 ? c.coop_parts : kDefaultParts;
+        if (const char* ev = std::getenv("QB_SERVER_PARTS")) parts = std::max(1, std::atoi(ev));
+        const int full_resid = resid_lockstep_grid(), full_qubo = qubo_lockstep_grid();
+        parts = std::max(1, std::min(parts, std::min(full_resid, full_qubo)));
+        S->parts = parts;
+        S->part_resid = parts > 1 ? full_resid / parts : 0;
+        S->part_qubo = parts > 1 ? full_qubo / parts : 0;
+        if (parts > 1) {
+            for (int k = 0; k < parts; ++k) {
+                cudaStream_t st;
+                QB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                S->part_streams.push_back(st);
+            }
+            S->part_run.assign(size_t(parts), nullptr);
+        }
         if (const char* fa = std::getenv("QB_SERVER_FAIL_ADMIT")) S->fail_admission = std::atoll(fa);
         qb_server* raw = S.release();
         raw->worker = std::thread(worker_main, raw);
@@ -763,8 +811,29 @@ extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_sche
         r->kind = p->kind;
         r->R = int(n_branches);
         r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
-        r->exclusive = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
+        r->coop = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
+        r->exclusive = r->coop && S->parts == 1;
         r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
+        if (r->coop && !r->exclusive && p->kind == QB_KIND_RESIDUAL) {
+            // a lockstep residual problem runs on one partition: plan it for
+            // that grid (same colouring, same branches) from its host copy;
+            // one without a host copy runs on the whole device
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                for (auto& kv : S->reqs)
+                    if (kv.second->prob == p && (kv.second->state == QB_REQ_PENDING || kv.second->state == QB_REQ_RUNNING))
+                        return fail(QB_EBUSY, "qb_server_submit: the problem already has a request in flight");
+                if (std::find(S->submitting.begin(), S->submitting.end(), p) != S->submitting.end())
+                    return fail(QB_EBUSY, "qb_server_submit: the problem is being submitted by another thread");
+                S->submitting.push_back(p);
+            }
+            qb_status ps = QB_OK;
+            if (p->host.row_ptr.empty()) r->exclusive = true;
+            else ps = replan_residual(p, S->part_resid);
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->submitting.erase(std::find(S->submitting.begin(), S->submitting.end(), p));
+            if (ps != QB_OK) return ps;
+        }
         r->seed0 = 1 + seed_offset;
         if (p->kind == QB_KIND_ISING) {
             r->charge_work = ising_work_bytes(p, r->R, r->sweeps);
@@ -953,6 +1022,10 @@ extern "C" void qb_server_destroy(qb_server* S) {
     if (S->h_tick) cudaFreeHost(S->h_tick);
     S->d_tick.release();
     for (cudaStream_t st : S->resid_streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    for (cudaStream_t st : S->part_streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }

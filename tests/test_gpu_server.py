@@ -206,9 +206,9 @@ def test_graph_and_direct_ticks_agree():
 
 
 def test_exclusive_requests_beside_ticks_are_the_same_alone():
-    """A lockstep-planned pyramid and a weighted QUBO run as whole-device
-    sweeps with nothing beside them; ising requests submitted around them
-    still finish, and every result equals its solve alone."""
+    """With coop_parts = 1 a lockstep-planned pyramid and a weighted QUBO run
+    as whole-device sweeps with nothing beside them; ising requests submitted
+    around them still finish, and every result equals its solve alone."""
     pyr = synth.tomography(synth.small_tomo_params(0.2, 24))
     q = synth.random_qubo(400, 2500, 17)
     g1, g2 = synth.random_regular(2000, 8, 5), synth.torus_pm1(40, 2)
@@ -217,7 +217,7 @@ def test_exclusive_requests_beside_ticks_are_the_same_alone():
     Pp = ResidualProblem.from_arrays(pyr, flags=DEFER)       # lockstep plan: exclusive
     Pq = QuboProblem.from_dict(q, flags=DEFER)                # exclusive
     P2 = IsingProblem(*g2, flags=DEFER)
-    S = Server()
+    S = Server(coop_parts=1)
     ids = [S.submit(P1, si, 16, 1), S.submit(Pp, sp, 20, 2), S.submit(Pq, sq, 40, 3), S.submit(P2, si, 8, 4)]
     for i in ids:
         S.wait(i, 120000)
@@ -232,6 +232,41 @@ def test_exclusive_requests_beside_ticks_are_the_same_alone():
     for rid, r in zip(ids, alone):
         assert (S.branches(rid) == r.branches()).all()
     np.testing.assert_allclose(S.energies(ids[2]), alone[2].energies(), rtol=1e-12)
+    S.close()
+
+
+def test_cooperative_requests_overlap_on_partitions_and_match_alone():
+    """Lockstep pyramids and weighted QUBOs run side by side on partitions of
+    the device (a deferred pyramid is planned again for its partition's grid
+    at submission), beside ising ticks; at least two of them overlap in time,
+    and every result equals its solve alone on the whole device."""
+    pyrs = [synth.tomography(synth.small_tomo_params(0.2 + 0.02 * k, 24)) for k in range(3)]
+    qs = [synth.random_qubo(400 + 100 * k, 2500, 17 + k) for k in range(2)]
+    g1 = synth.random_regular(2000, 8, 5)
+    sp, sq, si = Schedule(50.0, 1.0, 200, 50, 25), Schedule(3.0, 0.05, 600, 20, 32), Schedule(3.0, 0.05, 300, 0, 0)
+    Pp = [ResidualProblem.from_arrays(a, flags=DEFER) for a in pyrs]
+    Pq = [QuboProblem.from_dict(q, flags=DEFER) for q in qs]
+    Pi = IsingProblem(*g1, flags=DEFER)
+    S = Server(coop_parts=4)
+    ids = [S.submit(P, sp, 16 + 4 * k, k) for k, P in enumerate(Pp)]
+    ids += [S.submit(P, sq, 48, 10 + k) for k, P in enumerate(Pq)]
+    ids.append(S.submit(Pi, si, 16, 20))
+    for i in ids:
+        S.wait(i, 300000)
+    infos = [S.info(i) for i in ids]
+    coop = infos[:5]
+    overlaps = sum(1 for a in range(5) for b in range(a + 1, 5)
+                   if coop[a].t_admit < coop[b].t_done and coop[b].t_admit < coop[a].t_done)
+    assert overlaps >= 1
+    for k, a in enumerate(pyrs):
+        r = ResidualProblem.from_arrays(a).solve(sp, 16 + 4 * k, k)
+        assert (S.branches(ids[k]) == r.branches()).all(), k
+        np.testing.assert_allclose(S.energies(ids[k]), r.energies(), rtol=1e-12)
+    for k, q in enumerate(qs):
+        r = QuboProblem.from_dict(q).solve(sq, 48, 10 + k)
+        assert (S.branches(ids[3 + k]) == r.branches()).all(), k
+    r = IsingProblem(*g1).solve(si, 16, 20)
+    assert (S.branches(ids[5]) == r.branches()).all()
     S.close()
 
 
