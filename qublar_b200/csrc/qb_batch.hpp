@@ -89,8 +89,9 @@ qb_status launch_batch_marginals(const uint8_t* x, const BatchInstDev* inst, int
 // the launch's tables, in *keep (destroy it after the stream's work).
 qb_status packed_replicas(qb_problem* p, const qb_schedule& s, int R, uint64_t seed_offset, const qb_opts* opts,
                           qb_batch** keep, DevBuf& x, DevBuf& f, DevBuf& e, DevBuf& pm);
-// Whether packed_replicas serves R replicas of this plan (R >= 128 and a
-// group's state fits a CTA's shared memory).
+// Whether packed_replicas serves R replicas of this plan (asked for with
+// QB_PACKED_REPLICAS=1, R >= 128, and a group's state fits a CTA's shared
+// memory).
 bool packed_replicas_fit(const IsingPlan& P, int R);
 
 }  // namespace qb

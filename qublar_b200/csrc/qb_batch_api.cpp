@@ -529,7 +529,10 @@ void take(DevBuf& dst, DevBuf& src) {
 }  // namespace
 
 bool packed_replicas_fit(const IsingPlan& P, int R) {
-    if (R < kPackedMinReplicas || std::getenv("QB_PACKED_REPLICAS_OFF")) return false;
+    // opt-in (QB_PACKED_REPLICAS=1): on dense small graphs one CTA per replica
+    // with smaller CTAs is the faster form
+    const char* on = std::getenv("QB_PACKED_REPLICAS");
+    if (R < kPackedMinReplicas || !on || std::atoi(on) == 0) return false;
     const int cap = batch_max_smem();
     return cap > 0 && batch_item_smem(P.n, 1) <= size_t(std::min(cap, kDefaultSmem));
 }

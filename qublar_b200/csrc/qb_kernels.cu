@@ -582,19 +582,20 @@ struct LockStage {
     int32_t* nbr;    // kLockN
 };
 
-// Stage a chunk's entries, bit records and neighbour lists (async copies;
-// 16-byte copies for the entries where both ends allow, 8-byte ones at a
-// chunk's odd edge).
-__device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0, const int4 c1, const LockStage& S) {
+// Stage a chunk's entries, bit records and neighbour lists (async copies by
+// threads t0, t0 + stride, ...; 16-byte copies for the entries where both ends
+// allow, 8-byte ones at a chunk's odd edge).
+__device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0, const int4 c1, const LockStage& S,
+                                           int t0, int stride) {
     const int e0 = c1.x, e1 = c1.y;
     if ((e0 & 1) == 0) {
-        for (int e = e0 + 2 * int(threadIdx.x); e + 1 < e1; e += 2 * kLockThreads) cp_async16(&S.ent[e - e0], &A.ent[e]);
-        if (((e1 - e0) & 1) && threadIdx.x == 0) cp_async8(&S.ent[e1 - 1 - e0], &A.ent[e1 - 1]);
+        for (int e = e0 + 2 * t0; e + 1 < e1; e += 2 * stride) cp_async16(&S.ent[e - e0], &A.ent[e]);
+        if (((e1 - e0) & 1) && t0 == 0) cp_async8(&S.ent[e1 - 1 - e0], &A.ent[e1 - 1]);
     } else {
-        for (int e = e0 + int(threadIdx.x); e < e1; e += kLockThreads) cp_async8(&S.ent[e - e0], &A.ent[e]);
+        for (int e = e0 + t0; e < e1; e += stride) cp_async8(&S.ent[e - e0], &A.ent[e]);
     }
-    for (int k = 2 * c0.x + int(threadIdx.x); k < 2 * c0.y; k += kLockThreads) cp_async16(&S.meta[k - 2 * c0.x], &A.meta[k]);
-    for (int j = c1.z + int(threadIdx.x); j < c1.w; j += kLockThreads) cp_async4(&S.nbr[j - c1.z], &A.nbr[j]);
+    for (int k = 2 * c0.x + t0; k < 2 * c0.y; k += stride) cp_async16(&S.meta[k - 2 * c0.x], &A.meta[k]);
+    for (int j = c1.z + t0; j < c1.w; j += stride) cp_async4(&S.nbr[j - c1.z], &A.nbr[j]);
 }
 
 // Every CTA of a cooperative grid works its chunk list (a balanced slice of
@@ -632,10 +633,12 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     int32_t* s_segbit = reinterpret_cast<int32_t*>(s_amask + size_t(kLockB) * A.NG);    // kLockSegs: bit of each segment
     uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_segbit + kLockSegs);                  // kLockB x NG x 16 unlike counts
     __shared__ double s_trace[16 * kLockMaxNG];
-    // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`, into table `t`
+    // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`,
+    // into table `t`; the highest threads first (the low warps carry the
+    // phase-A items, so the draws fill the others' idle time)
     auto make_draws = [&](int t, int b0, int nb, int sw) {
         unsigned long long* d = s_draw + size_t(t) * kLockB * 16;
-        for (int q = tid; q < nb * 16; q += kLockThreads) {
+        for (int q = kLockThreads - 1 - tid; q < nb * 16; q += kLockThreads) {
             const int k = q >> 4, b = q & 15;
             if (b < A.R) d[q] = draw_u53(A.seed0 + uint64_t(b), uint32_t(__ldg(&A.order[b0 + k])), uint32_t(sw), 0u);
         }
@@ -662,7 +665,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         A.rp[k] = split_pair(-__dmul_rn(sqrt(fabs(A.w64[b])), A.d[b]));
     }
     for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
-    if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0));
+    if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0), tid, kLockThreads);
     cp_async_commit();
     if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
     grid_arrive_ways(A.bar, A.bar_ways);
@@ -715,9 +718,12 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             }
             const LockStage St = stage(gci & 1);
             // the other buffer was last read by the previous chunk, which every
-            // thread has finished: stage the next chunk into it now
-            lock_stage(A, cn0, cn1, stage((gci + 1) & 1));
+            // thread has finished: the upper half of the CTA (warps without
+            // phase-A items, mostly) stages the next chunk into it now
+            if (tid >= kLockThreads / 2)
+                lock_stage(A, cn0, cn1, stage((gci + 1) & 1), tid - kLockThreads / 2, kLockThreads / 2);
             cp_async_commit();
+            const int sweep_n = nx == 0 ? sweep + 1 : sweep;
             const int nb = c0.y - c0.x;
             const int nseg = c0.z;                       // segments of the chunk
             if (PHASES) t_a = clock64();
@@ -785,6 +791,9 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     for (int u = 0; u < kSeg / 2; ++u) held[u] = rv[u];
                 }
             }
+            // the next chunk's Philox draws (the next sweep's after the last
+            // chunk), mostly by warps that had no phase-A item
+            if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
             __syncthreads();
             if (PHASES) {
                 const long long t1 = clock64();
@@ -891,14 +900,10 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 ph_items += t1 - t_ph;
                 t_ph = t1;
             }
-            const int sweep_n = nx == 0 ? sweep + 1 : sweep;
             if (c0.w & 1) {
-                // arrive, make the next chunk's draws while the others arrive, then wait
                 grid_arrive_ways(A.bar, A.bar_ways);
-                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
             } else {
-                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
             }
             cur0 = cn0;
@@ -1048,7 +1053,23 @@ qb_status launch_ising_anneal(const IsingPlan& p, const SolveBuffers& b, int R, 
         A.f_scratch = static_cast<int32_t*>(b.scratch);
         A.s_scratch = reinterpret_cast<int8_t*>(A.f_scratch + size_t(R) * size_t(p.n));
     }
-    const dim3 grid(static_cast<unsigned>(R)), block(kIsingThreads);
+    // CTA size: 512 threads while the replicas fit one CTA per SM; with more
+    // replicas, 128-thread CTAs, several per SM (measured on the 800-node ER
+    // graph: 1,024 replicas take 16.7 ms at 128 threads, 28.1 at 256, 48.8 at
+    // 512; 16 replicas 11.8 ms at 512, 13.1 at 128). The decisions do not
+    // depend on the CTA size (integer sums are order-free). QB_ISING_THREADS
+    // overrides (a multiple of 32, 32..512).
+    int threads = kIsingThreads;
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (R > sms) threads = 128;
+        if (const char* t = std::getenv("QB_ISING_THREADS")) {
+            const int v = std::atoi(t);
+            if (v >= 32 && v <= kIsingThreads && v % 32 == 0) threads = v;
+        }
+    }
+    const dim3 grid(static_cast<unsigned>(R)), block(static_cast<unsigned>(threads));
     if (smem) {
         if (p.weight_bytes == 1) {
             QB_CUDA(allow_max_smem(ising_anneal_kernel<int8_t, true>));

@@ -13,7 +13,8 @@ fixtures:
 * ref_runs.npz -- outputs of the reference's own annealers run here through
   oracle/_ref: wising::anneal on the 800-node ER Max-Cut instance and
   anneal_branch on the small pyramid, 64 seeds each (final energies, per-sweep
-  energy traces, per-bit void fractions);
+  energy traces, per-bit void fractions), each in its own bit order and with
+  the bits relabelled into the GPU's colour-class order (suffix _colour);
 * ref_pyramid.npz -- anneal_branch of the reference on the benchmark pyramid
   (306,328 bits, 75,594 rays), seeds 1..64 with the posterior schedule (T 50
   -> 1 over 200 sweeps, 50 held): per-bit counts of branches with x = 1, final
@@ -88,34 +89,67 @@ def ree_text():
             f.write(data)
 
 
+def graph_colour_of_bits(n, eu, ev, ew):
+    """The plan's colour class of every vertex (qb_colour_ising) and its sweep order."""
+    import ctypes as C
+
+    from qublar_b200._abi import IsingDesc, lib, ptr
+    eu, ev, ew = (np.ascontiguousarray(v, np.int32) for v in (eu, ev, ew))
+    d = IsingDesc(int(n), int(eu.size), ptr(eu), ptr(ev), ptr(ew))
+    order = np.empty(n, np.int32)
+    cptr = np.empty(n + 1, np.int32)
+    nc = C.c_int32(0)
+    assert lib().qb_colour_ising(C.byref(d), ptr(order), ptr(cptr), C.byref(nc)) == 0
+    colour = np.empty(n, np.int32)
+    for c in range(nc.value):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    return colour, order
+
+
 def ref_runs():
     res = {}
-    # 800-node ER Max-Cut, T 3 -> 0.05 geometric over 1000 sweeps
-    g = O.Graph(*synth.erdos_renyi(800, 0.06, 1))
-    rg = O.RefGraph(g.rudy())
-    E, T = [], []
-    for s in range(1, SEEDS + 1):
-        x, e, tr = rg.trace(3.0, 0.05, 1000, 0, s)
-        E.append(e)
-        T.append(tr)
-    res["er800_energy"] = np.array(E, np.int64)
-    res["er800_trace_mean"] = np.mean(T, 0)
-    res["er800_trace_var"] = np.var(T, 0, ddof=1)
-    res["er800_m"] = np.int64(g.m)
-    # small pyramid, the posterior schedule 50 -> 1, 200 + 50
+    # 800-node ER Max-Cut, T 3 -> 0.05 geometric over 1000 sweeps; the second
+    # run relabels the vertices so that the reference's index-order sweep
+    # visits them in the GPU's colour-class order
+    n, eu, ev, ew = synth.erdos_renyi(800, 0.06, 1)
+    colour, order = graph_colour_of_bits(n, eu, ev, ew)
+    inv = np.empty(n, np.int32)
+    inv[order] = np.arange(n, dtype=np.int32)
+    for suffix, (u, v) in (("", (eu, ev)), ("_colour", (inv[eu], inv[ev]))):
+        g = O.Graph(n, u, v, ew)
+        rg = O.RefGraph(g.rudy())
+        E, T = [], []
+        for s in range(1, SEEDS + 1):
+            x, e, tr = rg.trace(3.0, 0.05, 1000, 0, s)
+            E.append(e)
+            T.append(tr)
+        res["er800_energy" + suffix] = np.array(E, np.int64)
+        res["er800_trace_mean" + suffix] = np.mean(T, 0)
+        res["er800_trace_var" + suffix] = np.var(T, 0, ddof=1)
+    res["er800_m"] = np.int64(eu.size)
+    res["er800_colour"] = colour
+    # small pyramid, the posterior schedule 50 -> 1, 200 + 50 (own order, and
+    # relabelled into the colour-class order)
     a = synth.tomography(synth.small_tomo_params())
-    rp = O.RefProblem(a)
-    X, T = [], []
-    for s in range(1, SEEDS + 1):
-        x, tr = rp.trace(50.0, 1.0, 200, 50, s)
-        X.append(x)
-        T.append(tr)
-    X = np.array(X, np.uint8)
-    res["tomo_small_frac"] = X.mean(0)
-    res["tomo_small_energy"] = np.array([t[-1] for t in T])
-    res["tomo_small_trace_mean"] = np.mean(T, 0)
-    res["tomo_small_trace_var"] = np.var(T, 0, ddof=1)
+    tcol, torder = colour_of_bits(a)
+    for suffix, prob in (("", a), ("_colour", relabel(a, torder))):
+        rp = O.RefProblem(prob)
+        X, T = [], []
+        for s in range(1, SEEDS + 1):
+            x, tr = rp.trace(50.0, 1.0, 200, 50, s)
+            X.append(x)
+            T.append(tr)
+        X = np.array(X, np.uint8)
+        if suffix:
+            Xo = np.empty_like(X)
+            Xo[:, torder] = X
+            X = Xo
+        res["tomo_small_frac" + suffix] = X.mean(0)
+        res["tomo_small_energy" + suffix] = np.array([t[-1] for t in T])
+        res["tomo_small_trace_mean" + suffix] = np.mean(T, 0)
+        res["tomo_small_trace_var" + suffix] = np.var(T, 0, ddof=1)
     res["tomo_small_n"] = np.int64(X.shape[1])
+    res["tomo_small_colour"] = tcol
     np.savez_compressed(os.path.join(OUT, "ref_runs.npz"), **res)
 
 
@@ -186,6 +220,10 @@ if __name__ == "__main__":
         sys.exit("make_golden.py: set QUBLAR_REFERENCE to the root of the reference tree")
     if "--pyramid-only" in sys.argv:
         ref_pyramid()
+        print("golden fixtures written to", OUT)
+        sys.exit(0)
+    if "--runs-only" in sys.argv:
+        ref_runs()
         print("golden fixtures written to", OUT)
         sys.exit(0)
     ree()

@@ -122,20 +122,23 @@ def test_batch_reaches_the_single_solve_energies_on_a_large_torus():
 
 
 def test_many_replicas_route_equals_the_cta_per_replica_sweep(monkeypatch):
-    """qb_solve with 128 or more replicas of a graph whose groups fit a CTA's
-    shared memory runs them as work items of the packed kernel; branches,
-    tracked energies, fields and marginals equal those of one CTA per replica
-    (QB_PACKED_REPLICAS_OFF forces that form)."""
+    """qb_solve with 128 or more replicas (QB_PACKED_REPLICAS=1) runs them as
+    work items of the packed kernel; branches, tracked energies, fields and
+    marginals equal those of one CTA per replica, whatever the CTA size."""
     from qublar_b200 import Budget
     n, eu, ev, ew = synth.erdos_renyi(800, 0.06, 1)
     P = IsingProblem(n, eu, ev, ew)
     b = Budget(3.0, 0.05, 100, 0)
+    monkeypatch.setenv("QB_PACKED_REPLICAS", "1")
     r = P.solve(b, 256, 7)
-    assert r.info().launches == 4   # the packed route: anneal, marginals, energies, conversion
     X, E, F, p = r.branches(), r.energies_tracked(), r.fields(), r.marginals()
-    monkeypatch.setenv("QB_PACKED_REPLICAS_OFF", "1")
+    monkeypatch.delenv("QB_PACKED_REPLICAS")
+    for threads in ("512", "128"):
+        monkeypatch.setenv("QB_ISING_THREADS", threads)
+        o = P.solve(b, 256, 7)
+        assert (o.branches() == X).all() and (o.energies_tracked() == E).all(), threads
+    monkeypatch.delenv("QB_ISING_THREADS")
     q = P.solve(b, 256, 7)
-    assert q.info().launches == 3
     assert (q.branches() == X).all()
     assert (q.energies_tracked() == E).all() and (q.fields() == F).all()
     assert (q.marginals() == p).all()

@@ -15,6 +15,10 @@ and the small pyramid, made by the reference compiled here
 * statistical: the GPU's per-sweep mean energy over 64 branches agrees with
   the reference's within Welch |z| < 4.5 at every sweep (a Bonferroni-style
   bound over the 1000 / 250 sweeps, whose values are strongly correlated).
+  The reference run compared is the one with the bits relabelled into the
+  GPU's colour-class order: in the first hot sweeps a coloured sweep (a class
+  moves all its bits from one state) and an index-order sweep differ by
+  construction, so the trace is held against the same visiting order.
 """
 import os
 
@@ -28,6 +32,13 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 Z_MAX = 4.5
 TRACE_RTOL = 1e-9
+
+
+def _colour_of_bits(order, cptr, n):
+    colour = np.empty(n, np.int32)
+    for c in range(cptr.size - 1):
+        colour[order[cptr[c]:cptr[c + 1]]] = c
+    return colour
 
 
 def _welch_z(m_g, v_g, n_g, m_r, v_r, n_r):
@@ -44,7 +55,7 @@ def test_ising_er800_trace_exact_and_vs_reference():
     b = Budget(3.0, 0.05, 1000, 0)
     g = O.Graph(*gen)
     P = IsingProblem(*gen)
-    order, _ = P.colouring()
+    order, cptr = P.colouring()
     temps = O.temperatures(b.t_hot, b.t_cold, b.anneal_sweeps, b.hold_sweeps)
     r = P.solve(b, 64, trace=True)
     T = r.energy_trace()
@@ -55,7 +66,8 @@ def test_ising_er800_trace_exact_and_vs_reference():
         _, _, e, tr = g.anneal_coloured(order, temps, k + 1, trace=True)
         assert (T[k] == tr).all(), k
     G = np.load(os.path.join(GOLD, "ref_runs.npz"))
-    z = _welch_z(T.mean(0), T.var(0, ddof=1), 64, G["er800_trace_mean"], G["er800_trace_var"], 64)
+    assert (_colour_of_bits(order, cptr, P.n) == G["er800_colour"]).all(), "regenerate the fixture"
+    z = _welch_z(T.mean(0), T.var(0, ddof=1), 64, G["er800_trace_mean_colour"], G["er800_trace_var_colour"], 64)
     assert np.abs(z).max() < Z_MAX, (np.abs(z).argmax(), np.abs(z).max())
 
 
@@ -93,7 +105,10 @@ def test_residual_small_trace_vs_reference():
     r = P.solve(Schedule(), 64, trace=True)
     T = r.energy_trace()
     G = np.load(os.path.join(GOLD, "ref_runs.npz"))
-    z = _welch_z(T.mean(0), T.var(0, ddof=1), 64, G["tomo_small_trace_mean"], G["tomo_small_trace_var"], 64)
+    order, cptr = P.colouring()
+    assert (_colour_of_bits(order, cptr, P.n) == G["tomo_small_colour"]).all(), "regenerate the fixture"
+    z = _welch_z(T.mean(0), T.var(0, ddof=1), 64, G["tomo_small_trace_mean_colour"],
+                 G["tomo_small_trace_var_colour"], 64)
     assert np.abs(z).max() < Z_MAX, (np.abs(z).argmax(), np.abs(z).max())
 
 
