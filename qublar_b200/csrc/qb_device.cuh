@@ -46,47 +46,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned r
     return s_ok != 0;
 }
 
-// A grid barrier whose arrivals are spread over `ways` counters kWayStride
-// bytes apart (CTA p arrives on counter p % ways), so fewer CTAs add into
-// one L2 line; a poll reads every counter (the loads are independent). Round
-// `round` is complete when the counters sum to round * per_round.
-constexpr int kWayStride = 512;   // bytes between the counters
-constexpr int kMaxWays = 8;
-
-__device__ __forceinline__ unsigned* way_counter(unsigned* bar, int k) {
-    return reinterpret_cast<unsigned*>(reinterpret_cast<char*>(bar) + size_t(k) * kWayStride);
-}
-
-__device__ __forceinline__ void grid_arrive_ways(unsigned* bar, int ways) {
-    __syncthreads();
-    if (threadIdx.x == 0) red_release_gpu(way_counter(bar, int(blockIdx.x) % ways), 1u);
-}
-
-__device__ __forceinline__ bool grid_wait_ways(unsigned* bar, int ways, int* err, unsigned round, unsigned per_round,
-                                               unsigned limit) {
-    __shared__ int s_ok3;
-    if (threadIdx.x == 0) {
-        const unsigned target = round * per_round;
-        unsigned spins = 0;
-        int ok = 1;
-        for (;;) {
-            unsigned sum = 0;
-#pragma unroll
-            for (int k = 0; k < kMaxWays; ++k)
-                if (k < ways) sum += ld_acquire_gpu(way_counter(bar, k));
-            if (sum >= target) break;
-            if (++spins > limit || *reinterpret_cast<volatile int*>(err)) {
-                atomicExch(err, 1);
-                ok = 0;
-                break;
-            }
-        }
-        s_ok3 = ok;
-    }
-    __syncthreads();
-    return s_ok3 != 0;
-}
-
 // The two halves of grid_barrier, so a CTA can work between its arrival and
 // the wait: grid_arrive after the CTA's last write of the phase, grid_wait
 // before its first read of the next phase. Every thread calls both.

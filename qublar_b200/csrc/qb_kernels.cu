@@ -557,7 +557,6 @@ struct ResidLockArgs {
     int* status;                // nullable: set to QB_ETIMEDOUT when a barrier times out
     unsigned bar_extra;         // arrivals a barrier round waits for beyond the grid (0; test hook)
     unsigned spin_limit;        // polls of a barrier before it gives up
-    int bar_ways;               // barrier counters the arrivals are spread over (grid_arrive_ways)
     uint8_t* x_out;
     float* drift;
     unsigned long long* accepts;
@@ -633,12 +632,10 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     int32_t* s_segbit = reinterpret_cast<int32_t*>(s_amask + size_t(kLockB) * A.NG);    // kLockSegs: bit of each segment
     uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_segbit + kLockSegs);                  // kLockB x NG x 16 unlike counts
     __shared__ double s_trace[16 * kLockMaxNG];
-    // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`,
-    // into table `t`; the highest threads first (the low warps carry the
-    // phase-A items, so the draws fill the others' idle time)
+    // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`, into table `t`
     auto make_draws = [&](int t, int b0, int nb, int sw) {
         unsigned long long* d = s_draw + size_t(t) * kLockB * 16;
-        for (int q = kLockThreads - 1 - tid; q < nb * 16; q += kLockThreads) {
+        for (int q = tid; q < nb * 16; q += kLockThreads) {
             const int k = q >> 4, b = q & 15;
             if (b < A.R) d[q] = draw_u53(A.seed0 + uint64_t(b), uint32_t(__ldg(&A.order[b0 + k])), uint32_t(sw), 0u);
         }
@@ -668,8 +665,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0), tid, kLockThreads);
     cp_async_commit();
     if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
-    grid_arrive_ways(A.bar, A.bar_ways);
-    bool ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
+    bool ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
     int4 cur0 = make_int4(0, 0, 0, 0), cur1 = make_int4(0, 0, 0, 0);   // descriptor of the chunk in hand
     if (n_chunks > 0) {
@@ -695,8 +691,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (dv > 0.0f) atomicMax(reinterpret_cast<int*>(&A.drift[j]), __float_as_int(dv));
                 __stcg(&A.rp[k], split_pair(v));
             }
-            grid_arrive_ways(A.bar, A.bar_ways);
-            ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
+            ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
             if (!ok) break;
         }
         const double T = A.temp[sweep];
@@ -791,9 +786,6 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     for (int u = 0; u < kSeg / 2; ++u) held[u] = rv[u];
                 }
             }
-            // the next chunk's Philox draws (the next sweep's after the last
-            // chunk), mostly by warps that had no phase-A item
-            if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
             __syncthreads();
             if (PHASES) {
                 const long long t1 = clock64();
@@ -819,17 +811,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
                     const int s0 = int(m1.w);
-                    // the segment sums in order; eight loads at a time so the adds
-                    // wait on one shared-memory round trip per eight segments
                     float h = 0.0f;
-                    for (int q0 = 0; q0 < nsg; q0 += 8) {
-                        float v[8];
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) v[u] = q0 + u < nsg ? hseg[((s0 + q0 + u) * A.NG + g) * 16 + br] : 0.0f;
-#pragma unroll
-                        for (int u = 0; u < 8; ++u)
-                            if (q0 + u < nsg) h = __fadd_rn(h, v[u]);
-                    }
+                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * A.NG + g) * 16 + br]);
                     const float delta = xi ? -1.0f : 1.0f;
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
                     const float prior = __fmul_rn(A.lambda, float(ne - 2 * unlike));
@@ -901,9 +884,12 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 t_ph = t1;
             }
             if (c0.w & 1) {
-                grid_arrive_ways(A.bar, A.bar_ways);
-                ok = grid_wait_ways(A.bar, A.bar_ways, A.err, ++round, per_round, A.spin_limit);
+                // arrive, make the next chunk's draws while the others arrive, then wait
+                grid_arrive(A.bar);
+                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
+                ok = grid_wait(A.bar, A.err, ++round, per_round, A.spin_limit);
             } else {
+                if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
             }
             cur0 = cn0;
@@ -1255,9 +1241,8 @@ int resid_lockstep_grid() {
 }
 
 // The scratch of a lockstep solve starts with a control block: the barrier
-// counters (kMaxWays of them, kWayStride bytes apart) and, at +16, the
-// timeout flag.
-constexpr size_t kLockCtl = size_t(kMaxWays) * kWayStride;
+// counter and, at +16, the timeout flag.
+constexpr size_t kLockCtl = 256;
 
 size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
     const int NG = (R + 15) / 16;
@@ -1270,9 +1255,6 @@ size_t resid_lockstep_scratch(const ResidualPlan& p, int R) {
 void lock_barrier_settings(ResidLockArgs& A) {
     A.bar_extra = 0;
     A.spin_limit = kSpinLimit;
-    // QB_BARRIER_WAYS=k: spread the barrier's arrivals over k counters
-    A.bar_ways = 1;
-    if (const char* w = std::getenv("QB_BARRIER_WAYS")) A.bar_ways = std::min(kMaxWays, std::max(1, std::atoi(w)));
     const char* v = std::getenv("QB_TEST_BARRIER_STALL");
     if (v && std::atoi(v) > 0) {
         A.bar_extra = 1;
@@ -1318,7 +1300,6 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     // the barrier counters restart per launch; the timeout flag (+16) is
     // zeroed once per solve by the caller, so a timeout of any launch shows
     QB_CUDA(cudaMemsetAsync(A.bar, 0, 16, st));
-    QB_CUDA(cudaMemsetAsync(sc + kWayStride, 0, kLockCtl - kWayStride, st));
     const int grid = p.lock_grid;
     if (grid < 1) return fail(QB_ENOTSUP, "residual lockstep sweep: no co-resident grid");
     DevBuf phase;
