@@ -380,7 +380,7 @@ def batch_cpu_baseline(graphs, items, R, S):
 
 # ---- serve: a Poisson request stream through the serving loop -----------------------------------
 
-SERVE_LOCKSTEP_BITS = int(os.environ.get("QB_SERVE_LOCKSTEP_BITS", "40000"))
+SERVE_LOCKSTEP_BITS = int(os.environ.get("QB_SERVE_LOCKSTEP_BITS", "10000"))
 SERVE_QUBO_MAXCUT_BITS = 50000
 SERVE_WORKLOAD = ("Poisson request stream: N log-uniform 1,000..300,000, half tomography-style pyramids, half "
                   "sparse +-1 Max-Cut (d-regular, d 3..12), sweeps 500..5000, branches 8..32")
@@ -445,9 +445,14 @@ def _serve_run(probs, specs, scheds, rate, seed):
     return out
 
 
-def run_serve(args):
+def serve_measure(n_requests, rates=(0.5, 0.8), plain_sample=24, warm=3):
+    """The serving stream of n_requests through a fresh server, saturated
+    (everything submitted at once) and at Poisson rates that are fractions of
+    the measured capacity; the plain form (each request alone through
+    qb_solve) on a sample of plain_sample requests (all of them when 0 or more
+    than the stream); the served results against the plain ones."""
     from qublar_b200 import synth
-    specs = synth.serve_specs(args.requests)
+    specs = synth.serve_specs(n_requests)
     t0 = time.perf_counter()
     data = _spawn_map(synth.build_request, specs)
     log(f"[serve] built {len(data)} requests in {time.perf_counter() - t0:.1f} s")
@@ -461,9 +466,9 @@ def run_serve(args):
         # one partition of the device (several side by side); smaller ones one
         # cluster per branch beside the rest. Max-Cut graphs of 50,000 bits and
         # more run as the equal weighted QUBO on a partition (identical
-        # branches); smaller ones in ticks.
-        # The plain form (served=False) is the same problem solved alone; its
-        # pyramids always take the lockstep sweep, qb_solve's default plan.
+        # branches); smaller ones in ticks. The plain form (served=False) is
+        # the same problem solved alone; its pyramids always take the lockstep
+        # sweep, qb_solve's default plan.
         sp = specs[k]
         fl = OPT_DEFER_UPLOAD if served else 0
         if sp["kind"] == "tomography":
@@ -481,26 +486,25 @@ def run_serve(args):
     attempts = [sp["branches"] * sch.sweeps * P.n for sp, sch, P in zip(specs, scheds, probs)]
     total = float(sum(attempts))
     # warm-up: a few small requests through a server
-    small = sorted(range(len(probs)), key=lambda k: attempts[k])[:max(3, args.warmup)]
-    for _ in range(1):
-        w = _serve_run([probs[k] for k in small], [specs[k] for k in small], [scheds[k] for k in small], None, 0)
-        w["server"].close()
+    small = sorted(range(len(probs)), key=lambda k: attempts[k])[:max(3, warm)]
+    w = _serve_run([probs[k] for k in small], [specs[k] for k in small], [scheds[k] for k in small], None, 0)
+    w["server"].close()
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
     sat = _serve_run(probs, specs, scheds, None, 1)
     clocks = sampler.stop()
     value = total / sat["makespan"]
-    # check: served results equal the plain solve of the same plan (sampled)
+    # served results against the plain solve of the same problem (sampled)
     mu = len(probs) / sat["makespan"]
     S = sat["server"]
-    sample = [int(j) for j in np.linspace(0, len(probs) - 1, min(24, len(probs)))]
+    n_plain = len(probs) if plain_sample <= 0 else min(plain_sample, len(probs))
+    sample = [int(j) for j in np.linspace(0, len(probs) - 1, n_plain)]
     same = 0
     e_rel = []
     p_att, p_s = 0.0, 0.0
     for k in sample:
         x_served = S.branches(sat["ids"][k])
         e_served = S.energies(sat["ids"][k])
-        # plain form: this request alone through qb_solve
         Q = make(k, served=False)
         r = Q.solve(scheds[k], specs[k]["branches"], k)
         inf = r.info()
@@ -508,8 +512,8 @@ def run_serve(args):
         p_s += inf.total_ms / 1e3
         x_plain = r.branches()
         e_plain = r.energies()
-        if specs[k]["kind"] != "tomography":
-            same += int((x_plain == x_served).all())
+        if specs[k]["kind"] != "tomography" or probs[k].info().variant == 1:
+            same += int((x_plain == x_served).all())   # the same sweep: identical branches
         else:
             same += 1 if abs(e_plain.mean() - e_served.mean()) <= 0.05 * abs(e_plain.mean()) + 1e-9 else 0
         e_rel.append(float((e_served.mean() - e_plain.mean()) / max(1e-12, abs(e_plain.mean()))))
@@ -518,42 +522,54 @@ def run_serve(args):
     plain = p_att / p_s
     S.close()
     lat_sat = sat["lat"]
-    rates = {}
-    for frac in (0.5, 0.8):
+    at_rates = {}
+    for frac in rates:
         run = _serve_run(probs, specs, scheds, frac * mu, 2)
-        rates[f"{frac:.1f}x capacity"] = {"rate_per_s": frac * mu, "p50_s": float(np.percentile(run["lat"], 50)),
-                                          "p99_s": float(np.percentile(run["lat"], 99)),
-                                          "throughput": total / run["makespan"]}
+        at_rates[f"{frac:.1f}x capacity"] = {"rate_per_s": frac * mu, "p50_s": float(np.percentile(run["lat"], 50)),
+                                             "p99_s": float(np.percentile(run["lat"], 99)),
+                                             "throughput": total / run["makespan"]}
         run["server"].close()
+    return {"requests": len(probs), "total_attempts": total, "value": value, "makespan_s": sat["makespan"],
+            "warm": len(small), "plain": plain, "plain_sample": len(sample), "vs_plain": value / plain,
+            "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
+                                      "p99_s": float(np.percentile(lat_sat, 99))}, **at_rates},
+            "equal_energy": {"checked": len(sample), "agree": same,
+                             "mean_rel_energy_diff": float(np.mean(e_rel)) if e_rel else None,
+                             "rule": "Max-Cut and lockstep pyramids: identical branches; cluster pyramids: mean "
+                                     "energy within 5% (cluster vs lockstep summation order)"},
+            "ticks": sat["ticks"], "peak_bytes": sat["peak_bytes"], "paths_saturated": sat["paths"],
+            "clocks": clocks}
+
+
+SERVE_POLICY = (f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: lockstep sweep on one of 4 SM partitions, side by side; "
+                "smaller pyramids: one cluster per branch; Max-Cut >= "
+                f"{SERVE_QUBO_MAXCUT_BITS} bits: the equal weighted QUBO on a partition; smaller Max-Cut: ticks of "
+                "the packed kernel")
+
+
+def run_serve(args):
+    m = serve_measure(args.requests)
     hbm, peak_kind = peaks()
     line = {
-        "metric": "spin-flip attempts/s; p50/p99 solve latency at equal energy, served vs plain", "value": value,
-        "unit": "attempts/s", "n_gpus": 1, "steps": 1, "warmup": len(small), "ms_per_step": sat["makespan"] * 1e3,
+        "metric": "spin-flip attempts/s; p50/p99 solve latency at equal energy, served vs plain", "value": m["value"],
+        "unit": "attempts/s", "n_gpus": 1, "steps": 1, "warmup": m["warm"], "ms_per_step": m["makespan_s"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed (int32 / f32)",
         "data": "synthetic",
-        "config": {"workload": SERVE_WORKLOAD, "requests": len(probs), "total_attempts": total,
-                   "policy": f"pyramids >= {SERVE_LOCKSTEP_BITS} bits: lockstep sweep on one of 4 SM partitions, "
-                             "side by side; smaller pyramids: one cluster per branch; Max-Cut >= "
-                             f"{SERVE_QUBO_MAXCUT_BITS} bits: the equal weighted QUBO on a partition; smaller Max-Cut: "
-                             "ticks of the packed kernel",
-                   "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
-        "latency": {"saturated": {"p50_s": float(np.percentile(lat_sat, 50)),
-                                  "p99_s": float(np.percentile(lat_sat, 99))}, **rates},
-        "plain": {"value": plain, "unit": "attempts/s",
+        "config": {"workload": SERVE_WORKLOAD, "requests": m["requests"], "total_attempts": m["total_attempts"],
+                   "policy": SERVE_POLICY, "budget": "150 GB (capped at 90% of free memory)", "parallelism": "1 GPU"},
+        "latency": m["latency"],
+        "plain": {"value": m["plain"], "unit": "attempts/s",
                   "form": "each request alone through qb_solve (lockstep sweep for pyramids, the whole-device "
                           f"QUBO sweep for Max-Cut >= {SERVE_QUBO_MAXCUT_BITS} bits, CTA per replica below)",
-                  "sample": f"{len(sample)} requests"},
-        "vs_plain": value / plain,
-        "equal_energy": {"checked": len(sample), "agree": same,
-                         "mean_rel_energy_diff": float(np.mean(e_rel)) if e_rel else None,
-                         "rule": "Max-Cut: identical branches; pyramids: mean energy within 5% (cluster vs "
-                                 "lockstep summation order)"},
-        "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                  "sample": f"{m['plain_sample']} requests"},
+        "vs_plain": m["vs_plain"],
+        "equal_energy": m["equal_energy"],
+        "e2e": {"value": m["value"], "unit": "attempts/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "requests enter as host problems (deferred upload) and the server uploads them at "
                         "admission inside the timed makespan"},
-        "server": {"ticks": sat["ticks"], "peak_bytes": sat["peak_bytes"], "paths_saturated": sat["paths"]},
+        "server": {"ticks": m["ticks"], "peak_bytes": m["peak_bytes"], "paths_saturated": m["paths_saturated"]},
         "peak_hbm_gbs": hbm, "peak_kind": peak_kind,
-        "clocks": clocks,
+        "clocks": m["clocks"],
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -754,6 +770,8 @@ def main():
     ap.add_argument("--instances", type=int, default=4096, help="batch: instances")
     ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch: sweeps per instance")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
+    ap.add_argument("--serve-requests", type=int, default=24,
+                    help="tomography: also measure served vs plain on a stream of this many requests (0 = skip)")
     ap.add_argument("--shape", default=None,
                     help="batch: fixed packed-kernel shape 'threads,smem_bytes,max_group' instead of autotuning")
     ap.add_argument("--qubo-sweeps", type=int, default=5000, help="qubo: sweeps (shorter runs are for profiling)")
@@ -896,6 +914,16 @@ def main():
         "max_energy_error": energy_err,
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        # the serving target on a stated stream of the mixed workload, recorded
+        # beside the pyramid line: served throughput against each request
+        # solved alone, latencies, identical results
+        m = serve_measure(args.serve_requests, rates=(0.5,), plain_sample=0)
+        line["serve"] = {"stream": f"{m['requests']} requests of the serving workload ({SERVE_WORKLOAD})",
+                         "policy": SERVE_POLICY, "total_attempts": m["total_attempts"],
+                         "served_attempts_per_s": m["value"], "plain_attempts_per_s": m["plain"],
+                         "served_vs_plain": m["vs_plain"], "makespan_s": m["makespan_s"], "latency": m["latency"],
+                         "equal_energy": m["equal_energy"], "clocks": m["clocks"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         branches = min(BRANCHES, threads)
