@@ -40,10 +40,11 @@ METRIC = "spin-flip attempts/s"
 BRANCHES = 16
 # DRAM bytes (read + write) per sweep of resid_lockstep_kernel from the
 # committed ncu capture of a 10-sweep launch on the same pyramid and 16
-# branches (profiles/resid_lockstep_pyramid.md): 1.924 GB + 6.3 MB over 10
-# sweeps. The bit->ray structure streams from DRAM once per sweep, so the
-# traffic of a full launch is this figure times its sweeps.
-NCU_TRAFFIC_PER_SWEEP = (1.931776e9 + 5.473536e6) / 10
+# branches (profiles/resid_lockstep_pyramid.md): 982.7 MB + 5.0 MB over 10
+# sweeps. The bit->ray structure (8-byte entries, 87 MB) streams from DRAM
+# once per sweep, so the traffic of a full launch is this figure times its
+# sweeps.
+NCU_TRAFFIC_PER_SWEEP = (982.714368e6 + 5.003776e6) / 10
 
 
 def log(*a):
@@ -116,21 +117,21 @@ class ClockSampler:
 def algorithmic_bytes(a, R, sweeps, refresh, accepted):
     """Bytes one launch of the lockstep residual sweep must move: the residual
     form's per-sweep figure with a replica tile of 16 branches (one stream
-    of the bit->ray CSR -- ray id + a, 8 B per entry -- serves 16 branches),
-    each branch's residuals read and written once per sweep (rays x 2 x 4 B),
-    its bits read and written (2 x 1/8 B each), the prior's neighbour lists
-    once per tile (4 B per entry), plus every accepted flip's residual
-    read-modify-write (entries of the bit x 2 x 4 B, from the device's
-    accept count, at the mean entries per bit) and the fp64 refreshes
-    (ray-major CSR, 8 B per entry, once per tile)."""
+    of the bit->ray CSR -- ray id + a', 8 B per entry -- serves 16 branches),
+    each branch's compensated residuals (hi + lo, s_r = 8 B) read and written
+    once per sweep (rays x 2 x 8 B), its bits read and written (2 x 1/8 B
+    each), the prior's neighbour lists once per tile (4 B per entry), plus
+    every accepted flip's residual read-modify-write (entries of the bit x 2
+    x 8 B, from the device's accept count, at the mean entries per bit) and
+    the fp64 refreshes (ray-major CSR, 8 B per entry, once per tile)."""
     nnz = int(a["ray"].size)
     n = int(a["row_ptr"].size - 1)
     rays = int(a["d"].size)
     nbr = int(a["nbr"].size)
     tiles = (R + 15) // 16
-    per_sweep = nnz * 8 * tiles + R * (rays * 2 * 4 + n * 2 / 8) + nbr * 4 * tiles
+    per_sweep = nnz * 8 * tiles + R * (rays * 2 * 8 + n * 2 / 8) + nbr * 4 * tiles
     refreshes = (sweeps - 1) // refresh if refresh > 0 else 0
-    return per_sweep * sweeps + refreshes * tiles * nnz * 8 + accepted * (nnz / n) * 2 * 4
+    return per_sweep * sweeps + refreshes * tiles * nnz * 8 + accepted * (nnz / n) * 2 * 8
 
 
 def cpu_baseline(a, sched, threads, branches):

@@ -386,10 +386,11 @@ void qb_batch_destroy(qb_batch* b);
  *   - residual requests (planned with QB_OPT_RESID_CLUSTER) run as one
  *     cluster launch each on a pool of streams, beside the ticks;
  *   - lockstep residual and weighted QUBO requests run as cooperative grids
- *     of a fraction of the device (coop_parts), several side by side and
- *     beside the ticks; a deferred lockstep residual problem is planned again
- *     for that grid when it is submitted (the same colouring and branches),
- *     one without a host copy runs alone on the whole device.
+ *     sized to their problems (enough CTAs for about one round of work per
+ *     colour class, at most half the device), several side by side and beside
+ *     the ticks; a deferred lockstep residual problem is planned again for
+ *     its grid when it is submitted (the same colouring and branches), one
+ *     without a host copy runs alone on the whole device.
  * A request's branches equal those of qb_solve on its own with the same
  * schedule and seeds, whatever else the server runs. All calls are
  * thread-safe. */
@@ -406,8 +407,9 @@ typedef struct qb_server_config {
     qb_batch_config batch;       /* packed-kernel shape (zeros = defaults) */
     int32_t max_pending;         /* requests waiting for admission at most; a submit beyond returns QB_EBUSY
                                     (0 = no limit) */
-    int32_t coop_parts;          /* cooperative sweeps (lockstep residual, weighted QUBO) run side by side on
-                                    this many equal partitions of the SMs, one request per partition
+    int32_t coop_parts;          /* cooperative sweeps (lockstep residual, weighted QUBO) run side by side, up
+                                    to this many at once, each on a grid sized to its problem (at most half the
+                                    device; the grids together within what the device holds at once)
                                     (0 = 4; 1 = each alone on the whole device) */
 } qb_server_config;
 

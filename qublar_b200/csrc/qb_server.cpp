@@ -80,7 +80,8 @@ struct Request {
     bool cancel = false;
     bool coop = false;            // a cooperative sweep (lockstep residual or weighted QUBO)
     bool exclusive = false;       // ... on the whole device, with nothing beside it (no partition plan)
-    int part = -1;                // the partition a partitioned cooperative sweep runs on
+    int part = -1;                // the stream a side-by-side cooperative sweep runs on
+    int ctas = 0;                 // ... and its grid (CTAs taken from the device's cooperative budget)
     // device memory (stream-ordered allocations)
     DevBuf d_x, d_f, d_e, d_p, d_temp, d_state, d_drift, d_accepts, d_ef64, d_etrack;
     // ising progress
@@ -124,10 +125,12 @@ struct qb_server {
     std::vector<Request*> running_ising;
     std::vector<Request*> running_resid;
     Request* exclusive_run = nullptr;
-    // cooperative sweeps side by side: `parts` partitions of the SMs, each
-    // running one request's grid of part_resid (residual) or part_qubo CTAs
+    // cooperative sweeps side by side: up to `parts` at once, each on its own
+    // stream with a grid sized to its problem, their grids together within the
+    // CTAs the device holds at once (coop_budget), one grid at most coop_cap
     int parts = 1;
-    int part_resid = 0, part_qubo = 0;
+    int coop_budget = 0, coop_cap = 0, coop_used = 0;
+    int full_resid = 0, full_qubo = 0;
     std::vector<cudaStream_t> part_streams;
     std::vector<Request*> part_run;
     std::vector<qb_problem*> submitting;   // problems being planned for a partition by a submitting thread
@@ -225,6 +228,26 @@ void plan_groups(qb_server* S, Request* r, double target_attempts) {
     }
     const double per_sweep = double(r->n) * gmax;
     r->slice = int(std::max(1.0, std::min(double(r->sweeps), std::floor(target_attempts / per_sweep))));
+}
+
+// The grid of a cooperative request that runs beside others: enough CTAs
+// that a colour class gives each of them about one round of warp items (a
+// residual bit takes about nnz / (16 n) + 1.5 items, a QUBO bit one warp
+// visit), at least 16, at most half the device.
+int coop_grid(const qb_server* S, const qb_problem* p) {
+    double per_class = 0.0, items_per_bit = 1.0, per_cta = 32.0;
+    int full = S->full_qubo;
+    if (p->kind == QB_KIND_RESIDUAL) {
+        const ResidualPlan& P = p->resid;
+        per_class = double(P.n) / std::max(1, P.col.n_colours());
+        items_per_bit = double(P.nnz) / std::max(1, P.n) / 16.0 + 1.5;
+        per_cta = 28.0;
+        full = S->full_resid;
+    } else {
+        per_class = double(p->qubo.n) / std::max(1, p->qubo.col.n_colours());
+    }
+    const int want = int(std::ceil(per_class * items_per_bit / per_cta));
+    return std::max(std::min(16, full), std::min({want, S->coop_cap, full}));
 }
 
 // ---- admission ---------------------------------------------------------------------------------
@@ -379,12 +402,13 @@ void admit_pending(qb_server* S) {
             for (Request* pr : S->part_run) parts_busy |= pr != nullptr;
             if (q->exclusive && (S->tick_inflight || !S->running_ising.empty() || !S->running_resid.empty() || parts_busy))
                 return;
-            if (q->coop && !q->exclusive) {   // a free partition, or wait at the head
+            if (q->coop && !q->exclusive) {   // a free stream and room for its grid, or wait at the head
                 int slot = -1;
                 for (int k = 0; k < int(S->part_run.size()) && slot < 0; ++k)
                     if (!S->part_run[size_t(k)]) slot = k;
-                if (slot < 0) return;
+                if (slot < 0 || S->coop_used + q->ctas > S->coop_budget) return;
                 q->part = slot;
+                S->coop_used += q->ctas;
             }
             S->pending.pop_front();
             S->bytes_in_use += need;
@@ -398,11 +422,12 @@ void admit_pending(qb_server* S) {
         const qb_status s = S->admissions == S->fail_admission
                                 ? fail(QB_ENOMEM, "injected admission failure (QB_SERVER_FAIL_ADMIT)")
                             : r->exclusive ? launch_coop(S, r, S->tick_stream, 0)
-                            : r->coop      ? launch_coop(S, r, S->part_streams[size_t(r->part)], S->part_qubo)
+                            : r->coop      ? launch_coop(S, r, S->part_streams[size_t(r->part)], r->ctas)
                             : r->kind == QB_KIND_ISING ? admit_ising(S, r)
                                                        : launch_resid(S, r);
         if (s != QB_OK) {
             const std::string msg = qb_last_error();
+            if (r->coop && !r->exclusive) S->coop_used -= r->ctas;   // its grid never ran
             drop_work(S, r);
             drop_results(r);
             std::lock_guard<std::mutex> lk(S->mu);
@@ -657,7 +682,10 @@ bool poll_coop(qb_server* S, Request* r) {
 void poll_exclusive(qb_server* S) {
     if (S->exclusive_run && poll_coop(S, S->exclusive_run)) S->exclusive_run = nullptr;
     for (Request*& r : S->part_run)
-        if (r && poll_coop(S, r)) r = nullptr;
+        if (r && poll_coop(S, r)) {
+            S->coop_used -= r->ctas;
+            r = nullptr;
+        }
 }
 
 // Cancelled ising requests leave between ticks.
@@ -775,8 +803,10 @@ extern "C" qb_status qb_server_create(const qb_server_config* cfg, qb_server** o
         const int full_resid = resid_lockstep_grid(), full_qubo = qubo_lockstep_grid();
         parts = std::max(1, std::min(parts, std::min(full_resid, full_qubo)));
         S->parts = parts;
-        S->part_resid = parts > 1 ? full_resid / parts : 0;
-        S->part_qubo = parts > 1 ? full_qubo / parts : 0;
+        S->full_resid = full_resid;
+        S->full_qubo = full_qubo;
+        S->coop_budget = std::min(full_resid, full_qubo);
+        S->coop_cap = std::max(1, S->coop_budget / 2);
         if (parts > 1) {
             for (int k = 0; k < parts; ++k) {
                 cudaStream_t st;
@@ -813,6 +843,7 @@ extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_sche
         r->n = p->kind == QB_KIND_ISING ? p->ising.n : p->kind == QB_KIND_QUBO ? p->qubo.n : p->resid.n;
         r->coop = p->kind == QB_KIND_QUBO || (p->kind == QB_KIND_RESIDUAL && p->resid.variant == QB_RESID_LOCKSTEP);
         r->exclusive = r->coop && S->parts == 1;
+        if (r->coop && !r->exclusive && p->kind == QB_KIND_QUBO) r->ctas = coop_grid(S, p);
         r->sweeps = sch->anneal_sweeps + sch->hold_sweeps;
         if (r->coop && !r->exclusive && p->kind == QB_KIND_RESIDUAL) {
             // a lockstep residual problem runs on one partition: plan it for
@@ -829,7 +860,7 @@ extern "C" qb_status qb_server_submit(qb_server* S, qb_problem* p, const qb_sche
             }
             qb_status ps = QB_OK;
             if (p->host.row_ptr.empty()) r->exclusive = true;
-            else ps = replan_residual(p, S->part_resid);
+            else ps = replan_residual(p, r->ctas = coop_grid(S, p));
             std::lock_guard<std::mutex> lk(S->mu);
             S->submitting.erase(std::find(S->submitting.begin(), S->submitting.end(), p));
             if (ps != QB_OK) return ps;
