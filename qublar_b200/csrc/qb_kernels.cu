@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         cur0 = chunks[0];
         cur1 = chunks[1];
     }
-    long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0, ph_a = 0, ph_b = 0, t_a = 0;
+    long long ph_wait = 0, ph_items = 0, ph_bar = 0, ph_n = 0, t_ph = 0, ph_a = 0, ph_b = 0, t_a = 0, ph_c = 0;
     for (int sweep = 0; ok && sweep < A.sweeps; ++sweep) {
         if (A.refresh > 0 && sweep > 0 && sweep % A.refresh == 0) {
             // fp64 refresh: thread per (ray, branch), the ray's set bits in
@@ -830,6 +830,8 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (A.trace && flip) atomicAdd(&s_trace[branch], double(dE));
             }
             __syncthreads();
+            long long t_c = 0;
+            if (PHASES) t_c = clock64();   // phase B ends here; phase C is counted apart
             // the sweep's tracked energy change, once per CTA per sweep
             if (A.trace && ci == n_chunks - 1 && tid < A.R) {
                 atomicAdd(&A.trace[size_t(tid) * A.sweeps + sweep], s_trace[tid]);
@@ -876,7 +878,9 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             // next chunk's writes
             if (PHASES) {
                 __syncthreads();
-                ph_b += clock64() - t_a;
+                const long long t1 = clock64();
+                ph_b += t1 - t_a;
+                ph_c += t1 - t_c;
             }
             if (PHASES) {
                 const long long t1 = clock64();
@@ -904,7 +908,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     asm volatile("cp.async.wait_all;" ::: "memory");
     if (PHASES && tid == 0) {
         unsigned long long* ph = A.phase + 8 * size_t(blockIdx.x);
-        ph[0] = ph_wait; ph[1] = ph_items; ph[2] = ph_bar; ph[3] = ph_n; ph[4] = ph_a; ph[5] = ph_b;
+        ph[0] = ph_wait; ph[1] = ph_items; ph[2] = ph_bar; ph[3] = ph_n; ph[4] = ph_a; ph[5] = ph_b; ph[6] = ph_c;
     }
     if (ok) {
         // branches out, original bit order
@@ -1318,14 +1322,15 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
         std::vector<unsigned long long> h(size_t(grid) * 8);
         QB_CUDA(cudaMemcpyAsync(h.data(), phase.p, phase.bytes, cudaMemcpyDeviceToHost, st));
         QB_CUDA(cudaStreamSynchronize(st));
-        double w = 0, it = 0, br = 0, ch = 0, pa = 0, pb = 0, itmax = 0;
+        double w = 0, it = 0, br = 0, ch = 0, pa = 0, pb = 0, pc = 0, itmax = 0;
         for (int c = 0; c < grid; ++c) {
             w += h[8 * c]; it += h[8 * c + 1]; br += h[8 * c + 2]; ch += h[8 * c + 3]; pa += h[8 * c + 4]; pb += h[8 * c + 5];
+            pc += h[8 * c + 6];
             itmax = std::max(itmax, double(h[8 * c + 1]) / std::max(1.0, double(h[8 * c + 3])));
         }
         std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: stage wait %.0f, items %.0f "
-                     "(A %.0f, B %.0f; slowest CTA's mean %.0f), barrier %.0f\n",
-                     ch / grid, w / ch, it / ch, pa / ch, pb / ch, itmax, br / ch);
+                     "(A %.0f, B %.0f, C %.0f; slowest CTA's mean %.0f), barrier %.0f\n",
+                     ch / grid, w / ch, it / ch, pa / ch, (pb - pc) / ch, pc / ch, itmax, br / ch);
     }
     return QB_OK;
 }
