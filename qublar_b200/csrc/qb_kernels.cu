@@ -609,8 +609,9 @@ __device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0
 //      TwoSum and store them (a class touches a residual at most once, so
 //      plain stores suffice and the result is deterministic).
 // A bounded grid barrier closes each class.
-template <bool PHASES>
+template <bool PHASES, int NG>
 __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLockArgs A) {
+    static_assert(NG >= 1 && NG <= kLockMaxNG, "16-branch groups: 1 .. kLockMaxNG");
     extern __shared__ __align__(16) unsigned char smem[];
     const int tid = int(threadIdx.x);
     const int lane = tid & 31;
@@ -620,17 +621,17 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     const int half = lane >> 4;         // entry parity
     const int P = int(gridDim.x);
     const int p = int(blockIdx.x);
-    const int RP = 16 * A.NG;           // residual row pitch (pairs)
+    const int RP = 16 * NG;           // residual row pitch (pairs)
     constexpr size_t kStageBytes = size_t(kLockE) * 8 + size_t(kLockB) * 32 + size_t(kLockN) * 4;
     // one group of 16 branches: the Philox draws of the next chunk are made
     // while the grid barrier is pending and wait in two 16-branch tables
     unsigned long long* s_draw = reinterpret_cast<unsigned long long*>(smem + 2 * kStageBytes);
-    const bool pre_draw = A.NG == 1;
+    const bool pre_draw = NG == 1;
     float* hseg = reinterpret_cast<float*>(s_draw + (pre_draw ? 2 * size_t(kLockB) * 16 : 0));   // kLockSegs x NG x 16 segment sums
-    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * A.NG * 16);   // kLockB x NG bit words (before)
-    uint32_t* s_amask = s_xw + size_t(kLockB) * A.NG;                                   // kLockB x NG flipped branches
-    int32_t* s_segbit = reinterpret_cast<int32_t*>(s_amask + size_t(kLockB) * A.NG);    // kLockSegs: bit of each segment
-    uint8_t* s_unl = reinterpret_cast<uint8_t*>(s_segbit + kLockSegs);                  // kLockB x NG x 16 unlike counts
+    uint32_t* s_xw = reinterpret_cast<uint32_t*>(hseg + size_t(kLockSegs) * NG * 16);   // kLockB x NG bit words (before)
+    uint32_t* s_amask = s_xw + size_t(kLockB) * NG;                                   // kLockB x NG flipped branches
+    uint8_t* s_map = reinterpret_cast<uint8_t*>(s_amask + size_t(kLockB) * NG);         // 2 x kLockSegs: bit of each segment
+    uint8_t* s_unl = s_map + 2 * kLockSegs;                                            // kLockB x NG x 16 unlike counts
     __shared__ double s_trace[16 * kLockMaxNG];
     // the draws of the chunk that starts at bit b0 with nb bits in sweep `sw`, into table `t`
     auto make_draws = [&](int t, int b0, int nb, int sw) {
@@ -638,6 +639,17 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         for (int q = tid; q < nb * 16; q += kLockThreads) {
             const int k = q >> 4, b = q & 15;
             if (b < A.R) d[q] = draw_u53(A.seed0 + uint64_t(b), uint32_t(__ldg(&A.order[b0 + k])), uint32_t(sw), 0u);
+        }
+    };
+    // the segment -> bit map of the chunk staged in buffer b (bits per chunk
+    // <= kLockB = 256 fit a byte), built before the chunk runs so that a
+    // segment item finds its bit with one shared load
+    auto seg_map = [&](int b, const int4 n0) {
+        const uint4* meta = reinterpret_cast<const uint4*>(smem + size_t(b) * kStageBytes + size_t(kLockE) * 8);
+        uint8_t* m = s_map + b * kLockSegs;
+        for (int k = tid; k < n0.y - n0.x; k += kLockThreads) {
+            const int s0 = int(meta[2 * k + 1].w), ns = (int(meta[2 * k].y) + kSeg - 1) / kSeg;
+            for (int j = 0; j < ns; ++j) m[s0 + j] = uint8_t(k);
         }
     };
     auto stage = [&](int b) {
@@ -661,11 +673,14 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         const int b = int(k / RP);
         A.rp[k] = split_pair(-__dmul_rn(sqrt(fabs(A.w64[b])), A.d[b]));
     }
-    for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
+    for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * NG; k += size_t(P) * kLockThreads) A.xb[k] = 0u;
     if (n_chunks > 0) lock_stage(A, chunks[0], chunks[1], stage(0), tid, kLockThreads);
     cp_async_commit();
     if (pre_draw && n_chunks > 0 && A.sweeps > 0) make_draws(0, chunks[0].x, chunks[0].y - chunks[0].x, 0);
-    bool ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    bool ok = grid_barrier(A.bar, A.err, ++round, per_round, A.spin_limit);   // also publishes the first stage
+    if (n_chunks > 0) seg_map(0, chunks[0]);
+    __syncthreads();
     int gci = 0;   // chunk counter over all sweeps: staging buffer gci & 1
     int4 cur0 = make_int4(0, 0, 0, 0), cur1 = make_int4(0, 0, 0, 0);   // descriptor of the chunk in hand
     if (n_chunks > 0) {
@@ -684,7 +699,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 const double sw = sqrt(fabs(A.w64[b]));
                 double acc = 0.0;
                 for (int e = A.rrow[b]; e < A.rrow[b + 1]; ++e)
-                    if ((__ldcg(&A.xb[size_t(A.rbit[e]) * A.NG + g]) >> l) & 1u) acc = __dadd_rn(acc, double(scaled_coef(sw, A.ra[e])));
+                    if ((__ldcg(&A.xb[size_t(A.rbit[e]) * NG + g]) >> l) & 1u) acc = __dadd_rn(acc, double(scaled_coef(sw, A.ra[e])));
                 const double v = __dsub_rn(acc, __dmul_rn(sw, A.d[b]));
                 const float2 cur = __ldcg(&A.rp[k]);
                 const float dv = __double2float_rn(fabs(__dsub_rn(__dadd_rn(double(cur.x), double(cur.y)), v)));
@@ -724,38 +739,32 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             if (PHASES) t_a = clock64();
             // A. segment sums, and per (bit, group) the bit word and the
             // unlike-neighbour counts, in one round of loads
-            const int nseg_items = nseg * A.NG;
+            const int nseg_items = nseg * NG;
             float2 held[kSeg / 2];   // the pairs of this warp's first segment item, for phase C
             int held_it = -1;
 #pragma unroll
             for (int u = 0; u < kSeg / 2; ++u) held[u] = make_float2(0.0f, 0.0f);
-            for (int it = warp; it < nseg_items + nb * A.NG; it += kWarps) {
+            for (int it = warp; it < nseg_items + nb * NG; it += kWarps) {
                 if (it >= nseg_items) {
-                    const int k = (it - nseg_items) / A.NG, g = (it - nseg_items) % A.NG;
+                    const int k = (it - nseg_items) / NG, g = (it - nseg_items) % NG;
                     const uint4 m0 = St.meta[2 * k];
                     const int ns = int(m0.z) - c1.z, nn = int(m0.w);
-                    const uint32_t xw = __ldcg(&A.xb[size_t(c0.x + k) * A.NG + g]);
+                    const uint32_t xw = __ldcg(&A.xb[size_t(c0.x + k) * NG + g]);
                     int unlike = 0;
                     for (int j0 = 0; j0 < nn; j0 += 32) {
-                        const uint32_t w = j0 + lane < nn ? __ldcg(&A.xb[size_t(St.nbr[ns + j0 + lane]) * A.NG + g]) : 0u;
+                        const uint32_t w = j0 + lane < nn ? __ldcg(&A.xb[size_t(St.nbr[ns + j0 + lane]) * NG + g]) : 0u;
                         const int m = min(32, nn - j0);
                         for (int u = 0; u < m; ++u) {
                             const uint32_t wu = __shfl_sync(kFull, w, u);
                             unlike += ((wu ^ xw) >> br) & 1u;
                         }
                     }
-                    if (half == 0) s_unl[(k * A.NG + g) * 16 + br] = uint8_t(unlike);
-                    if (lane == 0) s_xw[k * A.NG + g] = xw;
+                    if (half == 0) s_unl[(k * NG + g) * 16 + br] = uint8_t(unlike);
+                    if (lane == 0) s_xw[k * NG + g] = xw;
                     continue;
                 }
-                const int sg = it / A.NG, g = it % A.NG;
-                // the bit of segment sg: meta word 7 is the bit's first segment in the chunk
-                int lo = 0, hi = nb - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (int(St.meta[2 * mid + 1].w) <= sg) lo = mid; else hi = mid - 1;
-                }
-                if (g == 0 && lane == 0) s_segbit[sg] = lo;
+                const int sg = it / NG, g = it % NG;
+                const int lo = s_map[(gci & 1) * kLockSegs + sg];   // the bit of segment sg
                 const uint4 m0 = St.meta[2 * lo];
                 const int seg_in_bit = sg - int(St.meta[2 * lo + 1].w);
                 const int rs = int(m0.x) - c1.x + seg_in_bit * kSeg;
@@ -779,7 +788,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 for (int u = 0; u < kSeg / 2; ++u)
                     if (rs + half + 2 * u < re) acc = fmaf(cv[u], __fadd_rn(rv[u].x, rv[u].y), acc);
                 const float other = __shfl_xor_sync(kFull, acc, 16);
-                if (half == 0) hseg[(sg * A.NG + g) * 16 + br] = __fadd_rn(acc, other);
+                if (half == 0) hseg[(sg * NG + g) * 16 + br] = __fadd_rn(acc, other);
                 if (held_it < 0) {
                     held_it = it;
 #pragma unroll
@@ -793,16 +802,16 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 t_a = t1;
             }
             // B. decide, a warp per (bit, group)
-            for (int it = warp; it < nb * A.NG; it += kWarps) {
-                const int k = it / A.NG, g = it % A.NG;
+            for (int it = warp; it < nb * NG; it += kWarps) {
+                const int k = it / NG, g = it % NG;
                 const int branch = 16 * g + br;
                 const bool live = branch < A.R && half == 0;
                 const uint4 m0 = St.meta[2 * k], m1 = St.meta[2 * k + 1];
                 const int i = c0.x + k;
                 const int ne = int(m0.w);
-                const uint32_t xw = s_xw[k * A.NG + g];
+                const uint32_t xw = s_xw[k * NG + g];
                 const uint32_t xi = (xw >> br) & 1u;
-                const int unlike = s_unl[(k * A.NG + g) * 16 + br];
+                const int unlike = s_unl[(k * NG + g) * 16 + br];
                 const uint64_t u53 = !live ? 0ull
                                      : pre_draw ? s_draw[size_t(gci & 1) * kLockB * 16 + size_t(k) * 16 + br]
                                                 : draw_u53(A.seed0 + uint64_t(branch), m1.z, uint32_t(sweep), 0u);
@@ -812,7 +821,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
                     const int s0 = int(m1.w);
                     float h = 0.0f;
-                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * A.NG + g) * 16 + br]);
+                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * NG + g) * 16 + br]);
                     const float delta = xi ? -1.0f : 1.0f;
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
                     const float prior = __fmul_rn(A.lambda, float(ne - 2 * unlike));
@@ -821,9 +830,9 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 }
                 const unsigned amask = __ballot_sync(kFull, flip) & 0xFFFFu;
                 if (lane == 0) {
-                    s_amask[k * A.NG + g] = amask;
+                    s_amask[k * NG + g] = amask;
                     if (amask) {
-                        __stcg(&A.xb[size_t(i) * A.NG + g], xw ^ amask);
+                        __stcg(&A.xb[size_t(i) * NG + g], xw ^ amask);
                         my_accepts += unsigned(__popc(amask));
                     }
                 }
@@ -839,12 +848,12 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             }
             // C. the flipped branches' residuals: rho += delta a' (TwoSum)
             for (int it = warp; it < nseg_items; it += kWarps) {
-                const int sg = it / A.NG, g = it % A.NG;
-                const int k = s_segbit[sg];
-                const uint32_t amask = s_amask[k * A.NG + g];
+                const int sg = it / NG, g = it % NG;
+                const int k = s_map[(gci & 1) * kLockSegs + sg];
+                const uint32_t amask = s_amask[k * NG + g];
                 if (!amask) continue;   // warp-uniform
                 const bool mine = (amask >> br) & 1u;
-                const float dl = ((s_xw[k * A.NG + g] >> br) & 1u) ? -1.0f : 1.0f;
+                const float dl = ((s_xw[k * NG + g] >> br) & 1u) ? -1.0f : 1.0f;
                 const uint4 m0 = St.meta[2 * k];
                 const int seg_in_bit = sg - int(St.meta[2 * k + 1].w);
                 const int rs = int(m0.x) - c1.x + seg_in_bit * kSeg;
@@ -887,12 +896,21 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 ph_items += t1 - t_ph;
                 t_ph = t1;
             }
+            // the next chunk's stage (issued at this chunk's start) is complete
+            // once every thread's copies are; the block barrier below publishes
+            // it, its segment map is built after that, and the closing block
+            // barrier publishes the map
+            asm volatile("cp.async.wait_all;" ::: "memory");
             if (c0.w & 1) {
-                // arrive, make the next chunk's draws while the others arrive, then wait
+                // arrive; build the map and make the next chunk's draws while
+                // the others arrive; then wait
                 grid_arrive(A.bar);
+                seg_map((gci + 1) & 1, cn0);
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 ok = grid_wait(A.bar, A.err, ++round, per_round, A.spin_limit);
             } else {
+                __syncthreads();
+                seg_map((gci + 1) & 1, cn0);
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
                 __syncthreads();
             }
@@ -914,7 +932,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         // branches out, original bit order
         for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n) * A.R; k += size_t(P) * kLockThreads) {
             const int i = int(k % A.n), b = int(k / A.n);
-            A.x_out[size_t(b) * A.n + A.order[i]] = uint8_t((__ldcg(&A.xb[size_t(i) * A.NG + (b >> 4)]) >> (b & 15)) & 1u);
+            A.x_out[size_t(b) * A.n + A.order[i]] = uint8_t((__ldcg(&A.xb[size_t(i) * NG + (b >> 4)]) >> (b & 15)) & 1u);
         }
     } else if (tid == 0 && A.status) {
         *reinterpret_cast<volatile int*>(A.status) = int(QB_ETIMEDOUT);
@@ -1213,7 +1231,7 @@ qb_status resid_check_fit(const ResidualPlan& p) {
 
 size_t resid_lockstep_smem(int NG) {
     return 2 * (size_t(kLockE) * 8 + size_t(kLockB) * 32 + size_t(kLockN) * 4) + (NG == 1 ? 2 * size_t(kLockB) * 16 * 8 : 0) +
-           size_t(kLockSegs) * NG * 16 * 4 + size_t(kLockB) * NG * (4 + 4 + 16) + size_t(kLockSegs) * 4;
+           size_t(kLockSegs) * NG * 16 * 4 + size_t(kLockB) * NG * (4 + 4 + 16) + 2 * size_t(kLockSegs);
 }
 // The largest of those over the branch-group counts one launch serves.
 size_t resid_lockstep_smem_max() {
@@ -1221,6 +1239,32 @@ size_t resid_lockstep_smem_max() {
     for (int g = 1; g <= kLockMaxNG; ++g) m = std::max(m, resid_lockstep_smem(g));
     return m;
 }
+// The lockstep kernel for ng groups of 16 branches (the group count is a
+// compile-time constant of each instance, so the item index arithmetic is
+// shifts and multiplies).
+template <bool PHASES>
+const void* lockstep_kernel(int ng) {
+    switch (ng) {
+        case 1: return reinterpret_cast<const void*>(resid_lockstep_kernel<PHASES, 1>);
+        case 2: return reinterpret_cast<const void*>(resid_lockstep_kernel<PHASES, 2>);
+        case 3: return reinterpret_cast<const void*>(resid_lockstep_kernel<PHASES, 3>);
+        default: return reinterpret_cast<const void*>(resid_lockstep_kernel<PHASES, 4>);
+    }
+}
+
+// Raises the dynamic shared-memory limit of every lockstep instance.
+cudaError_t allow_lockstep_smem() {
+    for (int ng = 1; ng <= kLockMaxNG; ++ng) {
+        cudaError_t e = cudaFuncSetAttribute(lockstep_kernel<false>(ng), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(resid_lockstep_smem_max()));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(lockstep_kernel<true>(ng), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(resid_lockstep_smem_max()));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 int resid_lockstep_max_branches() { return 16 * kLockMaxNG; }
 int resid_lockstep_segment() { return kSeg; }
 int resid_lockstep_chunk_segments() { return kLockSegs; }
@@ -1232,15 +1276,16 @@ int resid_lockstep_grid() {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return 0;
-    if (cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(resid_lockstep_smem_max())) != cudaSuccess ||
-        cudaFuncSetAttribute(resid_lockstep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(resid_lockstep_smem_max())) != cudaSuccess)
-        return 0;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resid_lockstep_kernel<false>, kLockThreads,
-                                                      resid_lockstep_smem_max()) != cudaSuccess)
-        return 0;
+    if (allow_lockstep_smem() != cudaSuccess) return 0;
+    // every instance needs one co-resident CTA per SM
+    for (int ng = 1; ng <= kLockMaxNG; ++ng) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lockstep_kernel<false>(ng), kLockThreads,
+                                                          resid_lockstep_smem_max()) != cudaSuccess ||
+            per_sm < 1)
+            return 0;
+    }
+    int per_sm = 1;
     return per_sm >= 1 ? sms : 0;
 }
 
@@ -1314,8 +1359,7 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
         QB_CUDA(cudaMemsetAsync(phase.p, 0, phase.bytes, st));
         A.phase = phase.as<unsigned long long>();
     }
-    void* kern = phases ? reinterpret_cast<void*>(resid_lockstep_kernel<true>)
-                        : reinterpret_cast<void*>(resid_lockstep_kernel<false>);
+    const void* kern = phases ? lockstep_kernel<true>(A.NG) : lockstep_kernel<false>(A.NG);
     void* args[] = {&A};
     QB_CUDA(cudaLaunchCooperativeKernel(kern, dim3(unsigned(grid)), dim3(kLockThreads), args, resid_lockstep_smem(A.NG), st));
     if (phases) {
@@ -1504,10 +1548,9 @@ extern "C" qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_sch
         A.trace = nullptr;
         A.phase = nullptr;
         lock_barrier_settings(A);
-        QB_CUDA(cudaFuncSetAttribute(resid_lockstep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(resid_lockstep_smem_max())));
+        QB_CUDA(allow_lockstep_smem());
         void* args[] = {&A};
-        QB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resid_lockstep_kernel<false>),
+        QB_CUDA(cudaLaunchCooperativeKernel(lockstep_kernel<false>(A.NG),
                                             dim3(unsigned(P.lock_grid)), dim3(kLockThreads), args,
                                             resid_lockstep_smem(A.NG), cs));
         return QB_OK;
