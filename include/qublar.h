@@ -305,6 +305,15 @@ void qb_result_destroy(qb_result* r);
 qb_status qb_solve_residual_noalloc(const qb_problem* p, const qb_schedule* s, uint32_t n_branches,
                                     uint64_t seed_offset, uint8_t* x_out, int32_t* status, void* stream);
 
+/* Diagnostics: the sweeps' Metropolis test of n uphill moves, run on `device`.
+ * Move k draws u53[k] (53 bits) against dE[k] > 0 at temperature T[k]; dE is
+ * rounded to fp32 as the sweeps hold it. fast[k] = the fp32 verdict (1
+ * accept, 0 reject, 255 left to fp64), accept[k] = the sweeps' outcome,
+ * exact[k] = the plain fp64 test u53 * 2^-53 < exp(-dE / T); accept always
+ * equals exact. Host arrays of n entries; synchronous. */
+qb_status qb_metropolis_check(const uint64_t* u53, const double* dE, const double* T, int32_t n, int32_t device,
+                              uint8_t* fast, uint8_t* accept, uint8_t* exact);
+
 /* ---- batches: many ising instances in one persistent launch ----------------
  *
  * The reference anneals one instance per launch (gising::run_batch,

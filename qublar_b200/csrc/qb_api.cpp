@@ -1534,3 +1534,27 @@ extern "C" qb_status qb_energies_residual(const qb_problem* p, const uint8_t* x,
         return QB_OK;
     });
 }
+
+extern "C" qb_status qb_metropolis_check(const uint64_t* u53, const double* dE, const double* T, int32_t n,
+                                         int32_t device, uint8_t* fast, uint8_t* accept, uint8_t* exact) {
+    return guarded("metropolis_check", [&]() -> qb_status {
+        if (n < 0) return fail(QB_EINVAL, "metropolis_check: n must be non-negative");
+        if (n > 0 && (!u53 || !dE || !T || !fast || !accept || !exact))
+            return fail(QB_EINVAL, "metropolis_check: null array");
+        if (n == 0) return QB_OK;
+        QB_CUDA(cudaSetDevice(device));
+        DevBuf du, de, dt, dout;
+        qb_status s;
+        if ((s = upload(du, u53, size_t(n) * 8, nullptr)) || (s = upload(de, dE, size_t(n) * 8, nullptr)) ||
+            (s = upload(dt, T, size_t(n) * 8, nullptr)) || (s = dout.alloc(size_t(n) * 3)))
+            return s;
+        uint8_t* o = dout.as<uint8_t>();
+        if ((s = launch_metropolis_check(du.as<uint64_t>(), de.as<double>(), dt.as<double>(), n, o, o + n, o + 2 * size_t(n),
+                                         nullptr)))
+            return s;
+        QB_CUDA(cudaMemcpy(fast, o, size_t(n), cudaMemcpyDeviceToHost));
+        QB_CUDA(cudaMemcpy(accept, o + n, size_t(n), cudaMemcpyDeviceToHost));
+        QB_CUDA(cudaMemcpy(exact, o + 2 * size_t(n), size_t(n), cudaMemcpyDeviceToHost));
+        return QB_OK;
+    });
+}

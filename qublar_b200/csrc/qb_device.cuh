@@ -76,20 +76,32 @@ __device__ __forceinline__ bool grid_wait(unsigned* bar, int* err, unsigned roun
 
 // The Metropolis test of an uphill move, u53 * 2^-53 < exp(-dE / T) with the
 // quotient and the exp in fp64, settled in fp32 when the two sides are far
-// apart. p = __expf(-dE * inv_T) (inv_T = fp32 1/T) is within a relative
-// 3e-5 of exp(-dE / T) wherever it is a normal number: the argument's
-// roundings cost |x| * 2e-7 with |x| < 88, and __expf's documented error is
-// 2 + 1.173 |x| ulp. u = hi * 2^-32 (hi = the draw's top 32 bits) is at most
-// 2^-32 below u53 * 2^-53. So u + 2^-32 < 0.999 p proves acceptance and
-// u > 1.001 p proves rejection (also after p underflows: a draw of 2^-32 or
-// more exceeds exp(-87)); a zero draw, non-finite values and the narrow band
-// between take the fp64 test. The outcome is always the fp64 test's.
-__device__ __forceinline__ bool uphill_accept(uint64_t u53, double dE, double T, float inv_T) {
+// apart. With x = fp32(dE) * inv_T (inv_T = fp32 1/T, dE > 0), p =
+// __expf(-x) is within a relative (2 + 2.2 x) 2^-23 of exp(-dE / T) wherever
+// it is a normal number: the two roundings of the argument cost x 2^-23, and
+// __expf's documented error is 2 + 1.173 |x| ulp (an ulp is at most 2^-23 of
+// a normal result). u = fp32(hi) * 2^-32 (hi = the draw's top 32 bits) is at
+// most 2^-32 + u 2^-24 below u53 * 2^-53 and at most u 2^-24 above it. With
+// r = (8 + 4 x) 2^-23, which covers both and the roundings of the tests
+// themselves, u + 2^-32 < p (1 - r) proves acceptance and u > p (1 + r)
+// proves rejection (also after p underflows: a draw of 2^-32 or more exceeds
+// exp(-87)). A zero draw, non-finite values and the narrow band between take
+// the fp64 test, so the outcome is always the fp64 test's. The band is narrow
+// because a class step waits for the slowest of its warps: a wide band sends
+// some warp of nearly every step through the fp64 division and exp.
+// The fp32 part: 1 accept, 0 reject, -1 undecided (the fp64 test decides).
+__device__ __forceinline__ int uphill_fast(uint64_t u53, float dE, float inv_T) {
     const float u = __uint2float_rn(uint32_t(u53 >> 21)) * 0x1p-32f;
-    const float p = __expf(-(float(dE) * inv_T));
-    if (u + 0x1p-32f < 0.999f * p) return true;
-    if (u > 1.001f * p) return false;
-    return double(u53) * 0x1.0p-53 < exp(-dE / T);
+    const float x = dE * inv_T;
+    const float p = __expf(-x);
+    const float r = __fmaf_rn(4.0f, x, 8.0f) * 0x1p-23f;
+    if (u + 0x1p-32f < p * (1.0f - r)) return 1;
+    if (u > p * (1.0f + r)) return 0;
+    return -1;
+}
+__device__ __forceinline__ bool uphill_accept(uint64_t u53, double dE, double T, float inv_T) {
+    const int f = uphill_fast(u53, float(dE), inv_T);
+    return f >= 0 ? f != 0 : double(u53) * 0x1.0p-53 < exp(-dE / T);
 }
 
 // ---- compensated residuals of the residual-form sweeps ----------------------------

@@ -1379,6 +1379,30 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
     return QB_OK;
 }
 
+// Diagnostics of the Metropolis test (qb_metropolis_check): per move the
+// fp32 verdict, the sweeps' outcome and the plain fp64 test, with dE rounded
+// to fp32 and inv_T = fp32(1/T) as the sweeps have them.
+__global__ void metropolis_check_kernel(const uint64_t* u53, const double* dE, const double* T, int n, uint8_t* fast,
+                                        uint8_t* accept, uint8_t* exact) {
+    for (int k = int(blockIdx.x * blockDim.x + threadIdx.x); k < n; k += int(gridDim.x * blockDim.x)) {
+        const float d = __double2float_rn(dE[k]);
+        const double t = T[k];
+        const float inv_t = float(1.0 / t);
+        const int f = uphill_fast(u53[k], d, inv_t);
+        fast[k] = f < 0 ? 255u : uint8_t(f);
+        accept[k] = uphill_accept(u53[k], double(d), t, inv_t) ? 1u : 0u;
+        exact[k] = double(u53[k]) * 0x1.0p-53 < exp(-double(d) / t) ? 1u : 0u;
+    }
+}
+
+qb_status launch_metropolis_check(const uint64_t* u53, const double* dE, const double* T, int n, uint8_t* fast,
+                                  uint8_t* accept, uint8_t* exact, cudaStream_t st) {
+    if (n <= 0) return QB_OK;
+    metropolis_check_kernel<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(u53, dE, T, n, fast, accept, exact);
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+}
+
 qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st) {
     if (K == 0) return QB_OK;
     ResidEnergyArgs A{};

@@ -63,6 +63,8 @@ size_t resid_lockstep_scratch(const ResidualPlan& p, int R);
 qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, int R, int sweeps, int refresh,
                                 uint64_t seed0, cudaStream_t st);
 qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st);
+qb_status launch_metropolis_check(const uint64_t* u53, const double* dE, const double* T, int n, uint8_t* fast,
+                                  uint8_t* accept, uint8_t* exact, cudaStream_t st);
 
 qb_status launch_marginals(const uint8_t* x, int R, int n, float* p, cudaStream_t st);
 qb_status launch_tristate(const float* p, int n, float lo, float hi, uint8_t* out, cudaStream_t st);
