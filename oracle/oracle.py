@@ -58,6 +58,7 @@ def orc() -> C.CDLL:
         sig = {
             "orc_splitmix": (U64, [P]), "orc_uniform": (D, [P]),
             "orc_philox4x32_10": (None, [P, P, P]), "orc_draw_u53": (U64, [U64, C.c_uint32, C.c_uint32, C.c_uint32]),
+            "orc_draw_u53_hi": (U64, [U64, C.c_uint32, C.c_uint32, C.c_uint32]),
             "orc_temperature": (D, [D, D, C.c_int, C.c_int]),
             "orc_build_csr": (None, [C.c_int, I64, P, P, P, P, P, P]),
             "orc_cut_of": (I64, [I64, P, P, P, P]),
@@ -74,8 +75,8 @@ def orc() -> C.CDLL:
             "orc_classify": (None, [P, I64, C.c_float, C.c_float, P]),
             "orc_fractions": (None, [P, C.c_int, I64, P]),
             "orc_qubo_energy": (D, [C.c_int, I64, P, P, P, P, D, P]),
-            "orc_qubo_anneal_coloured": (D, [C.c_int, I64, P, P, P, P, P, P, C.c_int, P, C.c_int, C.c_int, U64, P,
-                                             P]),
+            "orc_qubo_anneal_coloured": (D, [C.c_int, I64, P, P, P, P, P, P, C.c_int, P, C.c_int, C.c_int, U64,
+                                             C.c_int, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -213,6 +214,10 @@ def draw_u53(seed, bit, sweep, stream=0) -> int:
     return int(orc().orc_draw_u53(seed, bit, sweep, stream))
 
 
+def draw_u53_hi(seed, bit, sweep, stream=0) -> int:
+    return int(orc().orc_draw_u53_hi(seed, bit, sweep, stream))
+
+
 def philox(ctr, key):
     c = np.array(ctr, np.uint32)
     k = np.array(key, np.uint32)
@@ -287,9 +292,11 @@ def qubo_energy(q: dict, x) -> float:
                                        float(q.get("offset", 0.0)), _p(x)))
 
 
-def qubo_anneal_coloured(q: dict, order, class_ptr, temps, refresh, seed):
+def qubo_anneal_coloured(q: dict, order, class_ptr, temps, refresh, seed, half=0):
     """The GPU's compensated-field weighted-QUBO sweep for one replica:
-    returns (x, tracked sum of accepted dE, max fp32-vs-fp64 field drift)."""
+    returns (x, tracked sum of accepted dE, max fp32-vs-fp64 field drift).
+    The replica draws half `half` of the Philox blocks keyed by `seed`
+    (qubo_key_half gives both for a branch of a solve)."""
     eu, ev = np.ascontiguousarray(q["eu"], np.int32), np.ascontiguousarray(q["ev"], np.int32)
     ew = np.ascontiguousarray(q["ew"], np.float32)
     h = None if q.get("h") is None else np.ascontiguousarray(q["h"], np.float32)
@@ -301,8 +308,16 @@ def qubo_anneal_coloured(q: dict, order, class_ptr, temps, refresh, seed):
     drift = C.c_float(0.0)
     track = orc().orc_qubo_anneal_coloured(n, int(eu.size), _p(eu), _p(ev), _p(ew), _p(h), _p(order), _p(cptr),
                                            int(cptr.size - 1), _p(temps), int(temps.size), int(refresh), int(seed),
-                                           _p(x), C.byref(drift))
+                                           int(half), _p(x), C.byref(drift))
     return x, float(track), float(drift.value)
+
+
+def qubo_key_half(branch: int, seed_offset: int = 0):
+    """The Philox key and half of branch `branch` of a weighted-QUBO solve
+    (qb_qubo.cu): launches of 64 replicas, replica r and r + 32 of a launch
+    share key seed_base + r (seed_base = 1 + seed_offset + 64 per launch)."""
+    r = branch % 64
+    return 1 + seed_offset + branch - (32 if r >= 32 else 0), 1 if r >= 32 else 0
 
 
 def fractions(X) -> np.ndarray:

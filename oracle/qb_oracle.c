@@ -65,6 +65,16 @@ uint64_t orc_draw_u53(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t stre
     return (((uint64_t)o[1] << 32) | (uint64_t)o[0]) >> 11;
 }
 
+/* The other half of the same block: the top 53 bits of words 3:2
+ * (qb_philox.cuh draw_u53_pair). */
+uint64_t orc_draw_u53_hi(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t stream) {
+    const uint32_t ctr[4] = {bit, sweep, stream, 0u};
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    orc_philox4x32_10(ctr, key, o);
+    return (((uint64_t)o[3] << 32) | (uint64_t)o[2]) >> 11;
+}
+
 /* Temperature of a sweep: ising_recon.hpp:129-131, ising_weighted.hpp:255-257. */
 double orc_temperature(double t_hot, double t_cold, int anneal, int sweep) {
     const int den = anneal - 1 > 1 ? anneal - 1 : 1;
@@ -494,12 +504,14 @@ double orc_qubo_energy(int n, int64_t m, const int32_t* eu, const int32_t* ev, c
  * neighbours that flipped at their latest visit (CSR built from the edge list
  * in edge order, TwoSum into the fp32 pair hi + lo), every `refresh` sweeps
  * (sweep > 0) recomputes the field in fp64 and records |fp32 - fp64|, then
- * accepts if dE <= 0 or u53 * 2^-53 < exp(-dE / T). Returns the tracked sum of
- * accepted dE in fp64. */
+ * accepts if dE <= 0 or u53 * 2^-53 < exp(-dE / T), u53 the half `half` (0:
+ * words 1:0, 1: words 3:2) of the Philox block of (seed, bit, sweep) -- the
+ * kernel's replicas r and r + 32 share a key and take one half each. Returns
+ * the tracked sum of accepted dE in fp64. */
 double orc_qubo_anneal_coloured(int n, int64_t m, const int32_t* eu, const int32_t* ev, const float* ew,
                                 const float* h, const int32_t* order, const int32_t* class_ptr, int nc,
-                                const double* temps, int sweeps, int refresh, uint64_t seed, uint8_t* x_out,
-                                float* drift_out) {
+                                const double* temps, int sweeps, int refresh, uint64_t seed, int half,
+                                uint8_t* x_out, float* drift_out) {
     int64_t* row = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
     for (int64_t e = 0; e < m; ++e) { row[eu[e] + 1]++; row[ev[e] + 1]++; }
     for (int i = 0; i < n; ++i) row[i + 1] += row[i];
@@ -539,9 +551,9 @@ double orc_qubo_anneal_coloured(int n, int64_t m, const int32_t* eu, const int32
                 }
                 const float Lf = H + L;
                 const float dE = x[i] ? -Lf : Lf;
-                const int acc = dE <= 0.0f ||
-                                (double)orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u) * 0x1.0p-53 <
-                                    exp(-(double)dE / T);
+                const uint64_t u53 = half ? orc_draw_u53_hi(seed, (uint32_t)i, (uint32_t)sweep, 0u)
+                                          : orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u);
+                const int acc = dE <= 0.0f || (double)u53 * 0x1.0p-53 < exp(-(double)dE / T);
                 f[i] = (uint8_t)acc;
                 if (acc) {
                     x[i] ^= 1u;

@@ -713,14 +713,13 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
         const float inv_T = float(1.0 / T);
         for (int ci = 0; ci < n_chunks; ++ci, ++gci) {
             const int4 c0 = cur0, c1 = cur1;
-            // stage the next chunk (wrapping into the next sweep), then wait for this one;
-            // its descriptor is fetched now and used after this chunk's work
+            // the next chunk (wrapping into the next sweep) is staged while this
+            // one runs; its descriptor is fetched now and used after this chunk's work
             const int nx = ci + 1 < n_chunks ? ci + 1 : 0;
             const int4 cn0 = __ldg(&chunks[2 * nx]), cn1 = __ldg(&chunks[2 * nx + 1]);
             if (PHASES) t_ph = clock64();
-            // this chunk was staged during the previous chunk's barrier
-            asm volatile("cp.async.wait_all;" ::: "memory");
-            __syncthreads();
+            // this chunk's stage was waited for and published before the
+            // previous chunk's block barriers (or the first grid barrier)
             if (PHASES) {
                 const long long t1 = clock64();
                 ph_wait += t1 - t_ph;

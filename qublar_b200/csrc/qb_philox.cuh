@@ -65,4 +65,13 @@ QB_HD uint64_t draw_u53(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t st
     return z >> 11;
 }
 
+// Both halves of one draw block: *lo = draw_u53 (words 1:0), *hi = the top 53
+// bits of words 3:2. Two replicas that share a key take one half each, so one
+// Philox evaluation serves both.
+QB_HD void draw_u53_pair(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t stream, uint64_t* lo, uint64_t* hi) {
+    const Philox4 o = philox4x32_10(bit, sweep, stream, 0u, uint32_t(seed), uint32_t(seed >> 32));
+    *lo = ((uint64_t(o.v[1]) << 32) | uint64_t(o.v[0])) >> 11;
+    *hi = ((uint64_t(o.v[3]) << 32) | uint64_t(o.v[2])) >> 11;
+}
+
 }  // namespace qb

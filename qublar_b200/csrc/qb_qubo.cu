@@ -22,9 +22,12 @@
 // Every `refresh` sweeps a visit also recomputes L_i from scratch in fp64,
 // records |fp32 - fp64| (the drift) and restarts hi + lo from it. The final
 // energies are recomputed in fp64 from scratch by a separate kernel.
-// Acceptance: dE <= 0, else u53 * 2^-53 < exp(-dE / T) in double, u53 the
-// Philox draw of (replica seed, original bit, sweep); uphill_accept settles
-// most draws in fp32 with the same outcome.
+// Acceptance: dE <= 0, else u53 * 2^-53 < exp(-dE / T) in double, u53 a
+// half of the Philox block of (key, original bit, sweep): of the 64 replicas
+// of a launch, replica r < 32 takes words 1:0 of key seed0 + r and replica
+// r + 32 words 3:2 of the same key (branch b of a solve: key seed_base + b -
+// 32 [b mod 64 >= 32]), so one evaluation serves both replicas of a lane;
+// uphill_accept settles most draws in fp32 with the same outcome.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A)
     const int tw = int(gridDim.x) * wpc;
     const int r0 = lane, r1 = lane + 32;
     const bool has0 = r0 < A.R, has1 = r1 < A.R;
-    const uint64_t seed_a = A.seed0 + uint64_t(r0), seed_b = A.seed0 + uint64_t(r1);
+    const uint64_t key = A.seed0 + uint64_t(r0);   // replicas r0 and r1 share the draw block
     float eh0 = 0.0f, el0 = 0.0f, eh1 = 0.0f, el1 = 0.0f;
     unsigned long long acc_a = 0, acc_b = 0;
     float dr0 = 0.0f, dr1 = 0.0f;
@@ -209,11 +212,11 @@ __global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A)
                 const float L0 = __fadd_rn(hi0, lo0), L1 = __fadd_rn(hi1, lo1);
                 const float dE0 = b0 ? -L0 : L0, dE1 = b1 ? -L1 : L1;
                 const uint32_t oj = uint32_t(__ldg(A.order + j));
-                bool acc0 = false, acc1 = false;
-                if (has0)
-                    acc0 = dE0 <= 0.0f || uphill_accept(draw_u53(seed_a, oj, uint32_t(sweep), 0u), double(dE0), T, inv_T);
-                if (has1)
-                    acc1 = dE1 <= 0.0f || uphill_accept(draw_u53(seed_b, oj, uint32_t(sweep), 0u), double(dE1), T, inv_T);
+                const bool up0 = has0 && !(dE0 <= 0.0f), up1 = has1 && !(dE1 <= 0.0f);   // uphill (or NaN: rejected)
+                uint64_t u0 = 0, u1 = 0;
+                if (up0 || up1) draw_u53_pair(key, oj, uint32_t(sweep), 0u, &u0, &u1);
+                const bool acc0 = has0 && (!up0 || uphill_accept(u0, double(dE0), T, inv_T));
+                const bool acc1 = has1 && (!up1 || uphill_accept(u1, double(dE1), T, inv_T));
                 const unsigned m0 = __ballot_sync(kFullMask, acc0), m1 = __ballot_sync(kFullMask, acc1);
                 const unsigned long long mask = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
                 if (lane == 0) {

@@ -28,6 +28,24 @@ def test_philox_draws_uniform():
     assert len(set(u.tolist())) == u.size
 
 
+def test_draw_halves_are_the_philox_words():
+    """draw_u53 takes words 1:0 of the Philox block of (seed, bit, sweep),
+    draw_u53_hi words 3:2 (the weighted-QUBO kernel's second replica of a lane)."""
+    for seed, bit, sweep in [(1, 0, 0), (77, 123456, 4999), (2 ** 40 + 3, 7, 1)]:
+        o = O.philox([bit, sweep, 0, 0], [seed & 0xFFFFFFFF, seed >> 32])
+        assert O.draw_u53(seed, bit, sweep) == ((o[1] << 32) | o[0]) >> 11
+        assert O.draw_u53_hi(seed, bit, sweep) == ((o[3] << 32) | o[2]) >> 11
+
+
+def test_qubo_branch_keys():
+    """Branch b of a weighted-QUBO solve: launches of 64 replicas; replica r
+    and r + 32 of a launch share one key (words 1:0 and 3:2)."""
+    assert O.qubo_key_half(0) == (1, 0) and O.qubo_key_half(31) == (32, 0)
+    assert O.qubo_key_half(32) == (1, 1) and O.qubo_key_half(63) == (32, 1)
+    assert O.qubo_key_half(64) == (65, 0) and O.qubo_key_half(96) == (65, 1)
+    assert O.qubo_key_half(69, 5) == (75, 0)
+
+
 def test_splitmix_matches_reference_stream():
     s = synth.SplitMix(1)
     v = [s.next() for _ in range(5)]
