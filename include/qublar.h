@@ -187,6 +187,13 @@ qb_status qb_problem_create_residual(const qb_residual_desc* desc, const qb_opts
 qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_opts* opts, qb_problem** out);
 void qb_problem_destroy(qb_problem* p);
 
+/* The device memory of problems and solves comes from a stream-ordered pool
+ * the library keeps per device: destroyed problems and results return their
+ * buffers to it, and later ones reuse them without mapping memory afresh
+ * (qb_problem_destroy waits for the device before it returns them). This call
+ * waits for `device` and hands the memory the pool holds back to the driver. */
+qb_status qb_device_trim(int32_t device);
+
 typedef struct qb_problem_info {
     int32_t kind;           /* QB_KIND_* */
     int32_t n;              /* bits */

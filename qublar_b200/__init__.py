@@ -29,7 +29,7 @@ from ._abi import (KIND_ISING, KIND_QUBO, KIND_RESIDUAL, OPT_DEFER_UPLOAD, OPT_R
                    ServerStats, check, check_edge_lengths, check_residual_lengths, lib, ptr)
 
 __all__ = ["QBError", "Schedule", "Budget", "IsingProblem", "ResidualProblem", "QuboProblem", "Result", "RunOut", "BatchOut",
-           "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "lib",
+           "branch_fractions", "anneal_branch", "anneal", "run_batch", "classify", "device_count", "device_trim", "lib",
            "Batch", "solve_batch", "autotune_batch", "Server", "OPT_DEFER_UPLOAD", "OPT_RESID_CLUSTER", "OPT_TRACE", "parse_rudy",
            "freeze_rock", "roi_qubo", "enumerate_qubo", "parse_qubo_text", "write_qubo_text", "write_ising_out",
            "write_roi_text"]
@@ -68,6 +68,12 @@ class Budget(Schedule):
 
 def device_count() -> int:
     return int(lib().qb_device_count())
+
+
+def device_trim(device: int = 0) -> None:
+    """Hands the device memory the library's pool keeps for reuse back to the
+    driver (qb_device_trim)."""
+    check(lib().qb_device_trim(device))
 
 
 def _opts(device: int = -1, stream=None, flags: int = 0) -> Opts:

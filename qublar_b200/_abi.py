@@ -185,6 +185,7 @@ SIGNATURES = {
     "qb_energies_qubo": (C.c_int, [_P, _P, C.c_int32, _P]),
     "qb_solve_residual_noalloc": (C.c_int, [_P, C.POINTER(ScheduleC), C.c_uint32, C.c_uint64, _P, _P, _P]),
     "qb_metropolis_check": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, _P, _P, _P]),
+    "qb_device_trim": (C.c_int, [C.c_int32]),
     "qb_batch_autotune": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.c_int32, C.POINTER(Opts),
                                     C.POINTER(BatchConfig)]),
     "qb_solve_batch": (C.c_int, [C.POINTER(BatchItem), C.c_int32, C.POINTER(BatchConfig), C.POINTER(Opts),

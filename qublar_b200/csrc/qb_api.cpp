@@ -43,7 +43,11 @@ qb_status select_device(const qb_opts* o, int* dev_out) {
 qb_status alloc_async(DevBuf& b, size_t bytes, cudaStream_t st) {
     b.release();
     if (bytes == 0) return QB_OK;
-    QB_CUDA(cudaMallocAsync(&b.p, bytes, st));
+    int dev = 0;
+    QB_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool = library_pool(dev);
+    if (pool) QB_CUDA(cudaMallocFromPoolAsync(&b.p, bytes, pool, st));
+    else QB_CUDA(cudaMallocAsync(&b.p, bytes, st));
     b.bytes = bytes;
     b.pooled = true;
     b.pool_stream = st;
@@ -1001,11 +1005,12 @@ extern "C" qb_status qb_problem_create_ising(const qb_ising_desc* desc, const qb
             p->host.ew.assign(desc->ew, desc->ew + m);
             p->device_bytes = ising_device_bytes(p->ising);
         } else if (s == QB_OK) {
+            AsyncAllocScope pool(stream_of(opts), true);   // returned at destroy, after a device synchronise
             s = upload_ising(p->ising, desc, stream_of(opts), &p->device_bytes);
             p->uploaded = s == QB_OK;
         }
         if (s != QB_OK) {
-            delete p;
+            qb_problem_destroy(p);   // waits for any copy the failed upload queued
             return s;
         }
         *out = p;
@@ -1053,6 +1058,7 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
             h.kappa = desc->kappa;
             p->device_bytes = residual_device_bytes(p->resid);
         } else if (s == QB_OK) {
+            AsyncAllocScope pool(stream_of(opts), true);   // returned at destroy, after a device synchronise
             s = upload_residual(p->resid, desc, stream_of(opts), &p->device_bytes);
             p->uploaded = s == QB_OK;
         }
@@ -1060,7 +1066,7 @@ extern "C" qb_status qb_problem_create_residual(const qb_residual_desc* desc, co
             std::fprintf(stderr, "[qb plan] check %.1f ms, plan %.1f ms, upload %.1f ms\n", ms(t0, t1), ms(t1, t2),
                          ms(t2, now()));
         if (s != QB_OK) {
-            delete p;
+            qb_problem_destroy(p);   // waits for any copy the failed upload queued
             return s;
         }
         *out = p;
@@ -1088,11 +1094,12 @@ extern "C" qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_o
             h.offset = desc->offset;
             p->device_bytes = qubo_device_bytes(p->qubo);
         } else if (s == QB_OK) {
+            AsyncAllocScope pool(stream_of(opts), true);   // returned at destroy, after a device synchronise
             s = upload_qubo(p->qubo, desc, stream_of(opts), &p->device_bytes);
             p->uploaded = s == QB_OK;
         }
         if (s != QB_OK) {
-            delete p;
+            qb_problem_destroy(p);   // waits for any copy the failed upload queued
             return s;
         }
         *out = p;
@@ -1103,6 +1110,9 @@ extern "C" qb_status qb_problem_create_qubo(const qb_qubo_desc* desc, const qb_o
 extern "C" void qb_problem_destroy(qb_problem* p) {
     if (!p) return;
     cudaSetDevice(p->device);
+    // the problem's buffers go back to the library's pool: no work that reads
+    // them may still be queued (cudaFree used to wait for the device the same way)
+    cudaDeviceSynchronize();
     delete p;
 }
 
@@ -1555,6 +1565,15 @@ extern "C" qb_status qb_metropolis_check(const uint64_t* u53, const double* dE, 
         QB_CUDA(cudaMemcpy(fast, o, size_t(n), cudaMemcpyDeviceToHost));
         QB_CUDA(cudaMemcpy(accept, o + n, size_t(n), cudaMemcpyDeviceToHost));
         QB_CUDA(cudaMemcpy(exact, o + 2 * size_t(n), size_t(n), cudaMemcpyDeviceToHost));
+        return QB_OK;
+    });
+}
+
+extern "C" qb_status qb_device_trim(int32_t device) {
+    return guarded("qb_device_trim", [&]() -> qb_status {
+        QB_CUDA(cudaSetDevice(device));
+        QB_CUDA(cudaDeviceSynchronize());
+        if (cudaMemPool_t pool = library_pool(device)) QB_CUDA(cudaMemPoolTrimTo(pool, 0));
         return QB_OK;
     });
 }

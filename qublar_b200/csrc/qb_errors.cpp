@@ -1,6 +1,7 @@
 // Status codes and the thread-local error message of the C ABI. The reference
 // exits on a CUDA error (src/ising_gpu.cuh:44-52); the library reports it.
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "qb_internal.hpp"
@@ -10,17 +11,44 @@ namespace qb {
 namespace {
 thread_local std::string g_last_error;
 thread_local bool g_async_on = false;
+thread_local bool g_free_legacy = false;
 thread_local cudaStream_t g_async_stream = nullptr;
+constexpr int kMaxPoolDevices = 64;
 }
 
-AsyncAllocScope::AsyncAllocScope(cudaStream_t st) : prev(g_async_stream), prev_on(g_async_on) {
+AsyncAllocScope::AsyncAllocScope(cudaStream_t st, bool free_on_legacy)
+    : prev(g_async_stream), prev_on(g_async_on), prev_legacy(g_free_legacy) {
     g_async_on = true;
     g_async_stream = st;
+    g_free_legacy = free_on_legacy;
 }
 
 AsyncAllocScope::~AsyncAllocScope() {
     g_async_on = prev_on;
     g_async_stream = prev;
+    g_free_legacy = prev_legacy;
+}
+
+cudaMemPool_t library_pool(int dev) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[kMaxPoolDevices] = {};
+    if (dev < 0 || dev >= kMaxPoolDevices) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps pr{};
+        pr.allocType = cudaMemAllocationTypePinned;
+        pr.location.type = cudaMemLocationTypeDevice;
+        pr.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &pr) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = ~uint64_t(0);   // freed memory stays in the pool
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
 }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
@@ -43,9 +71,11 @@ qb_status DevBuf::alloc(size_t n) {
     if (n == 0) return QB_OK;
     cudaError_t e;
     if (g_async_on) {
-        e = cudaMallocAsync(&p, n, g_async_stream);
+        int dev = 0;
+        cudaMemPool_t pool = cudaGetDevice(&dev) == cudaSuccess ? library_pool(dev) : nullptr;
+        e = pool ? cudaMallocFromPoolAsync(&p, n, pool, g_async_stream) : cudaMallocAsync(&p, n, g_async_stream);
         pooled = e == cudaSuccess;
-        pool_stream = g_async_stream;
+        pool_stream = g_free_legacy ? nullptr : g_async_stream;
     } else {
         e = cudaMalloc(&p, n);
     }

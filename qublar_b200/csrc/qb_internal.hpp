@@ -48,18 +48,28 @@ qb_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 
 // ---- device buffer (RAII, library-owned) -------------------------------------
 
-// Allocations of a DevBuf are stream-ordered (cudaMallocAsync / cudaFreeAsync)
-// while an AsyncAllocScope is open on the allocating thread: a server thread
-// takes and returns request memory without the device-wide synchronisation of
-// cudaMalloc/cudaFree, so work on other streams keeps running.
+// Allocations of a DevBuf are stream-ordered (from the library's pool on
+// stream st, returned with cudaFreeAsync) while an AsyncAllocScope is open on
+// the allocating thread: a server thread takes and returns request memory
+// without the device-wide synchronisation of cudaMalloc/cudaFree, so work on
+// other streams keeps running, and repeated problems reuse the pool's memory
+// instead of mapping it afresh. free_on_legacy: the buffers are returned on the
+// legacy default stream (for buffers that outlive the caller's stream; their
+// owner synchronises the device first).
 struct AsyncAllocScope {
-    explicit AsyncAllocScope(cudaStream_t st);
+    explicit AsyncAllocScope(cudaStream_t st, bool free_on_legacy = false);
     ~AsyncAllocScope();
     AsyncAllocScope(const AsyncAllocScope&) = delete;
     AsyncAllocScope& operator=(const AsyncAllocScope&) = delete;
     cudaStream_t prev;
     bool prev_on;
+    bool prev_legacy;
 };
+
+// The library's stream-ordered memory pool of a device (created on first use;
+// it keeps freed memory for reuse until qb_device_trim), or null if the device
+// has none.
+cudaMemPool_t library_pool(int dev);
 
 struct DevBuf {
     void* p = nullptr;
