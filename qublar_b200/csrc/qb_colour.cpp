@@ -183,38 +183,43 @@ Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* ro
     }
     // First fit: the lowest colour on none of the bit's rays and on none of its
     // prior neighbours.
+    // the ray and neighbour lists gathered into visit order (in parallel), so
+    // that the first-fit loop streams them instead of fetching every bit's
+    // lists from a random place of the caller's arrays
+    std::vector<int64_t> vrow(size_t(n) + 1, 0), vnb(size_t(n) + 1, 0);
+    for (int v = 0; v < n; ++v) {
+        const int i = vis[size_t(v)];
+        vrow[size_t(v) + 1] = vrow[size_t(v)] + (row_ptr[i + 1] - row_ptr[i]);
+        vnb[size_t(v) + 1] = vnb[size_t(v)] + (nbr_ptr[i + 1] - nbr_ptr[i]);
+    }
+    RawVec<int32_t> vray(size_t(vrow[size_t(n)]) + 1), vnbr(size_t(vnb[size_t(n)]) + 1);
+#pragma omp parallel for schedule(static, 1024)
+    for (int v = 0; v < n; ++v) {
+        const int i = vis[size_t(v)];
+        std::memcpy(vray.data() + vrow[size_t(v)], ray + row_ptr[i], sizeof(int32_t) * size_t(row_ptr[i + 1] - row_ptr[i]));
+        std::memcpy(vnbr.data() + vnb[size_t(v)], nbr + nbr_ptr[i], sizeof(int32_t) * size_t(nbr_ptr[i + 1] - nbr_ptr[i]));
+    }
     std::vector<uint64_t> forbid;
     for (size_t v = 0; v < vis.size(); ++v) {
         const int i = vis[v];
-        // a pipeline of prefetches, each stage on data the one before brought
-        // in: the offsets of the bit 12 visits ahead, the ray and neighbour
-        // lists of the bit 6 ahead, and the rows of the bit 2 ahead (random
-        // rays)
-        if (v + 12 < vis.size()) {
-            const int i12 = vis[v + 12];
-            __builtin_prefetch(row_ptr + i12);
-            __builtin_prefetch(nbr_ptr + i12);
-        }
-        if (v + 6 < vis.size()) {
-            const int i6 = vis[v + 6];
-            for (int k = row_ptr[i6]; k < row_ptr[i6 + 1]; k += 16) __builtin_prefetch(ray + k);
-            if (nbr_ptr[i6] < nbr_ptr[i6 + 1]) __builtin_prefetch(nbr + nbr_ptr[i6]);
-        }
-        if (v + 2 < vis.size()) {
-            const int i2 = vis[v + 2];
-            for (int k = row_ptr[i2]; k < row_ptr[i2 + 1]; ++k)
-                __builtin_prefetch(used + size_t(ray[k]) * size_t(words), 1);
-            for (int k = nbr_ptr[i2]; k < nbr_ptr[i2 + 1]; ++k) __builtin_prefetch(c.colour.data() + nbr[k]);
+        const int32_t* rl = vray.data() + vrow[v];
+        const int nrl = int(vrow[v + 1] - vrow[v]);
+        const int32_t* nl = vnbr.data() + vnb[v];
+        const int nnl = int(vnb[v + 1] - vnb[v]);
+        // the rows (random rays) and neighbour colours of the bit 3 visits ahead
+        if (v + 3 < vis.size()) {
+            for (int64_t k = vrow[v + 3]; k < vrow[v + 4]; ++k) __builtin_prefetch(used + size_t(vray[size_t(k)]) * size_t(words), 1);
+            for (int64_t k = vnb[v + 3]; k < vnb[v + 4]; ++k) __builtin_prefetch(c.colour.data() + vnbr[size_t(k)]);
         }
         int cc = -1;
         if (words == kColourWords) {
             uint64_t f[kColourWords] = {};
-            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
-                const uint64_t* u = used + size_t(ray[k]) * kColourWords;
+            for (int k = 0; k < nrl; ++k) {
+                const uint64_t* u = used + size_t(rl[k]) * kColourWords;
                 for (int q = 0; q < kColourWords; ++q) f[q] |= u[q];
             }
-            for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
-                const int cj = c.colour[size_t(nbr[k])];
+            for (int k = 0; k < nnl; ++k) {
+                const int cj = c.colour[size_t(nl[k])];
                 if (cj >= 0) f[cj >> 6] |= uint64_t(1) << (cj & 63);
             }
             for (int q = 0; q < kColourWords && cc < 0; ++q)
@@ -223,12 +228,12 @@ Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* ro
         }
         while (cc < 0) {
             forbid.assign(size_t(words), 0);
-            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
-                const uint64_t* u = used + size_t(ray[k]) * size_t(words);
+            for (int k = 0; k < nrl; ++k) {
+                const uint64_t* u = used + size_t(rl[k]) * size_t(words);
                 for (int q = 0; q < words; ++q) forbid[size_t(q)] |= u[q];
             }
-            for (int k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
-                const int cj = c.colour[size_t(nbr[k])];
+            for (int k = 0; k < nnl; ++k) {
+                const int cj = c.colour[size_t(nl[k])];
                 if (cj >= 0) forbid[size_t(cj >> 6)] |= uint64_t(1) << (cj & 63);
             }
             for (int q = 0; q < words && cc < 0; ++q)
@@ -236,8 +241,7 @@ Colouring colour_residual(int n, int n_rays, int* max_ray_len, const int32_t* ro
             if (cc < 0) alloc_rows(words * 2);
         }
         c.colour[size_t(i)] = cc;
-        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
-            used[size_t(ray[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
+        for (int k = 0; k < nrl; ++k) used[size_t(rl[k]) * size_t(words) + size_t(cc >> 6)] |= uint64_t(1) << (cc & 63);
     }
     finish_colouring(c, n);
     return c;
