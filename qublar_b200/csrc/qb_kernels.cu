@@ -526,6 +526,7 @@ constexpr int kLockB = 256;    // staged bits per chunk
 constexpr int kLockN = 1536;   // staged neighbour entries per chunk
 constexpr int kSeg = 16;       // entries per segment: one warp, one batch of loads
 constexpr int kLockSegs = kLockE / kSeg + kLockB;   // segments a chunk can hold
+constexpr int kStageWarps = 2;                       // warps that stage the next chunk
 constexpr int kLockMaxNG = 4;  // branch groups of 16 one launch serves (64 branches)
 constexpr uint32_t kRayMask = 0x7FFFFFFFu;   // entry word 0: ray | (w < 0) << 31
 
@@ -727,10 +728,12 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             }
             const LockStage St = stage(gci & 1);
             // the other buffer was last read by the previous chunk, which every
-            // thread has finished: the upper half of the CTA (warps without
-            // phase-A items, mostly) stages the next chunk into it now
-            if (tid >= kLockThreads / 2)
-                lock_stage(A, cn0, cn1, stage((gci + 1) & 1), tid - kLockThreads / 2, kLockThreads / 2);
+            // thread has finished: the CTA's last kStageWarps warps (without
+            // phase-A items, mostly: items go to the lowest warps first) stage
+            // the next chunk into it now, so no segment item waits behind the
+            // copies' issue
+            if (tid >= kLockThreads - 32 * kStageWarps)
+                lock_stage(A, cn0, cn1, stage((gci + 1) & 1), tid - (kLockThreads - 32 * kStageWarps), 32 * kStageWarps);
             cp_async_commit();
             const int sweep_n = nx == 0 ? sweep + 1 : sweep;
             const int nb = c0.y - c0.x;
