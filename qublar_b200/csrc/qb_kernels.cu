@@ -613,6 +613,8 @@ __device__ __forceinline__ void lock_stage(const ResidLockArgs& A, const int4 c0
 template <bool PHASES, int NG>
 __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLockArgs A) {
     static_assert(NG >= 1 && NG <= kLockMaxNG, "16-branch groups: 1 .. kLockMaxNG");
+    __shared__ unsigned s_seen_round;   // the last class barrier this CTA saw complete
+    __shared__ int s_wait_fail;
     extern __shared__ __align__(16) unsigned char smem[];
     const int tid = int(threadIdx.x);
     const int lane = tid & 31;
@@ -667,7 +669,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
     unsigned round = 0;
     unsigned long long my_accepts = 0;
     __shared__ unsigned long long s_acc_count;
-    if (tid == 0) s_acc_count = 0;
+    if (tid == 0) {
+        s_acc_count = 0;
+        s_seen_round = 0;
+        s_wait_fail = 0;
+    }
     if (tid < 16 * kLockMaxNG) s_trace[tid] = 0.0;
     // x = 0: rho_b = -sqrt|w_b| d_b for every branch
     for (size_t k = size_t(p) * kLockThreads + tid; k < size_t(A.n_rays) * RP; k += size_t(P) * kLockThreads) {
@@ -909,7 +915,7 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 grid_arrive(A.bar);
                 seg_map((gci + 1) & 1, cn0);
                 if (pre_draw && sweep_n < A.sweeps) make_draws((gci + 1) & 1, cn0.x, cn0.y - cn0.x, sweep_n);
-                ok = grid_wait(A.bar, A.err, ++round, per_round, A.spin_limit);
+                ok = grid_wait2(A.bar, A.err, ++round, per_round, A.spin_limit, &s_seen_round, &s_wait_fail);
             } else {
                 __syncthreads();
                 seg_map((gci + 1) & 1, cn0);
