@@ -828,8 +828,16 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
                 if (live) {
                     const int nsg = (int(m0.y) + kSeg - 1) / kSeg;
                     const int s0 = int(m1.w);
+                    // the first four segment sums loaded together, then every sum
+                    // added in order (most bits have at most four segments)
+                    float hv[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) hv[q] = q < nsg ? hseg[((s0 + q) * NG + g) * 16 + br] : 0.0f;
                     float h = 0.0f;
-                    for (int q = 0; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * NG + g) * 16 + br]);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (q < nsg) h = __fadd_rn(h, hv[q]);
+                    for (int q = 4; q < nsg; ++q) h = __fadd_rn(h, hseg[((s0 + q) * NG + g) * 16 + br]);
                     const float delta = xi ? -1.0f : 1.0f;
                     const float t = __fadd_rn(__uint_as_float(m1.x), h);
                     const float prior = __fmul_rn(A.lambda, float(ne - 2 * unlike));
