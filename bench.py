@@ -40,11 +40,11 @@ METRIC = "spin-flip attempts/s"
 BRANCHES = 16
 # DRAM bytes (read + write) per sweep of resid_lockstep_kernel from the
 # committed ncu capture of a 10-sweep launch on the same pyramid and 16
-# branches (profiles/resid_lockstep_pyramid.md): 1049.2 MB + 4.5 MB over 10
+# branches (profiles/resid_lockstep_pyramid.md): 1040.9 MB + 4.6 MB over 10
 # sweeps. The bit->ray structure (8-byte entries, 87 MB) streams from DRAM
 # once per sweep, so the traffic of a full launch is this figure times its
 # sweeps.
-NCU_TRAFFIC_PER_SWEEP = (1049.175e6 + 4.531968e6) / 10
+NCU_TRAFFIC_PER_SWEEP = (1040.907e6 + 4.588288e6) / 10
 
 
 def log(*a):
