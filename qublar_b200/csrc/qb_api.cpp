@@ -972,18 +972,21 @@ qb_status qb::replan_residual(qb_problem* p, int slices) {
 
 void qb::problem_release_device(qb_problem* p) {
     IsingPlan& I = p->ising;
-    DevBuf* ib[] = {&I.d_row, &I.d_adj, &I.d_w, &I.d_f0, &I.d_order, &I.d_class_ptr, &I.d_eu, &I.d_ev, &I.d_ew};
-    for (DevBuf* b : ib) b->release();
     ResidualPlan& R = p->resid;
-    DevBuf* rb[] = {&R.d_row, &R.d_ent, &R.d_lin, &R.d_q, &R.d_nbr_ptr, &R.d_nbr_home, &R.d_order, &R.d_class_ptr,
-                    &R.d_chunks, &R.d_chunk_ptr, &R.d_d, &R.d_w64, &R.d_rrow, &R.d_rbit, &R.d_ra, &R.d_meta,
-                    &R.d_nbr_new, &R.d_rbit_new, &R.d_o_row, &R.d_o_ray, &R.d_o_a, &R.d_o_nbr_ptr, &R.d_o_nbr,
-                    &R.d_o_lin, &R.d_o_rbit};
-    for (DevBuf* b : rb) b->release();
     QuboPlan& Q = p->qubo;
-    DevBuf* qbf[] = {&Q.d_row, &Q.d_adj, &Q.d_J, &Q.d_h, &Q.d_order, &Q.d_class_ptr, &Q.d_eu, &Q.d_ev, &Q.d_ew, &Q.d_ho};
-    for (DevBuf* b : qbf) b->release();
-    p->d_temp.release();
+    DevBuf* all[] = {&I.d_row, &I.d_adj, &I.d_w, &I.d_f0, &I.d_order, &I.d_class_ptr, &I.d_eu, &I.d_ev, &I.d_ew,
+                     &R.d_row, &R.d_ent, &R.d_lin, &R.d_q, &R.d_nbr_ptr, &R.d_nbr_home, &R.d_order, &R.d_class_ptr,
+                     &R.d_chunks, &R.d_chunk_ptr, &R.d_d, &R.d_w64, &R.d_rrow, &R.d_rbit, &R.d_ra, &R.d_meta,
+                     &R.d_nbr_new, &R.d_rbit_new, &R.d_o_row, &R.d_o_ray, &R.d_o_a, &R.d_o_nbr_ptr, &R.d_o_nbr,
+                     &R.d_o_lin, &R.d_o_rbit,
+                     &Q.d_row, &Q.d_adj, &Q.d_J, &Q.d_h, &Q.d_order, &Q.d_class_ptr, &Q.d_eu, &Q.d_ev, &Q.d_ew, &Q.d_ho,
+                     &p->d_temp};
+    // buffers of the plain create path go back to the pool on the legacy
+    // stream: no queued work may still read them
+    bool wait = false;
+    for (DevBuf* b : all) wait |= b->sync_free;
+    if (wait) cudaDeviceSynchronize();
+    for (DevBuf* b : all) b->release();
     p->uploaded = false;
 }
 

@@ -75,6 +75,7 @@ qb_status DevBuf::alloc(size_t n) {
         cudaMemPool_t pool = cudaGetDevice(&dev) == cudaSuccess ? library_pool(dev) : nullptr;
         e = pool ? cudaMallocFromPoolAsync(&p, n, pool, g_async_stream) : cudaMallocAsync(&p, n, g_async_stream);
         pooled = e == cudaSuccess;
+        sync_free = pooled && g_free_legacy;
         pool_stream = g_free_legacy ? nullptr : g_async_stream;
     } else {
         e = cudaMalloc(&p, n);

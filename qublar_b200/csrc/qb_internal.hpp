@@ -75,14 +75,17 @@ struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
     bool pooled = false;              // from cudaMallocAsync: returned with cudaFreeAsync
+    bool sync_free = false;           // returned on the legacy stream: its owner waits for the device first
     cudaStream_t pool_stream = nullptr;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), pooled(o.pooled), pool_stream(o.pool_stream) {
+    DevBuf(DevBuf&& o) noexcept
+        : p(o.p), bytes(o.bytes), pooled(o.pooled), sync_free(o.sync_free), pool_stream(o.pool_stream) {
         o.p = nullptr;
         o.bytes = 0;
         o.pooled = false;
+        o.sync_free = false;
     }
     DevBuf& operator=(DevBuf&& o) noexcept {
         if (this != &o) {
@@ -90,10 +93,12 @@ struct DevBuf {
             p = o.p;
             bytes = o.bytes;
             pooled = o.pooled;
+            sync_free = o.sync_free;
             pool_stream = o.pool_stream;
             o.p = nullptr;
             o.bytes = 0;
             o.pooled = false;
+            o.sync_free = false;
         }
         return *this;
     }
@@ -104,6 +109,7 @@ struct DevBuf {
             else cudaFree(p);
         }
         pooled = false;
+        sync_free = false;
         p = nullptr;
         bytes = 0;
     }
