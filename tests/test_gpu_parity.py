@@ -113,6 +113,23 @@ def test_residual_small_bit_exact():
     assert (r.tristate() == O.classify(p)).all()
 
 
+@pytest.mark.parametrize("R", [40, 64], ids=["three_groups", "four_groups"])
+def test_residual_branch_groups_bit_exact(R):
+    """The lockstep sweep serves 16-branch groups with one compiled instance
+    per group count: with 40 (three groups) and 64 branches, branches of every
+    group equal the oracle's coloured-Philox run of the same seed bit for bit."""
+    a = _small_tomo()
+    P = ResidualProblem.from_arrays(a)
+    s = Schedule(50.0, 1.0, 60, 20, 20)
+    r = P.solve(s, R, 5)
+    X = r.branches()
+    order, _ = P.colouring()
+    temps = O.temperatures(s.t_hot, s.t_cold, s.anneal_sweeps, s.hold_sweeps)
+    for k in sorted({0, 15, 16, 31, 32, R - 1}):
+        x, _ = O.resid_anneal_coloured(a, order, temps, s.refresh_sweeps, k + 1 + 5, mode=P.info().variant)
+        assert (X[k] == x).all(), k
+
+
 def test_residual_small_statistical_vs_reference():
     """64 branches against the reference's anneal_branch over seeds 1..64:
     per-bit void fractions within binomial error (two-sample z < 4.5 for
