@@ -562,7 +562,7 @@ struct ResidLockArgs {
     float* drift;
     unsigned long long* accepts;
     double* trace;              // nullable: R x sweeps, the sum of accepted dE of each sweep
-    unsigned long long* phase;  // PHASES builds: per CTA {stage wait, items, barrier, chunks} clock64 sums
+    unsigned long long* phase;  // PHASES builds: per CTA {stage wait, items, barrier, chunks, A, A-C, C} clock64 sums
 };
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -727,11 +727,6 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             if (PHASES) t_ph = clock64();
             // this chunk's stage was waited for and published before the
             // previous chunk's block barriers (or the first grid barrier)
-            if (PHASES) {
-                const long long t1 = clock64();
-                ph_wait += t1 - t_ph;
-                t_ph = t1;
-            }
             const LockStage St = stage(gci & 1);
             // the other buffer was last read by the previous chunk, which every
             // thread has finished: the CTA's last kStageWarps warps (without
@@ -916,7 +911,11 @@ __global__ void __launch_bounds__(kLockThreads, 1) resid_lockstep_kernel(ResidLo
             // once every thread's copies are; the block barrier below publishes
             // it, its segment map is built after that, and the closing block
             // barrier publishes the map
-            asm volatile("cp.async.wait_all;" ::: "memory");
+            {
+                const long long tw = PHASES ? clock64() : 0;
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                if (PHASES) ph_wait += clock64() - tw;
+            }
             if (c0.w & 1) {
                 // arrive; build the map and make the next chunk's draws while
                 // the others arrive; then wait
@@ -1388,9 +1387,9 @@ qb_status launch_resid_lockstep(const ResidualPlan& p, const SolveBuffers& b, in
             pc += h[8 * c + 6];
             itmax = std::max(itmax, double(h[8 * c + 1]) / std::max(1.0, double(h[8 * c + 3])));
         }
-        std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: stage wait %.0f, items %.0f "
-                     "(A %.0f, B %.0f, C %.0f; slowest CTA's mean %.0f), barrier %.0f\n",
-                     ch / grid, w / ch, it / ch, pa / ch, (pb - pc) / ch, pc / ch, itmax, br / ch);
+        std::fprintf(stderr, "[qublar] lockstep phases per CTA: chunks %.0f, cycles per chunk: items %.0f "
+                     "(A %.0f, B %.0f, C %.0f; slowest CTA's mean %.0f), barrier %.0f (of which the next stage's wait %.0f)\n",
+                     ch / grid, it / ch, pa / ch, (pb - pc) / ch, pc / ch, itmax, br / ch, w / ch);
     }
     return QB_OK;
 }
