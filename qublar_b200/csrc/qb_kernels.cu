@@ -987,24 +987,45 @@ __device__ double block_sum_f64(double v, double* red) {
     return t;
 }
 
-__global__ void __launch_bounds__(1024) resid_energy_kernel(ResidEnergyArgs A) {
+// Partial sums of state s over block j's share of the rays (data term) and of
+// the bits (prior term); grid = (blocks per state, states), so every SM takes
+// part. The partials are added in block order afterwards.
+__global__ void __launch_bounds__(256) resid_energy_part_kernel(ResidEnergyArgs A, double* part) {
     __shared__ double red[32];
-    const uint8_t* x = A.X + size_t(blockIdx.x) * size_t(A.n);
+    const int st = int(blockIdx.y), j = int(blockIdx.x), nb = int(gridDim.x);
+    const uint8_t* x = A.X + size_t(st) * size_t(A.n);
+    const int r0 = int(int64_t(A.n_rays) * j / nb), r1 = int(int64_t(A.n_rays) * (j + 1) / nb);
+    const int i0 = int(int64_t(A.n) * j / nb), i1 = int(int64_t(A.n) * (j + 1) / nb);
     double data = 0.0, prior = 0.0;
-    for (int b = int(threadIdx.x); b < A.n_rays; b += blockDim.x) {
+    for (int b = r0 + int(threadIdx.x); b < r1; b += blockDim.x) {
         double r = -A.d[b];
         for (int k = A.rrow[b]; k < A.rrow[b + 1]; ++k)
             if (x[A.rbit[k]]) r += double(A.ra[k]);
         data += 0.5 * A.w[b] * r * r;
     }
-    for (int i = int(threadIdx.x); i < A.n; i += blockDim.x) {
+    for (int i = i0 + int(threadIdx.x); i < i1; i += blockDim.x) {
         prior += A.lin[i] * double(x[i]);
         for (int k = A.nbr_ptr[i]; k < A.nbr_ptr[i + 1]; ++k)
             if (A.nbr[k] > i && x[A.nbr[k]] != x[i]) prior += A.lambda;
     }
     const double sd = block_sum_f64(data, red);
     const double sp = block_sum_f64(prior, red);
-    if (threadIdx.x == 0) A.e[blockIdx.x] = sd + sp;
+    if (threadIdx.x == 0) {
+        part[(size_t(st) * size_t(nb) + size_t(j)) * 2] = sd;
+        part[(size_t(st) * size_t(nb) + size_t(j)) * 2 + 1] = sp;
+    }
+}
+
+// e_s = (data partials in block order) + (prior partials in block order).
+__global__ void resid_energy_final_kernel(const double* part, int nb, int K, double* e) {
+    const int st = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (st >= K) return;
+    double sd = 0.0, sp = 0.0;
+    for (int j = 0; j < nb; ++j) {
+        sd += part[(size_t(st) * size_t(nb) + size_t(j)) * 2];
+        sp += part[(size_t(st) * size_t(nb) + size_t(j)) * 2 + 1];
+    }
+    e[st] = sd + sp;
 }
 
 // ---- results ----------------------------------------------------------------------------
@@ -1434,8 +1455,24 @@ qb_status launch_resid_energies(const ResidualPlan& p, const uint8_t* x, int K, 
     A.nbr = p.d_o_nbr.as<int32_t>();
     A.X = x;
     A.e = e;
-    resid_energy_kernel<<<unsigned(K), 1024, 0, st>>>(A);
-    QB_CUDA(cudaGetLastError());
+    // blocks per state: about four CTAs of work per SM in all
+    int dev = 0, sms = 148;
+    QB_CUDA(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int nb = std::max(1, std::min(256, (4 * sms + K - 1) / K));
+    const size_t bytes = size_t(K) * size_t(nb) * 2 * sizeof(double);
+    double* part = nullptr;
+    cudaMemPool_t pool = library_pool(dev);
+    if (pool) QB_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&part), bytes, pool, st));
+    else QB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), bytes, st));
+    resid_energy_part_kernel<<<dim3(unsigned(nb), unsigned(K)), 256, 0, st>>>(A, part);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        resid_energy_final_kernel<<<unsigned((K + 127) / 128), 128, 0, st>>>(part, nb, K, e);
+        err = cudaGetLastError();
+    }
+    cudaFreeAsync(part, st);
+    QB_CUDA(err);
     return QB_OK;
 }
 
