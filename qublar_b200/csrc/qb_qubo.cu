@@ -269,26 +269,42 @@ __global__ void __launch_bounds__(kQThreads, 1) qubo_lockstep_kernel(QuboArgs A)
 }
 
 // E(x) = offset + sum_i h_i x_i + sum_e J_e x_u x_v in fp64 from scratch
-// (qubo_energy, src/check_ree_qubo.cu:158-163), one CTA per state, a fixed
-// reduction shape.
-__global__ void qubo_energy_kernel(const int32_t* eu, const int32_t* ev, const float* ew, int64_t m, const float* h,
-                                   int n, double offset, const uint8_t* X, double* e) {
+// (qubo_energy, src/check_ree_qubo.cu:158-163). Grid = (blocks per state,
+// states): block j of state st sums its share of the bits (linear terms) and
+// of the edges into part[st * nb + j]; qubo_energy_final_kernel adds the
+// partials in block order. The shape is fixed by (K, SM count), so the sums
+// are deterministic.
+__global__ void __launch_bounds__(256) qubo_energy_part_kernel(const int32_t* eu, const int32_t* ev, const float* ew,
+                                                               int64_t m, const float* h, int n, const uint8_t* X,
+                                                               double* part) {
     __shared__ double red[256 / 32];
-    const uint8_t* x = X + size_t(blockIdx.x) * size_t(n);
+    const int st = int(blockIdx.y), j = int(blockIdx.x), nb = int(gridDim.x);
+    const uint8_t* x = X + size_t(st) * size_t(n);
+    const int i0 = int(int64_t(n) * j / nb), i1 = int(int64_t(n) * (j + 1) / nb);
+    const int64_t k0 = m * j / nb, k1 = m * (j + 1) / nb;
     double acc = 0.0;
-    for (int i = int(threadIdx.x); i < n; i += int(blockDim.x))
+    for (int i = i0 + int(threadIdx.x); i < i1; i += int(blockDim.x))
         if (x[i]) acc += double(h[i]);
-    for (int64_t k = threadIdx.x; k < m; k += blockDim.x)
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x)
         if (x[eu[k]] && x[ev[k]]) acc += double(ew[k]);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
     if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = offset;
+        double t = 0.0;
         for (int q = 0; q < int(blockDim.x >> 5); ++q) t += red[q];
-        e[blockIdx.x] = t;
+        part[size_t(st) * size_t(nb) + size_t(j)] = t;
     }
+}
+
+// e_st = offset + the partials of state st in block order.
+__global__ void qubo_energy_final_kernel(const double* part, int nb, int K, double offset, double* e) {
+    const int st = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (st >= K) return;
+    double t = offset;
+    for (int j = 0; j < nb; ++j) t += part[size_t(st) * size_t(nb) + size_t(j)];
+    e[st] = t;
 }
 
 }  // namespace
@@ -346,9 +362,25 @@ qb_status launch_qubo_lockstep(const QuboPlan& p, const QuboBuffers& b, int R, i
 
 qb_status launch_qubo_energies(const QuboPlan& p, const uint8_t* x, int K, double* e, cudaStream_t st) {
     if (K == 0) return QB_OK;
-    qubo_energy_kernel<<<dim3(unsigned(K)), 256, 0, st>>>(p.d_eu.as<int32_t>(), p.d_ev.as<int32_t>(), p.d_ew.as<float>(),
-                                                        p.m, p.d_ho.as<float>(), p.n, p.offset, x, e);
-    QB_CUDA(cudaGetLastError());
+    // blocks per state: about four CTAs of work per SM in all
+    int dev = 0, sms = 148;
+    QB_CUDA(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int nb = std::max(1, std::min(256, (4 * sms + K - 1) / K));
+    const size_t bytes = size_t(K) * size_t(nb) * sizeof(double);
+    double* part = nullptr;
+    cudaMemPool_t pool = library_pool(dev);
+    if (pool) QB_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&part), bytes, pool, st));
+    else QB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), bytes, st));
+    qubo_energy_part_kernel<<<dim3(unsigned(nb), unsigned(K)), 256, 0, st>>>(
+        p.d_eu.as<int32_t>(), p.d_ev.as<int32_t>(), p.d_ew.as<float>(), p.m, p.d_ho.as<float>(), p.n, x, part);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        qubo_energy_final_kernel<<<unsigned((K + 127) / 128), 128, 0, st>>>(part, nb, K, p.offset, e);
+        err = cudaGetLastError();
+    }
+    cudaFreeAsync(part, st);
+    QB_CUDA(err);
     return QB_OK;
 }
 
