@@ -20,7 +20,10 @@
  *   - sweeps visit the bits in colour-class order (a greedy distance-1
  *     colouring of the conflict graph), not in index order;
  *   - the Metropolis draw of (branch, bit, sweep) is Philox4x32-10 keyed by the
- *     branch seed, not the reference's sequential splitmix64 stream.
+ *     branch seed, not the reference's sequential splitmix64 stream; two
+ *     branches share a key and take one half of each Philox block each
+ *     (integer Ising: branches 2k and 2k + 1; weighted QUBO: branches r and
+ *     r + 32 of every 64).
  * Energies and fields of any returned configuration are exact (integer) or
  * fp64 from scratch; trajectories agree with the reference statistically.
  */
@@ -237,7 +240,10 @@ qb_status qb_colour_residual(const qb_residual_desc* desc, int32_t* order, int32
 qb_status qb_schedule_scaled(const qb_problem* p, int32_t anneal_sweeps, int32_t hold_sweeps, qb_schedule* out);
 
 /* Anneal n_branches branches; branch b uses seed b + 1 + seed_offset, the
- * reference's convention (ising_recon.hpp:157, gpu_anneal.cu:143). Every
+ * reference's convention (ising_recon.hpp:157, gpu_anneal.cu:143), except
+ * that the branches sharing a Philox key (above) use the seed of the first of
+ * them: integer-Ising branch b draws words 1:0 (b even) or 3:2 (b odd) of the
+ * block of seed (b & ~1) + 1 + seed_offset. Every
  * branch starts from x = 0. The kernels are queued on opts->stream; the call
  * returns without waiting for them. Replaces anneal_branch /
  * branch_fractions (ising_recon.hpp:121-166), wising::anneal

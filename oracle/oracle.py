@@ -65,7 +65,7 @@ def orc() -> C.CDLL:
             "orc_energy_scratch": (I64, [C.c_int, P, P, P, P]),
             "orc_fields": (None, [C.c_int, P, P, P, P, P]),
             "orc_wising_anneal": (I64, [C.c_int, P, P, P, D, D, C.c_int, C.c_int, U64, P, P]),
-            "orc_ising_anneal_coloured": (I64, [C.c_int, P, P, P, P, P, C.c_int, U64, P, P, P]),
+            "orc_ising_anneal_coloured": (I64, [C.c_int, P, P, P, P, P, C.c_int, U64, C.c_int, P, P, P]),
             "orc_gray_check": (I64, [C.c_int, I64, P, P, P, P, P, P, P]),
             "orc_binary_energy": (D, [C.POINTER(ResidDesc), P]),
             "orc_binary_energy_batch": (None, [C.POINTER(ResidDesc), P, I64, P]),
@@ -189,14 +189,14 @@ class Graph:
                                     seed, _p(x), _p(tr))
         return (x, int(e), tr) if trace else (x, int(e))
 
-    def anneal_coloured(self, order, temps, seed, trace=False):
+    def anneal_coloured(self, order, temps, seed, trace=False, half=0):
         order = np.ascontiguousarray(order, np.int32)
         temps = np.ascontiguousarray(temps, np.float64)
         x = np.empty(self.n, np.uint8)
         f = np.empty(self.n, np.int64)
         tr = np.empty(temps.size, np.float64) if trace else None
         e = orc().orc_ising_anneal_coloured(self.n, _p(self.row), _p(self.col), _p(self.w), _p(order), _p(temps),
-                                            int(temps.size), seed, _p(x), _p(f), _p(tr))
+                                            int(temps.size), seed, int(half), _p(x), _p(f), _p(tr))
         return (x, f, int(e), tr) if trace else (x, f, int(e))
 
     def gray_check(self):
@@ -318,6 +318,13 @@ def qubo_key_half(branch: int, seed_offset: int = 0):
     share key seed_base + r (seed_base = 1 + seed_offset + 64 per launch)."""
     r = branch % 64
     return 1 + seed_offset + branch - (32 if r >= 32 else 0), 1 if r >= 32 else 0
+
+
+def ising_key_half(replica: int, seed_offset: int = 0):
+    """The Philox key and half of replica `replica` of an integer-Ising solve
+    (qb_solve, qb_solve_batch, the server): replicas 2k and 2k + 1 share key
+    1 + seed_offset + 2k, 2k taking half 0 and 2k + 1 half 1."""
+    return 1 + seed_offset + (replica & ~1), replica & 1
 
 
 def fractions(X) -> np.ndarray:

@@ -183,10 +183,12 @@ int64_t orc_wising_anneal(int n, const int64_t* row, const int32_t* col, const i
 }
 
 /* The coloured-Philox integer annealer: wising::anneal's Metropolis rule and
- * State, bits visited in colour-class order, draw = Philox(seed, bit, sweep).
+ * State, bits visited in colour-class order, draw = half `half` (0: words 1:0,
+ * 1: words 3:2) of the Philox block of (seed, bit, sweep) -- replicas 2k and
+ * 2k + 1 of a solve share a key and take one half each.
  * temps: the temperature of every sweep. */
 int64_t orc_ising_anneal_coloured(int n, const int64_t* row, const int32_t* col, const int32_t* w,
-                                  const int32_t* order, const double* temps, int sweeps, uint64_t seed,
+                                  const int32_t* order, const double* temps, int sweeps, uint64_t seed, int half,
                                   uint8_t* x_out, int64_t* f_out, double* trace) {
     orc_state st = {n, row, col, w, (int8_t*)malloc((size_t)n), (int64_t*)malloc(sizeof(int64_t) * (size_t)n), 0};
     st_init(&st);
@@ -195,8 +197,13 @@ int64_t orc_ising_anneal_coloured(int n, const int64_t* row, const int32_t* col,
         for (int k = 0; k < n; ++k) {
             const int i = order[k];
             const double dE = (double)st_dE(&st, i);
-            if (dE <= 0.0 || (double)orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u) * 0x1.0p-53 < exp(-dE / T))
+            if (dE <= 0.0) {
                 st_flip(&st, i);
+                continue;
+            }
+            const uint64_t u53 = half ? orc_draw_u53_hi(seed, (uint32_t)i, (uint32_t)sweep, 0u)
+                                      : orc_draw_u53(seed, (uint32_t)i, (uint32_t)sweep, 0u);
+            if ((double)u53 * 0x1.0p-53 < exp(-dE / T)) st_flip(&st, i);
         }
         if (trace) trace[sweep] = (double)st.energy;
     }

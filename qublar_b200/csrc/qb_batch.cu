@@ -40,6 +40,27 @@ __device__ __forceinline__ unsigned long long accept_threshold(int k, double T) 
     return (unsigned long long)ceil(p * 0x1.0p53);
 }
 
+// The item's outputs (kItemFinal: x and f in original bit order) and its kept
+// state (kItemKeep).
+template <bool GLOBAL>
+__device__ __forceinline__ void ising_item_out(const IsingItem& it, const int32_t* f, const int8_t* s, int tid, int bs) {
+    const int n = it.n, lg = it.log2g, G = 1 << lg, NG = n << lg;
+    if (it.flags & kItemFinal) {
+        for (int p = tid; p < NG; p += bs) {
+            const int i = p >> lg;
+            const size_t o = size_t(p & (G - 1)) * size_t(n) + size_t(it.order[i]);
+            it.x_out[o] = s[p] > 0 ? 1u : 0u;
+            it.f_out[o] = f[p];
+        }
+    }
+    if (!GLOBAL && (it.flags & kItemKeep)) {
+        for (int p = tid; p < NG; p += bs) {
+            it.f_state[p] = f[p];
+            it.s_state[p] = s[p];
+        }
+    }
+}
+
 template <typename WT, bool GLOBAL>
 __device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* smem, unsigned long long* thr,
                                            unsigned long long* e_sh, int* cls) {
@@ -83,10 +104,118 @@ __device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* s
         for (int c = tid; c <= n_colours; c += bs) cls[c] = class_ptr[c];
     if (tid < G) e_sh[tid] = 0ull;
     __syncthreads();
-    // bs is a multiple of G, so this thread always serves replica r
-    const int r = tid & (G - 1);
-    const uint64_t seed = it.seed0 + uint64_t(r);
     const bool table = bound <= kThrMax;
+    // the item's replica r is replica r0 + r of the solve: it draws from key
+    // ising_pair_key(base, r0 + r) = seed0 - m + ((m + r) & ~1), m = r0 & 1,
+    // the words of half (m + r) & 1
+    const int m = (flags & kItemOddBase) ? 1 : 0;
+    if (lg >= 1 && m == 0) {
+        // pairs: a thread carries replicas 2h and 2h + 1 of one bit, which
+        // share one Philox block (G / 2 threads per bit, the pair fastest).
+        // Threads of odd bit slots take replica 2h + 1 first, so the field
+        // accesses of two consecutive bits start on banks of opposite parity.
+        // The item's tables are read from the shared descriptor where they are
+        // used, to keep the registers for the two replicas' state. (Energy
+        // changes added to the replicas' shared sums at each flip instead of
+        // in registers made the sweep 1.4x slower: the lanes of different
+        // bits that carry the same replica hit one shared word.)
+        const int lh = lg - 1;
+        const int par = (tid >> lh) & 1;
+        const int ra = ((tid & ((G >> 1) - 1)) << 1) + par, rb = ra ^ 1;
+        long long Ea = 0, Eb = 0;
+        for (int sweep = sweep0; sweep < sweep1; ++sweep) {
+            const double T = it.temp[sweep];
+            if (table) {
+                for (int k = tid + 1; k <= bound; k += bs) thr[k] = accept_threshold(k, T);
+                __syncthreads();
+            }
+            for (int c = 0; c < n_colours; ++c) {
+                const int q0 = (cls_sh ? cls[c] : it.class_ptr[c]) << lh;
+                const int q1 = (cls_sh ? cls[c + 1] : it.class_ptr[c + 1]) << lh;
+                for (int q = q0 + tid; q < q1; q += bs) {
+                    const int i = q >> lh;
+                    const uint32_t oi = uint32_t(__ldg(order + i));
+                    const int pa = (i << lg) + ra, pb = (i << lg) + rb;
+                    const int sa = s[pa], sb = s[pb];
+                    const int dEa = -sa * f[pa], dEb = -sb * f[pb];
+                    bool acca = dEa <= 0, accb = dEb <= 0;
+                    unsigned long long ta = 0ull, tb = 0ull;
+                    if (!acca) {
+                        ta = table ? thr[dEa] : accept_threshold(dEa, T);
+                        acca = ta >= (1ull << 53);
+                    }
+                    if (!accb) {
+                        tb = table ? thr[dEb] : accept_threshold(dEb, T);
+                        accb = tb >= (1ull << 53);
+                    }
+                    const bool needa = !acca && ta != 0ull, needb = !accb && tb != 0ull;
+                    if (needa || needb) {
+                        uint64_t lo, hi;
+                        draw_u53_pair(it.seed0 + uint64_t(ra & ~1), oi, uint32_t(sweep), 0u, &lo, &hi);
+                        if (needa) acca = (par ? hi : lo) < ta;
+                        if (needb) accb = (par ? lo : hi) < tb;
+                    }
+                    if (acca) {
+                        s[pa] = int8_t(-sa);
+                        Ea += dEa;
+                    }
+                    if (accb) {
+                        s[pb] = int8_t(-sb);
+                        Eb += dEb;
+                    }
+                    if (acca || accb) {
+                        // f_j -= 2 w_ij s_i per flipped replica, wrap-around uint32
+                        const uint32_t msa = sa > 0 ? 0xFFFFFFFEu : 2u, msb = sb > 0 ? 0xFFFFFFFEu : 2u;
+                        const int32_t* __restrict__ row = it.row;
+                        const int32_t* __restrict__ adj = it.adj;
+                        const WT* __restrict__ w = static_cast<const WT*>(it.w);
+                        int k = __ldg(row + i);
+                        const int k1 = __ldg(row + i + 1);
+                        for (; k + 4 <= k1; k += 4) {
+                            int j[4];
+                            uint32_t d[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                j[u] = __ldg(adj + k + u) << lg;
+                                d[u] = uint32_t(int32_t(__ldg(w + k + u)));
+                            }
+                            if (acca) {
+#pragma unroll
+                                for (int u = 0; u < 4; ++u)
+                                    atomicAdd(reinterpret_cast<unsigned int*>(&f[j[u] + ra]), d[u] * msa);
+                            }
+                            if (accb) {
+#pragma unroll
+                                for (int u = 0; u < 4; ++u)
+                                    atomicAdd(reinterpret_cast<unsigned int*>(&f[j[u] + rb]), d[u] * msb);
+                            }
+                        }
+                        for (; k < k1; ++k) {
+                            const int j = __ldg(adj + k) << lg;
+                            const uint32_t d = uint32_t(int32_t(__ldg(w + k)));
+                            if (acca) atomicAdd(reinterpret_cast<unsigned int*>(&f[j + ra]), d * msa);
+                            if (accb) atomicAdd(reinterpret_cast<unsigned int*>(&f[j + rb]), d * msb);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        atomicAdd(&e_sh[ra], (unsigned long long)Ea);
+        atomicAdd(&e_sh[rb], (unsigned long long)Eb);
+        __syncthreads();
+        if (tid < G) {
+            const long long prev = init ? 0ll : it.e_acc[tid];
+            it.e_acc[tid] = prev + (long long)e_sh[tid];
+        }
+        ising_item_out<GLOBAL>(it, f, s, tid, bs);
+        return;
+    }
+    // one replica per thread (groups of one replica): bs is a multiple of G,
+    // so this thread always serves replica r
+    const int r = tid & (G - 1);
+    const uint64_t seed = it.seed0 - uint64_t(m) + uint64_t((m + r) & ~1);
+    const int half = (m + r) & 1;
     long long E = 0;
     for (int sweep = sweep0; sweep < sweep1; ++sweep) {
         const double T = temp[sweep];
@@ -106,7 +235,7 @@ __device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* s
                 if (!acc) {
                     const unsigned long long t = table ? thr[dE] : accept_threshold(dE, T);
                     if (t >= (1ull << 53)) acc = true;
-                    else if (t != 0ull) acc = draw_u53(seed, oi, uint32_t(sweep), 0u) < t;
+                    else if (t != 0ull) acc = draw_u53_half(seed, oi, uint32_t(sweep), 0u, half) < t;
                 }
                 if (acc) {
                     s[p] = int8_t(-si);
@@ -148,25 +277,16 @@ __device__ __forceinline__ void ising_item(const IsingItem& it, unsigned char* s
         const long long prev = init ? 0ll : it.e_acc[tid];
         it.e_acc[tid] = prev + (long long)e_sh[tid];
     }
-    if (flags & kItemFinal) {
-        for (int p = tid; p < NG; p += bs) {
-            const int i = p >> lg;
-            const size_t o = size_t(p & (G - 1)) * size_t(n) + size_t(order[i]);
-            it.x_out[o] = s[p] > 0 ? 1u : 0u;
-            it.f_out[o] = f[p];
-        }
-    }
-    if (!GLOBAL && (flags & kItemKeep)) {
-        for (int p = tid; p < NG; p += bs) {
-            it.f_state[p] = f[p];
-            it.s_state[p] = s[p];
-        }
-    }
+    ising_item_out<GLOBAL>(it, f, s, tid, bs);
 }
 
 // items are handed out by ctl[0]; their count is n_items, or ctl[1] when
 // n_items < 0 (a launch replayed from a graph reads it from device memory).
-__global__ void __launch_bounds__(kBatchThreadsMax) ising_batch_kernel(const IsingItem* __restrict__ items, int n_items,
+// MAXT: the largest CTA the instance serves, one CTA per SM (the item state
+// fills the shared memory): 1024 threads get 64 registers each, 512 up to
+// 128, room for the two-replica threads' state.
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) ising_batch_kernel(const IsingItem* __restrict__ items, int n_items,
                                                                       int* ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned long long thr[kThrMax + 1];
@@ -215,11 +335,17 @@ __global__ void batch_marginals_kernel(const uint8_t* __restrict__ x, const Batc
     }
 }
 
+using BatchKernel = void (*)(const IsingItem*, int, int*);
+
+BatchKernel batch_kernel(int threads) {
+    return threads > 512 ? ising_batch_kernel<kBatchThreadsMax> : ising_batch_kernel<512>;
+}
+
 }  // namespace
 
 qb_status launch_ising_batch_ctl(const IsingItem* d_items, int* d_ctl, const BatchShape& sh, cudaStream_t st) {
     if (sh.ctas <= 0) return fail(QB_EINVAL, "batch: the launch needs its CTA count");
-    ising_batch_kernel<<<dim3(unsigned(sh.ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, -1,
+    batch_kernel(sh.threads)<<<dim3(unsigned(sh.ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, -1,
                                                                                                         d_ctl);
     QB_CUDA(cudaGetLastError());
     return QB_OK;
@@ -240,7 +366,8 @@ int batch_max_smem() {
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, ising_batch_kernel) != cudaSuccess) return 0;
+    // both instances have the same static shared memory
+    if (cudaFuncGetAttributes(&fa, ising_batch_kernel<kBatchThreadsMax>) != cudaSuccess) return 0;
     return optin - int(fa.sharedSizeBytes);
 }
 
@@ -250,8 +377,9 @@ qb_status batch_ctas(const BatchShape& sh, int* ctas) {
     QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (sh.threads < 32 || sh.threads > kBatchThreadsMax || sh.threads % kBatchMaxGroup)
         return fail(QB_EINVAL, "batch: threads must be a multiple of 32 in [32, 1024]");
-    QB_CUDA(allow_max_smem(ising_batch_kernel));
-    QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ising_batch_kernel, sh.threads, size_t(sh.smem_bytes)));
+    QB_CUDA(allow_max_smem(batch_kernel(sh.threads)));
+    QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel(sh.threads), sh.threads,
+                                                          size_t(sh.smem_bytes)));
     if (occ < 1) return fail(QB_EREFUSED, "batch: the launch shape does not fit an SM");
     *ctas = occ * sms;
     return QB_OK;
@@ -264,12 +392,12 @@ qb_status launch_ising_batch(const IsingItem* d_items, int n_items, int* d_count
         qb_status s = batch_ctas(sh, &ctas);
         if (s != QB_OK) return s;
     } else {
-        QB_CUDA(allow_max_smem(ising_batch_kernel));
+        QB_CUDA(allow_max_smem(batch_kernel(sh.threads)));
     }
     if (n_items <= 0) return QB_OK;
     if (ctas > n_items) ctas = n_items;
     QB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
-    ising_batch_kernel<<<dim3(unsigned(ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, n_items,
+    batch_kernel(sh.threads)<<<dim3(unsigned(ctas)), dim3(unsigned(sh.threads)), size_t(sh.smem_bytes), st>>>(d_items, n_items,
                                                                                                       d_counter);
     QB_CUDA(cudaGetLastError());
     return QB_OK;

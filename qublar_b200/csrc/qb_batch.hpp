@@ -42,6 +42,10 @@ constexpr int kItemInit = 1;     // start from x = 0 (s = -1, f = f0, E = 0)
 constexpr int kItemGlobal = 2;   // the state stays in f_state/s_state (too large for shared memory)
 constexpr int kItemFinal = 4;    // write x_out, f_out at the end
 constexpr int kItemKeep = 8;     // write the shared-memory state back to f_state/s_state at the end
+// bit 8 of flags: the parity of the item's first replica r0 (its replicas'
+// Philox key pairing, ising_pair_key); seed0 is the solve's base + r0
+constexpr int kItemOddBase = 1 << 8;
+inline int item_rbase_flags(int r0) { return (r0 & 1) ? kItemOddBase : 0; }
 
 constexpr int kBatchMaxGroup = 32;
 

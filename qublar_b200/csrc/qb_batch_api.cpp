@@ -236,7 +236,7 @@ qb_status build_items(qb_batch* b, const qb_batch_config& c, int sample, const d
         it.log2g = log2i(u.G);
         it.sweep0 = 0;
         it.sweep1 = sample > 0 ? sample : I.sweeps;
-        it.flags = kItemInit | kItemFinal;
+        it.flags = kItemInit | kItemFinal | item_rbase_flags(u.r0);
         if (u.global) {
             unsigned char* base = b->d_state.as<unsigned char>() + u.state_off;
             it.f_state = reinterpret_cast<int32_t*>(base);

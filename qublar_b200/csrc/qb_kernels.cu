@@ -56,10 +56,10 @@ constexpr int kChunkN = 6144;   // stage neighbour entries per chunk
 constexpr uint32_t kSlotBits = 27;
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
 
-__device__ __forceinline__ bool metropolis(double dE, double T, float inv_T, uint64_t seed, uint32_t bit,
+__device__ __forceinline__ bool metropolis(double dE, double T, float inv_T, uint64_t seed, int half, uint32_t bit,
                                            uint32_t sweep) {
     if (dE <= 0.0) return true;
-    return uphill_accept(draw_u53(seed, bit, sweep, 0u), dE, T, inv_T);
+    return uphill_accept(draw_u53_half(seed, bit, sweep, 0u, half), dE, T, inv_T);
 }
 
 // ---- integer Ising ----------------------------------------------------------------
@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
     }
     if (threadIdx.x < 2) acc_count[threadIdx.x] = 0;
     __syncthreads();
-    const uint64_t seed = A.seed0 + uint64_t(rep);
+    const uint64_t seed = ising_pair_key(A.seed0, uint32_t(rep));
+    const int half = ising_pair_half(uint32_t(rep));
     const WT* w = static_cast<const WT*>(A.w);
     const int lane = int(threadIdx.x & 31u), warp = int(threadIdx.x >> 5), n_warps = int(blockDim.x >> 5);
     long long E = 0;
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kIsingThreads) ising_anneal_kernel(IsingArgs A
             for (int i = A.class_ptr[c] + int(threadIdx.x); i < c1; i += blockDim.x) {
                 const int si = s[i];
                 const long long dE = -(long long)si * (long long)f[i];
-                if (metropolis(double(dE), T, inv_T, seed, uint32_t(A.order[i]), uint32_t(sweep))) {
+                if (metropolis(double(dE), T, inv_T, seed, half, uint32_t(A.order[i]), uint32_t(sweep))) {
                     s[i] = int8_t(-si);
                     E += dE;
                     // f_j -= 2 w_ij s_i, in wrap-around uint32 arithmetic: the

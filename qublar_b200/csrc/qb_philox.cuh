@@ -74,4 +74,17 @@ QB_HD void draw_u53_pair(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t s
     *hi = ((uint64_t(o.v[3]) << 32) | uint64_t(o.v[2])) >> 11;
 }
 
+// One half of a draw block: words 1:0 (half 0, = draw_u53) or words 3:2 (half 1).
+QB_HD uint64_t draw_u53_half(uint64_t seed, uint32_t bit, uint32_t sweep, uint32_t stream, int half) {
+    const Philox4 o = philox4x32_10(bit, sweep, stream, 0u, uint32_t(seed), uint32_t(seed >> 32));
+    return half ? ((uint64_t(o.v[3]) << 32) | uint64_t(o.v[2])) >> 11
+                : ((uint64_t(o.v[1]) << 32) | uint64_t(o.v[0])) >> 11;
+}
+
+// Integer-Ising replica pairing: replicas 2k and 2k + 1 of a solve share the
+// Philox key base + 2k; 2k takes words 1:0 of each block and 2k + 1 words 3:2.
+// A thread that carries both replicas of a pair evaluates one block for the two.
+QB_HD uint64_t ising_pair_key(uint64_t base, uint32_t b) { return base + uint64_t(b & ~1u); }
+QB_HD int ising_pair_half(uint32_t b) { return int(b & 1u); }
+
 }  // namespace qb

@@ -523,7 +523,7 @@ qb_status launch_tick(qb_server* S) {
             it.sweep0 = s0;
             it.sweep1 = s1;
             it.flags = (s0 == 0 ? kItemInit : 0) | (s1 == r->sweeps ? kItemFinal : 0) |
-                       (g.global ? kItemGlobal : (s1 < r->sweeps ? kItemKeep : 0));
+                       (g.global ? kItemGlobal : (s1 < r->sweeps ? kItemKeep : 0)) | item_rbase_flags(g.r0);
             it.bound = int32_t(P.B);
             it.wbytes = P.weight_bytes;
             items.push_back(it);

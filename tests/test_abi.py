@@ -370,11 +370,28 @@ def write_adapter_inputs(d):
 
 
 def test_branch_range_covers_branches():
-    for R in (1, 5, 16, 64):
+    for R in (1, 5, 16, 64, 130):
         for W in (1, 2, 3, 8):
-            rs = [branch_range(R, W, r) for r in range(W)]
-            assert rs[0][0] == 0 and rs[-1][1] == R
-            assert all(rs[k][1] == rs[k + 1][0] for k in range(W - 1))
+            for g in (1, 2, 64):
+                rs = [branch_range(R, W, r, g) for r in range(W)]
+                assert rs[0][0] == 0 and rs[-1][1] == R
+                assert all(rs[k][1] == rs[k + 1][0] for k in range(W - 1))
+                assert all(b0 % g == 0 or b0 == R for b0, _ in rs)
+
+
+def test_draw_granules():
+    from oracle import oracle as O
+    from qublar_b200 import KIND_ISING, KIND_QUBO, KIND_RESIDUAL
+    from qublar_b200.dist import draw_granule
+
+    class P:
+        def __init__(self, kind):
+            self.kind = kind
+    assert [draw_granule(P(k)) for k in (KIND_ISING, KIND_QUBO, KIND_RESIDUAL)] == [2, 64, 1]
+    # a rank's solve with seed_offset + b0 draws the single solve's keys
+    for b0, _ in (branch_range(37, 3, r, 2) for r in range(3)):
+        for j in range(4):
+            assert O.ising_key_half(j, b0) == O.ising_key_half(b0 + j)
 
 
 def _gloo_worker(rank, world, port, X, out_path):

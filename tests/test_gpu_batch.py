@@ -77,7 +77,8 @@ def test_batch_matches_the_oracle(batch_case):
         temps = O.temperatures(sched.t_hot, sched.t_cold, sched.anneal_sweeps, sched.hold_sweeps)
         X = B.branches(k)
         for r in range(min(R, 4)):
-            x, f, e = g.anneal_coloured(order, temps, r + 1 + off)
+            key, half = O.ising_key_half(r, off)
+            x, f, e = g.anneal_coloured(order, temps, key, half=half)
             assert (X[r] == x).all(), (k, r)
 
 

@@ -35,7 +35,8 @@ def _check_ising(gen, R, budget=None, anneal=400, hold=20):
     order, _ = P.colouring()
     temps = O.temperatures(b.t_hot, b.t_cold, b.anneal_sweeps, b.hold_sweeps)
     for k in range(R):
-        x, f, e = g.anneal_coloured(order, temps, k + 1)
+        key, half = O.ising_key_half(k)
+        x, f, e = g.anneal_coloured(order, temps, key, half=half)
         assert (X[k] == x).all(), k
         assert E[k] == e and (F[k] == f).all(), k
         # exact energies and fields of the returned configuration

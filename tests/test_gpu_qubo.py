@@ -92,19 +92,23 @@ def test_final_energies_agree_with_the_reference_annealer():
 def test_maxcut_through_the_qubo_sweep_equals_the_ising_sweep(gen):
     """A Max-Cut graph as a weighted QUBO (h = -sum w, J = 2 w): with exact
     fp32 fields the compensated sweep makes the integer sweep's decisions, so
-    the branches are identical and the energies equal -cut. Both sweeps give
-    replica r < 32 of a launch words 1:0 of key seed0 + r; the QUBO sweep's
-    replicas 32..63 take words 3:2 of the keys of replicas 0..31 (one Philox
-    block per lane), so the two paths are compared on 32 replicas."""
+    the branches are identical and the energies equal -cut, replica for
+    replica of the same Philox key and half. The integer sweep pairs replicas
+    2k and 2k + 1 on key seed0 + 2k (words 1:0 and 3:2); the QUBO sweep pairs
+    replicas r and r + 32 of a launch on key seed0 + r. So integer replica 2k
+    is QUBO replica 2k and integer replica 2k + 1 is QUBO replica 2k + 32."""
     from qublar_b200 import IsingProblem
     n, eu, ev, ew = gen()
     I = IsingProblem(n, eu, ev, ew)
     sched = I.scaled_schedule(150, 10)
     ri = I.solve(sched, 32, 2)
     Q = QuboProblem.from_dict(synth.maxcut_qubo(n, eu, ev, ew))
-    rq = Q.solve(sched, 32, 2)
-    assert (rq.branches() == ri.branches()).all()
-    assert (rq.energies() == ri.energies_tracked().astype(np.float64)).all()
+    rq = Q.solve(sched, 64, 2)
+    same = [b if b % 2 == 0 else b - 1 + 32 for b in range(32)]
+    for b in range(32):
+        assert O.ising_key_half(b, 2) == O.qubo_key_half(same[b], 2)
+    assert (rq.branches()[same] == ri.branches()).all()
+    assert (rq.energies()[same] == ri.energies_tracked().astype(np.float64)).all()
     assert rq.info().max_energy_error == 0.0
 
 

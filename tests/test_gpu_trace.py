@@ -63,7 +63,8 @@ def test_ising_er800_trace_exact_and_vs_reference():
     assert T.shape == (64, 1000)
     assert (T[:, -1] == E.astype(np.float64)).all()
     for k in range(4):
-        _, _, e, tr = g.anneal_coloured(order, temps, k + 1, trace=True)
+        key, half = O.ising_key_half(k)
+        _, _, e, tr = g.anneal_coloured(order, temps, key, trace=True, half=half)
         assert (T[k] == tr).all(), k
     G = np.load(os.path.join(GOLD, "ref_runs.npz"))
     assert (_colour_of_bits(order, cptr, P.n) == G["er800_colour"]).all(), "regenerate the fixture"

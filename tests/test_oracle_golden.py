@@ -46,6 +46,14 @@ def test_qubo_branch_keys():
     assert O.qubo_key_half(69, 5) == (75, 0)
 
 
+def test_ising_replica_keys():
+    """Replica b of an integer-Ising solve: replicas 2k and 2k + 1 share key
+    1 + seed_offset + 2k (words 1:0 and 3:2)."""
+    assert O.ising_key_half(0) == (1, 0) and O.ising_key_half(1) == (1, 1)
+    assert O.ising_key_half(30) == (31, 0) and O.ising_key_half(31) == (31, 1)
+    assert O.ising_key_half(7, 5) == (12, 1)
+
+
 def test_splitmix_matches_reference_stream():
     s = synth.SplitMix(1)
     v = [s.next() for _ in range(5)]
