@@ -394,6 +394,70 @@ def test_draw_granules():
             assert O.ising_key_half(j, b0) == O.ising_key_half(b0 + j)
 
 
+class _OracleIsingProblem:
+    """A stand-in integer-Ising problem for the CPU: solve() anneals with the
+    oracle's coloured-Philox sweep under the library's replica keys (replicas
+    2k, 2k + 1 share a Philox key), as qb_solve does on a GPU."""
+    kind = 1   # KIND_ISING
+
+    def __init__(self, seed=3, n=40, m=120):
+        rng = np.random.default_rng(seed)
+        eu = rng.integers(0, n, m)
+        ev = (eu + 1 + rng.integers(0, n - 1, m)) % n
+        self.args = (n, eu.astype(np.int32), ev.astype(np.int32), rng.choice([-1, 1], m).astype(np.int32))
+        self.n = n
+
+    def solve(self, temps, R, seed_offset):
+        from oracle import oracle as O
+        g = O.Graph(*self.args)
+        order = np.arange(self.n, dtype=np.int32)
+        X = np.stack([g.anneal_coloured(order, temps, *O.ising_key_half(b, seed_offset))[0] for b in range(R)])
+
+        class _R:
+            def branches(self):
+                return X
+
+            def close(self):
+                pass
+        return _R()
+
+
+def _gloo_sharded_worker(rank, world, port, R, offset, out_path):
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+    from qublar_b200.dist import sharded_branch_fractions
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    frac, _, _ = sharded_branch_fractions(_OracleIsingProblem(), O.temperatures(4.0, 0.2, 20, 5), R, offset)
+    if rank == 0:
+        np.save(out_path, frac)
+    dist.destroy_process_group()
+
+
+def test_two_ranks_shard_an_ising_solve_like_one_process(tmp_path):
+    """An integer-Ising solve's branches split over two gloo ranks: each rank
+    starts on an even branch (6 branches: [0, 4) and [4, 6), where an even
+    split would start rank 1 at branch 3 and change its Philox keys), so the
+    summed counts give the single solve's fractions exactly."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    from oracle import oracle as O
+    R, offset = 6, 5
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "frac.npy")
+    mp.spawn(_gloo_sharded_worker, args=(2, port, R, offset, out), nprocs=2, join=True)
+    X = _OracleIsingProblem().solve(O.temperatures(4.0, 0.2, 20, 5), R, offset).branches()
+    assert (np.load(out) == O.fractions(X)).all()
+    # the draws of a rank that started at branch 3 would differ
+    P = _OracleIsingProblem()
+    T = O.temperatures(4.0, 0.2, 20, 5)
+    assert not (P.solve(T, 3, offset + 3).branches() == X[3:]).all()
+
+
 def _gloo_worker(rank, world, port, X, out_path):
     import torch.distributed as dist
     from qublar_b200.dist import allreduce_counts
