@@ -5,15 +5,18 @@
 // sorted by estimated cost, largest first), anneals its G replicas of one
 // instance over its sweep range, and takes another. The item's fields (int32)
 // and spins (int8) sit in the CTA's shared memory, laid out bit-major with the
-// replica fastest, so a warp covers 32 / G consecutive bits of a class for all
-// G replicas: neighbour updates of one accepted bit land in G consecutive
-// words, and the CSR row of a bit is read once for its G replicas. Items too
-// large for shared memory run in place on their global state.
+// replica fastest. A thread carries replicas 2h and 2h + 1 of one bit (items
+// of G >= 2), so a warp covers 64 / G consecutive bits of a class for all G
+// replicas: the two replicas share one Philox block and one walk of the bit's
+// CSR row, and neighbour updates of one accepted bit land in G consecutive
+// words. Items too large for shared memory run in place on their global
+// state.
 //
 // The decisions are those of the single-instance sweep (qb_kernels.cu): colour
 // classes in order, dE = -s_i f_i, accept if dE <= 0, else if u53 * 2^-53 <
-// exp(-dE / T) with u53 the Philox draw of (replica seed, original bit,
-// sweep). For |dE| <= 256 the comparison uses a per-sweep table of
+// exp(-dE / T) with u53 the Philox draw of (replica key, original bit, sweep),
+// words 1:0 or 3:2 of the block as the replica is even or odd
+// (ising_pair_key). For |dE| <= 256 the comparison uses a per-sweep table of
 // ceil(exp(-k / T) * 2^53), which is the same test on the integer u53 (the
 // scaling by 2^53 is exact), so a replica's trajectory does not depend on the
 // item it falls in, the launch shape, or the other instances of the batch.
