@@ -16,6 +16,12 @@ attempts per step = 16 * 250 * 306,328.
   --impl reference -- the reference's own CPU branch_fractions
              (oracle/_ref, compiled from the reference sources) on this host.
 
+The default run (one GPU) also records, beside the pyramid line, the batched
+4,096-instance Max-Cut stream ("batch": packed solve against one qb_solve per
+instance) and the weighted 200,000-bit lattice QUBO ("qubo"), each measured by
+its own ``--workload`` run in a child process with 3 warm-up steps and 1 timed
+step (``--no-side-workloads`` skips them).
+
 Multi-GPU: one process per GPU (torchrun); every rank solves its own copy of
 the workload (branches are independent: weak scaling, no collective on the
 data path); the timed region is bracketed by barriers and the slowest rank's
@@ -754,6 +760,44 @@ def run_maxcut(args):
     return 0
 
 
+SIDE_KEYS = ("value", "unit", "steps", "warmup", "ms_per_step", "dtype", "plain", "vs_plain", "e2e", "gpu_launches",
+             "roofline", "precision", "clocks")
+
+
+def side_workload(argv, timeout_s=900):
+    """One of the other benchmark workloads (its own ``--workload`` line), run
+    as a child process after the pyramid line is measured, so that the default
+    run records it too: a failure there is reported in its block and touches
+    nothing else. Returns the child's figures, or {"error": ...}."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT", "GROUP_RANK", "ROLE_RANK",
+                        "LOCAL_WORLD_SIZE") and not k.startswith("TORCHELASTIC")}
+    cmd = [sys.executable, os.path.abspath(__file__)] + list(argv)
+    t0 = time.perf_counter()
+    try:
+        r = subprocess.run(cmd, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout_s,
+                           text=True)
+    except subprocess.TimeoutExpired:
+        return {"command": "bench.py " + " ".join(argv), "error": f"no line within {timeout_s} s"}
+    wall = time.perf_counter() - t0
+    got = None
+    for ln in reversed(r.stdout.splitlines()):
+        if ln.startswith("{"):
+            try:
+                got = json.loads(ln)
+                break
+            except ValueError:
+                pass
+    if r.returncode != 0 or got is None:
+        tail = (r.stderr.strip().splitlines() or ["(no output)"])[-1]
+        return {"command": "bench.py " + " ".join(argv), "error": f"exit {r.returncode}: {tail[:300]}"}
+    out = {"command": "bench.py " + " ".join(argv), "wall_s": round(wall, 1)}
+    out.update({k: got[k] for k in SIDE_KEYS if k in got})
+    cfg = got.get("config", {})
+    out["config"] = {k: cfg[k] for k in ("workload", "shape", "l2") if k in cfg}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -778,6 +822,8 @@ def main():
     ap.add_argument("--qubo-sweeps", type=int, default=5000, help="qubo: sweeps (shorter runs are for profiling)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="batch/qubo: time the kernel only (no plain-form, end-to-end or CPU legs; for profiling)")
+    ap.add_argument("--no-side-workloads", action="store_true",
+                    help="tomography: skip the batched (C3) and weighted-QUBO (C4) lines recorded beside the pyramid")
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)
@@ -932,6 +978,11 @@ def main():
         line["cpu_baseline"] = {"value": rate, "unit": "attempts/s", "cores": threads, "kind": kind,
                                 "sample": f"{branches} of 16 branches, the full 250-sweep schedule, "
                                           f"{threads} threads, {wall:.1f} s"}
+    if rank == 0 and world == 1 and not args.no_side_workloads:
+        # the batched stream and the weighted lattice QUBO, each in its own
+        # process after this line's measurements (W = 3 warm-up steps, 1 timed)
+        line["batch"] = side_workload(["--workload", "batch", "--steps", "1", "--warmup", "3", "--no-cpu-baseline"])
+        line["qubo"] = side_workload(["--workload", "qubo", "--steps", "1", "--warmup", "3", "--no-cpu-baseline"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

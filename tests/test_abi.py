@@ -311,6 +311,20 @@ def test_benchmark_pyramid_sizes():
     assert 140 < a["ray"].size / a["d"].size < 160
 
 
+def test_benchmark_side_workload_failure_is_reported_not_raised():
+    """The default benchmark run records the batched and QUBO workloads from
+    child processes; a child that fails (here: no GPU, or an unknown
+    workload) leaves an error in its block and raises nothing."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("qb_bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    got = bench.side_workload(["--workload", "no-such-workload"], timeout_s=120)
+    assert got["command"] == "bench.py --workload no-such-workload"
+    assert got["error"].startswith("exit 2")
+    assert "value" not in got
+
+
 def test_adapter_compiles_and_fails_cleanly_without_a_device(tmp_path):
     exe = tmp_path / "adapter_check"
     cmd = ["g++", "-std=c++17", "-O1", "-I" + INCLUDE, os.path.join(ROOT, "tests", "adapter_check.cpp"),
